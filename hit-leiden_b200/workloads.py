@@ -1,0 +1,296 @@
+"""Seeded synthetic graphs and update batches with the shapes of the benchmark configs.
+
+None of the reference's datasets (SNAP ca-HepTh, uk-2007-05) is available, so
+these generators stand in for them with the same sizes and value distributions:
+
+* ``planted``: planted power-law communities with mixing mu, power-law degrees and
+  optional triangle closure (config 1: n=9,877, ~21.8k unit edges, mu=0.15,
+  clustering ~0.45; config 2 shape: 1M vertices / 20M f64 edges, mu=0.3).
+* ``rmat``: R-MAT edge sampling (config 3: scale 25, edge factor 16), produced
+  on the GPU with torch as input plumbing.
+* batch generators: uniform inserts, degree-preferential inserts and uniform
+  deletes of existing edges, all seeded.
+
+Graphs are returned as (n, src, dst, w) numpy arrays with src < dst, no
+self-loops and no duplicates.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _powerlaw_int(rng, n, exponent, lo, hi, mean=None):
+    """Draw n integers in [lo, hi] from a discrete power law p(x) ~ x^-exponent."""
+    xs = np.arange(lo, hi + 1, dtype=np.float64)
+    p = xs ** (-exponent)
+    p /= p.sum()
+    out = rng.choice(xs.astype(np.int64), size=n, p=p)
+    if mean is not None and out.mean() > 0:
+        scale = mean / out.mean()
+        out = np.clip(np.round(out * scale), lo if lo > 0 else 1, hi).astype(np.int64)
+    return out
+
+
+def _community_sizes(rng, n, exponent, lo, hi):
+    sizes = []
+    total = 0
+    while total < n:
+        s = int(_powerlaw_int(rng, 1, exponent, lo, hi)[0])
+        s = min(s, n - total)
+        if s < lo and sizes:
+            sizes[-1] += s
+        else:
+            sizes.append(s)
+        total += s
+    return np.array(sizes, dtype=np.int64)
+
+
+def _dedup(n, u, v, w=None):
+    a = np.minimum(u, v).astype(np.int64)
+    b = np.maximum(u, v).astype(np.int64)
+    keep = a != b
+    a, b = a[keep], b[keep]
+    if w is not None:
+        w = w[keep]
+    key = a * n + b
+    key, idx = np.unique(key, return_index=True)
+    a, b = key // n, key % n
+    if w is not None:
+        w = w[idx]
+    return a.astype(np.uint32), b.astype(np.uint32), w
+
+
+def planted(n, mean_degree, mu, seed, degree_exp=2.5, max_degree=None, comm_exp=1.5,
+            comm_min=2, comm_max=400, triangle_frac=0.0, weights=None):
+    """Planted-partition graph (LFR-style).
+
+    Each vertex gets a power-law target degree; a fraction 1-mu of its stubs is
+    wired inside its community (configuration model), the rest across the whole
+    graph.  ``triangle_frac`` of the intra edges are instead placed by closing
+    wedges, which raises the clustering coefficient.  ``weights`` = None gives
+    unit weights, or a (lo, hi) pair for uniform f64 weights.
+    """
+    rng = np.random.default_rng(seed)
+    if max_degree is None:
+        max_degree = max(8, int(np.sqrt(n) * 4))
+    deg = _powerlaw_int(rng, n, degree_exp, 1, max_degree, mean=mean_degree)
+    sizes = _community_sizes(rng, n, comm_exp, comm_min, comm_max)
+    perm = rng.permutation(n)
+    comm = np.empty(n, np.int64)
+    starts = np.concatenate([[0], np.cumsum(sizes)])
+    for c in range(len(sizes)):
+        comm[perm[starts[c]:starts[c + 1]]] = c
+    intra = rng.binomial(deg, 1.0 - mu)
+    inter = deg - intra
+    # Intra edges: shuffle stubs inside each community and pair them up.
+    order = np.argsort(comm, kind="stable")
+    stub_node = np.repeat(order, intra[order])
+    stub_comm = comm[stub_node]
+    key = stub_comm * 4.0 + rng.random(len(stub_node))
+    stub_node = stub_node[np.argsort(key, kind="stable")]
+    stub_comm = comm[stub_node]
+    m_pairs = len(stub_node) // 2
+    a, b = stub_node[0:2 * m_pairs:2], stub_node[1:2 * m_pairs:2]
+    same = comm[a] == comm[b]
+    iu, iv = a[same], b[same]
+    n_tri = int(len(iu) * triangle_frac)
+    if n_tri > 0:
+        iu, iv = iu[n_tri:], iv[n_tri:]
+    # Inter edges: global configuration model.
+    sn = np.repeat(np.arange(n), inter)
+    rng.shuffle(sn)
+    mp = len(sn) // 2
+    ou, ov = sn[0:2 * mp:2], sn[1:2 * mp:2]
+    u = np.concatenate([iu, ou])
+    v = np.concatenate([iv, ov])
+    if n_tri > 0:
+        # Close wedges: pick a vertex, two of its current intra neighbours.
+        a0, b0, _ = _dedup(n, u, v)
+        nb_src = np.concatenate([a0, b0]).astype(np.int64)
+        nb_dst = np.concatenate([b0, a0]).astype(np.int64)
+        same = comm[nb_src] == comm[nb_dst]
+        nb_src, nb_dst = nb_src[same], nb_dst[same]
+        o = np.argsort(nb_src, kind="stable")
+        nb_src, nb_dst = nb_src[o], nb_dst[o]
+        cnt = np.bincount(nb_src, minlength=n)
+        off = np.concatenate([[0], np.cumsum(cnt)])
+        cand = np.nonzero(cnt >= 2)[0]
+        centers = cand[rng.integers(0, len(cand), size=n_tri)]
+        c0 = off[centers]
+        dc = cnt[centers]
+        x = rng.integers(0, dc)
+        y = (x + 1 + rng.integers(0, np.maximum(dc - 1, 1))) % dc
+        tu, tv = nb_dst[c0 + x], nb_dst[c0 + y]
+        u = np.concatenate([u, tu])
+        v = np.concatenate([v, tv])
+    w = None
+    if weights is not None:
+        w = rng.uniform(weights[0], weights[1], size=len(u))
+    src, dst, w = _dedup(n, u, v, w)
+    if w is None:
+        w = np.ones(len(src), np.float64)
+    return n, src, dst, w.astype(np.float64), comm.astype(np.uint32)
+
+
+def config1(seed=0):
+    """n=9,877, ~21.8k unit edges, ~480 communities (sizes 2-400, exp 1.5),
+    mu=0.15, power-law degrees (exp 2.5, mean 4.4), triangle closure."""
+    n, s, d, w, comm = planted(9877, 4.9, 0.15, seed, degree_exp=2.5, max_degree=65,
+                               comm_exp=1.5, comm_min=2, comm_max=400, triangle_frac=0.35)
+    return n, s, d, w
+
+
+def config2(seed=0, n=1_000_000, mean_degree=40.0):
+    """LFR-style 1M vertices / ~20M edges, degree exp 2.5 (mean 40, max 2000),
+    community sizes exp 1.5 in [50, 5000], mu=0.3, f64 weights U[0.5, 2.0]."""
+    n, s, d, w, comm = planted(n, mean_degree * 1.02, 0.3, seed, degree_exp=2.5, max_degree=2000,
+                               comm_exp=1.5, comm_min=50, comm_max=5000, weights=(0.5, 2.0))
+    return n, s, d, w
+
+
+def uniform_inserts(n, k, seed, existing=None):
+    """k uniformly random new undirected unit edges (no self-loops)."""
+    rng = np.random.default_rng(seed)
+    out_u, out_v = [], []
+    seen = set()
+    ex = existing
+    while len(out_u) < k:
+        a = rng.integers(0, n, size=2 * k)
+        b = rng.integers(0, n, size=2 * k)
+        for x, y in zip(a.tolist(), b.tolist()):
+            if x == y:
+                continue
+            key = (min(x, y), max(x, y))
+            if key in seen or (ex is not None and key in ex):
+                continue
+            seen.add(key)
+            out_u.append(key[0])
+            out_v.append(key[1])
+            if len(out_u) == k:
+                break
+    return (np.array(out_u, np.uint32), np.array(out_v, np.uint32), np.ones(k, np.float64))
+
+
+class EdgeStore:
+    """Current weighted edge set of a dynamic graph (for generating deletes)."""
+
+    def __init__(self, n, src, dst, w):
+        self.n = n
+        self.key = (src.astype(np.int64) * n + dst.astype(np.int64))
+        self.w = w.astype(np.float64).copy()
+        self.deg = np.bincount(src, minlength=n) + np.bincount(dst, minlength=n)
+        self.extra = {}
+        self.removed = set()
+
+    def weight(self, a, b):
+        key = a * self.n + b
+        if key in self.extra:
+            return self.extra[key]
+        if key in self.removed:
+            return None
+        i = np.searchsorted(self.key, key)
+        if i < len(self.key) and self.key[i] == key:
+            return float(self.w[i])
+        return None
+
+    def apply(self, u, v, w):
+        for a, b, x in zip(u.tolist(), v.tolist(), w.tolist()):
+            a, b = min(a, b), max(a, b)
+            cur = self.weight(a, b)
+            new = (cur or 0.0) + x
+            key = a * self.n + b
+            if new > 1e-12:
+                self.extra[key] = new
+                self.removed.discard(key)
+            else:
+                self.extra.pop(key, None)
+                self.removed.add(key)
+
+    def random_existing(self, rng, k):
+        out = []
+        while len(out) < k:
+            i = int(rng.integers(0, len(self.key) + len(self.extra)))
+            if i < len(self.key):
+                key = int(self.key[i])
+            else:
+                key = list(self.extra.keys())[i - len(self.key)]
+            a, b = divmod(key, self.n)
+            w = self.weight(a, b)
+            if w is None or (a, b) in [(x[0], x[1]) for x in out]:
+                continue
+            out.append((a, b, w))
+        return out
+
+
+def mixed_batch(store: EdgeStore, k, insert_frac, seed, weights=None, preferential=True):
+    """k updates: insert_frac new edges (endpoints drawn by degree when
+    ``preferential``, uniform otherwise) and the rest deletes of existing edges
+    chosen uniformly (alpha = -current weight, which removes the edge)."""
+    rng = np.random.default_rng(seed)
+    n = store.n
+    ki = int(round(k * insert_frac))
+    kd = k - ki
+    if preferential:
+        p = store.deg.astype(np.float64) + 1.0
+        p /= p.sum()
+        a = rng.choice(n, size=2 * ki + 64, p=p)
+        b = rng.choice(n, size=2 * ki + 64, p=p)
+    else:
+        a = rng.integers(0, n, size=2 * ki + 64)
+        b = rng.integers(0, n, size=2 * ki + 64)
+    iu, iv = [], []
+    seen = set()
+    for x, y in zip(a.tolist(), b.tolist()):
+        if len(iu) == ki:
+            break
+        if x == y:
+            continue
+        key = (min(x, y), max(x, y))
+        if key in seen:
+            continue
+        seen.add(key)
+        iu.append(key[0])
+        iv.append(key[1])
+    if weights is None:
+        iw = np.ones(len(iu))
+    else:
+        iw = rng.uniform(weights[0], weights[1], size=len(iu))
+    dels = store.random_existing(rng, kd)
+    u = np.array(iu + [x[0] for x in dels], np.uint32)
+    v = np.array(iv + [x[1] for x in dels], np.uint32)
+    w = np.concatenate([iw, np.array([-x[2] for x in dels])]).astype(np.float64)
+    perm = rng.permutation(len(u))
+    u, v, w = u[perm], v[perm], w[perm]
+    store.apply(u, v, w)
+    return u, v, w
+
+
+def rmat_torch(scale, edge_factor, seed, a=0.57, b=0.19, c=0.19, device="cuda"):
+    """R-MAT edge list generated on the GPU with torch (input plumbing only):
+    symmetrised (src < dst), duplicates and self-loops removed.  Returns
+    device tensors (src, dst) of dtype int32 sorted by (src, dst)."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    n = 1 << scale
+    m = n * edge_factor
+    chunk = 1 << 26
+    keys = []
+    for start in range(0, m, chunk):
+        cnt = min(chunk, m - start)
+        src = torch.zeros(cnt, dtype=torch.int64, device=device)
+        dst = torch.zeros(cnt, dtype=torch.int64, device=device)
+        for lvl in range(scale):
+            r = torch.rand(cnt, generator=g, device=device)
+            bit_s = (r >= a + b).to(torch.int64)
+            bit_d = (((r >= a) & (r < a + b)) | (r >= a + b + c)).to(torch.int64)
+            src |= bit_s << lvl
+            dst |= bit_d << lvl
+        lo = torch.minimum(src, dst)
+        hi = torch.maximum(src, dst)
+        keep = lo != hi
+        keys.append(lo[keep] * n + hi[keep])
+        del src, dst, lo, hi
+    key = torch.unique(torch.cat(keys))
+    return n, (key // n).to(torch.int32), (key % n).to(torch.int32)
