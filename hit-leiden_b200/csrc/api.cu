@@ -1,0 +1,790 @@
+// api.cu — host orchestration (Algorithm 6 level loop, bootstrap) and the
+// C ABI declared in include/hl.h and include/hl_debug.h.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "../../include/hl_debug.h"
+#include "hl_engine.cuh"
+
+using namespace hl;
+
+static thread_local std::string g_err;
+
+
+namespace hl {
+
+u64 Engine::read_u64(const u64* d) {
+  HL_CUDA(cudaMemcpyAsync(hs.p, d, sizeof(u64), cudaMemcpyDeviceToHost, stream));
+  HL_CUDA(cudaStreamSynchronize(stream));
+  return hs.p[0];
+}
+u32 Engine::read_u32(const u32* d) {
+  HL_CUDA(cudaMemcpyAsync(hs.p, d, sizeof(u32), cudaMemcpyDeviceToHost, stream));
+  HL_CUDA(cudaStreamSynchronize(stream));
+  return (u32)(hs.p[0] & 0xFFFFFFFFull);
+}
+double Engine::read_f64(const double* d) {
+  HL_CUDA(cudaMemcpyAsync(hs.p, d, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  HL_CUDA(cudaStreamSynchronize(stream));
+  double x;
+  std::memcpy(&x, hs.p, sizeof(double));
+  return x;
+}
+void Engine::sync() { HL_CUDA(cudaStreamSynchronize(stream)); }
+
+}  // namespace hl
+
+namespace {
+
+// Owns the stream; declared first in Holder so it is destroyed last, after
+// every stream-ordered free of the engine's buffers.
+struct StreamOwner {
+  cudaStream_t s = nullptr;
+  ~StreamOwner() {
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+};
+
+struct Batchbufs {
+  DBuf<u32> u, v;
+  DBuf<double> w;
+  DBuf<u32> xu[2], xv[2];
+  DBuf<double> xw[2];
+};
+
+}  // namespace
+
+// The engine plus the buffers that live across calls.
+struct EngineBox {
+  StreamOwner so;
+  std::unique_ptr<Engine> E;
+  Batchbufs bb;
+};
+
+static void validate_config(const hl_config* c) {
+  require(c != nullptr, "config is NULL");
+  require(std::isfinite(c->resolution), "resolution must be finite");
+  if (c->mode != HL_MODE_THROUGHPUT)
+    throw Error(HL_ERR_UNSUPPORTED,
+                "only RunMode::Throughput runs on the GPU (Deterministic is sequential)");
+  require(c->max_levels >= 1 && c->max_levels <= 64, "max_levels must be in [1, 64]");
+}
+
+static void engine_init(EngineBox& B, const hl_config* cfg) {
+  validate_config(cfg);
+  int ndev = 0;
+  HL_CUDA(cudaGetDeviceCount(&ndev));
+  require(cfg->device >= 0 && cfg->device < ndev, "device ordinal out of range");
+  HL_CUDA(cudaSetDevice(cfg->device));
+  HL_CUDA(cudaStreamCreateWithFlags(&B.so.s, cudaStreamNonBlocking));
+  B.E.reset(new Engine());
+  Engine& E = *B.E;
+  E.cfg = *cfg;
+  if (!E.cfg.max_rounds) E.cfg.max_rounds = 20;
+  E.device = cfg->device;
+  E.stream = B.so.s;
+  E.mem.stream = B.so.s;
+  E.mem.budget = cfg->hbm_budget;
+  E.multilevel = cfg->max_levels > 1;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, cfg->device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  HL_CUDA(cudaEventCreate(&E.ev0));
+  HL_CUDA(cudaEventCreate(&E.ev1));
+  E.levels.reserve(70);
+}
+
+static void engine_free(EngineBox* B) {
+  if (!B) return;
+  if (B->E) {
+    cudaSetDevice(B->E->device);
+    if (B->E->ev0) cudaEventDestroy(B->E->ev0);
+    if (B->E->ev1) cudaEventDestroy(B->E->ev1);
+  }
+  delete B;  // members: bb, E (frees on the stream), then so (destroys the stream)
+}
+
+__global__ void k_count_u8(const u8* f, u32 n, u32* out) {
+  u32 local = 0;
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    local += f[i] ? 1u : 0u;
+  for (int o = 16; o; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+}
+
+static u32 count_flags(Engine& E, const u8* f, u32 n) {
+  if (!n) return 0;
+  E.sc.cnt.ensure(E.mem, 16);
+  HL_CUDA(cudaMemsetAsync(E.sc.cnt.p + 15, 0, sizeof(u32), E.stream));
+  u32 g = (n + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  k_count_u8<<<g, 256, 0, E.stream>>>(f, n, E.sc.cnt.p + 15);
+  HL_LAUNCH_CHECK();
+  return E.read_u32(E.sc.cnt.p + 15);
+}
+
+// Algorithm 6 (hit_leiden.rs:936-1018) for one batch already on the device.
+static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
+  Engine& E = *B.E;
+  hl_batch_stats& st = E.st;
+  const u32 P = (u32)E.levels.size();
+  if (!E.multilevel) {
+    // The reference's reachable configuration: one level (state.rs:42), so
+    // no aggregation, and def_update is a no-op (hit_leiden.rs:1773-1792).
+    Level& L = E.levels[0];
+    apply_delta(E, L, delta, L.g.n, (E.cfg.flags & HL_FLAG_KEEP_SELF_LOOPS) != 0);
+    MoveOut mo = inc_movement(E, L, delta, delta.k == 0, false);
+    st.changed = count_flags(E, E.sc.changed.p, L.g.n);
+    RefineOut ro = inc_refinement(E, L, false);
+    st.iterations += mo.iterations;
+    st.moves += mo.moves;
+    st.candidates += mo.candidates;
+    st.traversed += mo.traversed;
+    st.splits += ro.splits;
+    st.merges += ro.merges;
+    st.refined = ro.refined;
+    return;
+  }
+  DevEdges cur = delta;
+  u32 cur_n = E.levels[0].g.n;
+  for (u32 p = 0; p < P; ++p) {
+    Level& L = E.levels[p];
+    apply_delta(E, L, cur, cur_n > L.g.n ? cur_n : L.g.n, true);
+    MoveOut mo = inc_movement(E, L, cur, cur.k == 0, true);
+    if (p == 0) st.changed = count_flags(E, E.sc.changed.p, L.g.n);
+    RefineOut ro = inc_refinement(E, L, true);
+    st.iterations += mo.iterations;
+    st.moves += mo.moves;
+    st.candidates += mo.candidates;
+    st.traversed += mo.traversed;
+    st.splits += ro.splits;
+    st.merges += ro.merges;
+    if (p == 0) st.refined = ro.refined;
+    if (p + 1 >= P) break;
+    Level& H = E.levels[p + 1];
+    // Grow level p+1 to hold every sub-community id handed out at level p.
+    u32 need = 0;
+    {
+      u32* o = E.sc.cnt.p + 12;
+      u32* sc = L.s_cur.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceReduce::Max(t, b, sc, o, (int64_t)L.g.n, E.stream);
+      });
+      need = E.read_u32(o) + 1;
+      for (auto& xo : E.new_ids) need = need > xo.first + 1 ? need : xo.first + 1;
+    }
+    graph_grow_nodes(E, H, need);
+    inherit_new_nodes(E, H, E.new_ids);
+    project_up(E, L, H);
+    if (cur.k == 0 && ro.refined == 0) {  // should_skip_aggregation (:1020-1022)
+      cur = DevEdges{};
+      cur_n = H.g.n;
+      continue;
+    }
+    u32 nn = 0;
+    u64 cnt = inc_aggregation(E, L, cur, &nn, true, true);
+    int slot = (p + 1) & 1;
+    B.bb.xu[slot].ensure(E.mem, cnt ? cnt : 1);
+    B.bb.xv[slot].ensure(E.mem, cnt ? cnt : 1);
+    B.bb.xw[slot].ensure(E.mem, cnt ? cnt : 1);
+    if (cnt) {
+      HL_CUDA(cudaMemcpyAsync(B.bb.xu[slot].p, E.sc.eu2.p, sizeof(u32) * cnt,
+                              cudaMemcpyDeviceToDevice, E.stream));
+      HL_CUDA(cudaMemcpyAsync(B.bb.xv[slot].p, E.sc.ev2.p, sizeof(u32) * cnt,
+                              cudaMemcpyDeviceToDevice, E.stream));
+      HL_CUDA(cudaMemcpyAsync(B.bb.xw[slot].p, E.sc.ew2.p, sizeof(double) * cnt,
+                              cudaMemcpyDeviceToDevice, E.stream));
+    }
+    cur = DevEdges{B.bb.xu[slot].p, B.bb.xv[slot].p, B.bb.xw[slot].p, cnt};
+    cur_n = nn > H.g.n ? nn : H.g.n;
+  }
+  top_down(E);
+}
+
+// Multi-level bootstrap (the spec's Algorithm 1): Move, Refine, Aggregate per
+// level until a level no longer coarsens by 1% or max_levels is reached.
+static void bootstrap(EngineBox& B, u32 n, const DevEdges& G) {
+  Engine& E = *B.E;
+  E.levels.clear();
+  E.levels.emplace_back();
+  graph_init_empty(E, E.levels[0], n);
+  if (!E.multilevel) {
+    // PartitionState::identity + an empty supergraph + hit_leiden(G): the
+    // reference tests' bootstrap (hit_leiden.rs:3119-3126).
+    hit_leiden_batch(B, G);
+    return;
+  }
+  apply_delta(E, E.levels[0], G, n, true);
+  u32 p = 0;
+  while (true) {
+    Level& L = E.levels[p];
+    const u32 np = L.g.n;
+    MoveOut mo = inc_movement(E, L, DevEdges{}, true, true);
+    RefineOut ro = inc_refinement(E, L, true);
+    E.st.iterations += mo.iterations;
+    E.st.moves += mo.moves;
+    E.st.traversed += mo.traversed;
+    E.st.merges += ro.merges;
+    u32 smax = 0;
+    {
+      u32* o = E.sc.cnt.p + 12;
+      u32* sc = L.s_cur.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceReduce::Max(t, b, sc, o, (int64_t)np, E.stream);
+      });
+      smax = E.read_u32(o);
+    }
+    u32 nn = np ? rank_compact(E, L.s_cur.p, np, smax) : 0;
+    if (np)
+      HL_CUDA(cudaMemcpyAsync(L.s_pre.p, L.s_cur.p, sizeof(u32) * np, cudaMemcpyDeviceToDevice,
+                              E.stream));
+    if (p + 1 >= E.cfg.max_levels || nn <= 1 || (u64)nn * 100 >= (u64)np * 99) break;
+    u64 cnt = aggregate_full(E, L, L.s_cur.p, nullptr, nullptr, nullptr);
+    E.levels.emplace_back();
+    Level& H = E.levels[p + 1];
+    Level& Lr = E.levels[p];
+    graph_init_empty(E, H, nn);
+    apply_delta(E, H, DevEdges{E.sc.eu2.p, E.sc.ev2.p, E.sc.ew2.p, cnt}, nn, true);
+    project_up(E, Lr, H);
+    ++p;
+  }
+  top_down(E);
+}
+
+#define HL_TRY(...)                                            \
+  try {                                                        \
+    __VA_ARGS__;                                               \
+    g_err.clear();                                             \
+    return HL_OK;                                              \
+  } catch (const hl::Error& e) {                               \
+    g_err = e.what();                                          \
+    return e.status;                                           \
+  } catch (const std::exception& e) {                          \
+    g_err = e.what();                                          \
+    return HL_ERR_CUDA;                                        \
+  } catch (...) {                                              \
+    g_err = "unknown error";                                   \
+    return HL_ERR_CUDA;                                        \
+  }
+
+static EngineBox* box(hl_graph* g) { return reinterpret_cast<EngineBox*>(g); }
+static const EngineBox* box(const hl_graph* g) { return reinterpret_cast<const EngineBox*>(g); }
+
+static void upload_edges(EngineBox& B, const uint32_t* src, const uint32_t* dst, const double* w,
+                         uint64_t m, DevEdges& out) {
+  Engine& E = *B.E;
+  B.bb.u.ensure(E.mem, m ? m : 1);
+  B.bb.v.ensure(E.mem, m ? m : 1);
+  if (m) {
+    HL_CUDA(cudaMemcpyAsync(B.bb.u.p, src, sizeof(u32) * m, cudaMemcpyHostToDevice, E.stream));
+    HL_CUDA(cudaMemcpyAsync(B.bb.v.p, dst, sizeof(u32) * m, cudaMemcpyHostToDevice, E.stream));
+  }
+  const double* dw = nullptr;
+  if (w && m) {
+    B.bb.w.ensure(E.mem, m);
+    HL_CUDA(cudaMemcpyAsync(B.bb.w.p, w, sizeof(double) * m, cudaMemcpyHostToDevice, E.stream));
+    dw = B.bb.w.p;
+  }
+  out = DevEdges{B.bb.u.p, B.bb.v.p, dw, m};
+}
+
+static void finish_stats(EngineBox& B, hl_batch_stats* stats) {
+  Engine& E = *B.E;
+  HL_CUDA(cudaEventRecord(E.ev1, E.stream));
+  HL_CUDA(cudaEventSynchronize(E.ev1));
+  float ms = 0.f;
+  HL_CUDA(cudaEventElapsedTime(&ms, E.ev0, E.ev1));
+  E.st.device_ms = ms;
+  E.st.levels = (u32)E.levels.size();
+  E.st.edges = E.levels.empty() ? 0 : E.levels[0].g.nnz / 2;
+  E.st.modularity = NAN;
+  if (E.cfg.flags & HL_FLAG_BATCH_MODULARITY)
+    E.st.modularity = modularity(E, E.levels[0], E.levels[0].f.p);
+  if (stats) *stats = E.st;
+}
+
+static void create_impl(const hl_config* cfg, uint32_t n, const uint32_t* src, const uint32_t* dst,
+                        const double* w, uint64_t m, bool device_ptrs, hl_graph** out) {
+  require(out != nullptr, "out is NULL");
+  require(m == 0 || (src && dst), "src/dst are NULL");
+  std::unique_ptr<EngineBox> B(new EngineBox());
+  engine_init(*B, cfg);
+  Engine& E = *B->E;
+  DevEdges G;
+  if (device_ptrs)
+    G = DevEdges{src, dst, w, m};
+  else
+    upload_edges(*B, src, dst, w, m, G);
+  check_endpoints(E, G, n);
+  E.integral = edges_integral(E, G);
+  E.st = hl_batch_stats{};
+  HL_CUDA(cudaEventRecord(E.ev0, E.stream));
+  bootstrap(*B, n, G);
+  if (E.levels[0].tw >= 4503599627370496.0) E.integral = false;  // 2^52
+  finish_stats(*B, nullptr);
+  *out = reinterpret_cast<hl_graph*>(B.release());
+}
+
+static void apply_impl(hl_graph* g, const uint32_t* src, const uint32_t* dst, const double* w,
+                       uint64_t k, bool device_ptrs, hl_batch_stats* stats) {
+  require(g != nullptr, "graph handle is NULL");
+  require(k == 0 || (src && dst), "src/dst are NULL");
+  EngineBox& B = *box(g);
+  Engine& E = *B.E;
+  HL_CUDA(cudaSetDevice(E.device));
+  E.st = hl_batch_stats{};
+  HL_CUDA(cudaEventRecord(E.ev0, E.stream));
+  DevEdges D;
+  if (device_ptrs)
+    D = DevEdges{src, dst, w, k};
+  else
+    upload_edges(B, src, dst, w, k, D);
+  check_endpoints(E, D, E.levels[0].g.n);
+  if (E.integral && !edges_integral(E, D)) E.integral = false;
+  hit_leiden_batch(B, D);
+  if (E.levels[0].tw >= 4503599627370496.0) E.integral = false;
+  finish_stats(B, stats);
+}
+
+extern "C" {
+
+hl_status hl_config_default(hl_config* cfg) {
+  if (!cfg) {
+    g_err = "config is NULL";
+    return HL_ERR_INVALID_INPUT;
+  }
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->resolution = 1.0;
+  cfg->mode = HL_MODE_THROUGHPUT;
+  cfg->max_levels = 10;
+  cfg->max_rounds = 20;
+  cfg->flags = 0;
+  cfg->hbm_budget = 0;
+  cfg->device = 0;
+  return HL_OK;
+}
+
+hl_status hl_create(const hl_config* cfg, uint32_t n, const uint32_t* src, const uint32_t* dst,
+                    const double* w, uint64_t m, hl_graph** out) {
+  HL_TRY(create_impl(cfg, n, src, dst, w, m, false, out));
+}
+
+hl_status hl_create_device(const hl_config* cfg, uint32_t n, const uint32_t* src,
+                           const uint32_t* dst, const double* w, uint64_t m, hl_graph** out) {
+  HL_TRY(create_impl(cfg, n, src, dst, w, m, true, out));
+}
+
+hl_status hl_apply_batch(hl_graph* g, const uint32_t* src, const uint32_t* dst, const double* w,
+                         uint64_t k, hl_batch_stats* stats) {
+  HL_TRY(apply_impl(g, src, dst, w, k, false, stats));
+}
+
+hl_status hl_apply_batch_device(hl_graph* g, const uint32_t* src, const uint32_t* dst,
+                                const double* w, uint64_t k, hl_batch_stats* stats) {
+  HL_TRY(apply_impl(g, src, dst, w, k, true, stats));
+}
+
+hl_status hl_set_resolution(hl_graph* g, double gamma) {
+  HL_TRY(require(g != nullptr, "graph handle is NULL");
+         require(std::isfinite(gamma), "resolution must be finite");
+         box(g)->E->cfg.resolution = gamma);
+}
+
+hl_status hl_num_nodes(const hl_graph* g, uint32_t* n) {
+  HL_TRY(require(g && n, "NULL argument"); *n = box(g)->E->levels[0].g.n);
+}
+
+hl_status hl_num_levels(const hl_graph* g, uint32_t* levels) {
+  HL_TRY(require(g && levels, "NULL argument"); *levels = (uint32_t)box(g)->E->levels.size());
+}
+
+hl_status hl_level_size(const hl_graph* g, uint32_t level, uint32_t* n_level) {
+  HL_TRY(require(g && n_level, "NULL argument");
+         require(level < box(g)->E->levels.size(), "level out of range");
+         *n_level = box(g)->E->levels[level].g.n);
+}
+
+hl_status hl_num_edges(const hl_graph* g, uint32_t level, uint64_t* entries) {
+  HL_TRY(require(g && entries, "NULL argument");
+         require(level < box(g)->E->levels.size(), "level out of range");
+         *entries = box(g)->E->levels[level].g.nnz);
+}
+
+static void get_map_impl(const hl_graph* g, uint32_t level, uint32_t which, uint32_t* out) {
+  require(g && out, "NULL argument");
+  Engine& E = *const_cast<EngineBox*>(box(g))->E;
+  require(level < E.levels.size(), "level out of range");
+  HL_CUDA(cudaSetDevice(E.device));
+  Level& L = E.levels[level];
+  const u32* src = nullptr;
+  switch (which) {
+    case HL_MAP_COMMUNITY: src = L.f.p; break;
+    case HL_MAP_REFINED: src = L.gm.p; break;
+    case HL_MAP_SUB_PREVIOUS: src = L.s_pre.p; break;
+    case HL_MAP_SUB_CURRENT: src = L.s_cur.p; break;
+    default: require(false, "unknown map");
+  }
+  if (L.g.n)
+    HL_CUDA(cudaMemcpyAsync(out, src, sizeof(u32) * L.g.n, cudaMemcpyDeviceToHost, E.stream));
+  E.sync();
+}
+
+hl_status hl_get_map(const hl_graph* g, uint32_t level, uint32_t which, uint32_t* out) {
+  HL_TRY(get_map_impl(g, level, which, out));
+}
+
+static void get_partition_impl(const hl_graph* g, uint32_t* out) {
+  require(g && out, "NULL argument");
+  Engine& E = *const_cast<EngineBox*>(box(g))->E;
+  HL_CUDA(cudaSetDevice(E.device));
+  Level& L = E.levels[0];
+  u32 n = L.g.n;
+  if (!n) return;
+  DBuf<u32> tmp;
+  tmp.ensure(E.mem, n);
+  canonicalize_device(E, L.f.p, n, tmp.p);
+  HL_CUDA(cudaMemcpyAsync(out, tmp.p, sizeof(u32) * n, cudaMemcpyDeviceToHost, E.stream));
+  E.sync();
+}
+
+hl_status hl_get_partition(const hl_graph* g, uint32_t* out) { HL_TRY(get_partition_impl(g, out)); }
+
+static void get_csr_impl(const hl_graph* g, uint32_t level, uint64_t* off, uint32_t* col,
+                         double* w) {
+  require(g != nullptr, "NULL argument");
+  Engine& E = *const_cast<EngineBox*>(box(g))->E;
+  require(level < E.levels.size(), "level out of range");
+  HL_CUDA(cudaSetDevice(E.device));
+  DevGraph& G = E.levels[level].g;
+  if (off)
+    HL_CUDA(cudaMemcpyAsync(off, G.off.p, sizeof(u64) * ((size_t)G.n + 1), cudaMemcpyDeviceToHost,
+                            E.stream));
+  if (col && G.nnz)
+    HL_CUDA(cudaMemcpyAsync(col, G.col.p, sizeof(u32) * G.nnz, cudaMemcpyDeviceToHost, E.stream));
+  if (w && G.nnz)
+    HL_CUDA(cudaMemcpyAsync(w, G.w.p, sizeof(double) * G.nnz, cudaMemcpyDeviceToHost, E.stream));
+  E.sync();
+}
+
+hl_status hl_get_csr(const hl_graph* g, uint32_t level, uint64_t* off, uint32_t* col, double* w) {
+  HL_TRY(get_csr_impl(g, level, off, col, w));
+}
+
+static void modularity_impl(const hl_graph* g, const uint32_t* part, double* q) {
+  require(g && q, "NULL argument");
+  Engine& E = *const_cast<EngineBox*>(box(g))->E;
+  HL_CUDA(cudaSetDevice(E.device));
+  Level& L = E.levels[0];
+  if (!part) {
+    *q = modularity(E, L, L.f.p);
+    return;
+  }
+  DBuf<u32> tmp;
+  tmp.ensure(E.mem, L.g.n ? L.g.n : 1);
+  if (L.g.n)
+    HL_CUDA(cudaMemcpyAsync(tmp.p, part, sizeof(u32) * L.g.n, cudaMemcpyHostToDevice, E.stream));
+  *q = modularity(E, L, tmp.p);
+}
+
+hl_status hl_modularity(const hl_graph* g, double* q) { HL_TRY(modularity_impl(g, nullptr, q)); }
+
+hl_status hl_modularity_of(const hl_graph* g, const uint32_t* part, double* q) {
+  HL_TRY(require(part != nullptr, "part is NULL"); modularity_impl(g, part, q));
+}
+
+void hl_destroy(hl_graph* g) {
+  try {
+    engine_free(box(g));
+  } catch (...) {
+  }
+}
+
+const char* hl_last_error(void) { return g_err.c_str(); }
+
+const char* hl_version(void) { return "hit-leiden-b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Function-level entry points (include/hl_debug.h)
+// ---------------------------------------------------------------------------
+namespace {
+
+std::unique_ptr<EngineBox> scratch_engine(int32_t device) {
+  hl_config cfg;
+  hl_config_default(&cfg);
+  cfg.device = device;
+  std::unique_ptr<EngineBox> B(new EngineBox());
+  engine_init(*B, &cfg);
+  return B;
+}
+
+bool host_integral(const double* w, u64 n) {
+  if (!w) return true;
+  for (u64 i = 0; i < n; ++i)
+    if (!(w[i] == std::floor(w[i])) || std::fabs(w[i]) > 4294967296.0) return false;
+  return true;
+}
+
+template <typename T>
+void up(Engine& E, DBuf<T>& b, const T* h, size_t n) {
+  b.ensure(E.mem, n ? n : 1);
+  if (n && h) HL_CUDA(cudaMemcpyAsync(b.p, h, sizeof(T) * n, cudaMemcpyHostToDevice, E.stream));
+}
+
+template <typename T>
+void down(Engine& E, T* h, const T* d, size_t n) {
+  if (n && h) HL_CUDA(cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, E.stream));
+}
+
+void level_from_host(Engine& E, Level& L, u32 n, const u64* off, const u32* col, const double* w) {
+  graph_init_empty(E, L, n);
+  u64 nnz = off ? off[n] : 0;
+  L.g.nnz = nnz;
+  up(E, L.g.off, off, (size_t)n + 1);
+  up(E, L.g.col, col, nnz);
+  up(E, L.g.w, w, nnz);
+  u64 loops = 0;
+  for (u32 v = 0; v < n; ++v)
+    for (u64 p = off[v]; p < off[v + 1]; ++p)
+      if (col[p] == v) ++loops;
+  L.g.self_loop_entries = loops;
+  E.integral = host_integral(w, nnz);
+  recompute_all_degrees(E, L);
+}
+
+DevEdges edges_up(Engine& E, Batchbufs& bb, const u32* s, const u32* d, const double* w, u64 k) {
+  up(E, bb.u, s, k);
+  up(E, bb.v, d, k);
+  const double* dw = nullptr;
+  if (w && k) {
+    up(E, bb.w, w, k);
+    dw = bb.w.p;
+  }
+  return DevEdges{bb.u.p, bb.v.p, dw, k};
+}
+
+}  // namespace
+
+extern "C" {
+
+hl_status hl_dbg_tree_sum(int32_t device, const double* x, uint64_t n, double* out) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    DBuf<double> d;
+    up(E, d, x, n);
+    *out = tree_sum(E, d.p, n);
+  });
+}
+
+hl_status hl_dbg_move_eval(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
+                           const double* w, const uint32_t* f, const double* d, uint64_t d_len,
+                           const double* k, double tw, double gamma, const uint32_t* verts,
+                           uint64_t nv, uint32_t* out_to, double* out_gain) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    E.cfg.resolution = gamma;
+    Level L;
+    level_from_host(E, L, n, off, col, w);
+    up(E, L.f, f, n);
+    up(E, L.k, k, n);
+    L.tw = tw;
+    DBuf<double> dd;
+    up(E, dd, d, d_len);
+    DBuf<u32> vv, to;
+    DBuf<double> g;
+    up(E, vv, verts, nv);
+    to.ensure(E.mem, nv ? nv : 1);
+    g.ensure(E.mem, nv ? nv : 1);
+    run_eval(E, 0, vv.p, (u32)nv, L, L.s_cur.p, dd.p, nullptr, true, to.p, g.p, nullptr);
+    down(E, out_to, to.p, nv);
+    down(E, out_gain, g.p, nv);
+    E.sync();
+  });
+}
+
+hl_status hl_dbg_select_decoupled(int32_t device, const uint32_t* node, const uint32_t* from,
+                                  const uint32_t* to, const double* gain, uint64_t m,
+                                  uint32_t* out_nodes, uint64_t* out_count) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    // Rank order: gain descending, node ascending (throughput.rs:205-210).
+    std::vector<u64> order(m);
+    for (u64 i = 0; i < m; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](u64 a, u64 b) { return node[a] < node[b]; });
+    std::vector<u32> sn, sf, stt;
+    std::vector<double> sg;
+    for (u64 i : order)
+      if (gain[i] > 0.0) {
+        sn.push_back(node[i]);
+        sf.push_back(from[i]);
+        stt.push_back(to[i]);
+        sg.push_back(gain[i]);
+      }
+    std::vector<u64> rk(sn.size());
+    for (u64 i = 0; i < rk.size(); ++i) rk[i] = i;
+    std::stable_sort(rk.begin(), rk.end(), [&](u64 a, u64 b) { return sg[a] > sg[b]; });
+    u32 M = (u32)rk.size();
+    std::vector<u32> rf(M), rt(M), rn(M);
+    u32 mx = 0;
+    for (u32 r = 0; r < M; ++r) {
+      rf[r] = sf[rk[r]];
+      rt[r] = stt[rk[r]];
+      rn[r] = sn[rk[r]];
+      mx = std::max(mx, std::max(rf[r], rt[r]));
+    }
+    Scratch& S = E.sc;
+    S.cnt.ensure(E.mem, 16);
+    ensure_comm_arrays(E, (size_t)mx + 2);
+    up(E, S.sel_from, rf.data(), M);
+    up(E, S.sel_to, rt.data(), M);
+    S.status.ensure(E.mem, M ? M : 1);
+    S.nmask.ensure(E.mem, M ? M : 1);
+    u64 cntv = 0;
+    if (M) {
+      select_decoupled_dev(E, M);
+      std::vector<u8> stv(M);
+      down(E, stv.data(), S.status.p, M);
+      E.sync();
+      for (u32 r = 0; r < M; ++r)
+        if (stv[r] == 1) out_nodes[cntv++] = rn[r];
+    }
+    *out_count = cntv;
+  });
+}
+
+hl_status hl_dbg_apply_delta(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
+                             const double* w, uint32_t delta_n, const uint32_t* dsrc,
+                             const uint32_t* ddst, const double* dw, uint64_t dk,
+                             int32_t keep_self_loops, uint64_t* out_off, uint32_t* out_col,
+                             double* out_w, uint64_t cap, uint64_t* out_nnz) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    Level L;
+    level_from_host(E, L, n, off, col, w);
+    DevEdges D = edges_up(E, B->bb, dsrc, ddst, dw, dk);
+    if (!host_integral(dw, dk)) E.integral = false;
+    u32 nn = std::max(n, delta_n);
+    check_endpoints(E, D, nn);
+    apply_delta(E, L, D, nn, keep_self_loops != 0);
+    *out_nnz = L.g.nnz;
+    require(L.g.nnz <= cap, "output capacity too small");
+    down(E, out_off, L.g.off.p, (size_t)L.g.n + 1);
+    down(E, out_col, L.g.col.p, L.g.nnz);
+    down(E, out_w, L.g.w.p, L.g.nnz);
+    E.sync();
+  });
+}
+
+hl_status hl_dbg_inc_movement(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
+                              const double* w, const uint32_t* dsrc, const uint32_t* ddst,
+                              const double* dw, uint64_t dk, uint32_t* f, const uint32_t* s,
+                              double gamma, uint32_t max_rounds, int32_t mark_moved,
+                              uint8_t* changed, uint8_t* affected, uint32_t* iterations) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    E.cfg.resolution = gamma;
+    E.cfg.max_rounds = max_rounds ? max_rounds : 20;
+    Level L;
+    level_from_host(E, L, n, off, col, w);
+    up(E, L.f, f, n);
+    up(E, L.s_cur, s, n);
+    DevEdges D = edges_up(E, B->bb, dsrc, ddst, dw, dk);
+    MoveOut mo = inc_movement(E, L, D, dk == 0, mark_moved != 0);
+    down(E, f, L.f.p, n);
+    down(E, changed, E.sc.changed.p, n);
+    down(E, affected, E.sc.affected.p, n);
+    E.sync();
+    if (iterations) *iterations = mo.iterations;
+  });
+}
+
+hl_status hl_dbg_inc_refinement(int32_t device, uint32_t n, const uint64_t* off,
+                                const uint32_t* col, const double* w, const uint32_t* f,
+                                uint32_t* s, const uint8_t* affected, double gamma,
+                                int32_t cc_same_community, uint8_t* refined) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    E.cfg.resolution = gamma;
+    Level L;
+    level_from_host(E, L, n, off, col, w);
+    up(E, L.f, f, n);
+    up(E, L.s_cur, s, n);
+    up(E, E.sc.affected, affected, n);
+    inc_refinement(E, L, cc_same_community != 0);
+    down(E, s, L.s_cur.p, n);
+    down(E, refined, E.sc.refined.p, n);
+    E.sync();
+  });
+}
+
+hl_status hl_dbg_inc_aggregation(int32_t device, uint32_t n, const uint64_t* off,
+                                 const uint32_t* col, const double* w, const uint32_t* dsrc,
+                                 const uint32_t* ddst, const double* dw, uint64_t dk,
+                                 const uint32_t* s_pre, const uint32_t* s_cur,
+                                 const uint8_t* refined, int32_t changed_only,
+                                 int32_t edge_weight_loops, uint32_t* out_s_pre,
+                                 uint32_t* out_next_n, uint32_t* out_u, uint32_t* out_v,
+                                 double* out_w, uint64_t cap, uint64_t* out_count) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    Level L;
+    level_from_host(E, L, n, off, col, w);
+    up(E, L.s_pre, s_pre, n);
+    up(E, L.s_cur, s_cur, n);
+    up(E, E.sc.refined, refined, n);
+    DevEdges D = edges_up(E, B->bb, dsrc, ddst, dw, dk);
+    u32 nn = 0;
+    u64 cnt = inc_aggregation(E, L, D, &nn, changed_only != 0, edge_weight_loops != 0);
+    *out_count = cnt;
+    if (out_next_n) *out_next_n = nn;
+    require(cnt <= cap, "output capacity too small");
+    down(E, out_s_pre, L.s_pre.p, n);
+    down(E, out_u, E.sc.eu2.p, cnt);
+    down(E, out_v, E.sc.ev2.p, cnt);
+    down(E, out_w, E.sc.ew2.p, cnt);
+    E.sync();
+  });
+}
+
+hl_status hl_dbg_modularity(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
+                            const double* w, const uint32_t* part, double* q) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    Level L;
+    level_from_host(E, L, n, off, col, w);
+    DBuf<u32> pp;
+    up(E, pp, part, n);
+    *q = modularity(E, L, pp.p);
+  });
+}
+
+hl_status hl_canonicalize(int32_t device, uint32_t* labels, uint64_t n) {
+  HL_TRY({
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    DBuf<u32> a, b;
+    up(E, a, labels, n);
+    b.ensure(E.mem, n ? n : 1);
+    canonicalize_device(E, a.p, n, b.p);
+    down(E, labels, b.p, n);
+    E.sync();
+  });
+}
+
+}  // extern "C"

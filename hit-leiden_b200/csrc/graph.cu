@@ -1,0 +1,653 @@
+// graph.cu — device CSR maintenance: G ← G ⊕ ΔG (K1), degrees, 2m.
+//
+// apply_delta restates in_memory.rs:103-137: every ΔG edge is keyed by
+// (min, max); a key's new weight is its existing weight followed by the
+// batch's deltas in batch order (a stable sort keeps that order); keys whose
+// weight ends at <= 1e-12 disappear.  Instead of rebuilding a hash map of all
+// m edges, only the changed keys are resolved: weight updates are written in
+// place, and inserts/deletes become sorted row-operations that a warp-per-row
+// merge folds into a fresh CSR with rows still sorted by neighbour id.
+#include "hl_engine.cuh"
+
+namespace hl {
+
+__global__ void k_fill_u8(u8* p, u8 v, u64 n) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+__global__ void k_iota(u32* p, u32 n) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    p[i] = (u32)i;
+}
+
+__global__ void k_fill_u64_range(u64* p, u64 v, u64 lo, u64 hi) {
+  for (u64 i = lo + blockIdx.x * (u64)blockDim.x + threadIdx.x; i < hi;
+       i += (u64)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+__global__ void k_fill_f64_range(double* p, double v, u64 lo, u64 hi) {
+  for (u64 i = lo + blockIdx.x * (u64)blockDim.x + threadIdx.x; i < hi;
+       i += (u64)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+__global__ void k_iota_range(u32* p, u64 lo, u64 hi) {
+  for (u64 i = lo + blockIdx.x * (u64)blockDim.x + threadIdx.x; i < hi;
+       i += (u64)gridDim.x * blockDim.x)
+    p[i] = (u32)i;
+}
+
+static inline u32 grid_for(u64 n, u32 block = 256) {
+  u64 g = (n + block - 1) / block;
+  if (g > 148u * 64u) g = 148u * 64u;
+  return g ? (u32)g : 1u;
+}
+
+void graph_init_empty(Engine& E, Level& L, u32 n) {
+  L.g.n = n;
+  L.g.nnz = 0;
+  L.g.self_loop_entries = 0;
+  L.g.off.ensure(E.mem, (size_t)n + 1);
+  HL_CUDA(cudaMemsetAsync(L.g.off.p, 0, sizeof(u64) * ((size_t)n + 1), E.stream));
+  L.g.col.ensure(E.mem, 1);
+  L.g.w.ensure(E.mem, 1);
+  L.f.ensure(E.mem, n ? n : 1);
+  L.gm.ensure(E.mem, n ? n : 1);
+  L.s_pre.ensure(E.mem, n ? n : 1);
+  L.s_cur.ensure(E.mem, n ? n : 1);
+  L.k.ensure(E.mem, n ? n : 1);
+  if (n) {
+    k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.f.p, n);
+    k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.gm.p, n);
+    k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.s_pre.p, n);
+    k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.s_cur.p, n);
+    HL_CUDA(cudaMemsetAsync(L.k.p, 0, sizeof(double) * n, E.stream));
+  }
+  L.tw = 0.0;
+  HL_LAUNCH_CHECK();
+}
+
+// New nodes start isolated with identity maps (PartitionState::identity).
+void graph_grow_nodes(Engine& E, Level& L, u32 n) {
+  u32 old = L.g.n;
+  if (n <= old) return;
+  L.g.off.ensure(E.mem, (size_t)n + 1, true);
+  k_fill_u64_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.g.off.p, L.g.nnz, (u64)old + 1,
+                                                             (u64)n + 1);
+  L.f.ensure(E.mem, n, true);
+  L.gm.ensure(E.mem, n, true);
+  L.s_pre.ensure(E.mem, n, true);
+  L.s_cur.ensure(E.mem, n, true);
+  L.k.ensure(E.mem, n, true);
+  k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.f.p, old, n);
+  k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.gm.p, old, n);
+  k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.s_pre.p, old, n);
+  k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.s_cur.p, old, n);
+  k_fill_f64_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.k.p, 0.0, old, n);
+  L.g.n = n;
+  HL_LAUNCH_CHECK();
+}
+
+__device__ __forceinline__ u64 lower_bound_u32(const u32* a, u64 lo, u64 hi, u32 x) {
+  while (lo < hi) {
+    u64 mid = (lo + hi) >> 1;
+    if (a[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ u64 lower_bound_u64(const u64* a, u64 lo, u64 hi, u64 x) {
+  while (lo < hi) {
+    u64 mid = (lo + hi) >> 1;
+    if (a[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_check_endpoints(const u32* u, const u32* v, u64 k, u32 n, u32* bad) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < k; i += (u64)gridDim.x * blockDim.x)
+    if (u[i] >= n || v[i] >= n) atomicAdd(bad, 1u);
+}
+
+void check_endpoints(Engine& E, const DevEdges& b, u32 n) {
+  if (!b.k) return;
+  E.sc.cnt.ensure(E.mem, 16);
+  HL_CUDA(cudaMemsetAsync(E.sc.cnt.p, 0, sizeof(u32), E.stream));
+  k_check_endpoints<<<grid_for(b.k), 256, 0, E.stream>>>(b.u, b.v, b.k, n, E.sc.cnt.p);
+  HL_LAUNCH_CHECK();
+  u32 bad = E.read_u32(E.sc.cnt.p);
+  require(bad == 0, "edge endpoint exceeds node_count (" + std::to_string(bad) + " edges)");
+}
+
+__global__ void k_integral(const double* w, u64 k, u32* bad) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < k; i += (u64)gridDim.x * blockDim.x) {
+    double x = w[i];
+    if (!(x == floor(x)) || fabs(x) > 4294967296.0) atomicAdd(bad, 1u);
+  }
+}
+
+bool edges_integral(Engine& E, const DevEdges& b) {
+  if (!b.k || !b.w) return true;
+  E.sc.cnt.ensure(E.mem, 16);
+  HL_CUDA(cudaMemsetAsync(E.sc.cnt.p + 1, 0, sizeof(u32), E.stream));
+  k_integral<<<grid_for(b.k), 256, 0, E.stream>>>(b.w, b.k, E.sc.cnt.p + 1);
+  HL_LAUNCH_CHECK();
+  return E.read_u32(E.sc.cnt.p + 1) == 0;
+}
+
+__global__ void k_delta_keys(const u32* u, const u32* v, u64 k, u64* keys, u32* idx) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < k; i += (u64)gridDim.x * blockDim.x) {
+    u32 a = u[i], b = v[i];
+    u32 lo = a < b ? a : b, hi = a < b ? b : a;
+    keys[i] = ((u64)lo << 32) | hi;
+    idx[i] = (u32)i;
+  }
+}
+
+__global__ void k_heads(const u64* sk, u64 k, u32* head) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < k; i += (u64)gridDim.x * blockDim.x)
+    head[i] = (i == 0 || sk[i] != sk[i - 1]) ? 1u : 0u;
+}
+
+__global__ void k_seg_start(const u32* head, const u32* segid, u64 k, u32* seg_start) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < k; i += (u64)gridDim.x * blockDim.x)
+    if (head[i]) seg_start[segid[i]] = (u32)i;
+}
+
+enum : u8 { OP_NONE = 0, OP_UPD = 1, OP_INS = 2, OP_DEL = 3 };
+
+// One thread per distinct key: existing weight, then the batch's deltas in
+// batch order (in_memory.rs:133-137), then the > 1e-12 filter (:110).
+__global__ void k_resolve(u32 U, const u32* seg_start, u64 k, const u64* sk, const u32* sidx,
+                          const double* bw, const u64* off, const u32* col, double* w,
+                          bool keep_loops, u8* op, double* neww, u8* ktouched, u32* nops_del,
+                          u32* nops_ins, u32* loop_counts) {
+  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < U; j += (u64)gridDim.x * blockDim.x) {
+    u64 t0 = seg_start[j];
+    u64 t1 = (j + 1 < U) ? seg_start[j + 1] : k;
+    u64 key = sk[t0];
+    u32 a = (u32)(key >> 32), b = (u32)key;
+    u64 o0 = off[a], o1 = off[a + 1];
+    u64 p = lower_bound_u32(col, o0, o1, b);
+    bool present = p < o1 && col[p] == b;
+    if (a == b && !keep_loops) present = false;
+    double x = present ? w[p] : 0.0;
+    for (u64 t = t0; t < t1; ++t) x = __dadd_rn(x, bw ? bw[sidx[t]] : 1.0);
+    u8 o = OP_NONE;
+    u32 nd = 0, ni = 0;
+    if (present) {
+      if (x > 1e-12) {
+        o = OP_UPD;
+        w[p] = x;
+        if (a == b) {
+          w[p + 1] = x;
+        } else {
+          u64 q = lower_bound_u32(col, off[b], off[b + 1], a);
+          w[q] = x;
+        }
+      } else {
+        o = OP_DEL;
+        nd = 2;
+        if (a == b) atomicAdd(&loop_counts[1], 1u);
+      }
+    } else if (x > 1e-12) {
+      o = OP_INS;
+      ni = 2;
+      if (a == b) atomicAdd(&loop_counts[0], 1u);
+    }
+    op[j] = o;
+    neww[j] = x;
+    nops_del[j] = nd;
+    nops_ins[j] = ni;
+    if (o != OP_NONE) {
+      ktouched[a] = 1;
+      ktouched[b] = 1;
+    }
+  }
+}
+
+constexpr u32 DEL_MARK = 0xFFFFFFFFu;
+
+__global__ void k_emit_rowops(u32 U, const u32* seg_start, const u64* sk, const u8* op,
+                              const u32* pos_del, const u32* pos_ins, u64 ins_base, u64* rkeys,
+                              u32* rvals) {
+  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < U; j += (u64)gridDim.x * blockDim.x) {
+    u8 o = op[j];
+    if (o != OP_DEL && o != OP_INS) continue;
+    u64 key = sk[seg_start[j]];
+    u32 a = (u32)(key >> 32), b = (u32)key;
+    u64 p = (o == OP_DEL) ? pos_del[j] : ins_base + pos_ins[j];
+    u32 val = (o == OP_DEL) ? DEL_MARK : (u32)j;
+    rkeys[p] = ((u64)a << 32) | b;
+    rvals[p] = val;
+    rkeys[p + 1] = ((u64)b << 32) | a;
+    rvals[p + 1] = val;
+  }
+}
+
+__global__ void k_count_loops(u32 n, const u64* off, const u32* col, u32* total) {
+  u32 local = 0;
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
+    u64 o0 = off[v], o1 = off[v + 1];
+    u64 p = lower_bound_u32(col, o0, o1, (u32)v);
+    while (p < o1 && col[p] == (u32)v) {
+      ++local;
+      ++p;
+    }
+  }
+  if (local) atomicAdd(total, local);
+}
+
+// Existing self-loops are dropped by the reference's apply_delta
+// (collect_canonical_edges keeps node < neighbor only, in_memory.rs:125).
+__global__ void k_emit_loop_drops(u32 n, const u64* off, const u32* col, u64* rkeys, u32* rvals,
+                                  u64 base, u64 limit, u32* counter, u8* ktouched, u32* err) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
+    u64 o0 = off[v], o1 = off[v + 1];
+    u64 p = lower_bound_u32(col, o0, o1, (u32)v);
+    u32 c = 0;
+    while (p + c < o1 && col[p + c] == (u32)v) ++c;
+    if (c) {
+      u32 at = atomicAdd(counter, c);
+      for (u32 i = 0; i < c; ++i) {
+        if (base + at + i >= limit) {
+          atomicAdd(err, 1u);
+          break;
+        }
+        rkeys[base + at + i] = ((u64)v << 32) | (u32)v;
+        rvals[base + at + i] = DEL_MARK;
+      }
+      ktouched[v] = 1;
+    }
+  }
+}
+
+__global__ void k_rowop_flags(const u32* rvals, u64 R, u32* isdel, u32* isins) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < R; t += (u64)gridDim.x * blockDim.x) {
+    bool d = rvals[t] == DEL_MARK;
+    isdel[t] = d ? 1u : 0u;
+    isins[t] = d ? 0u : 1u;
+  }
+}
+
+__global__ void k_rowop_deg(const u64* rkeys, const u32* rvals, u64 R, int* ddeg, u8* touched) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < R; t += (u64)gridDim.x * blockDim.x) {
+    u32 r = (u32)(rkeys[t] >> 32);
+    atomicAdd(&ddeg[r], rvals[t] == DEL_MARK ? -1 : 1);
+    touched[r] = 1;
+  }
+}
+
+__global__ void k_new_degrees(u32 n, const u64* off, const int* ddeg, u64* nd) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v <= n; v += (u64)gridDim.x * blockDim.x)
+    nd[v] = v < n ? (u64)((long long)(off[v + 1] - off[v]) + ddeg[v]) : 0ull;
+}
+
+// Warp per row: untouched rows are copied; touched rows are merged with their
+// sorted row-operations (deleted entries skipped, inserted entries placed by
+// rank), so the output row is again sorted by neighbour id.
+__global__ void k_merge_rows(u32 n, const u64* off, const u32* col, const double* w,
+                             const u64* noff, u32* ncol, double* nw, const u8* touched,
+                             const u64* rkeys, const u32* rvals, u64 R, const u32* delpre,
+                             const u32* inspre, const double* neww, u64 nnz_new, u32* err) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 r = warp; r < n; r += nwarps) {
+    u64 o0 = off[r], o1 = off[r + 1], no = noff[r];
+    if (!touched[r]) {
+      if (no + (o1 - o0) > nnz_new) {
+        if (lane == 0) atomicAdd(err, 1u);
+        continue;
+      }
+      for (u64 q = o0 + lane; q < o1; q += 32) {
+        ncol[no + (q - o0)] = col[q];
+        nw[no + (q - o0)] = w[q];
+      }
+      continue;
+    }
+    u64 a = lower_bound_u64(rkeys, 0, R, (u64)r << 32);
+    u64 b = lower_bound_u64(rkeys, a, R, ((u64)r + 1) << 32);
+    u32 dbase = delpre[a], ibase = inspre[a];
+    for (u64 q = o0 + lane; q < o1; q += 32) {
+      u32 c = col[q];
+      u64 key = ((u64)r << 32) | c;
+      u64 lb = lower_bound_u64(rkeys, a, b, key);
+      bool deleted = lb < b && rkeys[lb] == key && rvals[lb] == DEL_MARK;
+      if (deleted) continue;
+      u64 out = no + (q - o0) - (delpre[lb] - dbase) + (inspre[lb] - ibase);
+      if (out >= nnz_new) {
+        atomicAdd(err, 1u);
+        continue;
+      }
+      ncol[out] = c;
+      nw[out] = w[q];
+    }
+    for (u64 t = a + lane; t < b; t += 32) {
+      if (rvals[t] == DEL_MARK) continue;
+      u32 c = (u32)rkeys[t];
+      u64 lb = lower_bound_u64(rkeys, a, b, ((u64)r << 32) | c);
+      u64 qc = lower_bound_u32(col, o0, o1, c);
+      u64 out = no + (qc - o0) - (delpre[lb] - dbase) + (inspre[t] - ibase);
+      if (out >= nnz_new) {
+        atomicAdd(err, 1u);
+        continue;
+      }
+      ncol[out] = c;
+      nw[out] = neww[rvals[t]];
+    }
+  }
+}
+
+// Row sums in CSR order (hit_leiden.rs:1063).  Serial per row: the exact
+// left-to-right rounding of the reference for any weights.
+__global__ void k_row_sum_serial(const u32* rows, u32 nr, const u64* off, const double* w,
+                                 double* k) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < nr; i += (u64)gridDim.x * blockDim.x) {
+    u32 v = rows[i];
+    double s = 0.0;
+    for (u64 p = off[v]; p < off[v + 1]; ++p) s = __dadd_rn(s, w[p]);
+    k[v] = s;
+  }
+}
+
+// Warp-parallel row sums; only used when every weight is integral, where any
+// summation order gives the same bits.
+__global__ void k_row_sum_warp(const u32* rows, u32 nr, const u64* off, const double* w,
+                               double* k) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 i = warp; i < nr; i += nwarps) {
+    u32 v = rows ? rows[i] : (u32)i;
+    double s = 0.0;
+    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32) s += w[p];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) k[v] = s;
+  }
+}
+
+__global__ void k_row_sum_serial_all(u32 n, const u64* off, const double* w, double* k) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (u64 p = off[v]; p < off[v + 1]; ++p) s = __dadd_rn(s, w[p]);
+    k[v] = s;
+  }
+}
+
+// Fixed-shape pairwise sum: tiles of 1024 (+0.0 padded) folded by stride
+// halving; repeated on the tile sums until one value remains.
+__global__ void k_tree_tile(const double* x, u64 n, double* out) {
+  __shared__ double s[1024];
+  u64 base = (u64)blockIdx.x * 1024;
+  for (u32 i = threadIdx.x; i < 1024; i += blockDim.x) {
+    u64 idx = base + i;
+    s[i] = idx < n ? x[idx] : 0.0;
+  }
+  __syncthreads();
+  for (u32 st = 512; st >= 1; st >>= 1) {
+    for (u32 i = threadIdx.x; i < st; i += blockDim.x) s[i] = __dadd_rn(s[i], s[i + st]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = s[0];
+}
+
+double tree_sum(Engine& E, const double* x, u64 n) {
+  if (n == 0) return 0.0;
+  u64 tiles = (n + 1023) / 1024;
+  E.sc.red.ensure(E.mem, tiles + 1);
+  E.sc.red2.ensure(E.mem, (tiles + 1023) / 1024 + 1);
+  const double* src = x;
+  double* a = E.sc.red.p;
+  double* b = E.sc.red2.p;
+  u64 cur = n;
+  while (true) {
+    u64 t = (cur + 1023) / 1024;
+    k_tree_tile<<<(u32)t, 256, 0, E.stream>>>(src, cur, a);
+    HL_LAUNCH_CHECK();
+    if (t == 1) break;
+    src = a;
+    cur = t;
+    std::swap(a, b);
+  }
+  return E.read_f64(a);
+}
+
+static void recompute_rows(Engine& E, Level& L, const u32* rows, u32 nr) {
+  if (!nr) return;
+  if (E.integral)
+    k_row_sum_warp<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p,
+                                                                  L.k.p);
+  else
+    k_row_sum_serial<<<grid_for(nr), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p, L.k.p);
+  HL_LAUNCH_CHECK();
+}
+
+void recompute_all_degrees(Engine& E, Level& L) {
+  u32 n = L.g.n;
+  if (n) {
+    if (E.integral)
+      k_row_sum_warp<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(nullptr, n, L.g.off.p, L.g.w.p,
+                                                                   L.k.p);
+    else
+      k_row_sum_serial_all<<<grid_for(n), 256, 0, E.stream>>>(n, L.g.off.p, L.g.w.p, L.k.p);
+    HL_LAUNCH_CHECK();
+  }
+  L.tw = tree_sum(E, L.k.p, n);
+}
+
+struct FlagToIndex {
+  const u8* f;
+  __host__ __device__ bool operator()(const u32& i) const { return f[i] != 0; }
+};
+
+void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_loops) {
+  Scratch& S = E.sc;
+  cudaStream_t st = E.stream;
+  if (new_n > L.g.n) graph_grow_nodes(E, L, new_n);
+  const u32 n = L.g.n;
+  const bool drop_loops = !keep_loops && L.g.self_loop_entries > 0;
+  if (b.k == 0 && !drop_loops) return;
+  const u64 k = b.k;
+
+  S.ktouched.ensure(E.mem, n ? n : 1);
+  HL_CUDA(cudaMemsetAsync(S.ktouched.p, 0, n ? n : 1, st));
+  S.cnt.ensure(E.mem, 16);
+  HL_CUDA(cudaMemsetAsync(S.cnt.p, 0, 16 * sizeof(u32), st));  // [0] ins loops [1] del loops [2] drops
+
+  u32 U = 0;
+  if (k) {
+    S.keys.ensure(E.mem, k);
+    S.keys2.ensure(E.mem, k);
+    S.idx.ensure(E.mem, k);
+    S.idx2.ensure(E.mem, k);
+    S.segid.ensure(E.mem, k);
+    S.seg_start.ensure(E.mem, k + 1);
+    S.rowlist.ensure(E.mem, k);
+    k_delta_keys<<<grid_for(k), 256, 0, st>>>(b.u, b.v, k, S.keys.p, S.idx.p);
+    HL_LAUNCH_CHECK();
+    u64* kin = S.keys.p;
+    u64* kout = S.keys2.p;
+    u32* vin = S.idx.p;
+    u32* vout = S.idx2.p;
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceRadixSort::SortPairs(t, bytes, kin, kout, vin, vout, (int64_t)k, 0, 64, st);
+    });
+    k_heads<<<grid_for(k), 256, 0, st>>>(kout, k, S.rowlist.p);
+    HL_LAUNCH_CHECK();
+    u32* head = S.rowlist.p;
+    u32* segid = S.segid.p;
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceScan::ExclusiveSum(t, bytes, head, segid, (int64_t)k, st);
+    });
+    k_seg_start<<<grid_for(k), 256, 0, st>>>(head, segid, k, S.seg_start.p);
+    HL_LAUNCH_CHECK();
+    u32 last_seg = E.read_u32(segid + (k - 1));
+    u32 last_head = E.read_u32(head + (k - 1));
+    U = last_seg + last_head;
+
+    S.op.ensure(E.mem, U);
+    S.neww.ensure(E.mem, U);
+    S.nops_del.ensure(E.mem, U + 1);
+    S.nops_ins.ensure(E.mem, U + 1);
+    S.pos_del.ensure(E.mem, U + 1);
+    S.pos_ins.ensure(E.mem, U + 1);
+    k_resolve<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, k, kout, vout, b.w, L.g.off.p,
+                                           L.g.col.p, L.g.w.p, keep_loops, S.op.p, S.neww.p,
+                                           S.ktouched.p, S.nops_del.p, S.nops_ins.p, S.cnt.p);
+    HL_LAUNCH_CHECK();
+    HL_CUDA(cudaMemsetAsync(S.nops_del.p + U, 0, sizeof(u32), st));
+    HL_CUDA(cudaMemsetAsync(S.nops_ins.p + U, 0, sizeof(u32), st));
+    u32* nd = S.nops_del.p;
+    u32* pd = S.pos_del.p;
+    u32* ni = S.nops_ins.p;
+    u32* pi = S.pos_ins.p;
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceScan::ExclusiveSum(t, bytes, nd, pd, (int64_t)U + 1, st);
+    });
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceScan::ExclusiveSum(t, bytes, ni, pi, (int64_t)U + 1, st);
+    });
+  }
+  u64 n_del_keys = U ? E.read_u32(S.pos_del.p + U) : 0;
+  u64 n_ins = U ? E.read_u32(S.pos_ins.p + U) : 0;
+
+  // Existing self-loops to drop (reference behaviour) — counted first.
+  u64 n_drop = 0;
+  if (drop_loops) {
+    HL_CUDA(cudaMemsetAsync(S.cnt.p + 3, 0, sizeof(u32), st));
+    k_count_loops<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, S.cnt.p + 3);
+    HL_LAUNCH_CHECK();
+    n_drop = E.read_u32(S.cnt.p + 3);
+  }
+  u64 R = n_del_keys + n_drop + n_ins;
+
+  if (R == 0) {
+    // Weight updates only: no structural change.
+    if (U) {
+      u32* rows = S.rowlist.p;
+      S.cnt.ensure(E.mem, 16);
+      u32* cnt = S.cnt.p + 8;
+      S.act.ensure(E.mem, n ? n : 1);
+      cub_run(E, [&](void* t, size_t& bytes) {
+        return cub::DeviceSelect::Flagged(t, bytes, cub::CountingInputIterator<u32>(0),
+                                          S.ktouched.p, S.act.p, cnt, (int64_t)n, st);
+      });
+      u32 nr = E.read_u32(cnt);
+      (void)rows;
+      recompute_rows(E, L, S.act.p, nr);
+      L.tw = tree_sum(E, L.k.p, n);
+    }
+    return;
+  }
+
+  S.rkeys.ensure(E.mem, R);
+  S.rkeys2.ensure(E.mem, R);
+  S.rvals.ensure(E.mem, R);
+  S.rvals2.ensure(E.mem, R);
+  if (U)
+    k_emit_rowops<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, S.keys2.p, S.op.p, S.pos_del.p,
+                                               S.pos_ins.p, n_del_keys + n_drop, S.rkeys.p,
+                                               S.rvals.p);
+  if (drop_loops && n_drop)
+    k_emit_loop_drops<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, S.rkeys.p, S.rvals.p,
+                                                   n_del_keys, n_del_keys + n_drop, S.cnt.p + 2,
+                                                   S.ktouched.p, S.cnt.p + 4);
+  HL_LAUNCH_CHECK();
+  {
+    u64* kin = S.rkeys.p;
+    u64* kout = S.rkeys2.p;
+    u32* vin = S.rvals.p;
+    u32* vout = S.rvals2.p;
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceRadixSort::SortPairs(t, bytes, kin, kout, vin, vout, (int64_t)R, 0, 64, st);
+    });
+  }
+  S.delpre.ensure(E.mem, R + 1);
+  S.inspre.ensure(E.mem, R + 1);
+  // reuse: flags in segid/rowlist-sized temporaries
+  DBuf<u32>& fdel = S.cand_idx;
+  DBuf<u32>& fins = S.cand_to;
+  fdel.ensure(E.mem, R + 1);
+  fins.ensure(E.mem, R + 1);
+  k_rowop_flags<<<grid_for(R), 256, 0, st>>>(S.rvals2.p, R, fdel.p, fins.p);
+  HL_LAUNCH_CHECK();
+  HL_CUDA(cudaMemsetAsync(fdel.p + R, 0, sizeof(u32), st));
+  HL_CUDA(cudaMemsetAsync(fins.p + R, 0, sizeof(u32), st));
+  {
+    u32* a = fdel.p;
+    u32* o = S.delpre.p;
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceScan::ExclusiveSum(t, bytes, a, o, (int64_t)R + 1, st);
+    });
+    u32* a2 = fins.p;
+    u32* o2 = S.inspre.p;
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceScan::ExclusiveSum(t, bytes, a2, o2, (int64_t)R + 1, st);
+    });
+  }
+  S.ddeg.ensure(E.mem, n ? n : 1);
+  S.touched.ensure(E.mem, n ? n : 1);
+  HL_CUDA(cudaMemsetAsync(S.ddeg.p, 0, sizeof(int) * (n ? n : 1), st));
+  HL_CUDA(cudaMemsetAsync(S.touched.p, 0, n ? n : 1, st));
+  k_rowop_deg<<<grid_for(R), 256, 0, st>>>(S.rkeys2.p, S.rvals2.p, R, S.ddeg.p, S.touched.p);
+  S.newoff.ensure(E.mem, (size_t)n + 1);
+  k_new_degrees<<<grid_for((u64)n + 1), 256, 0, st>>>(n, L.g.off.p, S.ddeg.p, S.newoff.p);
+  HL_LAUNCH_CHECK();
+  {
+    u64* a = S.newoff.p;
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceScan::ExclusiveSum(t, bytes, a, a, (int64_t)n + 1, st);
+    });
+  }
+  u64 nnz_new = E.read_u64(S.newoff.p + n);
+  DevGraph& G = L.g;
+  DBuf<u32> ncol;
+  DBuf<double> nw;
+  ncol.ensure(E.mem, nnz_new ? nnz_new : 1);
+  nw.ensure(E.mem, nnz_new ? nnz_new : 1);
+  if (n)
+    k_merge_rows<<<grid_for((u64)n * 32), 256, 0, st>>>(n, G.off.p, G.col.p, G.w.p, S.newoff.p,
+                                                         ncol.p, nw.p, S.touched.p, S.rkeys2.p,
+                                                         S.rvals2.p, R, S.delpre.p, S.inspre.p,
+                                                         S.neww.p, nnz_new, S.cnt.p + 4);
+  HL_LAUNCH_CHECK();
+  if (E.read_u32(S.cnt.p + 4) != 0)
+    throw Error(HL_ERR_CUDA, "internal error: CSR merge produced an out-of-range position");
+  G.col.swap(ncol);
+  G.w.swap(nw);
+  G.off.swap(S.newoff);
+  G.nnz = nnz_new;
+  ncol.release();
+  nw.release();
+  {
+    u32 ins_loops = E.read_u32(S.cnt.p + 0);
+    u32 del_loops = E.read_u32(S.cnt.p + 1);
+    if (drop_loops)
+      G.self_loop_entries = 2ull * ins_loops;
+    else
+      G.self_loop_entries = G.self_loop_entries + 2ull * ins_loops - 2ull * del_loops;
+  }
+  // Degrees of every row whose weights changed, then 2m.
+  {
+    u32* cnt = S.cnt.p + 8;
+    S.act.ensure(E.mem, n ? n : 1);
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceSelect::Flagged(t, bytes, cub::CountingInputIterator<u32>(0), S.ktouched.p,
+                                        S.act.p, cnt, (int64_t)n, st);
+    });
+    u32 nr = E.read_u32(cnt);
+    recompute_rows(E, L, S.act.p, nr);
+    L.tw = tree_sum(E, L.k.p, n);
+  }
+}
+
+}  // namespace hl

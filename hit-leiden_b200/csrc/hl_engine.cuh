@@ -1,0 +1,162 @@
+// hl_engine.cuh — device state of one graph handle and the stage entry points.
+#pragma once
+#include <cub/cub.cuh>
+
+#include "hl_internal.cuh"
+
+namespace hl {
+
+// Undirected weighted CSR on the device: both directions stored, rows sorted
+// by neighbour id, a self-loop stored twice in its row (in_memory.rs:20-72).
+struct DevGraph {
+  u32 n = 0;
+  u64 nnz = 0;
+  u64 self_loop_entries = 0;
+  DBuf<u64> off;  // n+1
+  DBuf<u32> col;
+  DBuf<double> w;
+};
+
+// One hierarchy level (state.rs:19-32): supergraph G^p and its maps.
+struct Level {
+  DevGraph g;
+  DBuf<u32> f;      // community_mapping_per_level[p]
+  DBuf<u32> gm;     // refined_community_mapping_per_level[p]
+  DBuf<u32> s_pre;  // previous_subcommunity_mapping_per_level[p]
+  DBuf<u32> s_cur;  // current_subcommunity_mapping_per_level[p]
+  DBuf<double> k;   // weighted degree of each level-p node
+  double tw = 0.0;  // 2m of G^p
+};
+
+// An edge list on the device (GraphInput): w == nullptr means weight 1.0.
+struct DevEdges {
+  const u32* u = nullptr;
+  const u32* v = nullptr;
+  const double* w = nullptr;
+  u64 k = 0;
+};
+
+// Scratch reused by every stage; grown on demand, never shrunk.
+struct Scratch {
+  DBuf<u8> cub_tmp;
+  // edge-list staging (host batches, aggregation output)
+  DBuf<u32> eu, ev, eu2, ev2;
+  DBuf<double> ew, ew2;
+  // delta application
+  DBuf<u64> keys, keys2, rkeys, rkeys2;
+  DBuf<u32> idx, idx2, segid, seg_start, rvals, rvals2;
+  DBuf<u8> op, touched, ktouched, isdel, isins;
+  DBuf<double> neww;
+  DBuf<u32> nops_del, nops_ins, pos_del, pos_ins;
+  DBuf<u32> delpre, inspre;
+  DBuf<int> ddeg;
+  DBuf<u64> newoff;
+  DBuf<u32> rowlist;
+  // node flags (level size)
+  DBuf<u8> active, next, changed, affected, refined;
+  DBuf<u32> act, cand_idx, cnt;
+  DBuf<u32> cand_to, cand_node;
+  DBuf<double> cand_gain, cand_k;
+  DBuf<u64> gkey, gkey2;
+  DBuf<u32> sel_from, sel_to, sel_node, order, order2;
+  DBuf<u8> status, nmask;
+  DBuf<u32> role;
+  DBuf<u64> res;
+  DBuf<double> d;       // community degrees (2n)
+  DBuf<u32> used, rank;
+  // refinement
+  DBuf<u32> par, csize, ncomp, newid, minmem;
+  DBuf<u64> keep;
+  DBuf<u8> affsc, cand_sc, blocked;
+  DBuf<u32> sizes;
+  DBuf<double> dS, wsp, dcomm;
+  DBuf<u32> upd_node, upd_to;
+  // reductions
+  DBuf<double> red, red2;
+  DBuf<u64> red64;
+  DBuf<u32> origin;
+};
+
+struct Engine {
+  hl_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  MemCtx mem;
+  Scratch sc;
+  std::vector<Level> levels;
+  bool multilevel = false;
+  bool integral = true;  // every weight integral: all FP64 sums exact in any order
+  HostScalars hs;
+  u64 epoch = 1;         // selection epochs (reservation keys)
+  u32 sel_round = 0;     // role tag of the current selection
+  u64 stats_sel_iters = 0;
+  // per-call statistics
+  hl_batch_stats st{};
+  std::vector<std::pair<u32, u32>> new_ids;  // (new sub-community id, origin) of the last refinement
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  u64 read_u64(const u64* dptr);
+  u32 read_u32(const u32* dptr);
+  double read_f64(const double* dptr);
+  void sync();
+};
+
+// CUB helper: query temp bytes, grow the shared temp buffer, run.
+template <typename F>
+inline void cub_run(Engine& E, F f) {
+  size_t bytes = 0;
+  HL_CUDA(f((void*)nullptr, bytes));
+  E.sc.cub_tmp.ensure(E.mem, bytes + 16);
+  HL_CUDA(f((void*)E.sc.cub_tmp.p, bytes));
+}
+
+// ---- stage entry points (one .cu file each) --------------------------------
+// graph.cu
+void graph_init_empty(Engine& E, Level& L, u32 n);
+void graph_grow_nodes(Engine& E, Level& L, u32 n);
+void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_loops);
+void recompute_all_degrees(Engine& E, Level& L);
+double tree_sum(Engine& E, const double* x, u64 n);
+bool edges_integral(Engine& E, const DevEdges& b);
+void check_endpoints(Engine& E, const DevEdges& b, u32 n);
+
+// move.cu
+struct MoveOut {
+  u32 iterations = 0;
+  u64 moves = 0, candidates = 0, traversed = 0, changed = 0;
+};
+MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active,
+                     bool mark_moved);
+void recompute_comm_degrees(Engine& E, Level& L, const u32* part, u32 ncomm_cap, double* d);
+void compact_labels_if_needed(Engine& E, u32* labels, u32 n, u32 limit);
+void select_decoupled_dev(Engine& E, u32 M);
+void ensure_comm_arrays(Engine& E, size_t ncap);
+void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
+              const double* d, const u8* blocked, bool allow_empty, u32* out_to, double* out_gain,
+              unsigned long long* traversed);
+
+// refine.cu
+struct RefineOut {
+  u64 splits = 0, merges = 0, refined = 0;
+  u32 smax_before = 0;
+};
+RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community);
+
+// aggregate.cu
+u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n,
+                    bool changed_only, bool edge_weight_loops);  // output in sc.eu2/ev2/ew2
+u64 aggregate_full(Engine& E, Level& L, const u32* s, u32* out_u, u32* out_v, double* out_w);
+void project_up(Engine& E, Level& lo, Level& hi);
+void top_down(Engine& E);
+void inherit_new_nodes(Engine& E, Level& hi, const std::vector<std::pair<u32, u32>>& ids);
+
+// modularity.cu
+double modularity(Engine& E, Level& L, const u32* part);
+void canonicalize_device(Engine& E, u32* labels, u64 n, u32* out);
+u32 rank_compact(Engine& E, u32* labels, u32 n, u32 id_bound);
+
+// kernels used by more than one stage
+__global__ void k_fill_u8(u8* p, u8 v, u64 n);
+__global__ void k_iota(u32* p, u32 n);
+
+}  // namespace hl

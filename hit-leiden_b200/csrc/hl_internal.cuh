@@ -1,0 +1,176 @@
+// hl_internal.cuh — shared definitions of the B200 HIT-Leiden library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/hl.h"
+
+namespace hl {
+
+using u8 = uint8_t;
+using u32 = uint32_t;
+using u64 = uint64_t;
+
+constexpr u32 NONE32 = 0xFFFFFFFFu;
+
+// ---------------------------------------------------------------------------
+// Errors: internal code throws hl::Error; the C ABI converts it to a status and
+// a thread-local message.  Nothing propagates across the boundary.
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  hl_status status;
+  Error(hl_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define HL_CUDA(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      if (_e == cudaErrorMemoryAllocation)                                                 \
+        throw ::hl::Error(HL_ERR_OUT_OF_MEMORY, std::string(#call ": ") +                   \
+                                                    cudaGetErrorString(_e));               \
+      throw ::hl::Error(HL_ERR_CUDA, std::string(__FILE__) + ":" + std::to_string(__LINE__) + \
+                                         " " #call ": " + cudaGetErrorString(_e));         \
+    }                                                                                      \
+  } while (0)
+
+#define HL_LAUNCH_CHECK() HL_CUDA(cudaGetLastError())
+
+inline void require(bool ok, const std::string& msg) {
+  if (!ok) throw Error(HL_ERR_INVALID_INPUT, msg);
+}
+
+// ---------------------------------------------------------------------------
+// Device memory: stream-ordered allocations charged against a per-handle HBM
+// budget.  Buffers only grow (geometric), so steady-state batches allocate
+// nothing.
+// ---------------------------------------------------------------------------
+struct MemCtx {
+  cudaStream_t stream = nullptr;
+  u64 used = 0;
+  u64 peak = 0;
+  u64 budget = 0;  // 0 = unlimited
+};
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  MemCtx* ctx = nullptr;
+
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), cap(o.cap), ctx(o.ctx) {
+    o.p = nullptr;
+    o.cap = 0;
+  }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      cap = o.cap;
+      ctx = o.ctx;
+      o.p = nullptr;
+      o.cap = 0;
+    }
+    return *this;
+  }
+  ~DBuf() { release(); }
+
+  void release() {
+    if (p && ctx) {
+      cudaFreeAsync(p, ctx->stream);
+      ctx->used -= cap * sizeof(T);
+    }
+    p = nullptr;
+    cap = 0;
+  }
+
+  // Ensure capacity for n elements.  Contents are NOT preserved unless keep.
+  void ensure(MemCtx& c, size_t n, bool keep = false) {
+    ctx = &c;
+    if (n <= cap) return;
+    size_t ncap = cap ? cap : 1;
+    while (ncap < n) ncap = ncap < (1u << 20) ? ncap * 4 : ncap + ncap / 2;
+    u64 bytes = (u64)ncap * sizeof(T);
+    if (c.budget && c.used - (u64)cap * sizeof(T) + bytes > c.budget)
+      throw Error(HL_ERR_OUT_OF_MEMORY, "HBM budget exceeded (" + std::to_string(c.used + bytes) +
+                                            " > " + std::to_string(c.budget) + " bytes)");
+    T* np = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&np, bytes, c.stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(HL_ERR_OUT_OF_MEMORY, std::string("device allocation of ") +
+                                            std::to_string(bytes) + " bytes failed: " +
+                                            cudaGetErrorString(e));
+    }
+    if (keep && p && cap) HL_CUDA(cudaMemcpyAsync(np, p, cap * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
+    if (p) {
+      cudaFreeAsync(p, c.stream);
+      c.used -= (u64)cap * sizeof(T);
+    }
+    p = np;
+    cap = ncap;
+    c.used += bytes;
+    if (c.used > c.peak) c.peak = c.used;
+  }
+  void swap(DBuf& o) {
+    std::swap(p, o.p);
+    std::swap(cap, o.cap);
+    std::swap(ctx, o.ctx);
+  }
+  T* get() const { return p; }
+};
+
+// Pinned host staging for small scalar read-backs.
+struct HostScalars {
+  u64* p = nullptr;
+  explicit HostScalars() { HL_CUDA(cudaMallocHost((void**)&p, 64 * sizeof(u64))); }
+  ~HostScalars() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+inline u32 div_up(u64 a, u64 b) { return (u32)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// FP64 arithmetic that rounds exactly like the reference's Rust expressions.
+// The library is compiled with -fmad=false; the explicit _rn intrinsics make
+// the evaluation order of every gain formula visible here as well.
+// ---------------------------------------------------------------------------
+// ΔQ(v: C→C', γ) = (w_to - w_cur)/2m + γ·k_v·(d_cur - k_v - d_to)/(2m)²
+// (parallel_frontier.rs:185-190; hit_leiden.rs:1135-1140, :1488-1495).
+__device__ __forceinline__ double move_gain(double w_to, double w_cur, double tw, double gamma,
+                                            double kv, double d_cur, double d_to) {
+  double a = __ddiv_rn(__dsub_rn(w_to, w_cur), tw);
+  double b = __dmul_rn(__dmul_rn(gamma, kv), __dsub_rn(__dsub_rn(d_cur, kv), d_to));
+  return __dadd_rn(a, __ddiv_rn(b, __dmul_rn(tw, tw)));
+}
+// Gain of moving to the empty community (parallel_frontier.rs:207-211).
+__device__ __forceinline__ double empty_gain(double w_cur, double tw, double gamma, double kv,
+                                             double d_cur) {
+  double a = __ddiv_rn(-w_cur, tw);
+  double b = __dmul_rn(__dmul_rn(gamma, kv), __dsub_rn(d_cur, kv));
+  return __dadd_rn(a, __ddiv_rn(b, __dmul_rn(tw, tw)));
+}
+// ΔQ(S→∅) of the T-filter (hit_leiden.rs:1545-1547, :1627-1629).
+__device__ __forceinline__ double remove_gain(double w_sc, double tw, double gamma, double ds,
+                                              double dpar) {
+  double a = __ddiv_rn(-w_sc, tw);
+  double b = __dmul_rn(__dmul_rn(gamma, ds), __dsub_rn(dpar, ds));
+  return __dadd_rn(a, __ddiv_rn(b, __dmul_rn(tw, tw)));
+}
+
+// Total order on doubles as unsigned keys (ascending).
+__device__ __forceinline__ u64 double_key(double x) {
+  u64 b = (u64)__double_as_longlong(x);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+
+}  // namespace hl

@@ -1,0 +1,869 @@
+// move.cu — inc-movement, throughput mode (hit_leiden.rs:1024-1101 →
+// throughput.rs:80-236 → parallel_frontier.rs:133-239).
+//
+// Per round, on a snapshot of f and d(C):
+//   1. every active vertex finds its best move (warp per vertex; neighbour
+//      communities accumulated in first-encounter CSR order so ties go to the
+//      earliest candidate, exactly like the reference's dirty list + strict >);
+//   2. positive candidates are sorted by (gain desc, node asc);
+//   3. the reference's sequential greedy "no move may leave an acceptor or
+//      enter an emitter" selection is reproduced exactly with deterministic
+//      reservations: a candidate is decided once it holds the minimum rank on
+//      every endpoint community whose role is still open;
+//   4. accepted moves are applied, d(C) updated in selected order, and the
+//      next frontier / K set marked.
+#include "hl_engine.cuh"
+
+namespace hl {
+
+static inline u32 grid_for(u64 n, u32 block = 256) {
+  u64 g = (n + block - 1) / block;
+  if (g > 148u * 64u) g = 148u * 64u;
+  return g ? (u32)g : 1u;
+}
+
+// ----------------------------------------------------------------------------
+// Seeding: inc_movement lines 2-8 (hit_leiden.rs:1037-1057).
+// ----------------------------------------------------------------------------
+__global__ void k_seed(const u32* u, const u32* v, const double* w, u64 k, const u32* f,
+                       const u32* s, u8* active, u8* affected) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < k; i += (u64)gridDim.x * blockDim.x) {
+    u32 a = u[i], b = v[i];
+    double al = w ? w[i] : 1.0;
+    bool same_f = f[a] == f[b];
+    if ((al > 0.0 && !same_f) || (al < 0.0 && same_f)) {
+      active[a] = 1;
+      active[b] = 1;
+    }
+    if (s[a] == s[b]) {
+      affected[a] = 1;
+      affected[b] = 1;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Community degrees d(C) = Σ_{f(v)=C} k_v (hit_leiden.rs:1060-1066).
+// ----------------------------------------------------------------------------
+__global__ void k_comm_deg_atomic(u32 n, const u32* part, const double* k, double* d) {
+  __shared__ double sk[256];
+  __shared__ u32 sc[256];
+  const u32 lane = threadIdx.x & 31;
+  const u32 wbase = threadIdx.x & ~31u;
+  for (u64 base = blockIdx.x * (u64)blockDim.x; base < n; base += (u64)gridDim.x * blockDim.x) {
+    u64 v = base + threadIdx.x;
+    bool ok = v < n;
+    u32 c = ok ? part[v] : NONE32;
+    double kv = ok ? k[v] : 0.0;
+    sk[threadIdx.x] = kv;
+    sc[threadIdx.x] = c;
+    __syncwarp();
+    u32 grp = __match_any_sync(0xffffffffu, c);
+    if (ok && lane == (u32)(__ffs(grp) - 1)) {
+      double s = 0.0;
+      for (u32 m = grp; m; m &= m - 1) s += sk[wbase + __ffs(m) - 1];
+      atomicAdd(&d[c], s);
+    }
+    __syncwarp();
+  }
+}
+
+// Ordered variant: nodes sorted by (community, node); one thread per community
+// sums its members' degrees in ascending node order.
+__global__ void k_comm_deg_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 n,
+                                   const u32* sorted_nodes, const double* k, double* d) {
+  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < nu; j += (u64)gridDim.x * blockDim.x) {
+    u32 a = ustart[j], b = (j + 1 < nu) ? ustart[j + 1] : n;
+    double s = 0.0;
+    for (u32 t = a; t < b; ++t) s = __dadd_rn(s, k[sorted_nodes[t]]);
+    d[ukeys[j]] = s;
+  }
+}
+
+__global__ void k_copy_u32(const u32* a, u32* b, u64 n) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+__global__ void k_heads_u32(const u32* sk, u64 n, u32* head) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    head[i] = (i == 0 || sk[i] != sk[i - 1]) ? 1u : 0u;
+}
+
+__global__ void k_seg_compact(const u32* head, const u32* segid, const u32* sk, u64 n,
+                              u32* ukeys, u32* ustart) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    if (head[i]) {
+      ukeys[segid[i]] = sk[i];
+      ustart[segid[i]] = (u32)i;
+    }
+}
+
+// d[c] for every c in [0, ncomm_cap): zeroed, then filled from `part`.
+void recompute_comm_degrees(Engine& E, Level& L, const u32* part, u32 ncomm_cap, double* d) {
+  cudaStream_t st = E.stream;
+  u32 n = L.g.n;
+  HL_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * (size_t)ncomm_cap, st));
+  if (!n) return;
+  if (E.integral) {
+    k_comm_deg_atomic<<<grid_for(n), 256, 0, st>>>(n, part, L.k.p, d);
+    HL_LAUNCH_CHECK();
+    return;
+  }
+  Scratch& S = E.sc;
+  S.order.ensure(E.mem, n);
+  S.order2.ensure(E.mem, n);
+  S.used.ensure(E.mem, n);
+  S.rank.ensure(E.mem, n);
+  S.cand_node.ensure(E.mem, n);
+  S.sel_node.ensure(E.mem, n);
+  S.segid.ensure(E.mem, n);
+  k_iota<<<grid_for(n), 256, 0, st>>>(S.order.p, n);
+  k_copy_u32<<<grid_for(n), 256, 0, st>>>(part, S.used.p, n);
+  HL_LAUNCH_CHECK();
+  u32* kin = S.used.p;
+  u32* kout = S.rank.p;
+  u32* vin = S.order.p;
+  u32* vout = S.order2.p;
+  cub_run(E, [&](void* t, size_t& b) {
+    return cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int64_t)n, 0, 32, st);
+  });
+  k_heads_u32<<<grid_for(n), 256, 0, st>>>(kout, n, S.cand_node.p);
+  HL_LAUNCH_CHECK();
+  u32* h = S.cand_node.p;
+  u32* sid = S.segid.p;
+  cub_run(E, [&](void* t, size_t& b) {
+    return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)n, st);
+  });
+  u32 nu = E.read_u32(sid + n - 1) + E.read_u32(h + n - 1);
+  k_seg_compact<<<grid_for(n), 256, 0, st>>>(h, sid, kout, n, S.used.p, S.sel_node.p);
+  k_comm_deg_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.used.p, S.sel_node.p, n, vout, L.k.p, d);
+  HL_LAUNCH_CHECK();
+}
+
+// ----------------------------------------------------------------------------
+// Label compaction by rank when some id reached >= limit.
+// ----------------------------------------------------------------------------
+__global__ void k_mark_used(const u32* lab, u32 n, u32* used) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    used[lab[i]] = 1;
+}
+__global__ void k_relabel(u32* lab, u32 n, const u32* rank) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    lab[i] = rank[lab[i]];
+}
+
+// Rank-compacts labels in place; returns the number of distinct labels.
+u32 rank_compact(Engine& E, u32* labels, u32 n, u32 id_bound) {
+  cudaStream_t st = E.stream;
+  Scratch& S = E.sc;
+  S.used.ensure(E.mem, (size_t)id_bound + 1);
+  S.rank.ensure(E.mem, (size_t)id_bound + 1);
+  HL_CUDA(cudaMemsetAsync(S.used.p, 0, sizeof(u32) * ((size_t)id_bound + 1), st));
+  k_mark_used<<<grid_for(n), 256, 0, st>>>(labels, n, S.used.p);
+  HL_LAUNCH_CHECK();
+  u32* a = S.used.p;
+  u32* r = S.rank.p;
+  cub_run(E, [&](void* t, size_t& b) {
+    return cub::DeviceScan::ExclusiveSum(t, b, a, r, (int64_t)id_bound + 1, st);
+  });
+  u32 distinct = E.read_u32(r + id_bound);
+  k_relabel<<<grid_for(n), 256, 0, st>>>(labels, n, S.rank.p);
+  HL_LAUNCH_CHECK();
+  return distinct;
+}
+
+static u32 max_label(Engine& E, const u32* labels, u32 n) {
+  if (!n) return 0;
+  u32* out = E.sc.cnt.p + 12;
+  cub_run(E, [&](void* t, size_t& b) {
+    return cub::DeviceReduce::Max(t, b, labels, out, (int64_t)n, E.stream);
+  });
+  return E.read_u32(out);
+}
+
+void compact_labels_if_needed(Engine& E, u32* labels, u32 n, u32 limit) {
+  if (!n) return;
+  E.sc.cnt.ensure(E.mem, 16);
+  u32 mx = max_label(E, labels, n);
+  if (mx < limit) return;
+  rank_compact(E, labels, n, mx);
+}
+
+// ----------------------------------------------------------------------------
+// Best-move evaluation (shared with refinement).
+// ----------------------------------------------------------------------------
+enum EvalKind { EVAL_MOVE = 0, EVAL_REFINE = 1 };
+
+struct EvalArgs {
+  const u32* verts;    // vertices to evaluate
+  u32 nv;
+  const u64* off;
+  const u32* col;
+  const double* w;
+  const u32* f;        // communities
+  const u32* s;        // sub-communities (refine keys)
+  const double* d;     // degrees of the key sets (d(C) or d(S))
+  const double* kdeg;  // vertex degrees
+  const u8* blocked;   // refine: T-filter blocked sub-communities
+  double tw, gamma;
+  u32 n;               // graph size (empty-community id = n + v)
+  bool allow_empty;
+  u32* out_to;
+  double* out_gain;
+  // global hash tables for high-degree vertices
+  const u64* tab_off;  // per vertex index (0 if not big)
+  u32* tkey;
+  u32* tpos;
+  double* tval;
+  unsigned long long* traversed;
+};
+
+constexpr u32 WARP_TAB = 512;  // entries per warp table in shared memory
+constexpr u32 WARPS_PER_BLOCK = 4;
+constexpr u32 SMALL_DEG = 32;
+constexpr u32 MID_DEG = WARP_TAB / 2;
+
+__device__ __forceinline__ u32 hash32(u32 x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// Warp-argmax key: larger gain wins; on equal gains the smaller CSR position.
+__device__ __forceinline__ void warp_best(double& g, u32& pos, u32& key) {
+  for (int o = 16; o; o >>= 1) {
+    double og = __shfl_xor_sync(0xffffffffu, g, o);
+    u32 op = __shfl_xor_sync(0xffffffffu, pos, o);
+    u32 ok = __shfl_xor_sync(0xffffffffu, key, o);
+    if (og > g || (og == g && op < pos)) {
+      g = og;
+      pos = op;
+      key = ok;
+    }
+  }
+}
+
+template <int KIND>
+__device__ __forceinline__ bool entry_key(const EvalArgs& A, u32 v, u32 nb, u32 fv, u32& key) {
+  if (KIND == EVAL_MOVE) {
+    if (nb == v) return false;  // self-loops skipped (parallel_frontier.rs:164-166)
+    key = A.f[nb];
+    return true;
+  } else {
+    if (A.f[nb] != fv) return false;  // same community only (throughput.rs:308-311)
+    key = A.s[nb];
+    return true;
+  }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_eval(EvalArgs A) {
+  __shared__ u32 s_key[WARPS_PER_BLOCK][WARP_TAB];
+  __shared__ u32 s_pos[WARPS_PER_BLOCK][WARP_TAB];
+  __shared__ double s_val[WARPS_PER_BLOCK][WARP_TAB];
+  __shared__ double s_w[WARPS_PER_BLOCK][32];
+  __shared__ unsigned long long s_trav;
+  const u32 lane = threadIdx.x & 31;
+  const u32 wib = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_trav = 0;
+  __syncthreads();
+  unsigned long long my_trav = 0;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 i = warp; i < A.nv; i += nwarps) {
+    const u32 v = A.verts[i];
+    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u64 deg = o1 - o0;
+    const u32 fv = A.f[v];
+    const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+    const double kv = A.kdeg[v];
+    if (lane == 0) my_trav += deg;
+    double wcur = 0.0;
+    double best_g = 0.0;
+    u32 best_pos = NONE32, best_key = cur;
+    if (deg <= SMALL_DEG) {
+      // One chunk: groups of lanes with equal key; the lowest lane is the
+      // first CSR occurrence, and the leader sums its group in lane order.
+      u32 key = NONE32;
+      double wv = 0.0;
+      bool has = false;
+      if (lane < deg) {
+        u32 nb = A.col[o0 + lane];
+        wv = A.w[o0 + lane];
+        has = entry_key<KIND>(A, v, nb, fv, key);
+        if (!has) key = NONE32;
+      }
+      s_w[wib][lane] = wv;
+      __syncwarp();
+      u32 grp = __match_any_sync(0xffffffffu, key);
+      bool leader = has && lane == (u32)(__ffs(grp) - 1);
+      double sum = 0.0;
+      if (leader)
+        for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, s_w[wib][__ffs(m) - 1]);
+      u32 cl = __ballot_sync(0xffffffffu, leader && key == cur);
+      if (cl) wcur = __shfl_sync(0xffffffffu, sum, __ffs(cl) - 1);
+      double g = -1.0;
+      u32 p = NONE32;
+      if (leader && key != cur && A.tw != 0.0) {
+        bool blk = (KIND == EVAL_REFINE) && A.blocked[key];
+        if (!blk) {
+          g = move_gain(sum, wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
+          p = lane;
+        }
+      }
+      u32 kk = key;
+      if (p == NONE32) g = -1.0;
+      warp_best(g, p, kk);
+      if (p != NONE32 && g > 0.0) {
+        best_g = g;
+        best_key = kk;
+        best_pos = p;
+      }
+      __syncwarp();
+    } else {
+      // Hash table: shared memory for mid degrees, a private global region
+      // for high-degree vertices.  Chunks are processed in CSR order and each
+      // key's sum is extended serially, preserving the reference's rounding.
+      u32* tk;
+      u32* tp;
+      double* tv;
+      u32 cap;
+      if (deg <= MID_DEG) {
+        tk = s_key[wib];
+        tp = s_pos[wib];
+        tv = s_val[wib];
+        cap = WARP_TAB;
+      } else {
+        u64 base = A.tab_off[i];
+        tk = A.tkey + base;
+        tp = A.tpos + base;
+        tv = A.tval + base;
+        cap = 2;
+        while (cap < 2 * deg) cap <<= 1;
+      }
+      const u32 mask = cap - 1;
+      for (u32 t = lane; t < cap; t += 32) tk[t] = NONE32;
+      __syncwarp();
+      for (u64 base = o0; base < o1; base += 32) {
+        u64 q = base + lane;
+        u32 key = NONE32;
+        double wv = 0.0;
+        bool has = false;
+        if (q < o1) {
+          u32 nb = A.col[q];
+          wv = A.w[q];
+          has = entry_key<KIND>(A, v, nb, fv, key);
+          if (!has) key = NONE32;
+        }
+        s_w[wib][lane] = wv;
+        __syncwarp();
+        u32 grp = __match_any_sync(0xffffffffu, key);
+        if (has && lane == (u32)(__ffs(grp) - 1)) {
+          u32 slot = hash32(key) & mask;
+          while (true) {
+            u32 prev = atomicCAS(&tk[slot], NONE32, key);
+            if (prev == NONE32) {
+              tp[slot] = (u32)(q - o0);
+              double sum = 0.0;
+              for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, s_w[wib][__ffs(m) - 1]);
+              tv[slot] = sum;
+              break;
+            }
+            if (prev == key) {
+              double sum = tv[slot];
+              for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, s_w[wib][__ffs(m) - 1]);
+              tv[slot] = sum;
+              break;
+            }
+            slot = (slot + 1) & mask;
+          }
+        }
+        __syncwarp();
+      }
+      // w(v, cur)
+      for (u32 t = lane; t < cap; t += 32)
+        if (tk[t] == cur) wcur = tv[t];
+      for (int o = 16; o; o >>= 1) {
+        double x = __shfl_xor_sync(0xffffffffu, wcur, o);
+        if (x != 0.0) wcur = x;
+      }
+      double g = -1.0;
+      u32 p = NONE32, kk = cur;
+      if (A.tw != 0.0) {
+        for (u32 t = lane; t < cap; t += 32) {
+          u32 key = tk[t];
+          if (key == NONE32 || key == cur) continue;
+          if (KIND == EVAL_REFINE && A.blocked[key]) continue;
+          double gn = move_gain(tv[t], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
+          u32 pp = tp[t];
+          if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+            g = gn;
+            p = pp;
+            kk = key;
+          }
+        }
+      }
+      if (p == NONE32) g = -1.0;
+      warp_best(g, p, kk);
+      if (p != NONE32 && g > 0.0) {
+        best_g = g;
+        best_key = kk;
+        best_pos = p;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      u32 to = best_key;
+      double g = best_g;
+      if (KIND == EVAL_MOVE && A.allow_empty && A.tw != 0.0) {
+        double eg = empty_gain(wcur, A.tw, A.gamma, kv, A.d[cur]);
+        if (eg > g) {
+          g = eg;
+          to = A.n + v;
+        }
+      }
+      (void)best_pos;
+      A.out_to[i] = to;
+      A.out_gain[i] = g;
+    }
+  }
+  if (A.traversed) {
+    if (lane == 0 && my_trav) atomicAdd(&s_trav, my_trav);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_trav) atomicAdd(A.traversed, s_trav);
+  }
+}
+
+__global__ void k_big_caps(const u32* verts, u32 nv, const u64* off, u64* cap) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < nv; i += (u64)gridDim.x * blockDim.x) {
+    u32 v = verts[i];
+    u64 deg = off[v + 1] - off[v];
+    u64 c = 0;
+    if (deg > MID_DEG) {
+      c = 2;
+      while (c < 2 * deg) c <<= 1;
+    }
+    cap[i] = c;
+  }
+}
+
+// Runs the evaluation kernel over `verts`; fills out_to / out_gain.
+void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
+              const double* d, const u8* blocked, bool allow_empty, u32* out_to, double* out_gain,
+              unsigned long long* traversed) {
+  if (!nv) return;
+  cudaStream_t st = E.stream;
+  Scratch& S = E.sc;
+  S.gkey.ensure(E.mem, (size_t)nv + 1);
+  k_big_caps<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.gkey.p);
+  HL_CUDA(cudaMemsetAsync(S.gkey.p + nv, 0, sizeof(u64), st));
+  HL_LAUNCH_CHECK();
+  u64* a = S.gkey.p;
+  S.gkey2.ensure(E.mem, (size_t)nv + 1);
+  u64* o = S.gkey2.p;
+  cub_run(E, [&](void* t, size_t& b) {
+    return cub::DeviceScan::ExclusiveSum(t, b, a, o, (int64_t)nv + 1, st);
+  });
+  u64 total = E.read_u64(o + nv);
+  DBuf<u32> tk, tp;
+  DBuf<double> tv;
+  if (total) {
+    S.res.ensure(E.mem, 1);
+    tk.ensure(E.mem, total);
+    tp.ensure(E.mem, total);
+    tv.ensure(E.mem, total);
+  }
+  EvalArgs A;
+  A.verts = verts;
+  A.nv = nv;
+  A.off = L.g.off.p;
+  A.col = L.g.col.p;
+  A.w = L.g.w.p;
+  A.f = L.f.p;
+  A.s = s;
+  A.d = d;
+  A.kdeg = L.k.p;
+  A.blocked = blocked;
+  A.tw = L.tw;
+  A.gamma = E.cfg.resolution;
+  A.n = L.g.n;
+  A.allow_empty = allow_empty;
+  A.out_to = out_to;
+  A.out_gain = out_gain;
+  A.tab_off = o;
+  A.tkey = tk.p;
+  A.tpos = tp.p;
+  A.tval = tv.p;
+  A.traversed = traversed;
+  u32 blocks = grid_for((u64)nv * 32, WARPS_PER_BLOCK * 32);
+  if (kind == EVAL_MOVE)
+    k_eval<EVAL_MOVE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(A);
+  else
+    k_eval<EVAL_REFINE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(A);
+  HL_LAUNCH_CHECK();
+  if (total) {
+    tk.release();
+    tp.release();
+    tv.release();
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Decoupled selection (throughput.rs:204-236) by deterministic reservations.
+// ----------------------------------------------------------------------------
+enum : u32 { ROLE_EMIT = 1, ROLE_ACC = 2 };
+enum : u8 { ST_UNDECIDED = 0, ST_ACCEPTED = 1, ST_REJECTED = 2 };
+
+__device__ __forceinline__ u32 role_bits(u32 r, u32 round) { return (r >> 2) == round ? (r & 3u) : 0u; }
+
+__global__ void k_reserve(u32 M, const u32* from, const u32* to, u8* status, u8* nmask,
+                          const u32* role, unsigned long long* res, u32 round, u64 e) {
+  for (u64 r = blockIdx.x * (u64)blockDim.x + threadIdx.x; r < M; r += (u64)gridDim.x * blockDim.x) {
+    if (status[r] != ST_UNDECIDED) continue;
+    u32 A = from[r], B = to[r];
+    u32 ba = role_bits(role[A], round), bb = role_bits(role[B], round);
+    if ((ba & ROLE_ACC) || (bb & ROLE_EMIT)) {
+      status[r] = ST_REJECTED;
+      continue;
+    }
+    unsigned long long key = ((unsigned long long)e << 32) | (unsigned long long)(0xFFFFFFFFu - (u32)r);
+    u8 m = 0;
+    if (ba == 0) {
+      m |= 1;
+      atomicMax(&res[A], key);
+    }
+    if (bb == 0) {
+      m |= 2;
+      atomicMax(&res[B], key);
+    }
+    nmask[r] = m;
+  }
+}
+
+__global__ void k_decide(u32 M, const u32* from, const u32* to, u8* status, const u8* nmask,
+                         u32* role, const unsigned long long* res, u32 round, u64 e,
+                         u32* undecided) {
+  u32 local = 0;
+  for (u64 r = blockIdx.x * (u64)blockDim.x + threadIdx.x; r < M; r += (u64)gridDim.x * blockDim.x) {
+    if (status[r] != ST_UNDECIDED) continue;
+    u32 A = from[r], B = to[r];
+    u8 m = nmask[r];
+    unsigned long long key = ((unsigned long long)e << 32) | (unsigned long long)(0xFFFFFFFFu - (u32)r);
+    bool ok = (!(m & 1) || res[A] == key) && (!(m & 2) || res[B] == key);
+    if (!ok) {
+      ++local;
+      continue;
+    }
+    status[r] = ST_ACCEPTED;
+    if (A == B) {
+      role[A] = (round << 2) | ROLE_EMIT | ROLE_ACC;
+    } else {
+      role[A] = (round << 2) | ROLE_EMIT;
+      role[B] = (round << 2) | ROLE_ACC;
+    }
+  }
+  if (local) atomicAdd(undecided, local);
+}
+
+// Exact sequential finish for whatever the reservation rounds left undecided
+// (every earlier-ranked candidate is already final, so the greedy rule can be
+// applied in rank order directly).
+__global__ void k_select_tail(u32 M, const u32* from, const u32* to, u8* status, u32* role,
+                              u32 round) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (u32 r = 0; r < M; ++r) {
+    if (status[r] != ST_UNDECIDED) continue;
+    u32 A = from[r], B = to[r];
+    u32 ba = role_bits(role[A], round), bb = role_bits(role[B], round);
+    if ((ba & ROLE_ACC) || (bb & ROLE_EMIT)) {
+      status[r] = ST_REJECTED;
+      continue;
+    }
+    status[r] = ST_ACCEPTED;
+    role[A] = (round << 2) | (role_bits(role[A], round) | ROLE_EMIT);
+    role[B] = (round << 2) | (role_bits(role[B], round) | ROLE_ACC);
+  }
+}
+
+__global__ void k_cand_flags(const double* gain, u32 na, u8* flag) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < na; i += (u64)gridDim.x * blockDim.x)
+    flag[i] = gain[i] > 0.0 ? 1 : 0;
+}
+
+__global__ void k_gain_keys(const u32* cidx, u32 M, const double* gain, u64* keys, u32* vals) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < M; i += (u64)gridDim.x * blockDim.x) {
+    keys[i] = ~double_key(gain[cidx[i]]);  // descending gain
+    vals[i] = cidx[i];
+  }
+}
+
+__global__ void k_gather_sel(const u32* order, u32 M, const u32* act, const u32* cand_to,
+                             const u32* f, u32* sel_node, u32* sel_from, u32* sel_to) {
+  for (u64 r = blockIdx.x * (u64)blockDim.x + threadIdx.x; r < M; r += (u64)gridDim.x * blockDim.x) {
+    u32 i = order[r];
+    u32 v = act[i];
+    sel_node[r] = v;
+    sel_from[r] = f[v];
+    sel_to[r] = cand_to[i];
+  }
+}
+
+// Apply accepted moves (throughput.rs:182-187).  d(C) changes are exact in
+// any order for integral weights; otherwise k_apply_ordered replays them in
+// selected order per community.
+__global__ void k_apply_moves(u32 M, const u8* status, const u32* sel_node, const u32* sel_from,
+                              const u32* sel_to, u32* f, const double* kdeg, double* d,
+                              bool atomic_d, u8* changed, u8* affected, bool mark_moved,
+                              u32* accepted) {
+  u32 local = 0;
+  for (u64 r = blockIdx.x * (u64)blockDim.x + threadIdx.x; r < M; r += (u64)gridDim.x * blockDim.x) {
+    if (status[r] != ST_ACCEPTED) continue;
+    u32 v = sel_node[r];
+    f[v] = sel_to[r];
+    changed[v] = 1;
+    if (mark_moved) affected[v] = 1;
+    if (atomic_d) {
+      double kv = kdeg[v];
+      atomicAdd(&d[sel_from[r]], -kv);
+      atomicAdd(&d[sel_to[r]], kv);
+    }
+    ++local;
+  }
+  if (local) atomicAdd(accepted, local);
+}
+
+__global__ void k_dops(u32 M, const u8* status, const u32* sel_from, const u32* sel_to,
+                       u32* okey, u32* oval) {
+  for (u64 r = blockIdx.x * (u64)blockDim.x + threadIdx.x; r < M; r += (u64)gridDim.x * blockDim.x) {
+    bool acc = status[r] == ST_ACCEPTED;
+    okey[2 * r] = acc ? sel_from[r] : NONE32;
+    okey[2 * r + 1] = acc ? sel_to[r] : NONE32;
+    oval[2 * r] = (u32)(2 * r);
+    oval[2 * r + 1] = (u32)(2 * r + 1);
+  }
+}
+
+__global__ void k_apply_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 total,
+                                const u32* ops, const u32* sel_node, const double* kdeg,
+                                double* d) {
+  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < nu; j += (u64)gridDim.x * blockDim.x) {
+    u32 c = ukeys[j];
+    if (c == NONE32) continue;
+    u32 a = ustart[j], b = (j + 1 < nu) ? ustart[j + 1] : total;
+    double x = d[c];
+    for (u32 t = a; t < b; ++t) {
+      u32 op = ops[t];
+      double kv = kdeg[sel_node[op >> 1]];
+      x = (op & 1) ? __dadd_rn(x, kv) : __dsub_rn(x, kv);
+    }
+    d[c] = x;
+  }
+}
+
+// Next frontier and K marks (throughput.rs:189-199), on f after all moves.
+__global__ void k_mark_next(u32 M, const u8* status, const u32* sel_node, const u32* sel_to,
+                            const u64* off, const u32* col, const u32* f, const u32* s, u8* next,
+                            u8* affected) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 r = warp; r < M; r += nwarps) {
+    if (status[r] != ST_ACCEPTED) continue;
+    u32 v = sel_node[r], to = sel_to[r];
+    u32 sv = s[v];
+    bool any_same = false;
+    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32) {
+      u32 nb = col[p];
+      if (f[nb] != to) next[nb] = 1;
+      if (s[nb] == sv) {
+        affected[nb] = 1;
+        any_same = true;
+      }
+    }
+    if (__any_sync(0xffffffffu, any_same) && lane == 0) affected[v] = 1;
+  }
+}
+
+void ensure_comm_arrays(Engine& E, size_t ncap) {
+  Scratch& S = E.sc;
+  size_t old_res = S.res.cap, old_role = S.role.cap;
+  S.d.ensure(E.mem, ncap);
+  S.res.ensure(E.mem, ncap);
+  S.role.ensure(E.mem, ncap);
+  if (S.res.cap != old_res) HL_CUDA(cudaMemsetAsync(S.res.p, 0, S.res.cap * sizeof(u64), E.stream));
+  if (S.role.cap != old_role) HL_CUDA(cudaMemsetAsync(S.role.p, 0, S.role.cap * sizeof(u32), E.stream));
+}
+
+// Decides every sorted candidate in S.sel_from / S.sel_to (rank order):
+// S.status[r] = accepted / rejected exactly as the sequential greedy would.
+void select_decoupled_dev(Engine& E, u32 M) {
+  Scratch& S = E.sc;
+  cudaStream_t st = E.stream;
+  u32* cnt = S.cnt.p;
+  HL_CUDA(cudaMemsetAsync(S.status.p, ST_UNDECIDED, M, st));
+  u32 round = ++E.sel_round;
+  if (round >= (1u << 29)) E.sel_round = round = 1;
+  u32 iters = 0;
+  while (true) {
+    for (int rep = 0; rep < 4; ++rep) {
+      u64 e = ++E.epoch;
+      HL_CUDA(cudaMemsetAsync(cnt + 6, 0, sizeof(u32), st));
+      k_reserve<<<grid_for(M), 256, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.nmask.p,
+                                             S.role.p, (unsigned long long*)S.res.p, round, e);
+      k_decide<<<grid_for(M), 256, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.nmask.p,
+                                            S.role.p, (const unsigned long long*)S.res.p, round, e,
+                                            cnt + 6);
+      HL_LAUNCH_CHECK();
+      ++iters;
+    }
+    u32 left = E.read_u32(cnt + 6);
+    if (!left) break;
+    if (iters >= 64) {
+      k_select_tail<<<1, 32, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.role.p, round);
+      HL_LAUNCH_CHECK();
+      break;
+    }
+  }
+  E.stats_sel_iters += iters;
+}
+
+MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active,
+                     bool mark_moved) {
+  MoveOut out;
+  Scratch& S = E.sc;
+  cudaStream_t st = E.stream;
+  const u32 n = L.g.n;
+  S.active.ensure(E.mem, n ? n : 1);
+  S.next.ensure(E.mem, n ? n : 1);
+  S.changed.ensure(E.mem, n ? n : 1);
+  S.affected.ensure(E.mem, n ? n : 1);
+  HL_CUDA(cudaMemsetAsync(S.active.p, all_active ? 1 : 0, n ? n : 1, st));
+  HL_CUDA(cudaMemsetAsync(S.changed.p, 0, n ? n : 1, st));
+  HL_CUDA(cudaMemsetAsync(S.affected.p, 0, n ? n : 1, st));
+  if (!n) return out;
+  if (delta.k)
+    k_seed<<<grid_for(delta.k), 256, 0, st>>>(delta.u, delta.v, delta.w, delta.k, L.f.p,
+                                               L.s_cur.p, S.active.p, S.affected.p);
+  HL_LAUNCH_CHECK();
+  // Community ids must stay below n so that n + v is a fresh empty community.
+  compact_labels_if_needed(E, L.f.p, n, n);
+  const size_t ncap = 2 * (size_t)n + 2;
+  ensure_comm_arrays(E, ncap);
+  recompute_comm_degrees(E, L, L.f.p, (u32)ncap, S.d.p);
+
+  S.act.ensure(E.mem, n);
+  S.cand_to.ensure(E.mem, n);
+  S.cand_gain.ensure(E.mem, n);
+  S.cand_idx.ensure(E.mem, n);
+  S.status.ensure(E.mem, n);
+  S.nmask.ensure(E.mem, n);
+  S.sel_node.ensure(E.mem, n);
+  S.sel_from.ensure(E.mem, n);
+  S.sel_to.ensure(E.mem, n);
+  S.order.ensure(E.mem, n);
+  S.order2.ensure(E.mem, n);
+  S.gkey.ensure(E.mem, n);
+  S.gkey2.ensure(E.mem, n);
+  S.cnt.ensure(E.mem, 16);
+  S.red64.ensure(E.mem, 4);
+  HL_CUDA(cudaMemsetAsync(S.red64.p, 0, sizeof(u64), st));
+  u32* cnt = S.cnt.p;
+
+  const u32 max_rounds = E.cfg.max_rounds ? E.cfg.max_rounds : 20;
+  u32 it = 0;
+  while (it < max_rounds) {
+    // Active list, ascending (iter_ones order).
+    cub_run(E, [&](void* t, size_t& b) {
+      return cub::DeviceSelect::Flagged(t, b, cub::CountingInputIterator<u32>(0), S.active.p,
+                                        S.act.p, cnt + 4, (int64_t)n, st);
+    });
+    u32 na = E.read_u32(cnt + 4);
+    if (!na) break;
+    run_eval(E, EVAL_MOVE, S.act.p, na, L, L.s_cur.p, S.d.p, nullptr, true, S.cand_to.p,
+             S.cand_gain.p, (unsigned long long*)S.red64.p);
+    // Candidates with positive gain, still in ascending node order.
+    u8* flag = S.status.p;
+    k_cand_flags<<<grid_for(na), 256, 0, st>>>(S.cand_gain.p, na, flag);
+    HL_LAUNCH_CHECK();
+    cub_run(E, [&](void* t, size_t& b) {
+      return cub::DeviceSelect::Flagged(t, b, cub::CountingInputIterator<u32>(0), flag,
+                                        S.cand_idx.p, cnt + 5, (int64_t)na, st);
+    });
+    u32 M = E.read_u32(cnt + 5);
+    out.candidates += M;
+    ++it;
+    if (!M) break;  // no positive candidate: nothing selected, frontier empties
+    k_gain_keys<<<grid_for(M), 256, 0, st>>>(S.cand_idx.p, M, S.cand_gain.p, S.gkey.p, S.order.p);
+    HL_LAUNCH_CHECK();
+    {
+      u64* ki = S.gkey.p;
+      u64* ko = S.gkey2.p;
+      u32* vi = S.order.p;
+      u32* vo = S.order2.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)M, 0, 64, st);
+      });
+    }
+    k_gather_sel<<<grid_for(M), 256, 0, st>>>(S.order2.p, M, S.act.p, S.cand_to.p, L.f.p,
+                                              S.sel_node.p, S.sel_from.p, S.sel_to.p);
+    HL_LAUNCH_CHECK();
+    select_decoupled_dev(E, M);
+    HL_CUDA(cudaMemsetAsync(cnt + 7, 0, sizeof(u32), st));
+    k_apply_moves<<<grid_for(M), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_from.p,
+                                               S.sel_to.p, L.f.p, L.k.p, S.d.p, E.integral,
+                                               S.changed.p, S.affected.p, mark_moved, cnt + 7);
+    HL_LAUNCH_CHECK();
+    if (!E.integral) {
+      // Replay d(C) -= k / += k in selected order, per community.
+      S.used.ensure(E.mem, 2 * (size_t)M);
+      S.rank.ensure(E.mem, 2 * (size_t)M);
+      S.cand_node.ensure(E.mem, 2 * (size_t)M);
+      S.segid.ensure(E.mem, 2 * (size_t)M);
+      S.rowlist.ensure(E.mem, 2 * (size_t)M);
+      S.seg_start.ensure(E.mem, 2 * (size_t)M);
+      S.idx.ensure(E.mem, 2 * (size_t)M);
+      S.idx2.ensure(E.mem, 2 * (size_t)M);
+      k_dops<<<grid_for(M), 256, 0, st>>>(M, S.status.p, S.sel_from.p, S.sel_to.p, S.used.p,
+                                          S.idx.p);
+      HL_LAUNCH_CHECK();
+      u32 M2 = 2 * M;
+      u32* ki = S.used.p;
+      u32* ko = S.rank.p;
+      u32* vi = S.idx.p;
+      u32* vo = S.idx2.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)M2, 0, 32, st);
+      });
+      k_heads_u32<<<grid_for(M2), 256, 0, st>>>(ko, M2, S.cand_node.p);
+      HL_LAUNCH_CHECK();
+      u32* h = S.cand_node.p;
+      u32* sid = S.segid.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)M2, st);
+      });
+      u32 nu = E.read_u32(sid + M2 - 1) + E.read_u32(h + M2 - 1);
+      k_seg_compact<<<grid_for(M2), 256, 0, st>>>(h, sid, ko, M2, S.rowlist.p, S.seg_start.p);
+      k_apply_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, M2, vo,
+                                                    S.sel_node.p, L.k.p, S.d.p);
+      HL_LAUNCH_CHECK();
+    }
+    u32 acc = E.read_u32(cnt + 7);
+    out.moves += acc;
+    if (!acc) break;
+    HL_CUDA(cudaMemsetAsync(S.next.p, 0, n, st));
+    k_mark_next<<<grid_for((u64)M * 32), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_to.p,
+                                                        L.g.off.p, L.g.col.p, L.f.p, L.s_cur.p,
+                                                        S.next.p, S.affected.p);
+    HL_LAUNCH_CHECK();
+    S.active.swap(S.next);
+  }
+  out.iterations = it;
+  out.traversed = E.read_u64(S.red64.p);
+  return out;
+}
+
+}  // namespace hl

@@ -1,0 +1,453 @@
+// refine.cu — inc-refinement, throughput mode (hit_leiden.rs:1265-1390,
+// :1554-1637; throughput.rs:239-359).
+//
+//  1. Sub-communities holding a K vertex are split into connected components
+//     over edges whose ends share the sub-community (and, in the multi-level
+//     mode, the community).  Components come from a lock-free union-find that
+//     always hooks the larger root under the smaller, so a root is its
+//     component's minimum vertex — the BFS start the reference would use.
+//  2. The largest component keeps the id; on equal sizes the last one in
+//     discovery order (largest minimum vertex) wins, as Rust's max_by_key
+//     does.  The others get max(s)+1, +2, … in (sub-community, minimum vertex)
+//     order.
+//  3. T-filter: a candidate sub-community S is blocked when
+//     ΔQ(S→∅) = -w(S,C)/2m + γ d_S (d_C - d_S)/(2m)^2 > 1e-9.
+//  4. Jacobi singleton merge: every refined singleton evaluates its best
+//     same-community neighbour sub-community on the snapshot; all positive
+//     moves are applied together.
+#include "hl_engine.cuh"
+
+namespace hl {
+
+static inline u32 grid_for(u64 n, u32 block = 256) {
+  u64 g = (n + block - 1) / block;
+  if (g > 148u * 64u) g = 148u * 64u;
+  return g ? (u32)g : 1u;
+}
+
+void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
+              const double* d, const u8* blocked, bool allow_empty, u32* out_to, double* out_gain,
+              unsigned long long* traversed);
+
+__global__ void k_mark_affected_sc(const u8* affected, const u32* s, u32 n, u8* affsc) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x)
+    if (affected[v]) affsc[s[v]] = 1;
+}
+
+__device__ __forceinline__ u32 uf_find(u32* par, u32 x) {
+  u32 p = par[x];
+  while (p != x) {
+    u32 gp = par[p];
+    if (gp != p) par[x] = gp;  // path halving (always an ancestor)
+    x = p;
+    p = gp;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void uf_unite(u32* par, u32 a, u32 b) {
+  while (true) {
+    a = uf_find(par, a);
+    b = uf_find(par, b);
+    if (a == b) return;
+    u32 lo = a < b ? a : b, hi = a < b ? b : a;
+    if (atomicCAS(&par[hi], hi, lo) == hi) return;
+  }
+}
+
+__global__ void k_uf_edges(u32 n, const u64* off, const u32* col, const u32* s, const u32* f,
+                           const u8* affsc, bool same_f, u32* par) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 v = warp; v < n; v += nwarps) {
+    u32 sv = s[v];
+    if (!affsc[sv]) continue;
+    u32 fv = f[v];
+    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32) {
+      u32 nb = col[p];
+      if (nb <= v) continue;  // each undirected edge once (self-loops irrelevant)
+      if (s[nb] != sv) continue;
+      if (same_f && f[nb] != fv) continue;
+      uf_unite(par, (u32)v, nb);
+    }
+  }
+}
+
+__global__ void k_uf_final(u32 n, const u32* s, const u8* affsc, u32* par, u32* csize) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
+    if (!affsc[s[v]]) continue;
+    u32 r = uf_find(par, (u32)v);
+    par[v] = r;
+    atomicAdd(&csize[r], 1u);
+  }
+}
+
+__global__ void k_keep(u32 n, const u32* s, const u8* affsc, const u32* par, const u32* csize,
+                       unsigned long long* keep) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
+    if (!affsc[s[v]] || par[v] != v) continue;
+    atomicMax(&keep[s[v]], ((unsigned long long)csize[v] << 32) | (u32)v);
+  }
+}
+
+__global__ void k_split_roots(u32 n, const u32* s, const u8* affsc, const u32* par,
+                              const unsigned long long* keep, u8* flag, u64* key) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
+    bool nk = affsc[s[v]] && par[v] == v && (u32)keep[s[v]] != (u32)v;
+    flag[v] = nk ? 1 : 0;
+    key[v] = ((u64)s[v] << 32) | (u32)v;
+  }
+}
+
+__global__ void k_gather_keys(const u32* roots, u32 m, const u64* key, u64* out) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < m; i += (u64)gridDim.x * blockDim.x)
+    out[i] = key[roots[i]];
+}
+
+__global__ void k_assign_newid(const u64* sorted, u32 m, u32 base, u32* newid, u32* origin_new,
+                               u32* origin_old) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < m; t += (u64)gridDim.x * blockDim.x) {
+    u32 r = (u32)sorted[t];
+    newid[r] = base + (u32)t;
+    origin_new[t] = base + (u32)t;
+    origin_old[t] = (u32)(sorted[t] >> 32);
+  }
+}
+
+__global__ void k_apply_split(u32 n, u32* s, const u8* affsc_snapshot, const u32* par,
+                              const u8* nkflag, const u32* newid, u8* refined) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
+    u32 sv = s[v];
+    if (!affsc_snapshot[sv]) continue;
+    u32 r = par[v];
+    if (nkflag[r]) {
+      s[v] = newid[r];
+      refined[v] = 1;
+    }
+  }
+}
+
+__global__ void k_not_identity(u32 n, const u32* s, u32* bad) {
+  u32 local = 0;
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x)
+    if (s[v] != (u32)v) ++local;
+  if (local) atomicAdd(bad, local);
+}
+
+__global__ void k_sizes(u32 n, const u32* s, u32* sizes) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x)
+    atomicAdd(&sizes[s[v]], 1u);
+}
+
+__global__ void k_singletons(const u32* rs, u32 nr, const u32* s, const u32* sizes, u8* flag) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < nr; i += (u64)gridDim.x * blockDim.x)
+    flag[i] = sizes[s[rs[i]]] == 1 ? 1 : 0;
+}
+
+// Candidate sub-communities of the T-filter (hit_leiden.rs:1567-1586).
+__global__ void k_t_candidates(const u32* single, u32 ns, const u64* off, const u32* col,
+                               const u32* f, const u32* s, u8* cand) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 i = warp; i < ns; i += nwarps) {
+    u32 v = single[i];
+    u32 fv = f[v], sv = s[v];
+    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32) {
+      u32 nb = col[p];
+      if (f[nb] != fv) continue;
+      u32 x = s[nb];
+      if (x != sv) cand[x] = 1;
+    }
+  }
+}
+
+__global__ void k_min_member(u32 n, const u32* s, const u8* cand, u32* minmem) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x)
+    if (cand[s[v]]) atomicMin(&minmem[s[v]], (u32)v);
+}
+
+// w(S, C_parent) with integral weights: per-member partial sums, any order.
+__global__ void k_wsp_atomic(u32 n, const u64* off, const u32* col, const double* w, const u32* f,
+                             const u32* s, const u8* cand, const u32* minmem, double* wsp) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 v = warp; v < n; v += nwarps) {
+    u32 S = s[v];
+    if (!cand[S]) continue;
+    u32 parent = f[minmem[S]];
+    double x = 0.0;
+    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32)
+      if (f[col[p]] == parent) x += w[p];
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0 && x != 0.0) atomicAdd(&wsp[S], x);
+  }
+}
+
+// Ordered w(S, C_parent): members ascending, rows in CSR order, one chain per S
+// (hit_leiden.rs:1618-1625).
+__global__ void k_wsp_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 total,
+                              const u32* members, const u64* off, const u32* col, const double* w,
+                              const u32* f, const u32* minmem, double* wsp) {
+  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < nu; j += (u64)gridDim.x * blockDim.x) {
+    u32 S = ukeys[j];
+    u32 a = ustart[j], b = (j + 1 < nu) ? ustart[j + 1] : total;
+    u32 parent = f[minmem[S]];
+    double x = 0.0;
+    for (u32 t = a; t < b; ++t) {
+      u32 v = members[t];
+      for (u64 p = off[v]; p < off[v + 1]; ++p)
+        if (f[col[p]] == parent) x = __dadd_rn(x, w[p]);
+    }
+    wsp[S] = x;
+  }
+}
+
+__global__ void k_blocked(u32 ns, const u8* cand, const double* dS, const double* wsp,
+                          const u32* minmem, const u32* f, const double* dcomm, double tw,
+                          double gamma, u8* blocked) {
+  for (u64 S = blockIdx.x * (u64)blockDim.x + threadIdx.x; S < ns; S += (u64)gridDim.x * blockDim.x) {
+    u8 b = 0;
+    if (cand[S]) {
+      double ds = dS[S];
+      if (ds > 0.0) {
+        double dpar = dcomm[f[minmem[S]]];
+        double dq = remove_gain(wsp[S], tw, gamma, ds, dpar);
+        b = dq > 1e-9 ? 1 : 0;
+      }
+    }
+    blocked[S] = b;
+  }
+}
+
+__global__ void k_member_keys(u32 n, const u32* s, const u8* cand, u8* flag) {
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x)
+    flag[v] = cand[s[v]] ? 1 : 0;
+}
+
+__global__ void k_gather_s(const u32* list, u32 m, const u32* s, u32* out) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < m; i += (u64)gridDim.x * blockDim.x)
+    out[i] = s[list[i]];
+}
+
+__global__ void k_heads_u32b(const u32* sk, u64 n, u32* head) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    head[i] = (i == 0 || sk[i] != sk[i - 1]) ? 1u : 0u;
+}
+
+__global__ void k_seg_compact_b(const u32* head, const u32* segid, const u32* sk, u64 n,
+                                u32* ukeys, u32* ustart) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    if (head[i]) {
+      ukeys[segid[i]] = sk[i];
+      ustart[segid[i]] = (u32)i;
+    }
+}
+
+__global__ void k_apply_merges(const u32* single, u32 ns, const u32* to, const double* gain,
+                               u32* s, u32* count) {
+  u32 local = 0;
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < ns; i += (u64)gridDim.x * blockDim.x)
+    if (gain[i] > 0.0) {
+      s[single[i]] = to[i];
+      ++local;
+    }
+  if (local) atomicAdd(count, local);
+}
+
+static u32 reduce_max_u32(Engine& E, const u32* x, u32 n, u32* out) {
+  cub_run(E, [&](void* t, size_t& b) {
+    return cub::DeviceReduce::Max(t, b, x, out, (int64_t)n, E.stream);
+  });
+  return E.read_u32(out);
+}
+
+static u32 select_flagged(Engine& E, const u8* flags, u32 n, u32* out, u32* cnt) {
+  cub_run(E, [&](void* t, size_t& b) {
+    return cub::DeviceSelect::Flagged(t, b, cub::CountingInputIterator<u32>(0), flags, out, cnt,
+                                      (int64_t)n, E.stream);
+  });
+  return E.read_u32(cnt);
+}
+
+RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
+  RefineOut out;
+  Scratch& S = E.sc;
+  cudaStream_t st = E.stream;
+  const u32 n = L.g.n;
+  E.new_ids.clear();
+  S.refined.ensure(E.mem, n ? n : 1);
+  HL_CUDA(cudaMemsetAsync(S.refined.p, 0, n ? n : 1, st));
+  if (!n) return out;
+  S.cnt.ensure(E.mem, 16);
+  u32* cnt = S.cnt.p;
+  u32* s = L.s_cur.p;
+
+  // ---- 1. connected-component split of affected sub-communities ----------
+  u32 smax = reduce_max_u32(E, s, n, cnt + 12);
+  out.smax_before = smax;
+  const size_t scap = (size_t)smax + 2 + n;
+  S.affsc.ensure(E.mem, scap);
+  HL_CUDA(cudaMemsetAsync(S.affsc.p, 0, scap, st));
+  k_mark_affected_sc<<<grid_for(n), 256, 0, st>>>(S.affected.p, s, n, S.affsc.p);
+  S.par.ensure(E.mem, n);
+  S.csize.ensure(E.mem, n);
+  k_iota<<<grid_for(n), 256, 0, st>>>(S.par.p, n);
+  HL_CUDA(cudaMemsetAsync(S.csize.p, 0, sizeof(u32) * n, st));
+  k_uf_edges<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, s, L.f.p, S.affsc.p,
+                                                     cc_same_community, S.par.p);
+  k_uf_final<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.csize.p);
+  S.keep.ensure(E.mem, scap);
+  HL_CUDA(cudaMemsetAsync(S.keep.p, 0, sizeof(u64) * scap, st));
+  k_keep<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.csize.p,
+                                      (unsigned long long*)S.keep.p);
+  S.status.ensure(E.mem, n);
+  S.gkey.ensure(E.mem, n);
+  S.gkey2.ensure(E.mem, n);
+  k_split_roots<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p,
+                                              (const unsigned long long*)S.keep.p, S.status.p,
+                                              S.gkey.p);
+  HL_LAUNCH_CHECK();
+  S.act.ensure(E.mem, n);
+  u32 m_new = select_flagged(E, S.status.p, n, S.act.p, cnt + 4);
+  S.newid.ensure(E.mem, n);
+  if (m_new) {
+    S.keys.ensure(E.mem, m_new);
+    S.keys2.ensure(E.mem, m_new);
+    S.used.ensure(E.mem, m_new);
+    S.rank.ensure(E.mem, m_new);
+    k_gather_keys<<<grid_for(m_new), 256, 0, st>>>(S.act.p, m_new, S.gkey.p, S.keys.p);
+    HL_LAUNCH_CHECK();
+    u64* ki = S.keys.p;
+    u64* ko = S.keys2.p;
+    cub_run(E, [&](void* t, size_t& b) {
+      return cub::DeviceRadixSort::SortKeys(t, b, ki, ko, (int64_t)m_new, 0, 64, st);
+    });
+    k_assign_newid<<<grid_for(m_new), 256, 0, st>>>(ko, m_new, smax + 1, S.newid.p, S.used.p,
+                                                     S.rank.p);
+    k_apply_split<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.status.p, S.newid.p,
+                                               S.refined.p);
+    HL_LAUNCH_CHECK();
+    std::vector<u32> a(m_new), b(m_new);
+    HL_CUDA(cudaMemcpyAsync(a.data(), S.used.p, sizeof(u32) * m_new, cudaMemcpyDeviceToHost, st));
+    HL_CUDA(cudaMemcpyAsync(b.data(), S.rank.p, sizeof(u32) * m_new, cudaMemcpyDeviceToHost, st));
+    E.sync();
+    E.new_ids.resize(m_new);
+    for (u32 i = 0; i < m_new; ++i) E.new_ids[i] = {a[i], b[i]};
+  }
+  out.splits = m_new;
+
+  // is_initial (hit_leiden.rs:1333-1339): s is the identity ⇒ R = all.
+  HL_CUDA(cudaMemsetAsync(cnt + 5, 0, sizeof(u32), st));
+  k_not_identity<<<grid_for(n), 256, 0, st>>>(n, s, cnt + 5);
+  HL_LAUNCH_CHECK();
+  if (E.read_u32(cnt + 5) == 0) HL_CUDA(cudaMemsetAsync(S.refined.p, 1, n, st));
+
+  // ---- 2. sizes, d_S, d_C -----------------------------------------------
+  u32 smax2 = m_new ? smax + m_new : smax;
+  const size_t s2cap = (size_t)smax2 + 1;
+  S.sizes.ensure(E.mem, s2cap);
+  HL_CUDA(cudaMemsetAsync(S.sizes.p, 0, sizeof(u32) * s2cap, st));
+  k_sizes<<<grid_for(n), 256, 0, st>>>(n, s, S.sizes.p);
+  HL_LAUNCH_CHECK();
+  S.dS.ensure(E.mem, s2cap);
+  recompute_comm_degrees(E, L, s, (u32)s2cap, S.dS.p);
+  const size_t fcap = 2 * (size_t)n + 2;
+  S.dcomm.ensure(E.mem, fcap);
+  recompute_comm_degrees(E, L, L.f.p, (u32)fcap, S.dcomm.p);
+
+  // ---- 3. refined singletons ---------------------------------------------
+  u32 nr = select_flagged(E, S.refined.p, n, S.act.p, cnt + 6);
+  out.refined = nr;
+  if (!nr) return out;
+  S.nmask.ensure(E.mem, nr);
+  k_singletons<<<grid_for(nr), 256, 0, st>>>(S.act.p, nr, s, S.sizes.p, S.nmask.p);
+  HL_LAUNCH_CHECK();
+  S.cand_idx.ensure(E.mem, nr);
+  u32 ns = 0;
+  {
+    u32* tmp = S.cand_idx.p;
+    cub_run(E, [&](void* t, size_t& b) {
+      return cub::DeviceSelect::Flagged(t, b, S.act.p, S.nmask.p, tmp, cnt + 7, (int64_t)nr, st);
+    });
+    ns = E.read_u32(cnt + 7);
+  }
+  if (!ns) return out;
+  u32* single = S.cand_idx.p;
+
+  // ---- 4. T-filter --------------------------------------------------------
+  S.cand_sc.ensure(E.mem, s2cap);
+  S.blocked.ensure(E.mem, s2cap);
+  S.minmem.ensure(E.mem, s2cap);
+  S.wsp.ensure(E.mem, s2cap);
+  HL_CUDA(cudaMemsetAsync(S.cand_sc.p, 0, s2cap, st));
+  HL_CUDA(cudaMemsetAsync(S.minmem.p, 0xFF, sizeof(u32) * s2cap, st));
+  HL_CUDA(cudaMemsetAsync(S.wsp.p, 0, sizeof(double) * s2cap, st));
+  k_t_candidates<<<grid_for((u64)ns * 32), 256, 0, st>>>(single, ns, L.g.off.p, L.g.col.p, L.f.p,
+                                                         s, S.cand_sc.p);
+  k_min_member<<<grid_for(n), 256, 0, st>>>(n, s, S.cand_sc.p, S.minmem.p);
+  HL_LAUNCH_CHECK();
+  if (E.integral) {
+    k_wsp_atomic<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, L.f.p, s,
+                                                         S.cand_sc.p, S.minmem.p, S.wsp.p);
+    HL_LAUNCH_CHECK();
+  } else {
+    // Members of candidate sub-communities, sorted by (S, v).
+    S.next.ensure(E.mem, n);
+    k_member_keys<<<grid_for(n), 256, 0, st>>>(n, s, S.cand_sc.p, S.next.p);
+    HL_LAUNCH_CHECK();
+    S.order.ensure(E.mem, n);
+    u32 nm = select_flagged(E, S.next.p, n, S.order.p, cnt + 8);
+    if (nm) {
+      S.order2.ensure(E.mem, nm);
+      S.used.ensure(E.mem, nm);
+      S.rank.ensure(E.mem, nm);
+      S.segid.ensure(E.mem, nm);
+      S.rowlist.ensure(E.mem, nm);
+      S.seg_start.ensure(E.mem, nm);
+      S.sel_node.ensure(E.mem, nm);
+      k_gather_s<<<grid_for(nm), 256, 0, st>>>(S.order.p, nm, s, S.used.p);
+      HL_LAUNCH_CHECK();
+      u32* ki = S.used.p;
+      u32* ko = S.rank.p;
+      u32* vi = S.order.p;
+      u32* vo = S.order2.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)nm, 0, 32, st);
+      });
+      k_heads_u32b<<<grid_for(nm), 256, 0, st>>>(ko, nm, S.sel_node.p);
+      HL_LAUNCH_CHECK();
+      u32* h = S.sel_node.p;
+      u32* sid = S.segid.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)nm, st);
+      });
+      u32 nu = E.read_u32(sid + nm - 1) + E.read_u32(h + nm - 1);
+      k_seg_compact_b<<<grid_for(nm), 256, 0, st>>>(h, sid, ko, nm, S.rowlist.p, S.seg_start.p);
+      k_wsp_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, nm, vo,
+                                                  L.g.off.p, L.g.col.p, L.g.w.p, L.f.p,
+                                                  S.minmem.p, S.wsp.p);
+      HL_LAUNCH_CHECK();
+    }
+  }
+  k_blocked<<<grid_for(s2cap), 256, 0, st>>>((u32)s2cap, S.cand_sc.p, S.dS.p, S.wsp.p, S.minmem.p,
+                                             L.f.p, S.dcomm.p, L.tw, E.cfg.resolution,
+                                             S.blocked.p);
+  HL_LAUNCH_CHECK();
+
+  // ---- 5. Jacobi singleton merge -------------------------------------------
+  S.cand_to.ensure(E.mem, ns);
+  S.cand_gain.ensure(E.mem, ns);
+  run_eval(E, 1, single, ns, L, s, S.dS.p, S.blocked.p, false, S.cand_to.p, S.cand_gain.p,
+           nullptr);
+  HL_CUDA(cudaMemsetAsync(cnt + 9, 0, sizeof(u32), st));
+  k_apply_merges<<<grid_for(ns), 256, 0, st>>>(single, ns, S.cand_to.p, S.cand_gain.p, s,
+                                               cnt + 9);
+  HL_LAUNCH_CHECK();
+  out.merges = E.read_u32(cnt + 9);
+  return out;
+}
+
+}  // namespace hl

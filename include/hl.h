@@ -1,0 +1,166 @@
+/* hl.h — C ABI of the B200 HIT-Leiden incremental update path.
+ *
+ * A graph lives on one GPU behind an opaque handle.  The caller loads it once
+ * (hl_create: load + bootstrap partition), then applies edge-update batches
+ * (hl_apply_batch) and reads back the hierarchical partition and modularity.
+ *
+ * The reference crate (Rust `hit_leiden` 0.1.0) has no FFI; these entry points
+ * replace its crate-level API for this path:
+ *   hl_create        ~ PartitionState::identity + InMemoryGraph::from + the
+ *                      first hit_leiden call (src/core/partition/state.rs:35-49,
+ *                      src/core/graph/in_memory.rs:30-72,
+ *                      src/core/algorithm/hit_leiden.rs:936-1018)
+ *   hl_apply_batch   ~ hit_leiden(&mut state, &delta, gamma, mode)
+ *                      (src/core/algorithm/hit_leiden.rs:936-941)
+ *   hl_get_partition ~ reading PartitionState's per-level vectors
+ *                      (src/core/partition/state.rs:19-32)
+ *   hl_modularity    ~ compute_modularity (src/core/algorithm/hit_leiden.rs:121-161)
+ *   hl_canonicalize  ~ canonicalize_community_ids_in_place (hit_leiden.rs:358-376)
+ * Error codes mirror HitLeidenError::InvalidInput (src/core/error.rs:19-27) and
+ * the endpoint check of run() (hit_leiden.rs:35-43); nothing panics or aborts
+ * across this boundary.
+ *
+ * Conventions: host buffers are copied in; output buffers are caller-allocated.
+ * A handle may be used by one thread at a time; different handles may be used
+ * concurrently (each owns its own CUDA stream).
+ */
+#ifndef HL_H
+#define HL_H
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HL_API __attribute__((visibility("default")))
+#else
+#define HL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  HL_OK = 0,
+  HL_ERR_INVALID_INPUT = 1, /* bad argument, endpoint >= n, bad config      */
+  HL_ERR_CUDA = 2,          /* CUDA runtime / kernel launch failure          */
+  HL_ERR_OUT_OF_MEMORY = 3, /* device allocation failed or HBM budget hit    */
+  HL_ERR_TIMEOUT = 4,       /* a bounded device wait gave up                 */
+  HL_ERR_UNSUPPORTED = 5    /* mode / feature not available on this path     */
+} hl_status;
+
+/* RunMode (src/core/config.rs:19-23).  The GPU path implements Throughput;
+ * Deterministic (sequential Gauss–Seidel) is rejected with HL_ERR_UNSUPPORTED. */
+typedef enum { HL_MODE_DETERMINISTIC = 0, HL_MODE_THROUGHPUT = 1 } hl_mode;
+
+/* Which per-level map hl_get_map returns (state.rs:19-32). */
+typedef enum {
+  HL_MAP_COMMUNITY = 0,      /* f^p  community_mapping_per_level            */
+  HL_MAP_REFINED = 1,        /* g^p  refined_community_mapping_per_level    */
+  HL_MAP_SUB_PREVIOUS = 2,   /* s_pre^p previous_subcommunity_mapping       */
+  HL_MAP_SUB_CURRENT = 3     /* s_cur^p current_subcommunity_mapping        */
+} hl_map;
+
+typedef struct {
+  double resolution;    /* gamma (RunConfig.resolution, config.rs:35); default 1.0 */
+  uint32_t mode;        /* hl_mode; default HL_MODE_THROUGHPUT                     */
+  uint32_t max_levels;  /* 1 = the reference's single-level state (state.rs:42);   */
+                        /* >1 = multi-level bootstrap, levels created on demand    */
+                        /* up to this cap (default 10, RunConfig.max_iterations)   */
+  uint32_t max_rounds;  /* throughput movement round cap (hit_leiden.rs:1077); 20  */
+  uint32_t flags;       /* HL_FLAG_*                                               */
+  uint64_t hbm_budget;  /* bytes this handle may allocate on the device; 0 = no cap */
+  int32_t device;       /* CUDA device ordinal                                     */
+} hl_config;
+
+/* Keep existing self-loops on apply_delta.  Off (the reference's behaviour,
+ * in_memory.rs:122-130 keeps node < neighbor only) for max_levels == 1; the
+ * multi-level mode always keeps them. */
+#define HL_FLAG_KEEP_SELF_LOOPS (1u << 0)
+/* Compute the level-0 modularity after every batch into hl_batch_stats
+ * (an extra pass over the graph; off by default). */
+#define HL_FLAG_BATCH_MODULARITY (1u << 1)
+
+typedef struct {
+  uint32_t iterations;   /* movement rounds summed over levels (hit_leiden return) */
+  uint32_t levels;       /* levels in the state                                    */
+  uint64_t moves;        /* accepted movement moves, all levels                    */
+  uint64_t candidates;   /* positive-gain candidates, all levels                   */
+  uint64_t traversed;    /* adjacency entries scanned by movement, all levels      */
+  uint64_t splits;       /* sub-community components split off                     */
+  uint64_t merges;       /* singleton refinement merges                            */
+  uint64_t changed;      /* |B^1| level-0 vertices whose community changed         */
+  uint64_t refined;      /* |R^1| level-0 vertices refined                         */
+  uint64_t edges;        /* undirected edges in G^1 after the batch                */
+  double modularity;     /* Q of the level-0 community partition after the batch   */
+  double device_ms;      /* device time of the call (CUDA events)                  */
+} hl_batch_stats;
+
+typedef struct hl_graph hl_graph;
+
+/* Default configuration (gamma 1, throughput, 10 levels, 20 rounds). */
+HL_API hl_status hl_config_default(hl_config* cfg);
+
+/* Load an undirected weighted graph of n vertices (m edges; w == NULL means
+ * every weight is 1.0, as GraphInput's None weight, in_memory.rs:49) and build
+ * the bootstrap partition.  Edges with an endpoint >= n are rejected. */
+HL_API hl_status hl_create(const hl_config* cfg, uint32_t n, const uint32_t* src, const uint32_t* dst,
+                    const double* w, uint64_t m, hl_graph** out);
+
+/* Same, but src/dst/w are device pointers on cfg->device (no host copies). */
+HL_API hl_status hl_create_device(const hl_config* cfg, uint32_t n, const uint32_t* d_src,
+                           const uint32_t* d_dst, const double* d_w, uint64_t m,
+                           hl_graph** out);
+
+/* Apply one edge-update batch (GraphInput delta encoding, types.rs:133-147:
+ * positive weight adds or strengthens, negative weakens or deletes; an edge
+ * whose weight falls to <= 1e-12 is removed) and update the partition.
+ * w == NULL means all weights are +1.0.  stats may be NULL. */
+HL_API hl_status hl_apply_batch(hl_graph* g, const uint32_t* src, const uint32_t* dst, const double* w,
+                         uint64_t k, hl_batch_stats* stats);
+
+/* Same with device pointers (on the handle's device). */
+HL_API hl_status hl_apply_batch_device(hl_graph* g, const uint32_t* d_src, const uint32_t* d_dst,
+                                const double* d_w, uint64_t k, hl_batch_stats* stats);
+
+/* Change gamma for subsequent batches (hit_leiden takes it per call,
+ * hit_leiden.rs:939). */
+HL_API hl_status hl_set_resolution(hl_graph* g, double gamma);
+
+HL_API hl_status hl_num_nodes(const hl_graph* g, uint32_t* n);
+HL_API hl_status hl_num_levels(const hl_graph* g, uint32_t* levels);
+HL_API hl_status hl_level_size(const hl_graph* g, uint32_t level, uint32_t* n_level);
+HL_API hl_status hl_num_edges(const hl_graph* g, uint32_t level, uint64_t* entries);
+
+/* Node-indexed community partition of the input vertices (f^1 after
+ * def-update), relabelled to 0..k-1 in first-seen order; out has n entries. */
+HL_API hl_status hl_get_partition(const hl_graph* g, uint32_t* out);
+
+/* Raw per-level map (no relabelling); out has hl_level_size(level) entries. */
+HL_API hl_status hl_get_map(const hl_graph* g, uint32_t level, uint32_t which, uint32_t* out);
+
+/* CSR of level `level`: off has n_level+1 entries, col/w hl_num_edges entries.
+ * Rows are sorted by neighbour id; a self-loop appears twice in its row. */
+HL_API hl_status hl_get_csr(const hl_graph* g, uint32_t level, uint64_t* off, uint32_t* col,
+                     double* w);
+
+/* Modularity of the level-0 community partition (compute_modularity). */
+HL_API hl_status hl_modularity(const hl_graph* g, double* q);
+
+/* Modularity of an arbitrary node-indexed partition of the level-0 graph. */
+HL_API hl_status hl_modularity_of(const hl_graph* g, const uint32_t* part, double* q);
+
+/* First-seen contiguous relabelling of n labels, on the GPU of `device`. */
+HL_API hl_status hl_canonicalize(int32_t device, uint32_t* labels, uint64_t n);
+
+HL_API void hl_destroy(hl_graph* g);
+
+/* Message for the last error on this thread (empty string if none). */
+HL_API const char* hl_last_error(void);
+
+/* Version string of the library build. */
+HL_API const char* hl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HL_H */

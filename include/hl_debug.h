@@ -1,0 +1,76 @@
+/* hl_debug.h — function-level entry points of libhl used by the parity tests.
+ *
+ * Each call runs ONE stage of the update path on the GPU, on host-provided
+ * inputs, with the same kernels the product path uses, so that every stage can
+ * be compared with its reference counterpart on a fixed snapshot.  Graphs are
+ * passed as canonical CSR (rows sorted by neighbour id, a self-loop twice in
+ * its row).  All pointers are host pointers; outputs are caller-allocated.
+ */
+#ifndef HL_DEBUG_H
+#define HL_DEBUG_H
+#include "hl.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Per-vertex best move on a fixed snapshot (f, d(C), k, 2m):
+ * parallel_frontier.rs:133-239 (`execute_shard`, one node).  out_to is the
+ * chosen community (n+v for the empty community), out_gain its gain; a gain
+ * <= 0 means no move. */
+HL_API hl_status hl_dbg_move_eval(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
+                           const double* w, const uint32_t* f, const double* d, uint64_t d_len,
+                           const double* k, double tw, double gamma, const uint32_t* verts,
+                           uint64_t nv, uint32_t* out_to, double* out_gain);
+
+/* Decoupled move selection: throughput.rs:204-236 (`select_decoupled_moves`).
+ * Writes the accepted nodes in selection order; *out_count their number. */
+HL_API hl_status hl_dbg_select_decoupled(int32_t device, const uint32_t* node, const uint32_t* from,
+                                  const uint32_t* to, const double* gain, uint64_t m,
+                                  uint32_t* out_nodes, uint64_t* out_count);
+
+/* G ⊕ ΔG: in_memory.rs:103-137 (`apply_delta`).  Returns the new CSR through
+ * out_off (n_out+1 entries), out_col / out_w (capacity cap); *out_nnz entries. */
+HL_API hl_status hl_dbg_apply_delta(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
+                             const double* w, uint32_t delta_n, const uint32_t* dsrc,
+                             const uint32_t* ddst, const double* dw, uint64_t dk,
+                             int32_t keep_self_loops, uint64_t* out_off, uint32_t* out_col,
+                             double* out_w, uint64_t cap, uint64_t* out_nnz);
+
+/* inc_movement, throughput mode: hit_leiden.rs:1024-1101.  f is updated in
+ * place; changed / affected (may be NULL) receive B and K as 0/1 bytes. */
+HL_API hl_status hl_dbg_inc_movement(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
+                              const double* w, const uint32_t* dsrc, const uint32_t* ddst,
+                              const double* dw, uint64_t dk, uint32_t* f, const uint32_t* s,
+                              double gamma, uint32_t max_rounds, int32_t mark_moved,
+                              uint8_t* changed, uint8_t* affected, uint32_t* iterations);
+
+/* inc_refinement, throughput mode: hit_leiden.rs:1265-1390 with
+ * throughput.rs:239-359.  s is updated in place; refined receives R. */
+HL_API hl_status hl_dbg_inc_refinement(int32_t device, uint32_t n, const uint64_t* off,
+                                const uint32_t* col, const double* w, const uint32_t* f,
+                                uint32_t* s, const uint8_t* affected, double gamma,
+                                int32_t cc_same_community, uint8_t* refined);
+
+/* inc_aggregation: hit_leiden.rs:1639-1731.  Writes the compressed ΔH (ascending
+ * (u,v), capacity cap), the updated s_pre and the next level's node count. */
+HL_API hl_status hl_dbg_inc_aggregation(int32_t device, uint32_t n, const uint64_t* off,
+                                 const uint32_t* col, const double* w, const uint32_t* dsrc,
+                                 const uint32_t* ddst, const double* dw, uint64_t dk,
+                                 const uint32_t* s_pre, const uint32_t* s_cur,
+                                 const uint8_t* refined, int32_t changed_only,
+                                 int32_t edge_weight_loops, uint32_t* out_s_pre,
+                                 uint32_t* out_next_n, uint32_t* out_u, uint32_t* out_v,
+                                 double* out_w, uint64_t cap, uint64_t* out_count);
+
+/* The fixed-shape pairwise sum used for 2m (tiles of 1024, stride halving). */
+HL_API hl_status hl_dbg_tree_sum(int32_t device, const double* x, uint64_t n, double* out);
+
+/* Modularity of `part` on the CSR (hit_leiden.rs:121-161). */
+HL_API hl_status hl_dbg_modularity(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
+                            const double* w, const uint32_t* part, double* q);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HL_DEBUG_H */

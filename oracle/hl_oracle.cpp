@@ -1584,12 +1584,12 @@ void or_move_eval(const or_graph* G, const uint32_t* f, const double* d, uint64_
 
 uint32_t or_inc_movement(const or_graph* G, const uint32_t* dsrc, const uint32_t* ddst,
                          const double* dw, uint64_t dk, uint32_t* f, const uint32_t* s,
-                         double gamma, int mode, uint32_t max_rounds, int compact,
+                         double gamma, int mode, uint32_t max_rounds, int compact, int mark_moved,
                          uint8_t* out_changed, uint8_t* out_affected) {
   const Graph& g = G->g;
   std::vector<u32> fv(f, f + g.n), sv(s, s + g.n);
   MoveOut mo = inc_movement(g, make_edges(dsrc, ddst, dw, dk), fv, sv, gamma, mode, max_rounds,
-                            compact != 0);
+                            compact != 0, mark_moved != 0);
   std::memcpy(f, fv.data(), sizeof(u32) * g.n);
   if (out_changed) std::memcpy(out_changed, mo.changed.data(), g.n);
   if (out_affected) std::memcpy(out_affected, mo.affected.data(), g.n);
@@ -1597,11 +1597,12 @@ uint32_t or_inc_movement(const or_graph* G, const uint32_t* dsrc, const uint32_t
 }
 
 void or_inc_refinement(const or_graph* G, const uint32_t* f, uint32_t* s, const uint8_t* affected,
-                       double gamma, int mode, int faithful, uint8_t* out_refined) {
+                       double gamma, int mode, int faithful, int cc_same_community,
+                       uint8_t* out_refined) {
   const Graph& g = G->g;
   std::vector<u32> fv(f, f + g.n), sv(s, s + g.n);
   std::vector<uint8_t> av(affected, affected + g.n);
-  RefineOut ro = inc_refinement(g, fv, sv, av, gamma, mode, faithful != 0);
+  RefineOut ro = inc_refinement(g, fv, sv, av, gamma, mode, faithful != 0, cc_same_community != 0);
   std::memcpy(s, sv.data(), sizeof(u32) * g.n);
   if (out_refined) std::memcpy(out_refined, ro.refined.data(), g.n);
 }

@@ -57,10 +57,11 @@ void or_move_eval(const or_graph* g, const uint32_t* f, const double* d, uint64_
                   uint32_t* out_to, double* out_gain);
 uint32_t or_inc_movement(const or_graph* g, const uint32_t* dsrc, const uint32_t* ddst,
                          const double* dw, uint64_t dk, uint32_t* f, const uint32_t* s,
-                         double gamma, int mode, uint32_t max_rounds, int compact,
+                         double gamma, int mode, uint32_t max_rounds, int compact, int mark_moved,
                          uint8_t* out_changed, uint8_t* out_affected);
 void or_inc_refinement(const or_graph* g, const uint32_t* f, uint32_t* s, const uint8_t* affected,
-                       double gamma, int mode, int faithful, uint8_t* out_refined);
+                       double gamma, int mode, int faithful, int cc_same_community,
+                       uint8_t* out_refined);
 uint64_t or_inc_aggregation(const or_graph* g, const uint32_t* dsrc, const uint32_t* ddst,
                             const double* dw, uint64_t dk, const uint32_t* s_pre,
                             const uint32_t* s_cur, const uint8_t* refined, uint32_t flags,

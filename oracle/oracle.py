@@ -84,8 +84,9 @@ def load():
                                      u32p, C.c_uint64, u32p, f64p]
         lib.or_inc_movement.restype = C.c_uint32
         lib.or_inc_movement.argtypes = [vp, u32p, u32p, vp, C.c_uint64, u32p, u32p, C.c_double,
-                                        C.c_int, C.c_uint32, C.c_int, u8p, u8p]
-        lib.or_inc_refinement.argtypes = [vp, u32p, u32p, u8p, C.c_double, C.c_int, C.c_int, u8p]
+                                        C.c_int, C.c_uint32, C.c_int, C.c_int, u8p, u8p]
+        lib.or_inc_refinement.argtypes = [vp, u32p, u32p, u8p, C.c_double, C.c_int, C.c_int, C.c_int,
+                                          u8p]
         lib.or_inc_aggregation.restype = C.c_uint64
         lib.or_inc_aggregation.argtypes = [vp, u32p, u32p, vp, C.c_uint64, u32p, u32p, u8p,
                                            C.c_uint32, u32p, C.POINTER(C.c_uint32), u32p, u32p,
@@ -231,7 +232,8 @@ def move_eval(graph: Graph, f, d, k, tw, gamma, verts):
     return to, gain
 
 
-def inc_movement(graph: Graph, dsrc, ddst, dw, f, s, gamma, mode, max_rounds=20, compact=True):
+def inc_movement(graph: Graph, dsrc, ddst, dw, f, s, gamma, mode, max_rounds=20, compact=True,
+                 mark_moved=False):
     n = graph.n
     ds, dd, dwa, dwp = _edges(dsrc, ddst, dw)
     f = np.array(f, dtype=np.uint32)
@@ -239,17 +241,19 @@ def inc_movement(graph: Graph, dsrc, ddst, dw, f, s, gamma, mode, max_rounds=20,
     changed = np.zeros(n, np.uint8)
     affected = np.zeros(n, np.uint8)
     it = load().or_inc_movement(graph.h, ds, dd, dwp, len(ds), f, s, gamma, mode, max_rounds,
-                                int(compact), changed, affected)
+                                int(compact), int(mark_moved), changed, affected)
     return f, changed.astype(bool), affected.astype(bool), it
 
 
-def inc_refinement(graph: Graph, f, s, affected, gamma, mode, faithful=False):
+def inc_refinement(graph: Graph, f, s, affected, gamma, mode, faithful=False,
+                   cc_same_community=False):
     n = graph.n
     f = np.ascontiguousarray(f, dtype=np.uint32)
     s = np.array(s, dtype=np.uint32)
     aff = np.ascontiguousarray(np.asarray(affected, dtype=np.uint8))
     refined = np.zeros(n, np.uint8)
-    load().or_inc_refinement(graph.h, f, s, aff, gamma, mode, int(faithful), refined)
+    load().or_inc_refinement(graph.h, f, s, aff, gamma, mode, int(faithful),
+                             int(cc_same_community), refined)
     return s, refined.astype(bool)
 
 
