@@ -157,17 +157,20 @@ __global__ void k_relabel(u32* lab, u32 n, const u32* rank) {
 u32 rank_compact(Engine& E, u32* labels, u32 n, u32 id_bound) {
   cudaStream_t st = E.stream;
   Scratch& S = E.sc;
-  S.used.ensure(E.mem, (size_t)id_bound + 1);
-  S.rank.ensure(E.mem, (size_t)id_bound + 1);
-  HL_CUDA(cudaMemsetAsync(S.used.p, 0, sizeof(u32) * ((size_t)id_bound + 1), st));
+  // One extra (zero) slot so that the exclusive scan's last entry is the
+  // number of distinct labels.
+  const size_t len = (size_t)id_bound + 2;
+  S.used.ensure(E.mem, len);
+  S.rank.ensure(E.mem, len);
+  HL_CUDA(cudaMemsetAsync(S.used.p, 0, sizeof(u32) * len, st));
   k_mark_used<<<grid_for(n), 256, 0, st>>>(labels, n, S.used.p);
   HL_LAUNCH_CHECK();
   u32* a = S.used.p;
   u32* r = S.rank.p;
   cub_run(E, [&](void* t, size_t& b) {
-    return cub::DeviceScan::ExclusiveSum(t, b, a, r, (int64_t)id_bound + 1, st);
+    return cub::DeviceScan::ExclusiveSum(t, b, a, r, (int64_t)len, st);
   });
-  u32 distinct = E.read_u32(r + id_bound);
+  u32 distinct = E.read_u32(r + id_bound + 1);
   k_relabel<<<grid_for(n), 256, 0, st>>>(labels, n, S.rank.p);
   HL_LAUNCH_CHECK();
   return distinct;
