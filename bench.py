@@ -1,0 +1,410 @@
+#!/usr/bin/env python3
+"""Benchmark of the HIT-Leiden incremental update path on B200.
+
+One step = one edge-update batch applied through hl_apply_batch (G ⊕ ΔG, then
+inc-movement, inc-refinement and inc-aggregation on every level, then the
+top-down level maps), on a graph already resident in HBM.
+
+Default workload (the mid-size plain-method configuration): LFR-style planted
+graph, 1M vertices / ~20M undirected edges, degree exponent 2.5 (mean 40, max
+2000), community sizes exponent 1.5 in [50, 5000], mixing 0.3, f64 weights
+U[0.5, 2.0]; batches of 10k updates (90% degree-preferential inserts, 10%
+uniform deletes of existing edges).  Synthetic, seeded: the reference's
+datasets are not available.
+
+Reported:
+  value   edge-updates/s with batches already on the device (hl_apply_batch_device),
+          timed by CUDA events on the library's stream, summed over the K steps;
+  e2e     edge-updates/s through the public host API (hl_apply_batch with host
+          arrays, host→device copies inside) plus a device→host read of the
+          level-0 community map every step, timed on the host clock;
+  roofline for the inc-movement evaluation kernel (algorithmic bytes / event time);
+  cpu_baseline: the CPU oracle (a C++ port of the reference's Rust) applying
+          one batch of the same stream from the same bootstrapped state.
+
+--impl reference runs that CPU port alone on the same configuration.
+Multi-GPU (--gpus N under torchrun): independent replicas, one graph per GPU,
+no collective on the data path; the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "lfr1m": {
+        "workload": "LFR-style planted graph, 1M vertices / ~20M edges, f64 weights U[0.5,2], "
+                    "batches of 10k updates (90% degree-preferential inserts, 10% deletes)",
+        "batch": 10000,
+    },
+    "ca_hepth": {
+        "workload": "planted graph shaped like ca-HepTh: 9,877 vertices / ~21.8k unit edges, "
+                    "mu 0.15, triangle closure; batches of 1,000 uniform inserts",
+        "batch": 1000,
+    },
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="lfr1m")
+    ap.add_argument("--levels", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-sample-batches", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-small", action="store_true",
+                    help="small case for ncu captures (100k vertices, 2 warm-up steps)")
+    return ap.parse_args()
+
+
+def make_graph(cfg_name, seed, small=False):
+    W = importlib.import_module("hit-leiden_b200.workloads")
+    if cfg_name == "lfr1m":
+        if small:
+            n, s, d, w = W.config2(seed, n=200_000)
+        else:
+            n, s, d, w = W.config2(seed)
+        return n, s, d, w, (0.5, 2.0), 0.9, True
+    n, s, d, w = W.config1(seed)
+    return n, s, d, w, None, 1.0, False
+
+
+def make_batches(n, s, d, w, weights, insert_frac, preferential, count, k, seed):
+    W = importlib.import_module("hit-leiden_b200.workloads")
+    store = W.EdgeStore(n, s, d, w)
+    out = []
+    for i in range(count):
+        if insert_frac >= 1.0 and not preferential:
+            ex = None
+            u, v, ww = W.uniform_inserts(n, k, seed * 1000 + i, ex)
+            store.apply(u, v, ww)
+        else:
+            u, v, ww = W.mixed_batch(store, k, insert_frac, seed * 1000 + i, weights=weights,
+                                     preferential=preferential)
+        out.append((u.astype(np.uint32), v.astype(np.uint32), ww.astype(np.float64)))
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                mx = max(mx, float(parts[2].split()[0]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        j = json.load(open(p))
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the evaluation kernel from the committed ncu
+    summary, scaled to the bench's launch (see profiles/)."""
+    p = os.path.join(ROOT, "profiles", "move_eval_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return None
+    return None
+
+
+def export_state(st):
+    """Per-level CSR and maps of a GPU state, for the CPU oracle."""
+    levels = []
+    subs_pre = st.previous_subcommunity_mapping_per_level
+    subs_cur = st.current_subcommunity_mapping_per_level
+    fs = st.community_mapping_per_level
+    gs = st.refined_community_mapping_per_level
+    for p in range(st.levels):
+        off, col, w = st.supergraph(p)
+        levels.append({"off": off, "col": col, "w": w, "f": fs[p], "g": gs[p],
+                       "s_pre": subs_pre[p], "s_cur": subs_cur[p]})
+    return levels
+
+
+def cpu_baseline(st, batches, levels_cfg, max_batches):
+    """Time the oracle port on the next batches from the GPU's state; check that
+    the GPU state after the same batches is identical (full-size parity)."""
+    from oracle import oracle as O
+    O.load()
+    ora = O.State(st.node_count, levels=1, mode=O.MODE_THROUGHPUT)
+    ora.import_levels(export_state(st))
+    t_cpu = 0.0
+    edges = 0
+    used = 0
+    for (u, v, w) in batches[:max_batches]:
+        t0 = time.perf_counter()
+        ora.hit_leiden(u, v, w)
+        t_cpu += time.perf_counter() - t0
+        edges += len(u)
+        used += 1
+        st.apply_batch(u, v, w)
+    same = st.levels == ora.levels and all(
+        np.array_equal(st.community_mapping_per_level[p], ora.get_map(p, O.MAP_F))
+        and np.array_equal(st.current_subcommunity_mapping_per_level[p],
+                           ora.get_map(p, O.MAP_S_CUR))
+        for p in range(ora.levels))
+    q_gpu = st.modularity()
+    q_cpu = ora.modularity(0)
+    return {"value": edges / t_cpu, "seconds": t_cpu, "batches": used, "edges": edges,
+            "parity_bit_exact": bool(same), "dq": abs(q_gpu - q_cpu)}
+
+
+def run_reference(args, cfg):
+    """CPU port of the reference path alone (bootstrap untimed, then K batches)."""
+    from oracle import oracle as O
+    O.load()
+    n, s, d, w, wts, ins, pref = make_graph(args.config, args.seed, args.ncu_small)
+    k = cfg["batch"]
+    steps = max(1, min(args.steps, 2))
+    warm = 0
+    batches = make_batches(n, s, d, w, wts, ins, pref, warm + steps, k, args.seed)
+    st = O.State(n, mode=O.MODE_THROUGHPUT)
+    if args.levels > 1:
+        st.bootstrap(s, d, w, max_levels=args.levels)
+    else:
+        st = O.State(n, levels=1, mode=O.MODE_THROUGHPUT)
+        st.push_empty_graph()
+        st.hit_leiden(s, d, w)
+    t = 0.0
+    for (u, v, ww) in batches[warm:]:
+        t0 = time.perf_counter()
+        st.hit_leiden(u, v, ww)
+        t += time.perf_counter() - t0
+    val = steps * k / t
+    line = {
+        "impl": "reference", "metric": "edge_updates_per_s", "value": val,
+        "unit": "edge-updates/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * t / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "levels": st.levels, "batch_edges": k},
+        "cpu_baseline": {"value": val, "unit": "edge-updates/s", "cores": 1, "kind": "port",
+                         "sample": f"{steps} batches of {k} updates after an untimed bootstrap"},
+        "e2e": {"value": val, "unit": "edge-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "modularity": st.modularity(0),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, cfg)
+        return
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    hl = importlib.import_module("hit-leiden_b200")
+    L = importlib.import_module("hit-leiden_b200._lib")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    n, s, d, w, wts, ins, pref = make_graph(args.config, args.seed, args.ncu_small)
+    k = cfg["batch"]
+    K, Wm = args.steps, args.warmup
+    n_cpu = 0 if (args.no_cpu_baseline or rank != 0 or world != 1) else args.cpu_sample_batches
+    batches = make_batches(n, s, d, w, wts, ins, pref, Wm + 2 * K + n_cpu, k, args.seed)
+
+    rc = hl.RunConfig(max_iterations=args.levels, device=local)
+    c = rc.to_c()
+    c.flags |= L.HL_FLAG_KERNEL_TIMING
+    h = C.c_void_p()
+    t0 = time.perf_counter()
+    L.check(L.lib.hl_create(C.byref(c), n, L.ptr(s), L.ptr(d), L.ptr(w), len(s), C.byref(h)))
+    boot_s = time.perf_counter() - t0
+    st = hl.PartitionState(h, n, rc)
+
+    for (u, v, ww) in batches[:Wm]:
+        st.apply_batch(u, v, ww)
+
+    # device-resident batches for the HBM-resident measurement
+    dev = []
+    for (u, v, ww) in batches[Wm:Wm + K]:
+        dev.append((torch.from_numpy(u.view(np.int32)).to(f"cuda:{local}"),
+                    torch.from_numpy(v.view(np.int32)).to(f"cuda:{local}"),
+                    torch.from_numpy(ww).to(f"cuda:{local}")))
+    torch.cuda.synchronize()
+    L.check(L.lib.hl_reset_kernel_stats(h))
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    dev_ms = []
+    launches = 0
+    stats = L.BatchStats()
+    for (du, dv, dw) in dev:
+        L.check(L.lib.hl_apply_batch_device(h, C.c_void_p(du.data_ptr()), C.c_void_p(dv.data_ptr()),
+                                            C.c_void_p(dw.data_ptr()), k, C.byref(stats)))
+        dev_ms.append(stats.device_ms)
+        launches += stats.launches
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    tot_ms = float(sum(dev_ms))
+    if dist is not None:
+        t = torch.tensor([tot_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    value = world * K * k / (tot_ms / 1000.0)
+
+    kst = (L.KernelStat * 8)()
+    cnt = C.c_uint32()
+    L.check(L.lib.hl_kernel_stats(h, kst, 8, C.byref(cnt)))
+    kernels = {kst[i].name.decode(): {"launches": kst[i].launches, "ms": kst[i].total_ms,
+                                      "bytes": kst[i].bytes} for i in range(cnt.value)}
+
+    # end to end through the host API
+    e2e_s = []
+    comm = np.zeros(n, np.uint32)
+    barrier()
+    torch.cuda.synchronize()
+    for (u, v, ww) in batches[Wm + K:Wm + 2 * K]:
+        t1 = time.perf_counter()
+        st.apply_batch(u, v, ww)
+        L.check(L.lib.hl_get_map(h, 0, L.HL_MAP_COMMUNITY, L.ptr(comm)))
+        e2e_s.append(time.perf_counter() - t1)
+    torch.cuda.synchronize()
+    barrier()
+    tot_e2e = float(sum(e2e_s))
+    if dist is not None:
+        t = torch.tensor([tot_e2e], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_e2e = float(t.item())
+    e2e_val = world * K * k / tot_e2e
+    lat = sorted(1000.0 * x for x in e2e_s)
+
+    ev = kernels.get("move_eval", {})
+    peak, peak_kind = measured_peak()
+    roof = None
+    if ev.get("launches"):
+        achieved = ev["bytes"] / (ev["ms"] / 1000.0) / 1e9
+        per_launch = ev["bytes"] / ev["launches"]
+        tr = committed_traffic()
+        traffic = None
+        if tr and tr.get("config") == args.config and tr.get("traffic_per_algorithmic_byte"):
+            traffic = per_launch * tr["traffic_per_algorithmic_byte"]
+        roof = {"kernel": "k_eval<EVAL_MOVE> (inc-movement best-move evaluation)",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "bytes_per_launch": per_launch, "avg_launch_ms": ev["ms"] / ev["launches"],
+                "traffic": traffic}
+
+    q = st.modularity()
+    cpu = None
+    if n_cpu:
+        cpu_res = cpu_baseline(st, batches[Wm + 2 * K:], args.levels, n_cpu)
+        cpu = {"value": cpu_res["value"], "unit": "edge-updates/s", "cores": 1, "kind": "port",
+               "sample": f"{cpu_res['batches']} batch(es) of {k} updates of the same stream, "
+                         f"from the GPU's state ({cpu_res['seconds']:.1f} s on 1 host core)",
+               "parity_bit_exact_after_sample": cpu_res["parity_bit_exact"],
+               "dq_after_sample": cpu_res["dq"]}
+
+    if rank == 0:
+        line = {
+            "metric": "edge_updates_per_s", "value": value, "unit": "edge-updates/s",
+            "n_gpus": world, "steps": K, "warmup": Wm, "ms_per_step": tot_ms / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": cfg["workload"], "vertices": n, "edges": int(len(s)),
+                       "batch_edges": k, "levels": st.levels, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (resident CSR > 126 MB)",
+                       "bootstrap_s": boot_s},
+            "e2e": {"value": e2e_val, "unit": "edge-updates/s",
+                    "h2d_bytes_per_step": int(k * (4 + 4 + 8)),
+                    "d2h_bytes_per_step": int(n * 4),
+                    "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1,
+                                                                    int(0.99 * len(lat)))]},
+            "gpu_launches": int(launches),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "modularity": q,
+            "kernels": kernels,
+        }
+        print(json.dumps(line), flush=True)
+    st.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -27,6 +27,12 @@ HL_MODE_THROUGHPUT = 1
 HL_MAP_COMMUNITY, HL_MAP_REFINED, HL_MAP_SUB_PREVIOUS, HL_MAP_SUB_CURRENT = 0, 1, 2, 3
 HL_FLAG_KEEP_SELF_LOOPS = 1 << 0
 HL_FLAG_BATCH_MODULARITY = 1 << 1
+HL_FLAG_KERNEL_TIMING = 1 << 2
+
+
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint64), ("total_ms", C.c_double),
+                ("bytes", C.c_uint64)]
 
 
 class Config(C.Structure):
@@ -39,7 +45,8 @@ class BatchStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("levels", C.c_uint32), ("moves", C.c_uint64),
                 ("candidates", C.c_uint64), ("traversed", C.c_uint64), ("splits", C.c_uint64),
                 ("merges", C.c_uint64), ("changed", C.c_uint64), ("refined", C.c_uint64),
-                ("edges", C.c_uint64), ("modularity", C.c_double), ("device_ms", C.c_double)]
+                ("edges", C.c_uint64), ("modularity", C.c_double), ("device_ms", C.c_double),
+                ("launches", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -71,6 +78,8 @@ def _load():
         "hl_apply_batch": (st, [vp, vp, vp, vp, C.c_uint64, C.POINTER(BatchStats)]),
         "hl_apply_batch_device": (st, [vp, vp, vp, vp, C.c_uint64, C.POINTER(BatchStats)]),
         "hl_set_resolution": (st, [vp, C.c_double]),
+        "hl_kernel_stats": (st, [vp, vp, C.c_uint32, p32]),
+        "hl_reset_kernel_stats": (st, [vp]),
         "hl_num_nodes": (st, [vp, p32]),
         "hl_num_levels": (st, [vp, p32]),
         "hl_level_size": (st, [vp, C.c_uint32, p32]),

@@ -150,7 +150,7 @@ static u64 compress_records(Engine& E, u64 R, double threshold) {
   S.rowlist.ensure(E.mem, R);
   S.segid.ensure(E.mem, R);
   S.seg_start.ensure(E.mem, R);
-  k_heads64<<<grid_for(R), 256, 0, st>>>(ko, R, S.rowlist.p);
+  ++E.nlaunch, k_heads64<<<grid_for(R), 256, 0, st>>>(ko, R, S.rowlist.p);
   HL_LAUNCH_CHECK();
   u32* h = S.rowlist.p;
   u32* sid = S.segid.p;
@@ -158,12 +158,12 @@ static u64 compress_records(Engine& E, u64 R, double threshold) {
     return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)R, st);
   });
   u32 U = E.read_u32(sid + R - 1) + E.read_u32(h + R - 1);
-  k_seg_start64<<<grid_for(R), 256, 0, st>>>(h, sid, R, S.seg_start.p);
+  ++E.nlaunch, k_seg_start64<<<grid_for(R), 256, 0, st>>>(h, sid, R, S.seg_start.p);
   S.eu.ensure(E.mem, U);
   S.ev.ensure(E.mem, U);
   S.ew.ensure(E.mem, U);
   S.op.ensure(E.mem, U);
-  k_compress<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, R, ko, vo, S.neww.p, threshold,
+  ++E.nlaunch, k_compress<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, R, ko, vo, S.neww.p, threshold,
                                           S.eu.p, S.ev.p, S.ew.p, S.op.p);
   HL_LAUNCH_CHECK();
   S.eu2.ensure(E.mem, U);
@@ -193,6 +193,7 @@ u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n, boo
   Scratch& S = E.sc;
   cudaStream_t st = E.stream;
   const u32 n = L.g.n;
+  cudaEvent_t kev = E.kt_begin();
   // next node count from the maps before s_pre is updated (:1716-1722)
   S.cnt.ensure(E.mem, 16);
   {
@@ -214,7 +215,7 @@ u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n, boo
   }
   S.newoff.ensure(E.mem, (size_t)n + 1);
   S.gkey2.ensure(E.mem, (size_t)n + 1);
-  k_agg_count<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, S.refined.p,
+  ++E.nlaunch, k_agg_count<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, S.refined.p,
                                            L.s_pre.p, L.s_cur.p, changed_only, edge_weight_loops,
                                            S.newoff.p);
   HL_CUDA(cudaMemsetAsync(S.newoff.p + n, 0, sizeof(u64), st));
@@ -233,17 +234,22 @@ u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n, boo
     S.idx2.ensure(E.mem, R);
     S.neww.ensure(E.mem, R);
     if (delta.k)
-      k_agg_lift<<<grid_for(delta.k), 256, 0, st>>>(delta.u, delta.v, delta.w, delta.k, L.s_pre.p,
+      ++E.nlaunch, k_agg_lift<<<grid_for(delta.k), 256, 0, st>>>(delta.u, delta.v, delta.w, delta.k, L.s_pre.p,
                                                     S.keys.p, S.neww.p, S.idx.p);
-    k_agg_emit<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, S.refined.p,
+    ++E.nlaunch, k_agg_emit<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, S.refined.p,
                                             L.s_pre.p, L.s_cur.p, changed_only,
                                             edge_weight_loops, pos, delta.k, S.keys.p, S.neww.p,
                                             S.idx.p);
     HL_LAUNCH_CHECK();
   }
   u64 out = compress_records(E, R, 1e-9);
-  k_set_spre<<<grid_for(n), 256, 0, st>>>(n, S.refined.p, L.s_cur.p, L.s_pre.p);
+  ++E.nlaunch, k_set_spre<<<grid_for(n), 256, 0, st>>>(n, S.refined.p, L.s_cur.p, L.s_pre.p);
   HL_LAUNCH_CHECK();
+  E.kt_end(KT_AGGREGATE, kev);
+  // ΔG lifted (u, v, w + two s_pre reads), refined rows scanned (maps, row
+  // entries), ΔH records written and read once, compressed output written.
+  E.kagg[KT_AGGREGATE].bytes += 32ull * delta.k + 13ull * n + 10ull * (L.g.nnz ? R2 / 2 : 0) * 2 +
+                                 32ull * R + 16ull * out;
   return out;
 }
 
@@ -284,7 +290,7 @@ u64 aggregate_full(Engine& E, Level& L, const u32* s, u32*, u32*, double*) {
   const u32 n = L.g.n;
   S.newoff.ensure(E.mem, (size_t)n + 1);
   S.gkey2.ensure(E.mem, (size_t)n + 1);
-  k_full_count<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, S.newoff.p);
+  ++E.nlaunch, k_full_count<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, S.newoff.p);
   HL_CUDA(cudaMemsetAsync(S.newoff.p + n, 0, sizeof(u64), st));
   HL_LAUNCH_CHECK();
   u64* a = S.newoff.p;
@@ -299,7 +305,7 @@ u64 aggregate_full(Engine& E, Level& L, const u32* s, u32*, u32*, double*) {
   S.idx.ensure(E.mem, R);
   S.idx2.ensure(E.mem, R);
   S.neww.ensure(E.mem, R);
-  k_full_emit<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, s, pos, S.keys.p,
+  ++E.nlaunch, k_full_emit<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, s, pos, S.keys.p,
                                            S.neww.p, S.idx.p);
   HL_LAUNCH_CHECK();
   return compress_records(E, R, -1.0);
@@ -323,8 +329,8 @@ void project_up(Engine& E, Level& lo, Level& hi) {
   u32 nh = hi.g.n;
   S.minmem.ensure(E.mem, (size_t)nh + 1);
   HL_CUDA(cudaMemsetAsync(S.minmem.p, 0, sizeof(u32) * ((size_t)nh + 1), E.stream));
-  k_last_member<<<grid_for(lo.g.n), 256, 0, E.stream>>>(lo.g.n, lo.s_cur.p, S.minmem.p);
-  k_project<<<grid_for(nh), 256, 0, E.stream>>>(nh, S.minmem.p, lo.f.p, hi.f.p);
+  ++E.nlaunch, k_last_member<<<grid_for(lo.g.n), 256, 0, E.stream>>>(lo.g.n, lo.s_cur.p, S.minmem.p);
+  ++E.nlaunch, k_project<<<grid_for(nh), 256, 0, E.stream>>>(nh, S.minmem.p, lo.f.p, hi.f.p);
   HL_LAUNCH_CHECK();
 }
 
@@ -340,11 +346,11 @@ __global__ void k_top_down(u32 n, const u32* s, const u32* fhi, const u32* ghi, 
 void top_down(Engine& E) {
   int P = (int)E.levels.size();
   Level& top = E.levels[P - 1];
-  k_iota<<<grid_for(top.g.n), 256, 0, E.stream>>>(top.gm.p, top.g.n);
+  ++E.nlaunch, k_iota<<<grid_for(top.g.n), 256, 0, E.stream>>>(top.gm.p, top.g.n);
   for (int p = P - 2; p >= 0; --p) {
     Level& lo = E.levels[p];
     Level& hi = E.levels[p + 1];
-    k_top_down<<<grid_for(lo.g.n), 256, 0, E.stream>>>(lo.g.n, lo.s_cur.p, hi.f.p, hi.gm.p, lo.f.p,
+    ++E.nlaunch, k_top_down<<<grid_for(lo.g.n), 256, 0, E.stream>>>(lo.g.n, lo.s_cur.p, hi.f.p, hi.gm.p, lo.f.p,
                                                         lo.gm.p);
   }
   HL_LAUNCH_CHECK();
@@ -372,7 +378,7 @@ void inherit_new_nodes(Engine& E, Level& hi, const std::vector<std::pair<u32, u3
   S.upd_to.ensure(E.mem, m);
   HL_CUDA(cudaMemcpyAsync(S.upd_node.p, xs.data(), sizeof(u32) * m, cudaMemcpyHostToDevice, E.stream));
   HL_CUDA(cudaMemcpyAsync(S.upd_to.p, os.data(), sizeof(u32) * m, cudaMemcpyHostToDevice, E.stream));
-  k_inherit<<<grid_for(m), 256, 0, E.stream>>>(S.upd_node.p, S.upd_to.p, m, hi.s_pre.p, hi.s_cur.p,
+  ++E.nlaunch, k_inherit<<<grid_for(m), 256, 0, E.stream>>>(S.upd_node.p, S.upd_to.p, m, hi.s_pre.p, hi.s_cur.p,
                                                hi.gm.p);
   HL_LAUNCH_CHECK();
   E.sync();  // host vectors go out of scope

@@ -34,6 +34,45 @@ double Engine::read_f64(const double* d) {
 }
 void Engine::sync() { HL_CUDA(cudaStreamSynchronize(stream)); }
 
+static cudaEvent_t pool_get(std::vector<cudaEvent_t>& pool) {
+  if (!pool.empty()) {
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  HL_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+cudaEvent_t Engine::kt_begin() {
+  if (!ktiming) return nullptr;
+  cudaEvent_t e = pool_get(ev_pool);
+  HL_CUDA(cudaEventRecord(e, stream));
+  return e;
+}
+
+void Engine::kt_end(int id, cudaEvent_t a) {
+  if (!ktiming || !a) return;
+  cudaEvent_t b = pool_get(ev_pool);
+  HL_CUDA(cudaEventRecord(b, stream));
+  ev_pending.push_back({id, {a, b}});
+}
+
+void Engine::kt_collect() {
+  if (ev_pending.empty()) return;
+  HL_CUDA(cudaStreamSynchronize(stream));
+  for (auto& r : ev_pending) {
+    float ms = 0.f;
+    HL_CUDA(cudaEventElapsedTime(&ms, r.second.first, r.second.second));
+    kagg[r.first].ms += ms;
+    kagg[r.first].launches += 1;
+    ev_pool.push_back(r.second.first);
+    ev_pool.push_back(r.second.second);
+  }
+  ev_pending.clear();
+}
+
 }  // namespace hl
 
 namespace {
@@ -91,6 +130,7 @@ static void engine_init(EngineBox& B, const hl_config* cfg) {
   E.mem.stream = B.so.s;
   E.mem.budget = cfg->hbm_budget;
   E.multilevel = cfg->max_levels > 1;
+  E.ktiming = (cfg->flags & HL_FLAG_KERNEL_TIMING) != 0;
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, cfg->device) == cudaSuccess) {
     uint64_t thr = UINT64_MAX;
@@ -107,6 +147,8 @@ static void engine_free(EngineBox* B) {
     cudaSetDevice(B->E->device);
     if (B->E->ev0) cudaEventDestroy(B->E->ev0);
     if (B->E->ev1) cudaEventDestroy(B->E->ev1);
+    B->E->kt_collect();
+    for (cudaEvent_t e : B->E->ev_pool) cudaEventDestroy(e);
   }
   delete B;  // members: bb, E (frees on the stream), then so (destroys the stream)
 }
@@ -125,7 +167,7 @@ static u32 count_flags(Engine& E, const u8* f, u32 n) {
   HL_CUDA(cudaMemsetAsync(E.sc.cnt.p + 15, 0, sizeof(u32), E.stream));
   u32 g = (n + 255) / 256;
   if (g > 148 * 32) g = 148 * 32;
-  k_count_u8<<<g, 256, 0, E.stream>>>(f, n, E.sc.cnt.p + 15);
+  ++E.nlaunch, k_count_u8<<<g, 256, 0, E.stream>>>(f, n, E.sc.cnt.p + 15);
   HL_LAUNCH_CHECK();
   return E.read_u32(E.sc.cnt.p + 15);
 }
@@ -302,6 +344,8 @@ static void finish_stats(EngineBox& B, hl_batch_stats* stats) {
   float ms = 0.f;
   HL_CUDA(cudaEventElapsedTime(&ms, E.ev0, E.ev1));
   E.st.device_ms = ms;
+  E.st.launches = E.nlaunch - E.launch_mark;
+  E.kt_collect();
   E.st.levels = (u32)E.levels.size();
   E.st.edges = E.levels.empty() ? 0 : E.levels[0].g.nnz / 2;
   E.st.modularity = NAN;
@@ -340,6 +384,7 @@ static void apply_impl(hl_graph* g, const uint32_t* src, const uint32_t* dst, co
   Engine& E = *B.E;
   HL_CUDA(cudaSetDevice(E.device));
   E.st = hl_batch_stats{};
+  E.launch_mark = E.nlaunch;
   HL_CUDA(cudaEventRecord(E.ev0, E.stream));
   DevEdges D;
   if (device_ptrs)
@@ -389,6 +434,25 @@ hl_status hl_apply_batch(hl_graph* g, const uint32_t* src, const uint32_t* dst, 
 hl_status hl_apply_batch_device(hl_graph* g, const uint32_t* src, const uint32_t* dst,
                                 const double* w, uint64_t k, hl_batch_stats* stats) {
   HL_TRY(apply_impl(g, src, dst, w, k, true, stats));
+}
+
+static const char* kernel_names[KT_COUNT] = {"move_eval", "refine_eval", "select_decoupled",
+                                             "csr_merge_rows", "aggregate_compress"};
+
+hl_status hl_kernel_stats(const hl_graph* g, hl_kernel_stat* out, uint32_t cap, uint32_t* count) {
+  HL_TRY(require(g && count, "NULL argument"); Engine& E = *const_cast<EngineBox*>(box(g))->E;
+         E.kt_collect(); *count = KT_COUNT; for (uint32_t i = 0; i < KT_COUNT && i < cap && out; ++i) {
+           std::memset(&out[i], 0, sizeof(out[i]));
+           std::strncpy(out[i].name, kernel_names[i], sizeof(out[i].name) - 1);
+           out[i].launches = E.kagg[i].launches;
+           out[i].total_ms = E.kagg[i].ms;
+           out[i].bytes = E.kagg[i].bytes;
+         });
+}
+
+hl_status hl_reset_kernel_stats(hl_graph* g) {
+  HL_TRY(require(g != nullptr, "NULL argument"); Engine& E = *box(g)->E; E.kt_collect();
+         for (auto& k : E.kagg) k = KernelAgg{});
 }
 
 hl_status hl_set_resolution(hl_graph* g, double gamma) {

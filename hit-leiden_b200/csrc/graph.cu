@@ -59,10 +59,10 @@ void graph_init_empty(Engine& E, Level& L, u32 n) {
   L.s_cur.ensure(E.mem, n ? n : 1);
   L.k.ensure(E.mem, n ? n : 1);
   if (n) {
-    k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.f.p, n);
-    k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.gm.p, n);
-    k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.s_pre.p, n);
-    k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.s_cur.p, n);
+    ++E.nlaunch, k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.f.p, n);
+    ++E.nlaunch, k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.gm.p, n);
+    ++E.nlaunch, k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.s_pre.p, n);
+    ++E.nlaunch, k_iota<<<grid_for(n), 256, 0, E.stream>>>(L.s_cur.p, n);
     HL_CUDA(cudaMemsetAsync(L.k.p, 0, sizeof(double) * n, E.stream));
   }
   L.tw = 0.0;
@@ -74,18 +74,18 @@ void graph_grow_nodes(Engine& E, Level& L, u32 n) {
   u32 old = L.g.n;
   if (n <= old) return;
   L.g.off.ensure(E.mem, (size_t)n + 1, true);
-  k_fill_u64_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.g.off.p, L.g.nnz, (u64)old + 1,
+  ++E.nlaunch, k_fill_u64_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.g.off.p, L.g.nnz, (u64)old + 1,
                                                              (u64)n + 1);
   L.f.ensure(E.mem, n, true);
   L.gm.ensure(E.mem, n, true);
   L.s_pre.ensure(E.mem, n, true);
   L.s_cur.ensure(E.mem, n, true);
   L.k.ensure(E.mem, n, true);
-  k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.f.p, old, n);
-  k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.gm.p, old, n);
-  k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.s_pre.p, old, n);
-  k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.s_cur.p, old, n);
-  k_fill_f64_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.k.p, 0.0, old, n);
+  ++E.nlaunch, k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.f.p, old, n);
+  ++E.nlaunch, k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.gm.p, old, n);
+  ++E.nlaunch, k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.s_pre.p, old, n);
+  ++E.nlaunch, k_iota_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.s_cur.p, old, n);
+  ++E.nlaunch, k_fill_f64_range<<<grid_for(n - old), 256, 0, E.stream>>>(L.k.p, 0.0, old, n);
   L.g.n = n;
   HL_LAUNCH_CHECK();
 }
@@ -121,7 +121,7 @@ void check_endpoints(Engine& E, const DevEdges& b, u32 n) {
   if (!b.k) return;
   E.sc.cnt.ensure(E.mem, 16);
   HL_CUDA(cudaMemsetAsync(E.sc.cnt.p, 0, sizeof(u32), E.stream));
-  k_check_endpoints<<<grid_for(b.k), 256, 0, E.stream>>>(b.u, b.v, b.k, n, E.sc.cnt.p);
+  ++E.nlaunch, k_check_endpoints<<<grid_for(b.k), 256, 0, E.stream>>>(b.u, b.v, b.k, n, E.sc.cnt.p);
   HL_LAUNCH_CHECK();
   u32 bad = E.read_u32(E.sc.cnt.p);
   require(bad == 0, "edge endpoint exceeds node_count (" + std::to_string(bad) + " edges)");
@@ -138,7 +138,7 @@ bool edges_integral(Engine& E, const DevEdges& b) {
   if (!b.k || !b.w) return true;
   E.sc.cnt.ensure(E.mem, 16);
   HL_CUDA(cudaMemsetAsync(E.sc.cnt.p + 1, 0, sizeof(u32), E.stream));
-  k_integral<<<grid_for(b.k), 256, 0, E.stream>>>(b.w, b.k, E.sc.cnt.p + 1);
+  ++E.nlaunch, k_integral<<<grid_for(b.k), 256, 0, E.stream>>>(b.w, b.k, E.sc.cnt.p + 1);
   HL_LAUNCH_CHECK();
   return E.read_u32(E.sc.cnt.p + 1) == 0;
 }
@@ -411,7 +411,7 @@ double tree_sum(Engine& E, const double* x, u64 n) {
   u64 cur = n;
   while (true) {
     u64 t = (cur + 1023) / 1024;
-    k_tree_tile<<<(u32)t, 256, 0, E.stream>>>(src, cur, a);
+    ++E.nlaunch, k_tree_tile<<<(u32)t, 256, 0, E.stream>>>(src, cur, a);
     HL_LAUNCH_CHECK();
     if (t == 1) break;
     src = a;
@@ -424,10 +424,10 @@ double tree_sum(Engine& E, const double* x, u64 n) {
 static void recompute_rows(Engine& E, Level& L, const u32* rows, u32 nr) {
   if (!nr) return;
   if (E.integral)
-    k_row_sum_warp<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p,
+    ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p,
                                                                   L.k.p);
   else
-    k_row_sum_serial<<<grid_for(nr), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p, L.k.p);
+    ++E.nlaunch, k_row_sum_serial<<<grid_for(nr), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p, L.k.p);
   HL_LAUNCH_CHECK();
 }
 
@@ -435,10 +435,10 @@ void recompute_all_degrees(Engine& E, Level& L) {
   u32 n = L.g.n;
   if (n) {
     if (E.integral)
-      k_row_sum_warp<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(nullptr, n, L.g.off.p, L.g.w.p,
+      ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(nullptr, n, L.g.off.p, L.g.w.p,
                                                                    L.k.p);
     else
-      k_row_sum_serial_all<<<grid_for(n), 256, 0, E.stream>>>(n, L.g.off.p, L.g.w.p, L.k.p);
+      ++E.nlaunch, k_row_sum_serial_all<<<grid_for(n), 256, 0, E.stream>>>(n, L.g.off.p, L.g.w.p, L.k.p);
     HL_LAUNCH_CHECK();
   }
   L.tw = tree_sum(E, L.k.p, n);
@@ -472,7 +472,7 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
     S.segid.ensure(E.mem, k);
     S.seg_start.ensure(E.mem, k + 1);
     S.rowlist.ensure(E.mem, k);
-    k_delta_keys<<<grid_for(k), 256, 0, st>>>(b.u, b.v, k, S.keys.p, S.idx.p);
+    ++E.nlaunch, k_delta_keys<<<grid_for(k), 256, 0, st>>>(b.u, b.v, k, S.keys.p, S.idx.p);
     HL_LAUNCH_CHECK();
     u64* kin = S.keys.p;
     u64* kout = S.keys2.p;
@@ -481,14 +481,14 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
     cub_run(E, [&](void* t, size_t& bytes) {
       return cub::DeviceRadixSort::SortPairs(t, bytes, kin, kout, vin, vout, (int64_t)k, 0, 64, st);
     });
-    k_heads<<<grid_for(k), 256, 0, st>>>(kout, k, S.rowlist.p);
+    ++E.nlaunch, k_heads<<<grid_for(k), 256, 0, st>>>(kout, k, S.rowlist.p);
     HL_LAUNCH_CHECK();
     u32* head = S.rowlist.p;
     u32* segid = S.segid.p;
     cub_run(E, [&](void* t, size_t& bytes) {
       return cub::DeviceScan::ExclusiveSum(t, bytes, head, segid, (int64_t)k, st);
     });
-    k_seg_start<<<grid_for(k), 256, 0, st>>>(head, segid, k, S.seg_start.p);
+    ++E.nlaunch, k_seg_start<<<grid_for(k), 256, 0, st>>>(head, segid, k, S.seg_start.p);
     HL_LAUNCH_CHECK();
     u32 last_seg = E.read_u32(segid + (k - 1));
     u32 last_head = E.read_u32(head + (k - 1));
@@ -500,7 +500,7 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
     S.nops_ins.ensure(E.mem, U + 1);
     S.pos_del.ensure(E.mem, U + 1);
     S.pos_ins.ensure(E.mem, U + 1);
-    k_resolve<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, k, kout, vout, b.w, L.g.off.p,
+    ++E.nlaunch, k_resolve<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, k, kout, vout, b.w, L.g.off.p,
                                            L.g.col.p, L.g.w.p, keep_loops, S.op.p, S.neww.p,
                                            S.ktouched.p, S.nops_del.p, S.nops_ins.p, S.cnt.p);
     HL_LAUNCH_CHECK();
@@ -524,7 +524,7 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   u64 n_drop = 0;
   if (drop_loops) {
     HL_CUDA(cudaMemsetAsync(S.cnt.p + 3, 0, sizeof(u32), st));
-    k_count_loops<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, S.cnt.p + 3);
+    ++E.nlaunch, k_count_loops<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, S.cnt.p + 3);
     HL_LAUNCH_CHECK();
     n_drop = E.read_u32(S.cnt.p + 3);
   }
@@ -554,11 +554,11 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   S.rvals.ensure(E.mem, R);
   S.rvals2.ensure(E.mem, R);
   if (U)
-    k_emit_rowops<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, S.keys2.p, S.op.p, S.pos_del.p,
+    ++E.nlaunch, k_emit_rowops<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, S.keys2.p, S.op.p, S.pos_del.p,
                                                S.pos_ins.p, n_del_keys + n_drop, S.rkeys.p,
                                                S.rvals.p);
   if (drop_loops && n_drop)
-    k_emit_loop_drops<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, S.rkeys.p, S.rvals.p,
+    ++E.nlaunch, k_emit_loop_drops<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, S.rkeys.p, S.rvals.p,
                                                    n_del_keys, n_del_keys + n_drop, S.cnt.p + 2,
                                                    S.ktouched.p, S.cnt.p + 4);
   HL_LAUNCH_CHECK();
@@ -578,7 +578,7 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   DBuf<u32>& fins = S.cand_to;
   fdel.ensure(E.mem, R + 1);
   fins.ensure(E.mem, R + 1);
-  k_rowop_flags<<<grid_for(R), 256, 0, st>>>(S.rvals2.p, R, fdel.p, fins.p);
+  ++E.nlaunch, k_rowop_flags<<<grid_for(R), 256, 0, st>>>(S.rvals2.p, R, fdel.p, fins.p);
   HL_LAUNCH_CHECK();
   HL_CUDA(cudaMemsetAsync(fdel.p + R, 0, sizeof(u32), st));
   HL_CUDA(cudaMemsetAsync(fins.p + R, 0, sizeof(u32), st));
@@ -598,9 +598,9 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   S.touched.ensure(E.mem, n ? n : 1);
   HL_CUDA(cudaMemsetAsync(S.ddeg.p, 0, sizeof(int) * (n ? n : 1), st));
   HL_CUDA(cudaMemsetAsync(S.touched.p, 0, n ? n : 1, st));
-  k_rowop_deg<<<grid_for(R), 256, 0, st>>>(S.rkeys2.p, S.rvals2.p, R, S.ddeg.p, S.touched.p);
+  ++E.nlaunch, k_rowop_deg<<<grid_for(R), 256, 0, st>>>(S.rkeys2.p, S.rvals2.p, R, S.ddeg.p, S.touched.p);
   S.newoff.ensure(E.mem, (size_t)n + 1);
-  k_new_degrees<<<grid_for((u64)n + 1), 256, 0, st>>>(n, L.g.off.p, S.ddeg.p, S.newoff.p);
+  ++E.nlaunch, k_new_degrees<<<grid_for((u64)n + 1), 256, 0, st>>>(n, L.g.off.p, S.ddeg.p, S.newoff.p);
   HL_LAUNCH_CHECK();
   {
     u64* a = S.newoff.p;
@@ -614,12 +614,16 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   DBuf<double> nw;
   ncol.ensure(E.mem, nnz_new ? nnz_new : 1);
   nw.ensure(E.mem, nnz_new ? nnz_new : 1);
+  cudaEvent_t kev = E.kt_begin();
   if (n)
-    k_merge_rows<<<grid_for((u64)n * 32), 256, 0, st>>>(n, G.off.p, G.col.p, G.w.p, S.newoff.p,
+    ++E.nlaunch, k_merge_rows<<<grid_for((u64)n * 32), 256, 0, st>>>(n, G.off.p, G.col.p, G.w.p, S.newoff.p,
                                                          ncol.p, nw.p, S.touched.p, S.rkeys2.p,
                                                          S.rvals2.p, R, S.delpre.p, S.inspre.p,
                                                          S.neww.p, nnz_new, S.cnt.p + 4);
   HL_LAUNCH_CHECK();
+  E.kt_end(KT_MERGE_ROWS, kev);
+  // old and new offsets, touched flags, old and new (col, w) entries
+  E.kagg[KT_MERGE_ROWS].bytes += 16ull * ((u64)n + 1) + n + 12ull * (G.nnz + nnz_new);
   if (E.read_u32(S.cnt.p + 4) != 0)
     throw Error(HL_ERR_CUDA, "internal error: CSR merge produced an out-of-range position");
   G.col.swap(ncol);

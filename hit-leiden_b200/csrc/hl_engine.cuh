@@ -77,6 +77,22 @@ struct Scratch {
   DBuf<u32> origin;
 };
 
+// Per-kernel device timing (CUDA events on the engine's stream), enabled by
+// HL_FLAG_KERNEL_TIMING; bytes are the algorithmic bytes the stage moved.
+struct KernelAgg {
+  u64 launches = 0;
+  double ms = 0.0;
+  u64 bytes = 0;
+};
+enum KernelId : int {
+  KT_MOVE_EVAL = 0,
+  KT_REFINE_EVAL,
+  KT_SELECT,
+  KT_MERGE_ROWS,
+  KT_AGGREGATE,
+  KT_COUNT
+};
+
 struct Engine {
   hl_config cfg{};
   int device = 0;
@@ -90,10 +106,20 @@ struct Engine {
   u64 epoch = 1;         // selection epochs (reservation keys)
   u32 sel_round = 0;     // role tag of the current selection
   u64 stats_sel_iters = 0;
+  u64 nlaunch = 0;       // launches of this library's kernels
+  u64 launch_mark = 0;
   // per-call statistics
   hl_batch_stats st{};
   std::vector<std::pair<u32, u32>> new_ids;  // (new sub-community id, origin) of the last refinement
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // kernel timing
+  bool ktiming = false;
+  KernelAgg kagg[KT_COUNT];
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+  cudaEvent_t kt_begin();
+  void kt_end(int id, cudaEvent_t a);
+  void kt_collect();
 
   u64 read_u64(const u64* dptr);
   u32 read_u32(const u32* dptr);

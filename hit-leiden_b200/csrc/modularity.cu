@@ -93,8 +93,8 @@ static double dd_sum(Engine& E, const double* x, u64 n) {
   if (blocks > 1024) blocks = 1024;
   S.red.ensure(E.mem, 2 * (size_t)blocks + 4);
   S.red2.ensure(E.mem, 4);
-  k_dd_reduce<<<blocks, 256, 0, E.stream>>>(x, nullptr, n, S.red.p, S.red.p + blocks);
-  k_dd_reduce<<<1, 256, 0, E.stream>>>(S.red.p, S.red.p + blocks, blocks, S.red2.p, S.red2.p + 1);
+  ++E.nlaunch, k_dd_reduce<<<blocks, 256, 0, E.stream>>>(x, nullptr, n, S.red.p, S.red.p + blocks);
+  ++E.nlaunch, k_dd_reduce<<<1, 256, 0, E.stream>>>(S.red.p, S.red.p + blocks, blocks, S.red2.p, S.red2.p + 1);
   HL_LAUNCH_CHECK();
   double hi = E.read_f64(S.red2.p);
   double lo = E.read_f64(S.red2.p + 1);
@@ -109,7 +109,7 @@ double modularity(Engine& E, Level& L, const u32* part) {
   // intra
   DBuf<double> rows;
   rows.ensure(E.mem, n);
-  k_row_intra<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, part,
+  ++E.nlaunch, k_row_intra<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, part,
                                                       rows.p);
   HL_LAUNCH_CHECK();
   double intra = dd_sum(E, rows.p, n);
@@ -124,7 +124,7 @@ double modularity(Engine& E, Level& L, const u32* part) {
   d.ensure(E.mem, nc);
   terms.ensure(E.mem, nc);
   recompute_comm_degrees(E, L, part, nc, d.p);
-  k_sq_terms<<<grid_for(nc), 256, 0, st>>>(nc, d.p, L.tw, terms.p);
+  ++E.nlaunch, k_sq_terms<<<grid_for(nc), 256, 0, st>>>(nc, d.p, L.tw, terms.p);
   HL_LAUNCH_CHECK();
   double expected = dd_sum(E, terms.p, nc);
   return (intra - expected) / L.tw;
@@ -159,15 +159,15 @@ void canonicalize_device(Engine& E, u32* labels, u64 n, u32* out) {
   flag.ensure(E.mem, n);
   rank.ensure(E.mem, n);
   HL_CUDA(cudaMemsetAsync(first.p, 0xFF, sizeof(u32) * nc, st));
-  k_first_index<<<grid_for(n), 256, 0, st>>>(labels, n, first.p);
-  k_is_first<<<grid_for(n), 256, 0, st>>>(labels, n, first.p, flag.p);
+  ++E.nlaunch, k_first_index<<<grid_for(n), 256, 0, st>>>(labels, n, first.p);
+  ++E.nlaunch, k_is_first<<<grid_for(n), 256, 0, st>>>(labels, n, first.p, flag.p);
   HL_LAUNCH_CHECK();
   u32* a = flag.p;
   u32* r = rank.p;
   cub_run(E, [&](void* t, size_t& b) {
     return cub::DeviceScan::ExclusiveSum(t, b, a, r, (int64_t)n, st);
   });
-  k_apply_first<<<grid_for(n), 256, 0, st>>>(labels, n, first.p, rank.p, out);
+  ++E.nlaunch, k_apply_first<<<grid_for(n), 256, 0, st>>>(labels, n, first.p, rank.p, out);
   HL_LAUNCH_CHECK();
   E.sync();
 }

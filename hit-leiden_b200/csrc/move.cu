@@ -106,7 +106,7 @@ void recompute_comm_degrees(Engine& E, Level& L, const u32* part, u32 ncomm_cap,
   HL_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * (size_t)ncomm_cap, st));
   if (!n) return;
   if (E.integral) {
-    k_comm_deg_atomic<<<grid_for(n), 256, 0, st>>>(n, part, L.k.p, d);
+    ++E.nlaunch, k_comm_deg_atomic<<<grid_for(n), 256, 0, st>>>(n, part, L.k.p, d);
     HL_LAUNCH_CHECK();
     return;
   }
@@ -118,8 +118,8 @@ void recompute_comm_degrees(Engine& E, Level& L, const u32* part, u32 ncomm_cap,
   S.cand_node.ensure(E.mem, n);
   S.sel_node.ensure(E.mem, n);
   S.segid.ensure(E.mem, n);
-  k_iota<<<grid_for(n), 256, 0, st>>>(S.order.p, n);
-  k_copy_u32<<<grid_for(n), 256, 0, st>>>(part, S.used.p, n);
+  ++E.nlaunch, k_iota<<<grid_for(n), 256, 0, st>>>(S.order.p, n);
+  ++E.nlaunch, k_copy_u32<<<grid_for(n), 256, 0, st>>>(part, S.used.p, n);
   HL_LAUNCH_CHECK();
   u32* kin = S.used.p;
   u32* kout = S.rank.p;
@@ -128,7 +128,7 @@ void recompute_comm_degrees(Engine& E, Level& L, const u32* part, u32 ncomm_cap,
   cub_run(E, [&](void* t, size_t& b) {
     return cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int64_t)n, 0, 32, st);
   });
-  k_heads_u32<<<grid_for(n), 256, 0, st>>>(kout, n, S.cand_node.p);
+  ++E.nlaunch, k_heads_u32<<<grid_for(n), 256, 0, st>>>(kout, n, S.cand_node.p);
   HL_LAUNCH_CHECK();
   u32* h = S.cand_node.p;
   u32* sid = S.segid.p;
@@ -136,8 +136,8 @@ void recompute_comm_degrees(Engine& E, Level& L, const u32* part, u32 ncomm_cap,
     return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)n, st);
   });
   u32 nu = E.read_u32(sid + n - 1) + E.read_u32(h + n - 1);
-  k_seg_compact<<<grid_for(n), 256, 0, st>>>(h, sid, kout, n, S.used.p, S.sel_node.p);
-  k_comm_deg_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.used.p, S.sel_node.p, n, vout, L.k.p, d);
+  ++E.nlaunch, k_seg_compact<<<grid_for(n), 256, 0, st>>>(h, sid, kout, n, S.used.p, S.sel_node.p);
+  ++E.nlaunch, k_comm_deg_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.used.p, S.sel_node.p, n, vout, L.k.p, d);
   HL_LAUNCH_CHECK();
 }
 
@@ -163,7 +163,7 @@ u32 rank_compact(Engine& E, u32* labels, u32 n, u32 id_bound) {
   S.used.ensure(E.mem, len);
   S.rank.ensure(E.mem, len);
   HL_CUDA(cudaMemsetAsync(S.used.p, 0, sizeof(u32) * len, st));
-  k_mark_used<<<grid_for(n), 256, 0, st>>>(labels, n, S.used.p);
+  ++E.nlaunch, k_mark_used<<<grid_for(n), 256, 0, st>>>(labels, n, S.used.p);
   HL_LAUNCH_CHECK();
   u32* a = S.used.p;
   u32* r = S.rank.p;
@@ -171,7 +171,7 @@ u32 rank_compact(Engine& E, u32* labels, u32 n, u32 id_bound) {
     return cub::DeviceScan::ExclusiveSum(t, b, a, r, (int64_t)len, st);
   });
   u32 distinct = E.read_u32(r + id_bound + 1);
-  k_relabel<<<grid_for(n), 256, 0, st>>>(labels, n, S.rank.p);
+  ++E.nlaunch, k_relabel<<<grid_for(n), 256, 0, st>>>(labels, n, S.rank.p);
   HL_LAUNCH_CHECK();
   return distinct;
 }
@@ -219,7 +219,7 @@ struct EvalArgs {
   u32* tkey;
   u32* tpos;
   double* tval;
-  unsigned long long* traversed;
+  unsigned long long* traversed;  // [0] adjacency entries scanned, [1] candidates evaluated
 };
 
 constexpr u32 WARP_TAB = 512;  // entries per warp table in shared memory
@@ -269,12 +269,15 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_eval(EvalArgs A) {
   __shared__ u32 s_pos[WARPS_PER_BLOCK][WARP_TAB];
   __shared__ double s_val[WARPS_PER_BLOCK][WARP_TAB];
   __shared__ double s_w[WARPS_PER_BLOCK][32];
-  __shared__ unsigned long long s_trav;
+  __shared__ unsigned long long s_trav, s_cand;
   const u32 lane = threadIdx.x & 31;
   const u32 wib = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_trav = 0;
+  if (threadIdx.x == 0) {
+    s_trav = 0;
+    s_cand = 0;
+  }
   __syncthreads();
-  unsigned long long my_trav = 0;
+  unsigned long long my_trav = 0, my_cand = 0;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 i = warp; i < A.nv; i += nwarps) {
@@ -316,6 +319,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_eval(EvalArgs A) {
         if (!blk) {
           g = move_gain(sum, wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
           p = lane;
+          ++my_cand;
         }
       }
       u32 kk = key;
@@ -402,6 +406,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_eval(EvalArgs A) {
           if (key == NONE32 || key == cur) continue;
           if (KIND == EVAL_REFINE && A.blocked[key]) continue;
           double gn = move_gain(tv[t], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
+          ++my_cand;
           u32 pp = tp[t];
           if (p == NONE32 || gn > g || (gn == g && pp < p)) {
             g = gn;
@@ -436,8 +441,12 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_eval(EvalArgs A) {
   }
   if (A.traversed) {
     if (lane == 0 && my_trav) atomicAdd(&s_trav, my_trav);
+    if (my_cand) atomicAdd(&s_cand, my_cand);
     __syncthreads();
-    if (threadIdx.x == 0 && s_trav) atomicAdd(A.traversed, s_trav);
+    if (threadIdx.x == 0) {
+      if (s_trav) atomicAdd(&A.traversed[0], s_trav);
+      if (s_cand) atomicAdd(&A.traversed[1], s_cand);
+    }
   }
 }
 
@@ -462,7 +471,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   cudaStream_t st = E.stream;
   Scratch& S = E.sc;
   S.gkey.ensure(E.mem, (size_t)nv + 1);
-  k_big_caps<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.gkey.p);
+  ++E.nlaunch, k_big_caps<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.gkey.p);
   HL_CUDA(cudaMemsetAsync(S.gkey.p + nv, 0, sizeof(u64), st));
   HL_LAUNCH_CHECK();
   u64* a = S.gkey.p;
@@ -503,11 +512,13 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   A.tval = tv.p;
   A.traversed = traversed;
   u32 blocks = grid_for((u64)nv * 32, WARPS_PER_BLOCK * 32);
+  cudaEvent_t ev = E.kt_begin();
   if (kind == EVAL_MOVE)
-    k_eval<EVAL_MOVE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(A);
+    ++E.nlaunch, k_eval<EVAL_MOVE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(A);
   else
-    k_eval<EVAL_REFINE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(A);
+    ++E.nlaunch, k_eval<EVAL_REFINE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(A);
   HL_LAUNCH_CHECK();
+  E.kt_end(kind == EVAL_MOVE ? KT_MOVE_EVAL : KT_REFINE_EVAL, ev);
   if (total) {
     tk.release();
     tp.release();
@@ -707,6 +718,7 @@ void select_decoupled_dev(Engine& E, u32 M) {
   Scratch& S = E.sc;
   cudaStream_t st = E.stream;
   u32* cnt = S.cnt.p;
+  cudaEvent_t ev = E.kt_begin();
   HL_CUDA(cudaMemsetAsync(S.status.p, ST_UNDECIDED, M, st));
   u32 round = ++E.sel_round;
   if (round >= (1u << 29)) E.sel_round = round = 1;
@@ -715,9 +727,9 @@ void select_decoupled_dev(Engine& E, u32 M) {
     for (int rep = 0; rep < 4; ++rep) {
       u64 e = ++E.epoch;
       HL_CUDA(cudaMemsetAsync(cnt + 6, 0, sizeof(u32), st));
-      k_reserve<<<grid_for(M), 256, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.nmask.p,
+      ++E.nlaunch, k_reserve<<<grid_for(M), 256, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.nmask.p,
                                              S.role.p, (unsigned long long*)S.res.p, round, e);
-      k_decide<<<grid_for(M), 256, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.nmask.p,
+      ++E.nlaunch, k_decide<<<grid_for(M), 256, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.nmask.p,
                                             S.role.p, (const unsigned long long*)S.res.p, round, e,
                                             cnt + 6);
       HL_LAUNCH_CHECK();
@@ -726,12 +738,14 @@ void select_decoupled_dev(Engine& E, u32 M) {
     u32 left = E.read_u32(cnt + 6);
     if (!left) break;
     if (iters >= 64) {
-      k_select_tail<<<1, 32, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.role.p, round);
+      ++E.nlaunch, k_select_tail<<<1, 32, 0, st>>>(M, S.sel_from.p, S.sel_to.p, S.status.p, S.role.p, round);
       HL_LAUNCH_CHECK();
       break;
     }
   }
   E.stats_sel_iters += iters;
+  E.kt_end(KT_SELECT, ev);
+  E.kagg[KT_SELECT].bytes += (u64)M * 9 * iters;  // from/to/status/nmask per iteration
 }
 
 MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active,
@@ -749,7 +763,7 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   HL_CUDA(cudaMemsetAsync(S.affected.p, 0, n ? n : 1, st));
   if (!n) return out;
   if (delta.k)
-    k_seed<<<grid_for(delta.k), 256, 0, st>>>(delta.u, delta.v, delta.w, delta.k, L.f.p,
+    ++E.nlaunch, k_seed<<<grid_for(delta.k), 256, 0, st>>>(delta.u, delta.v, delta.w, delta.k, L.f.p,
                                                L.s_cur.p, S.active.p, S.affected.p);
   HL_LAUNCH_CHECK();
   // Community ids must stay below n so that n + v is a fresh empty community.
@@ -773,7 +787,8 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   S.gkey2.ensure(E.mem, n);
   S.cnt.ensure(E.mem, 16);
   S.red64.ensure(E.mem, 4);
-  HL_CUDA(cudaMemsetAsync(S.red64.p, 0, sizeof(u64), st));
+  HL_CUDA(cudaMemsetAsync(S.red64.p, 0, 2 * sizeof(u64), st));
+  u64 sum_nv = 0;
   u32* cnt = S.cnt.p;
 
   const u32 max_rounds = E.cfg.max_rounds ? E.cfg.max_rounds : 20;
@@ -786,11 +801,12 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     });
     u32 na = E.read_u32(cnt + 4);
     if (!na) break;
+    sum_nv += na;
     run_eval(E, EVAL_MOVE, S.act.p, na, L, L.s_cur.p, S.d.p, nullptr, true, S.cand_to.p,
              S.cand_gain.p, (unsigned long long*)S.red64.p);
     // Candidates with positive gain, still in ascending node order.
     u8* flag = S.status.p;
-    k_cand_flags<<<grid_for(na), 256, 0, st>>>(S.cand_gain.p, na, flag);
+    ++E.nlaunch, k_cand_flags<<<grid_for(na), 256, 0, st>>>(S.cand_gain.p, na, flag);
     HL_LAUNCH_CHECK();
     cub_run(E, [&](void* t, size_t& b) {
       return cub::DeviceSelect::Flagged(t, b, cub::CountingInputIterator<u32>(0), flag,
@@ -800,7 +816,7 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     out.candidates += M;
     ++it;
     if (!M) break;  // no positive candidate: nothing selected, frontier empties
-    k_gain_keys<<<grid_for(M), 256, 0, st>>>(S.cand_idx.p, M, S.cand_gain.p, S.gkey.p, S.order.p);
+    ++E.nlaunch, k_gain_keys<<<grid_for(M), 256, 0, st>>>(S.cand_idx.p, M, S.cand_gain.p, S.gkey.p, S.order.p);
     HL_LAUNCH_CHECK();
     {
       u64* ki = S.gkey.p;
@@ -811,12 +827,12 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
         return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)M, 0, 64, st);
       });
     }
-    k_gather_sel<<<grid_for(M), 256, 0, st>>>(S.order2.p, M, S.act.p, S.cand_to.p, L.f.p,
+    ++E.nlaunch, k_gather_sel<<<grid_for(M), 256, 0, st>>>(S.order2.p, M, S.act.p, S.cand_to.p, L.f.p,
                                               S.sel_node.p, S.sel_from.p, S.sel_to.p);
     HL_LAUNCH_CHECK();
     select_decoupled_dev(E, M);
     HL_CUDA(cudaMemsetAsync(cnt + 7, 0, sizeof(u32), st));
-    k_apply_moves<<<grid_for(M), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_from.p,
+    ++E.nlaunch, k_apply_moves<<<grid_for(M), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_from.p,
                                                S.sel_to.p, L.f.p, L.k.p, S.d.p, E.integral,
                                                S.changed.p, S.affected.p, mark_moved, cnt + 7);
     HL_LAUNCH_CHECK();
@@ -830,7 +846,7 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
       S.seg_start.ensure(E.mem, 2 * (size_t)M);
       S.idx.ensure(E.mem, 2 * (size_t)M);
       S.idx2.ensure(E.mem, 2 * (size_t)M);
-      k_dops<<<grid_for(M), 256, 0, st>>>(M, S.status.p, S.sel_from.p, S.sel_to.p, S.used.p,
+      ++E.nlaunch, k_dops<<<grid_for(M), 256, 0, st>>>(M, S.status.p, S.sel_from.p, S.sel_to.p, S.used.p,
                                           S.idx.p);
       HL_LAUNCH_CHECK();
       u32 M2 = 2 * M;
@@ -841,7 +857,7 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
       cub_run(E, [&](void* t, size_t& b) {
         return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)M2, 0, 32, st);
       });
-      k_heads_u32<<<grid_for(M2), 256, 0, st>>>(ko, M2, S.cand_node.p);
+      ++E.nlaunch, k_heads_u32<<<grid_for(M2), 256, 0, st>>>(ko, M2, S.cand_node.p);
       HL_LAUNCH_CHECK();
       u32* h = S.cand_node.p;
       u32* sid = S.segid.p;
@@ -849,8 +865,8 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
         return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)M2, st);
       });
       u32 nu = E.read_u32(sid + M2 - 1) + E.read_u32(h + M2 - 1);
-      k_seg_compact<<<grid_for(M2), 256, 0, st>>>(h, sid, ko, M2, S.rowlist.p, S.seg_start.p);
-      k_apply_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, M2, vo,
+      ++E.nlaunch, k_seg_compact<<<grid_for(M2), 256, 0, st>>>(h, sid, ko, M2, S.rowlist.p, S.seg_start.p);
+      ++E.nlaunch, k_apply_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, M2, vo,
                                                     S.sel_node.p, L.k.p, S.d.p);
       HL_LAUNCH_CHECK();
     }
@@ -858,7 +874,7 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     out.moves += acc;
     if (!acc) break;
     HL_CUDA(cudaMemsetAsync(S.next.p, 0, n, st));
-    k_mark_next<<<grid_for((u64)M * 32), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_to.p,
+    ++E.nlaunch, k_mark_next<<<grid_for((u64)M * 32), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_to.p,
                                                         L.g.off.p, L.g.col.p, L.f.p, L.s_cur.p,
                                                         S.next.p, S.affected.p);
     HL_LAUNCH_CHECK();
@@ -866,6 +882,11 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   }
   out.iterations = it;
   out.traversed = E.read_u64(S.red64.p);
+  // Algorithmic bytes of the evaluation kernel: per active vertex its list
+  // entry, offsets, f, k, d(f) and outputs; per adjacency entry the neighbour,
+  // weight and neighbour community; per evaluated candidate its d(C).
+  u64 ncand = E.read_u64(S.red64.p + 1);
+  E.kagg[KT_MOVE_EVAL].bytes += 52ull * sum_nv + 16ull * out.traversed + 8ull * ncand;
   return out;
 }
 

@@ -291,22 +291,22 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   const size_t scap = (size_t)smax + 2 + n;
   S.affsc.ensure(E.mem, scap);
   HL_CUDA(cudaMemsetAsync(S.affsc.p, 0, scap, st));
-  k_mark_affected_sc<<<grid_for(n), 256, 0, st>>>(S.affected.p, s, n, S.affsc.p);
+  ++E.nlaunch, k_mark_affected_sc<<<grid_for(n), 256, 0, st>>>(S.affected.p, s, n, S.affsc.p);
   S.par.ensure(E.mem, n);
   S.csize.ensure(E.mem, n);
-  k_iota<<<grid_for(n), 256, 0, st>>>(S.par.p, n);
+  ++E.nlaunch, k_iota<<<grid_for(n), 256, 0, st>>>(S.par.p, n);
   HL_CUDA(cudaMemsetAsync(S.csize.p, 0, sizeof(u32) * n, st));
-  k_uf_edges<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, s, L.f.p, S.affsc.p,
+  ++E.nlaunch, k_uf_edges<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, s, L.f.p, S.affsc.p,
                                                      cc_same_community, S.par.p);
-  k_uf_final<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.csize.p);
+  ++E.nlaunch, k_uf_final<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.csize.p);
   S.keep.ensure(E.mem, scap);
   HL_CUDA(cudaMemsetAsync(S.keep.p, 0, sizeof(u64) * scap, st));
-  k_keep<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.csize.p,
+  ++E.nlaunch, k_keep<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.csize.p,
                                       (unsigned long long*)S.keep.p);
   S.status.ensure(E.mem, n);
   S.gkey.ensure(E.mem, n);
   S.gkey2.ensure(E.mem, n);
-  k_split_roots<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p,
+  ++E.nlaunch, k_split_roots<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p,
                                               (const unsigned long long*)S.keep.p, S.status.p,
                                               S.gkey.p);
   HL_LAUNCH_CHECK();
@@ -318,16 +318,16 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
     S.keys2.ensure(E.mem, m_new);
     S.used.ensure(E.mem, m_new);
     S.rank.ensure(E.mem, m_new);
-    k_gather_keys<<<grid_for(m_new), 256, 0, st>>>(S.act.p, m_new, S.gkey.p, S.keys.p);
+    ++E.nlaunch, k_gather_keys<<<grid_for(m_new), 256, 0, st>>>(S.act.p, m_new, S.gkey.p, S.keys.p);
     HL_LAUNCH_CHECK();
     u64* ki = S.keys.p;
     u64* ko = S.keys2.p;
     cub_run(E, [&](void* t, size_t& b) {
       return cub::DeviceRadixSort::SortKeys(t, b, ki, ko, (int64_t)m_new, 0, 64, st);
     });
-    k_assign_newid<<<grid_for(m_new), 256, 0, st>>>(ko, m_new, smax + 1, S.newid.p, S.used.p,
+    ++E.nlaunch, k_assign_newid<<<grid_for(m_new), 256, 0, st>>>(ko, m_new, smax + 1, S.newid.p, S.used.p,
                                                      S.rank.p);
-    k_apply_split<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.status.p, S.newid.p,
+    ++E.nlaunch, k_apply_split<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.status.p, S.newid.p,
                                                S.refined.p);
     HL_LAUNCH_CHECK();
     std::vector<u32> a(m_new), b(m_new);
@@ -341,7 +341,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
 
   // is_initial (hit_leiden.rs:1333-1339): s is the identity ⇒ R = all.
   HL_CUDA(cudaMemsetAsync(cnt + 5, 0, sizeof(u32), st));
-  k_not_identity<<<grid_for(n), 256, 0, st>>>(n, s, cnt + 5);
+  ++E.nlaunch, k_not_identity<<<grid_for(n), 256, 0, st>>>(n, s, cnt + 5);
   HL_LAUNCH_CHECK();
   if (E.read_u32(cnt + 5) == 0) HL_CUDA(cudaMemsetAsync(S.refined.p, 1, n, st));
 
@@ -350,7 +350,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   const size_t s2cap = (size_t)smax2 + 1;
   S.sizes.ensure(E.mem, s2cap);
   HL_CUDA(cudaMemsetAsync(S.sizes.p, 0, sizeof(u32) * s2cap, st));
-  k_sizes<<<grid_for(n), 256, 0, st>>>(n, s, S.sizes.p);
+  ++E.nlaunch, k_sizes<<<grid_for(n), 256, 0, st>>>(n, s, S.sizes.p);
   HL_LAUNCH_CHECK();
   S.dS.ensure(E.mem, s2cap);
   recompute_comm_degrees(E, L, s, (u32)s2cap, S.dS.p);
@@ -363,7 +363,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   out.refined = nr;
   if (!nr) return out;
   S.nmask.ensure(E.mem, nr);
-  k_singletons<<<grid_for(nr), 256, 0, st>>>(S.act.p, nr, s, S.sizes.p, S.nmask.p);
+  ++E.nlaunch, k_singletons<<<grid_for(nr), 256, 0, st>>>(S.act.p, nr, s, S.sizes.p, S.nmask.p);
   HL_LAUNCH_CHECK();
   S.cand_idx.ensure(E.mem, nr);
   u32 ns = 0;
@@ -385,18 +385,18 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   HL_CUDA(cudaMemsetAsync(S.cand_sc.p, 0, s2cap, st));
   HL_CUDA(cudaMemsetAsync(S.minmem.p, 0xFF, sizeof(u32) * s2cap, st));
   HL_CUDA(cudaMemsetAsync(S.wsp.p, 0, sizeof(double) * s2cap, st));
-  k_t_candidates<<<grid_for((u64)ns * 32), 256, 0, st>>>(single, ns, L.g.off.p, L.g.col.p, L.f.p,
+  ++E.nlaunch, k_t_candidates<<<grid_for((u64)ns * 32), 256, 0, st>>>(single, ns, L.g.off.p, L.g.col.p, L.f.p,
                                                          s, S.cand_sc.p);
-  k_min_member<<<grid_for(n), 256, 0, st>>>(n, s, S.cand_sc.p, S.minmem.p);
+  ++E.nlaunch, k_min_member<<<grid_for(n), 256, 0, st>>>(n, s, S.cand_sc.p, S.minmem.p);
   HL_LAUNCH_CHECK();
   if (E.integral) {
-    k_wsp_atomic<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, L.f.p, s,
+    ++E.nlaunch, k_wsp_atomic<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, L.f.p, s,
                                                          S.cand_sc.p, S.minmem.p, S.wsp.p);
     HL_LAUNCH_CHECK();
   } else {
     // Members of candidate sub-communities, sorted by (S, v).
     S.next.ensure(E.mem, n);
-    k_member_keys<<<grid_for(n), 256, 0, st>>>(n, s, S.cand_sc.p, S.next.p);
+    ++E.nlaunch, k_member_keys<<<grid_for(n), 256, 0, st>>>(n, s, S.cand_sc.p, S.next.p);
     HL_LAUNCH_CHECK();
     S.order.ensure(E.mem, n);
     u32 nm = select_flagged(E, S.next.p, n, S.order.p, cnt + 8);
@@ -408,7 +408,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
       S.rowlist.ensure(E.mem, nm);
       S.seg_start.ensure(E.mem, nm);
       S.sel_node.ensure(E.mem, nm);
-      k_gather_s<<<grid_for(nm), 256, 0, st>>>(S.order.p, nm, s, S.used.p);
+      ++E.nlaunch, k_gather_s<<<grid_for(nm), 256, 0, st>>>(S.order.p, nm, s, S.used.p);
       HL_LAUNCH_CHECK();
       u32* ki = S.used.p;
       u32* ko = S.rank.p;
@@ -417,7 +417,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
       cub_run(E, [&](void* t, size_t& b) {
         return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)nm, 0, 32, st);
       });
-      k_heads_u32b<<<grid_for(nm), 256, 0, st>>>(ko, nm, S.sel_node.p);
+      ++E.nlaunch, k_heads_u32b<<<grid_for(nm), 256, 0, st>>>(ko, nm, S.sel_node.p);
       HL_LAUNCH_CHECK();
       u32* h = S.sel_node.p;
       u32* sid = S.segid.p;
@@ -425,14 +425,14 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
         return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)nm, st);
       });
       u32 nu = E.read_u32(sid + nm - 1) + E.read_u32(h + nm - 1);
-      k_seg_compact_b<<<grid_for(nm), 256, 0, st>>>(h, sid, ko, nm, S.rowlist.p, S.seg_start.p);
-      k_wsp_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, nm, vo,
+      ++E.nlaunch, k_seg_compact_b<<<grid_for(nm), 256, 0, st>>>(h, sid, ko, nm, S.rowlist.p, S.seg_start.p);
+      ++E.nlaunch, k_wsp_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, nm, vo,
                                                   L.g.off.p, L.g.col.p, L.g.w.p, L.f.p,
                                                   S.minmem.p, S.wsp.p);
       HL_LAUNCH_CHECK();
     }
   }
-  k_blocked<<<grid_for(s2cap), 256, 0, st>>>((u32)s2cap, S.cand_sc.p, S.dS.p, S.wsp.p, S.minmem.p,
+  ++E.nlaunch, k_blocked<<<grid_for(s2cap), 256, 0, st>>>((u32)s2cap, S.cand_sc.p, S.dS.p, S.wsp.p, S.minmem.p,
                                              L.f.p, S.dcomm.p, L.tw, E.cfg.resolution,
                                              S.blocked.p);
   HL_LAUNCH_CHECK();
@@ -443,7 +443,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   run_eval(E, 1, single, ns, L, s, S.dS.p, S.blocked.p, false, S.cand_to.p, S.cand_gain.p,
            nullptr);
   HL_CUDA(cudaMemsetAsync(cnt + 9, 0, sizeof(u32), st));
-  k_apply_merges<<<grid_for(ns), 256, 0, st>>>(single, ns, S.cand_to.p, S.cand_gain.p, s,
+  ++E.nlaunch, k_apply_merges<<<grid_for(ns), 256, 0, st>>>(single, ns, S.cand_to.p, S.cand_gain.p, s,
                                                cnt + 9);
   HL_LAUNCH_CHECK();
   out.merges = E.read_u32(cnt + 9);

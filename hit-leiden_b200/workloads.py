@@ -135,7 +135,7 @@ def planted(n, mean_degree, mu, seed, degree_exp=2.5, max_degree=None, comm_exp=
 def config1(seed=0):
     """n=9,877, ~21.8k unit edges, ~480 communities (sizes 2-400, exp 1.5),
     mu=0.15, power-law degrees (exp 2.5, mean 4.4), triangle closure."""
-    n, s, d, w, comm = planted(9877, 4.9, 0.15, seed, degree_exp=2.5, max_degree=65,
+    n, s, d, w, comm = planted(9877, 5.3, 0.15, seed, degree_exp=2.5, max_degree=65,
                                comm_exp=1.5, comm_min=2, comm_max=400, triangle_frac=0.35)
     return n, s, d, w
 
@@ -143,7 +143,7 @@ def config1(seed=0):
 def config2(seed=0, n=1_000_000, mean_degree=40.0):
     """LFR-style 1M vertices / ~20M edges, degree exp 2.5 (mean 40, max 2000),
     community sizes exp 1.5 in [50, 5000], mu=0.3, f64 weights U[0.5, 2.0]."""
-    n, s, d, w, comm = planted(n, mean_degree * 1.02, 0.3, seed, degree_exp=2.5, max_degree=2000,
+    n, s, d, w, comm = planted(n, mean_degree * 1.13, 0.3, seed, degree_exp=2.5, max_degree=2000,
                                comm_exp=1.5, comm_min=50, comm_max=5000, weights=(0.5, 2.0))
     return n, s, d, w
 
@@ -207,18 +207,22 @@ class EdgeStore:
                 self.removed.add(key)
 
     def random_existing(self, rng, k):
+        """k distinct edges of the base edge set that are still present, drawn
+        uniformly, with their current weights."""
         out = []
+        chosen = set()
         while len(out) < k:
-            i = int(rng.integers(0, len(self.key) + len(self.extra)))
-            if i < len(self.key):
+            idx = rng.integers(0, len(self.key), size=2 * (k - len(out)) + 8)
+            for i in idx.tolist():
                 key = int(self.key[i])
-            else:
-                key = list(self.extra.keys())[i - len(self.key)]
-            a, b = divmod(key, self.n)
-            w = self.weight(a, b)
-            if w is None or (a, b) in [(x[0], x[1]) for x in out]:
-                continue
-            out.append((a, b, w))
+                if key in chosen or key in self.removed:
+                    continue
+                w = self.extra.get(key, float(self.w[i]))
+                a, b = divmod(key, self.n)
+                out.append((a, b, w))
+                chosen.add(key)
+                if len(out) == k:
+                    break
         return out
 
 

@@ -79,6 +79,9 @@ typedef struct {
 /* Compute the level-0 modularity after every batch into hl_batch_stats
  * (an extra pass over the graph; off by default). */
 #define HL_FLAG_BATCH_MODULARITY (1u << 1)
+/* Time the main kernels with CUDA events on the handle's stream and count
+ * their algorithmic bytes (read with hl_kernel_stats). */
+#define HL_FLAG_KERNEL_TIMING (1u << 2)
 
 typedef struct {
   uint32_t iterations;   /* movement rounds summed over levels (hit_leiden return) */
@@ -93,7 +96,16 @@ typedef struct {
   uint64_t edges;        /* undirected edges in G^1 after the batch                */
   double modularity;     /* Q of the level-0 community partition after the batch   */
   double device_ms;      /* device time of the call (CUDA events)                  */
+  uint64_t launches;     /* kernels of this library launched by the call           */
 } hl_batch_stats;
+
+/* Accumulated per-kernel device time and algorithmic bytes. */
+typedef struct {
+  char name[32];
+  uint64_t launches;
+  double total_ms;
+  uint64_t bytes;
+} hl_kernel_stat;
 
 typedef struct hl_graph hl_graph;
 
@@ -121,6 +133,13 @@ HL_API hl_status hl_apply_batch(hl_graph* g, const uint32_t* src, const uint32_t
 /* Same with device pointers (on the handle's device). */
 HL_API hl_status hl_apply_batch_device(hl_graph* g, const uint32_t* d_src, const uint32_t* d_dst,
                                 const double* d_w, uint64_t k, hl_batch_stats* stats);
+
+/* Per-kernel statistics since creation or the last reset (needs
+ * HL_FLAG_KERNEL_TIMING; otherwise launches stay 0).  *count receives the
+ * number of entries; at most cap are written. */
+HL_API hl_status hl_kernel_stats(const hl_graph* g, hl_kernel_stat* out, uint32_t cap,
+                                 uint32_t* count);
+HL_API hl_status hl_reset_kernel_stats(hl_graph* g);
 
 /* Change gamma for subsequent batches (hit_leiden takes it per call,
  * hit_leiden.rs:939). */

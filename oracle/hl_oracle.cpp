@@ -114,29 +114,84 @@ static Graph graph_from_edges(u32 n, const std::vector<Edge>& edges) {
 // existing self-loop is dropped; self-loops carried by the delta survive.
 static Graph apply_delta(const Graph& g, u32 delta_n, const std::vector<Edge>& delta,
                          bool keep_self_loops) {
-  std::map<std::pair<u32, u32>, double> edge_map;
+  // Existing canonical edges, already in ascending (u, v) order because rows
+  // are sorted and scanned in node order; a repeated key keeps the last
+  // weight, as HashMap::insert does.
+  struct KW {
+    u64 key;
+    double w;
+  };
+  std::vector<KW> ex;
+  ex.reserve(g.col.size() / 2 + 1);
   for (u32 v = 0; v < g.n; ++v) {
     for (u64 p = g.off[v]; p < g.off[v + 1]; ++p) {
       u32 nb = g.col[p];
-      if (v < nb || (keep_self_loops && v == nb)) edge_map[{v, nb}] = g.w[p];  // insert: last wins
+      if (v < nb || (keep_self_loops && v == nb)) {
+        u64 key = ((u64)v << 32) | nb;
+        if (!ex.empty() && ex.back().key == key)
+          ex.back().w = g.w[p];
+        else
+          ex.push_back({key, g.w[p]});
+      }
     }
   }
-  for (const Edge& e : delta) {
-    std::pair<u32, u32> key = e.u <= e.v ? std::make_pair(e.u, e.v) : std::make_pair(e.v, e.u);
-    auto it = edge_map.find(key);
-    if (it == edge_map.end()) {
-      edge_map.emplace(key, 0.0 + e.w);
+  // Delta keys in batch order, stably sorted by key.
+  std::vector<std::pair<u64, u64>> dk(delta.size());
+  for (size_t i = 0; i < delta.size(); ++i) {
+    u32 a = std::min(delta[i].u, delta[i].v), b = std::max(delta[i].u, delta[i].v);
+    dk[i] = {((u64)a << 32) | b, (u64)i};
+  }
+  std::stable_sort(dk.begin(), dk.end(),
+                   [](const std::pair<u64, u64>& x, const std::pair<u64, u64>& y) {
+                     return x.first < y.first;
+                   });
+  std::vector<Edge> edges;
+  edges.reserve(ex.size() + dk.size());
+  size_t i = 0, j = 0;
+  while (i < ex.size() || j < dk.size()) {
+    u64 key;
+    double x;
+    if (j >= dk.size() || (i < ex.size() && ex[i].key < dk[j].first)) {
+      key = ex[i].key;
+      x = ex[i].w;
+      ++i;
     } else {
-      it->second += e.w;
+      key = dk[j].first;
+      x = 0.0;
+      if (i < ex.size() && ex[i].key == key) {
+        x = ex[i].w;
+        ++i;
+      }
+      while (j < dk.size() && dk[j].first == key) {
+        x += delta[dk[j].second].w;  // existing weight first, then batch order
+        ++j;
+      }
     }
+    if (x > 1e-12) edges.push_back({(u32)(key >> 32), (u32)key, x});
   }
   u32 n = std::max(g.n, delta_n);
-  std::vector<Edge> edges;
-  edges.reserve(edge_map.size());
-  for (const auto& kv : edge_map) {
-    if (kv.second > 1e-12) edges.push_back({kv.first.first, kv.first.second, kv.second});
-  }
   return graph_from_edges(n, edges);
+}
+
+// Sum records per (min, max) key in push order; ascending key output.
+static std::vector<Edge> compress_sum(const std::vector<Edge>& recs, double threshold) {
+  std::vector<std::pair<u64, u64>> idx(recs.size());
+  for (size_t i = 0; i < recs.size(); ++i) {
+    u32 a = std::min(recs[i].u, recs[i].v), b = std::max(recs[i].u, recs[i].v);
+    idx[i] = {((u64)a << 32) | b, (u64)i};
+  }
+  std::stable_sort(idx.begin(), idx.end(),
+                   [](const std::pair<u64, u64>& x, const std::pair<u64, u64>& y) {
+                     return x.first < y.first;
+                   });
+  std::vector<Edge> out;
+  for (size_t t = 0; t < idx.size();) {
+    u64 key = idx[t].first;
+    double x = 0.0;
+    while (t < idx.size() && idx[t].first == key) x += recs[idx[t++].second].w;
+    if (std::fabs(x) > threshold) out.push_back({(u32)(key >> 32), (u32)key, x});
+  }
+  return out;
 }
 
 // Per-vertex weighted degree: left-to-right sum over the row in CSR order
@@ -201,19 +256,29 @@ static double modularity_edges(u32 n, const std::vector<Edge>& edges, const u32*
 
 // Same quantity on the resident CSR (each edge appears twice there, a
 // self-loop twice in its row): intra and degrees agree with the edge-list form.
+// The per-community totals are the reference's node-order sums; the two outer
+// sums are accumulated in long double (the reference adds them in hash order,
+// so only their accurately rounded value is order-free).
 static double modularity_csr(const Graph& g, const u32* part) {
   std::vector<double> k = node_degrees(g);
   double tw = twice_total_weight(k);
   if (tw == 0.0) return 0.0;
-  double intra = 0.0;
+  long double intra = 0.0L;
   for (u32 v = 0; v < g.n; ++v)
     for (u64 p = g.off[v]; p < g.off[v + 1]; ++p)
       if (part[v] == part[g.col[p]]) intra += g.w[p];
-  std::map<u32, double> cds;
-  for (u32 i = 0; i < g.n; ++i) cds[part[i]] += k[i];
-  double expected = 0.0;
-  for (const auto& kv : cds) expected += kv.second * kv.second / tw;
-  return (intra - expected) / tw;
+  u32 mx = 0;
+  for (u32 i = 0; i < g.n; ++i) mx = std::max(mx, part[i]);
+  std::vector<double> cds((size_t)mx + 1, 0.0);
+  std::vector<uint8_t> seen((size_t)mx + 1, 0);
+  for (u32 i = 0; i < g.n; ++i) {
+    cds[part[i]] += k[i];
+    seen[part[i]] = 1;
+  }
+  long double expected = 0.0L;
+  for (size_t c = 0; c < cds.size(); ++c)
+    if (seen[c]) expected += (long double)(cds[c] * cds[c] / tw);
+  return (double)((intra - expected) / (long double)tw);
 }
 
 // hit_leiden.rs:358-376: first-seen contiguous relabel.
@@ -561,15 +626,22 @@ static std::vector<uint8_t> compute_blocked(const Graph& g, const std::vector<u3
       }
     }
   }
-  std::map<u32, double> dcomm;
-  for (u32 i = 0; i < n; ++i) dcomm[f[i]] += k[i];
   std::vector<uint8_t> blocked(dS.size(), 0);
   if (cand_list.empty()) return blocked;
+  u32 fmax = 0;
+  for (u32 i = 0; i < n; ++i) fmax = std::max(fmax, f[i]);
+  std::vector<double> dcomm((size_t)fmax + 1, 0.0);
+  for (u32 i = 0; i < n; ++i) dcomm[f[i]] += k[i];
   // Members of every candidate, ascending.
-  std::unordered_map<u32, std::vector<u32>> members;
+  std::vector<u32> mstart(dS.size() + 1, 0), mlist;
   if (!faithful) {
     for (u32 i = 0; i < n; ++i)
-      if (cand[s[i]]) members[s[i]].push_back(i);
+      if (cand[s[i]]) mstart[s[i] + 1] += 1;
+    for (size_t c = 0; c < dS.size(); ++c) mstart[c + 1] += mstart[c];
+    mlist.assign(mstart.back(), 0);
+    std::vector<u32> fill(mstart.begin(), mstart.end() - 1);
+    for (u32 i = 0; i < n; ++i)
+      if (cand[s[i]]) mlist[fill[s[i]]++] = i;
   }
   std::sort(cand_list.begin(), cand_list.end());
   for (u32 S : cand_list) {
@@ -580,10 +652,10 @@ static std::vector<uint8_t> compute_blocked(const Graph& g, const std::vector<u3
       for (u32 i = 0; i < n; ++i)
         if (s[i] == S) mem.push_back(i);
     } else {
-      mem = members[S];
+      mem.assign(mlist.begin() + mstart[S], mlist.begin() + mstart[S + 1]);
     }
     u32 parent = mem.empty() ? 0 : f[mem[0]];
-    double dpar = dcomm.count(parent) ? dcomm[parent] : 0.0;
+    double dpar = parent < dcomm.size() ? dcomm[parent] : 0.0;
     double wsp = 0.0;
     for (u32 i : mem)
       for (u64 p = g.off[i]; p < g.off[i + 1]; ++p)
@@ -667,14 +739,26 @@ static RefineOut inc_refinement(const Graph& g, const std::vector<u32>& f, std::
   RefineOut out;
   out.refined.assign(n, 0);
   // Affected sub-communities and their members (ascending).
-  std::set<u32> aff;
-  for (u32 v = 0; v < n; ++v)
-    if (affected[v]) aff.insert(s[v]);
-  std::map<u32, std::vector<u32>> nodes;
-  for (u32 i = 0; i < n; ++i)
-    if (aff.count(s[i])) nodes[s[i]].push_back(i);
   u32 mx = 0;
   for (u32 x : s) mx = std::max(mx, x);
+  std::vector<uint8_t> aff((size_t)mx + 1, 0);
+  for (u32 v = 0; v < n; ++v)
+    if (affected[v]) aff[s[v]] = 1;
+  // Members of each affected sub-community, ascending, grouped by id.
+  std::vector<std::pair<u32, u32>> mem;
+  for (u32 i = 0; i < n; ++i)
+    if (aff[s[i]]) mem.push_back({s[i], i});
+  std::stable_sort(mem.begin(), mem.end(),
+                   [](const std::pair<u32, u32>& a, const std::pair<u32, u32>& b) {
+                     return a.first < b.first;
+                   });
+  std::vector<std::pair<u32, std::vector<u32>>> nodes;
+  for (size_t t = 0; t < mem.size();) {
+    u32 S = mem[t].first;
+    std::vector<u32> vs;
+    while (t < mem.size() && mem[t].first == S) vs.push_back(mem[t++].second);
+    nodes.push_back({S, std::move(vs)});
+  }
   u64 next_id = n ? (u64)mx + 1 : 1;
   std::vector<uint8_t> visited(n, 0);
   for (auto& kv : nodes) {
@@ -834,18 +918,7 @@ static std::vector<Edge> inc_aggregation(const Graph& g, const std::vector<Edge>
   s_pre_next = s_pre;
   for (u32 v = 0; v < g.n; ++v)
     if (refined[v]) s_pre_next[v] = s_cur[v];
-  std::map<std::pair<u32, u32>, double> comp;
-  for (const Edge& e : dh) {
-    std::pair<u32, u32> key = e.u <= e.v ? std::make_pair(e.u, e.v) : std::make_pair(e.v, e.u);
-    auto it = comp.find(key);
-    if (it == comp.end())
-      comp.emplace(key, 0.0 + e.w);
-    else
-      it->second += e.w;
-  }
-  std::vector<Edge> out;
-  for (const auto& kv : comp)
-    if (std::fabs(kv.second) > 1e-9) out.push_back({kv.first.first, kv.first.second, kv.second});
+  std::vector<Edge> out = compress_sum(dh, 1e-9);
   u32 mx = 0;
   for (u32 x : s_cur) mx = std::max(mx, x);
   for (u32 x : s_pre) mx = std::max(mx, x);
@@ -1111,24 +1184,16 @@ static void bootstrap_ml(State& st, u32 n, const std::vector<Edge>& edges, doubl
     u32 nn = (u32)ids.size();
     if (p + 1 >= max_levels || nn <= 1 || (u64)nn * 100 >= (u64)np * 99) break;
     // Aggregate G^p by s^p (intra edges become self-loops of weight w).
-    std::vector<Edge> agg;
-    std::map<std::pair<u32, u32>, double> em;
+    std::vector<Edge> recs;
     for (u32 v = 0; v < np; ++v)
       for (u64 q = G.off[v]; q < G.off[v + 1]; ++q) {
         u32 nb = G.col[q];
         if (nb < v) continue;
-        double w = G.w[q];
-        if (nb == v) {
-          // a self-loop appears twice in its row; count it once
-          if (q + 1 < G.off[v + 1] && G.col[q + 1] == v) continue;
-        }
-        u32 a = s[v], b = s[nb];
-        std::pair<u32, u32> key = a <= b ? std::make_pair(a, b) : std::make_pair(b, a);
-        auto it = em.find(key);
-        if (it == em.end()) em.emplace(key, 0.0 + w);
-        else it->second += w;
+        // a self-loop appears twice in its row; count it once
+        if (nb == v && q + 1 < G.off[v + 1] && G.col[q + 1] == v) continue;
+        recs.push_back({s[v], s[nb], G.w[q]});
       }
-    for (auto& kv : em) agg.push_back({kv.first.first, kv.first.second, kv.second});
+    std::vector<Edge> agg = compress_sum(recs, -1.0);
     Graph gn;
     gn.n = nn;
     gn.off.assign((size_t)nn + 1, 0);
@@ -1696,6 +1761,37 @@ int or_hit_leiden(or_state* S, uint32_t delta_n, const uint32_t* src, const uint
 }
 
 uint32_t or_state_levels(const or_state* S) { return S->st.levels; }
+
+// Replace the state by `levels` levels imported level by level (used to start
+// the CPU baseline from an already bootstrapped state).
+void or_state_import_begin(or_state* S, uint32_t levels, uint32_t flags) {
+  S->st = State();
+  S->st.levels = levels;
+  S->st.sg.resize(levels);
+  S->st.f.resize(levels);
+  S->st.g.resize(levels);
+  S->st.s_pre.resize(levels);
+  S->st.s_cur.resize(levels);
+  S->flags = flags;
+}
+
+int or_state_import_level(or_state* S, uint32_t level, uint32_t n, const uint64_t* off,
+                          const uint32_t* col, const double* w, const uint32_t* f,
+                          const uint32_t* g, const uint32_t* s_pre, const uint32_t* s_cur) {
+  State& st = S->st;
+  if (level >= st.levels) return -1;
+  Graph& G = st.sg[level];
+  G.n = n;
+  G.off.assign(off, off + (size_t)n + 1);
+  G.col.assign(col, col + off[n]);
+  G.w.assign(w, w + off[n]);
+  st.f[level].assign(f, f + n);
+  st.g[level].assign(g, g + n);
+  st.s_pre[level].assign(s_pre, s_pre + n);
+  st.s_cur[level].assign(s_cur, s_cur + n);
+  if (level == 0) st.node_to_comm = st.g[0];
+  return 0;
+}
 
 int or_state_bootstrap(or_state* S, uint32_t n, const uint32_t* src, const uint32_t* dst,
                        const double* w, uint64_t m, uint32_t max_levels, or_stats* stats) {

@@ -77,6 +77,10 @@ void or_state_push_empty_graph(or_state* s, uint32_t n);
 int or_hit_leiden(or_state* s, uint32_t delta_n, const uint32_t* src, const uint32_t* dst,
                   const double* w, uint64_t k, or_stats* stats);
 uint32_t or_state_levels(const or_state* s);
+void or_state_import_begin(or_state* s, uint32_t levels, uint32_t flags);
+int or_state_import_level(or_state* s, uint32_t level, uint32_t n, const uint64_t* off,
+                          const uint32_t* col, const double* w, const uint32_t* f,
+                          const uint32_t* g, const uint32_t* s_pre, const uint32_t* s_cur);
 int or_state_bootstrap(or_state* s, uint32_t n, const uint32_t* src, const uint32_t* dst,
                        const double* w, uint64_t m, uint32_t max_levels, or_stats* stats);
 uint32_t or_state_level_nodes(const or_state* s, uint32_t level, int which);

@@ -103,6 +103,10 @@ def load():
         lib.or_state_bootstrap.restype = C.c_int
         lib.or_state_bootstrap.argtypes = [vp, C.c_uint32, u32p, u32p, vp, C.c_uint64, C.c_uint32,
                                            C.POINTER(Stats)]
+        lib.or_state_import_begin.argtypes = [vp, C.c_uint32, C.c_uint32]
+        lib.or_state_import_level.restype = C.c_int
+        lib.or_state_import_level.argtypes = [vp, C.c_uint32, C.c_uint32, u64p, u32p, f64p, u32p,
+                                              u32p, u32p, u32p]
         lib.or_state_levels.restype = C.c_uint32
         lib.or_state_levels.argtypes = [vp]
         lib.or_state_level_nodes.restype = C.c_uint32
@@ -321,6 +325,17 @@ class State:
     @property
     def levels(self):
         return self.lib.or_state_levels(self.h)
+
+    def import_levels(self, levels, flags=None):
+        """levels: list of dicts with off, col, w, f, g, s_pre, s_cur arrays."""
+        fl = (FLAG_MULTILEVEL if len(levels) > 1 else 0) if flags is None else flags
+        self.lib.or_state_import_begin(self.h, len(levels), fl)
+        for p, lv in enumerate(levels):
+            n = len(lv["f"])
+            a = [np.ascontiguousarray(lv[k], dt) for k, dt in
+                 (("off", np.uint64), ("col", np.uint32), ("w", np.float64), ("f", np.uint32),
+                  ("g", np.uint32), ("s_pre", np.uint32), ("s_cur", np.uint32))]
+            self.lib.or_state_import_level(self.h, p, n, *a)
 
     def get_map(self, level, which):
         n = self.lib.or_state_level_nodes(self.h, level, which)
