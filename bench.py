@@ -311,11 +311,13 @@ def main():
     dev_ms = []
     launches = 0
     stats = L.BatchStats()
+    torch.cuda.nvtx.range_push("hl_timed")
     for (du, dv, dw) in dev:
         L.check(L.lib.hl_apply_batch_device(h, C.c_void_p(du.data_ptr()), C.c_void_p(dv.data_ptr()),
                                             C.c_void_p(dw.data_ptr()), k, C.byref(stats)))
         dev_ms.append(stats.device_ms)
         launches += stats.launches
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()

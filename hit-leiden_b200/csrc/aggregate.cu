@@ -28,28 +28,6 @@ __device__ __forceinline__ bool agg_emit(u32 v, u32 nb, const u8* refined, const
   return changed_only && !refined[nb];
 }
 
-__global__ void k_agg_count(u32 n, const u64* off, const u32* col, const double* w,
-                            const u8* refined, const u32* s_pre, const u32* s_cur,
-                            bool changed_only, bool edge_weight_loops, u64* cnt) {
-  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
-    u64 c = 0;
-    if (agg_vertex((u32)v, refined, s_pre, s_cur, changed_only)) {
-      double slw = 0.0;
-      for (u64 p = off[v]; p < off[v + 1]; ++p) {
-        u32 nb = col[p];
-        if (nb == v) {
-          slw = __dadd_rn(slw, w[p]);
-          continue;
-        }
-        if (agg_emit((u32)v, nb, refined, s_pre, s_cur, changed_only)) c += 2;
-      }
-      if (edge_weight_loops) slw = slw / 2.0;
-      if (fabs(slw) > 1e-12) c += 2;
-    }
-    cnt[v] = c;
-  }
-}
-
 __device__ __forceinline__ u64 pair_key(u32 a, u32 b) {
   return a <= b ? (((u64)a << 32) | b) : (((u64)b << 32) | a);
 }
@@ -63,42 +41,64 @@ __global__ void k_agg_lift(const u32* u, const u32* v, const double* w, u64 k, c
   }
 }
 
-__global__ void k_agg_emit(u32 n, const u64* off, const u32* col, const double* w,
+// Warp per refined vertex: its adjacency is scanned 32 entries at a time in
+// CSR order; each emitting entry writes its (-w, +w) pair at the position
+// given by the ballot prefix, so the records keep the reference's push order.
+// With `pos == nullptr` only the per-vertex record count is produced.
+__global__ void k_agg_rows(u32 n, const u64* off, const u32* col, const double* w,
                            const u8* refined, const u32* s_pre, const u32* s_cur,
-                           bool changed_only, bool edge_weight_loops, const u64* pos, u64 base,
-                           u64* keys, double* vals, u32* seq) {
-  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
-    if (!agg_vertex((u32)v, refined, s_pre, s_cur, changed_only)) continue;
-    u64 o = base + pos[v];
-    double slw = 0.0;
-    u32 sp = s_pre[v], sc = s_cur[v];
-    for (u64 p = off[v]; p < off[v + 1]; ++p) {
-      u32 nb = col[p];
-      double x = w[p];
-      if (nb == v) {
-        slw = __dadd_rn(slw, x);
-        continue;
-      }
-      if (!agg_emit((u32)v, nb, refined, s_pre, s_cur, changed_only)) continue;
-      keys[o] = pair_key(sp, s_pre[nb]);
-      vals[o] = -x;
-      seq[o] = (u32)o;
-      ++o;
-      keys[o] = pair_key(sc, s_cur[nb]);
-      vals[o] = x;
-      seq[o] = (u32)o;
-      ++o;
+                           bool changed_only, bool edge_weight_loops, u64* cnt, const u64* pos,
+                           u64 base, u64* keys, double* vals, u32* seq) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 v = warp; v < n; v += nwarps) {
+    if (!agg_vertex((u32)v, refined, s_pre, s_cur, changed_only)) {
+      if (!pos && lane == 0) cnt[v] = 0;
+      continue;
     }
+    const u64 o0 = off[v], o1 = off[v + 1];
+    const u32 sp = s_pre[v], sc = s_cur[v];
+    u64 o = pos ? base + pos[v] : 0;
+    u64 c = 0;
+    for (u64 b0 = o0; b0 < o1; b0 += 32) {
+      u64 p = b0 + lane;
+      bool emit = false;
+      u32 nb = 0;
+      double x = 0.0;
+      if (p < o1) {
+        nb = col[p];
+        x = w[p];
+        emit = nb != (u32)v && agg_emit((u32)v, nb, refined, s_pre, s_cur, changed_only);
+      }
+      u32 m = __ballot_sync(0xffffffffu, emit);
+      if (pos && emit) {
+        u64 at = o + 2ull * __popc(m & ((1u << lane) - 1u));
+        keys[at] = pair_key(sp, s_pre[nb]);
+        vals[at] = -x;
+        seq[at] = (u32)at;
+        keys[at + 1] = pair_key(sc, s_cur[nb]);
+        vals[at + 1] = x;
+        seq[at + 1] = (u32)(at + 1);
+      }
+      o += 2ull * __popc(m);
+      c += 2ull * __popc(m);
+    }
+    double slw = warp_ordered_sum(o0, o1, 0.0, [&](u64 p) { return w[p]; },
+                                  [&](u64 p) { return col[p] == (u32)v; });
     if (edge_weight_loops) slw = slw / 2.0;
-    if (fabs(slw) > 1e-12) {
-      keys[o] = pair_key(sp, sp);
-      vals[o] = -slw;
-      seq[o] = (u32)o;
-      ++o;
-      keys[o] = pair_key(sc, sc);
-      vals[o] = slw;
-      seq[o] = (u32)o;
-      ++o;
+    bool loop = fabs(slw) > 1e-12;
+    if (lane == 0) {
+      if (!pos) {
+        cnt[v] = c + (loop ? 2 : 0);
+      } else if (loop) {
+        keys[o] = pair_key(sp, sp);
+        vals[o] = -slw;
+        seq[o] = (u32)o;
+        keys[o + 1] = pair_key(sc, sc);
+        vals[o + 1] = slw;
+        seq[o + 1] = (u32)(o + 1);
+      }
     }
   }
 }
@@ -117,15 +117,25 @@ __global__ void k_seg_start64(const u32* head, const u32* segid, u64 n, u32* sta
 __global__ void k_compress(u32 U, const u32* start, u64 total, const u64* sk, const u32* sseq,
                            const double* vals, double threshold, u32* ou, u32* ov, double* ow,
                            u8* keepf) {
-  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < U; j += (u64)gridDim.x * blockDim.x) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 j = warp; j < U; j += nwarps) {
     u64 a = start[j], b = (j + 1 < U) ? start[j + 1] : total;
     double x = 0.0;
-    for (u64 t = a; t < b; ++t) x = __dadd_rn(x, vals[sseq[t]]);
-    u64 key = sk[a];
-    ou[j] = (u32)(key >> 32);
-    ov[j] = (u32)key;
-    ow[j] = x;
-    keepf[j] = fabs(x) > threshold ? 1 : 0;
+    if (b - a == 1) {
+      x = vals[sseq[a]];
+    } else {
+      x = warp_ordered_sum(a, b, 0.0, [&](u64 t) { return vals[sseq[t]]; },
+                           [](u64) { return true; });
+    }
+    if (lane == 0) {
+      u64 key = sk[a];
+      ou[j] = (u32)(key >> 32);
+      ov[j] = (u32)key;
+      ow[j] = x;
+      keepf[j] = fabs(x) > threshold ? 1 : 0;
+    }
   }
 }
 
@@ -163,7 +173,7 @@ static u64 compress_records(Engine& E, u64 R, double threshold) {
   S.ev.ensure(E.mem, U);
   S.ew.ensure(E.mem, U);
   S.op.ensure(E.mem, U);
-  ++E.nlaunch, k_compress<<<grid_for(U), 256, 0, st>>>(U, S.seg_start.p, R, ko, vo, S.neww.p, threshold,
+  ++E.nlaunch, k_compress<<<grid_for((u64)U * 32), 256, 0, st>>>(U, S.seg_start.p, R, ko, vo, S.neww.p, threshold,
                                           S.eu.p, S.ev.p, S.ew.p, S.op.p);
   HL_LAUNCH_CHECK();
   S.eu2.ensure(E.mem, U);
@@ -215,9 +225,9 @@ u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n, boo
   }
   S.newoff.ensure(E.mem, (size_t)n + 1);
   S.gkey2.ensure(E.mem, (size_t)n + 1);
-  ++E.nlaunch, k_agg_count<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, S.refined.p,
-                                           L.s_pre.p, L.s_cur.p, changed_only, edge_weight_loops,
-                                           S.newoff.p);
+  ++E.nlaunch, k_agg_rows<<<grid_for((u64)n * 32), 256, 0, st>>>(
+      n, L.g.off.p, L.g.col.p, L.g.w.p, S.refined.p, L.s_pre.p, L.s_cur.p, changed_only,
+      edge_weight_loops, S.newoff.p, nullptr, 0, nullptr, nullptr, nullptr);
   HL_CUDA(cudaMemsetAsync(S.newoff.p + n, 0, sizeof(u64), st));
   HL_LAUNCH_CHECK();
   u64* a = S.newoff.p;
@@ -236,10 +246,9 @@ u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n, boo
     if (delta.k)
       ++E.nlaunch, k_agg_lift<<<grid_for(delta.k), 256, 0, st>>>(delta.u, delta.v, delta.w, delta.k, L.s_pre.p,
                                                     S.keys.p, S.neww.p, S.idx.p);
-    ++E.nlaunch, k_agg_emit<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, S.refined.p,
-                                            L.s_pre.p, L.s_cur.p, changed_only,
-                                            edge_weight_loops, pos, delta.k, S.keys.p, S.neww.p,
-                                            S.idx.p);
+    ++E.nlaunch, k_agg_rows<<<grid_for((u64)n * 32), 256, 0, st>>>(
+        n, L.g.off.p, L.g.col.p, L.g.w.p, S.refined.p, L.s_pre.p, L.s_cur.p, changed_only,
+        edge_weight_loops, nullptr, pos, delta.k, S.keys.p, S.neww.p, S.idx.p);
     HL_LAUNCH_CHECK();
   }
   u64 out = compress_records(E, R, 1e-9);

@@ -1,0 +1,655 @@
+// eval.cu — best-move evaluation on a fixed snapshot, shared by inc-movement
+// (parallel_frontier.rs:133-239) and the refinement merge
+// (throughput.rs:291-359).
+//
+// For every listed vertex v: Σw(v, X) per neighbour key X (community for the
+// movement, sub-community inside v's community for the refinement), each sum
+// extended in CSR order; then the argmax of the FP64 gain with the reference's
+// tie rule (strict '>' in first-encounter order = on equal gains the smallest
+// first CSR position); then, for the movement, the empty community n+v on a
+// strict improvement.
+//
+// Vertices are binned by degree so that no lane idles on short rows and no
+// vertex waits on a table far larger than it needs:
+//   deg <= 8, 16, 32    sub-warp groups of 8 / 16 / 32 lanes, one chunk, no table;
+//   33 .. MID_MAX       a warp per vertex, shared-memory table sized 2·deg;
+//   larger              a block per vertex: 256-entry adjacency tiles staged in
+//                       shared memory by all warps, keys accumulated in a
+//                       shared table (2048 entries up to degree 1024, 8192 up
+//                       to 4096, a global table above).  With integral weights
+//                       every warp inserts its chunk at once (exact in any
+//                       order); otherwise each warp owns a hash partition of the
+//                       keys and folds the tile in CSR order, so every key's
+//                       sum keeps the reference's rounding.
+#include <cstring>
+
+#include "hl_engine.cuh"
+
+namespace hl {
+
+static inline u32 grid_for(u64 n, u32 block = 256) {
+  u64 g = (n + block - 1) / block;
+  if (g > 148u * 64u) g = 148u * 64u;
+  return g ? (u32)g : 1u;
+}
+
+enum EvalKind { EVAL_MOVE = 0, EVAL_REFINE = 1 };
+
+struct EvalArgs {
+  const u32* verts;   // vertex ids
+  const u32* idx;     // indices into verts handled by this launch
+  u32 nidx;
+  const u64* off;
+  const u32* col;
+  const double* w;
+  const u32* f;
+  const u32* s;
+  const double* d;
+  const double* kdeg;
+  const u8* blocked;
+  double tw, gamma;
+  u32 n;
+  bool allow_empty;
+  bool concurrent;  // integral weights: order-free accumulation allowed
+  u32* out_to;
+  double* out_gain;
+  const u64* tab_off;  // global table offset per idx position (big vertices)
+  u32* tkey;
+  u32* tpos;
+  double* tval;
+  unsigned long long* counters;  // [0] entries scanned, [1] candidates evaluated
+};
+
+constexpr u32 MID_MAX = 128;
+constexpr u32 MID_TAB = 256;  // per-warp table entries (>= 2 * MID_MAX)
+constexpr u32 MID_WARPS = 8;
+constexpr u32 BIG_THREADS = 256;
+constexpr u32 BIG1_TAB = 2048;  // shared table of the block kernel, degrees up to 1024
+constexpr u32 BIG_TAB = 8192;   // shared table for larger degrees (global above 4096)
+
+__device__ __forceinline__ u32 hash32(u32 x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+template <int KIND>
+__device__ __forceinline__ bool entry_key(const EvalArgs& A, u32 v, u32 nb, u32 fv, u32& key) {
+  if (KIND == EVAL_MOVE) {
+    if (nb == v) return false;  // self-loops skipped (parallel_frontier.rs:164-166)
+    key = A.f[nb];
+    return true;
+  } else {
+    if (A.f[nb] != fv) return false;  // same community only (throughput.rs:308-311)
+    key = A.s[nb];
+    return true;
+  }
+}
+
+// Final decision of one vertex from its best neighbour candidate.
+template <int KIND>
+__device__ __forceinline__ void finish(const EvalArgs& A, u32 i, u32 v, u32 cur, double kv,
+                                       double wcur, double best_g, u32 best_key, bool has_best) {
+  u32 to = cur;
+  double g = 0.0;
+  if (has_best && best_g > 0.0) {
+    g = best_g;
+    to = best_key;
+  }
+  if (KIND == EVAL_MOVE && A.allow_empty && A.tw != 0.0) {
+    double eg = empty_gain(wcur, A.tw, A.gamma, kv, A.d[cur]);
+    if (eg > g) {
+      g = eg;
+      to = A.n + v;
+    }
+  }
+  A.out_to[i] = to;
+  A.out_gain[i] = g;
+}
+
+__device__ __forceinline__ void block_count(const EvalArgs& A, unsigned long long trav,
+                                            unsigned long long cand) {
+  if (!A.counters) return;
+  for (int o = 16; o; o >>= 1) {
+    trav += __shfl_xor_sync(0xffffffffu, trav, o);
+    cand += __shfl_xor_sync(0xffffffffu, cand, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (trav) atomicAdd(&A.counters[0], trav);
+    if (cand) atomicAdd(&A.counters[1], cand);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Small degrees: groups of G lanes, one vertex per group, one chunk.
+// ---------------------------------------------------------------------------
+template <int KIND, int G>
+__global__ void __launch_bounds__(256) k_eval_small(EvalArgs A) {
+  __shared__ double s_w[256];
+  const u32 lane = threadIdx.x & 31;
+  const u32 grp_in_warp = lane / G;
+  const u32 gl = lane % G;
+  const u32 gbase = lane - gl;  // first lane of this group
+  const u32 gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  constexpr u32 GPW = 32 / G;
+  unsigned long long trav = 0, ncand = 0;
+  for (u64 base = warp * GPW; base < A.nidx; base += nwarps * GPW) {
+    const u64 t = base + grp_in_warp;
+    const bool live = t < A.nidx;
+    u32 i = 0, v = 0, cur = 0, fv = 0;
+    u64 o0 = 0, deg = 0;
+    double kv = 0.0;
+    if (live) {
+      i = A.idx[t];
+      v = A.verts[i];
+      o0 = A.off[v];
+      deg = A.off[v + 1] - o0;
+      fv = A.f[v];
+      cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+      kv = A.kdeg[v];
+      if (gl == 0) trav += deg;
+    }
+    u32 key = NONE32;
+    double wv = 0.0;
+    bool has = false;
+    if (live && gl < deg) {
+      u32 nb = A.col[o0 + gl];
+      wv = A.w[o0 + gl];
+      has = entry_key<KIND>(A, v, nb, fv, key);
+    }
+    s_w[threadIdx.x] = wv;
+    __syncwarp();
+    unsigned long long mv = has ? (((unsigned long long)grp_in_warp << 32) | key)
+                                : (0x8000000000000000ull | lane);
+    u32 grp = __match_any_sync(0xffffffffu, mv);
+    bool leader = has && lane == (u32)(__ffs(grp) - 1);
+    double sum = 0.0;
+    if (leader)
+      for (u32 m = grp; m; m &= m - 1)
+        sum = __dadd_rn(sum, s_w[(threadIdx.x & ~31u) + __ffs(m) - 1]);
+    u32 curm = __ballot_sync(0xffffffffu, leader && key == cur) & gmask;
+    double wc = __shfl_sync(0xffffffffu, sum, curm ? (__ffs(curm) - 1) : lane);
+    double wcur = curm ? wc : 0.0;
+    double g = -1.0;
+    u32 p = NONE32, kk = key;
+    if (leader && key != cur && A.tw != 0.0) {
+      bool blk = (KIND == EVAL_REFINE) && A.blocked[key];
+      if (!blk) {
+        g = move_gain(sum, wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
+        p = gl;
+        ++ncand;
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) {
+      double og = __shfl_xor_sync(0xffffffffu, g, o);
+      u32 op = __shfl_xor_sync(0xffffffffu, p, o);
+      u32 ok = __shfl_xor_sync(0xffffffffu, kk, o);
+      if (op != NONE32 && (p == NONE32 || og > g || (og == g && op < p))) {
+        g = og;
+        p = op;
+        kk = ok;
+      }
+    }
+    if (live && gl == 0) finish<KIND>(A, i, v, cur, kv, wcur, g, kk, p != NONE32);
+    __syncwarp();
+  }
+  block_count(A, trav, ncand);
+}
+
+// ---------------------------------------------------------------------------
+// Mid degrees: a warp per vertex with a shared table sized to the vertex.
+// ---------------------------------------------------------------------------
+template <int KIND>
+__global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
+  __shared__ u32 s_key[MID_WARPS][MID_TAB];
+  __shared__ u32 s_pos[MID_WARPS][MID_TAB];
+  __shared__ double s_val[MID_WARPS][MID_TAB];
+  __shared__ double s_w[MID_WARPS][32];
+  const u32 lane = threadIdx.x & 31;
+  const u32 wib = threadIdx.x >> 5;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  unsigned long long trav = 0, ncand = 0;
+  u32* tk = s_key[wib];
+  u32* tp = s_pos[wib];
+  double* tv = s_val[wib];
+  for (u64 t = warp; t < A.nidx; t += nwarps) {
+    const u32 i = A.idx[t];
+    const u32 v = A.verts[i];
+    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u64 deg = o1 - o0;
+    const u32 fv = A.f[v];
+    const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+    const double kv = A.kdeg[v];
+    if (lane == 0) trav += deg;
+    u32 cap = 64;
+    while (cap < 2 * deg) cap <<= 1;
+    const u32 mask = cap - 1;
+    for (u32 x = lane; x < cap; x += 32) tk[x] = NONE32;
+    __syncwarp();
+    for (u64 b0 = o0; b0 < o1; b0 += 32) {
+      u64 q = b0 + lane;
+      u32 key = NONE32;
+      double wv = 0.0;
+      bool has = false;
+      if (q < o1) {
+        u32 nb = A.col[q];
+        wv = A.w[q];
+        has = entry_key<KIND>(A, v, nb, fv, key);
+        if (!has) key = NONE32;
+      }
+      s_w[wib][lane] = wv;
+      __syncwarp();
+      u32 grp = __match_any_sync(0xffffffffu, key);
+      if (has && lane == (u32)(__ffs(grp) - 1)) {
+        u32 slot = hash32(key) & mask;
+        while (true) {
+          u32 prev = atomicCAS(&tk[slot], NONE32, key);
+          if (prev == NONE32 || prev == key) {
+            double sum = prev == NONE32 ? 0.0 : tv[slot];
+            for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, s_w[wib][__ffs(m) - 1]);
+            tv[slot] = sum;
+            if (prev == NONE32) tp[slot] = (u32)(q - o0);
+            break;
+          }
+          slot = (slot + 1) & mask;
+        }
+      }
+      __syncwarp();
+    }
+    double wcur = 0.0;
+    bool found = false;
+    for (u32 x = lane; x < cap; x += 32)
+      if (tk[x] == cur) {
+        wcur = tv[x];
+        found = true;
+      }
+    u32 fm = __ballot_sync(0xffffffffu, found);
+    wcur = __shfl_sync(0xffffffffu, wcur, fm ? __ffs(fm) - 1 : 0);
+    if (!fm) wcur = 0.0;
+    double g = -1.0;
+    u32 p = NONE32, kk = cur;
+    if (A.tw != 0.0) {
+      for (u32 x = lane; x < cap; x += 32) {
+        u32 key = tk[x];
+        if (key == NONE32 || key == cur) continue;
+        if (KIND == EVAL_REFINE && A.blocked[key]) continue;
+        double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
+        ++ncand;
+        u32 pp = tp[x];
+        if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+          g = gn;
+          p = pp;
+          kk = key;
+        }
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      double og = __shfl_xor_sync(0xffffffffu, g, o);
+      u32 op = __shfl_xor_sync(0xffffffffu, p, o);
+      u32 ok = __shfl_xor_sync(0xffffffffu, kk, o);
+      if (op != NONE32 && (p == NONE32 || og > g || (og == g && op < p))) {
+        g = og;
+        p = op;
+        kk = ok;
+      }
+    }
+    if (lane == 0) finish<KIND>(A, i, v, cur, kv, wcur, g, kk, p != NONE32);
+    __syncwarp();
+  }
+  block_count(A, trav, ncand);
+}
+
+// ---------------------------------------------------------------------------
+// Large degrees: a block per vertex, adjacency staged in shared tiles.
+// ---------------------------------------------------------------------------
+template <int KIND, u32 TAB>
+__global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
+  extern __shared__ unsigned char smem_raw[];
+  u32* s_tk = reinterpret_cast<u32*>(smem_raw);                       // TAB
+  u32* s_tp = s_tk + TAB;                                              // TAB
+  double* s_tv = reinterpret_cast<double*>(s_tp + TAB);                // TAB
+  u32* s_key = reinterpret_cast<u32*>(s_tv + TAB);                     // BIG_THREADS
+  double* s_w = reinterpret_cast<double*>(s_key + BIG_THREADS);        // BIG_THREADS
+  __shared__ double r_g[BIG_THREADS / 32];
+  __shared__ u32 r_p[BIG_THREADS / 32], r_k[BIG_THREADS / 32];
+  __shared__ double s_wcur;
+  const u32 lane = threadIdx.x & 31;
+  const u32 wib = threadIdx.x >> 5;
+  unsigned long long trav = 0, ncand = 0;
+  for (u64 t = blockIdx.x; t < A.nidx; t += gridDim.x) {
+    const u32 i = A.idx[t];
+    const u32 v = A.verts[i];
+    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u64 deg = o1 - o0;
+    const u32 fv = A.f[v];
+    const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+    const double kv = A.kdeg[v];
+    if (threadIdx.x == 0) trav += deg;
+    u32* tk;
+    u32* tp;
+    double* tv;
+    u64 cap = 2;
+    while (cap < 2 * deg) cap <<= 1;
+    if (2 * deg <= TAB) {
+      tk = s_tk;
+      tp = s_tp;
+      tv = s_tv;
+    } else {
+      u64 gb = A.tab_off[t];
+      tk = A.tkey + gb;
+      tp = A.tpos + gb;
+      tv = A.tval + gb;
+    }
+    const u64 mask = cap - 1;
+    for (u64 x = threadIdx.x; x < cap; x += BIG_THREADS) {
+      tk[x] = NONE32;
+      tp[x] = NONE32;
+      tv[x] = 0.0;
+    }
+    __syncthreads();
+    for (u64 b0 = o0; b0 < o1; b0 += BIG_THREADS) {
+      u64 q = b0 + threadIdx.x;
+      u32 key = NONE32;
+      double wv = 0.0;
+      if (q < o1) {
+        u32 nb = A.col[q];
+        wv = A.w[q];
+        if (!entry_key<KIND>(A, v, nb, fv, key)) key = NONE32;
+      }
+      s_key[threadIdx.x] = key;
+      s_w[threadIdx.x] = wv;
+      __syncthreads();
+      const u32 nch = (u32)((o1 - b0 + 31) / 32 < BIG_THREADS / 32 ? (o1 - b0 + 31) / 32
+                                                                   : BIG_THREADS / 32);
+      // Integral weights: every warp inserts its own chunk at once (atomic,
+      // exact in any order).  Otherwise each warp owns the keys whose hash
+      // falls in its partition and folds the tile's chunks in CSR order, so
+      // every key's sum is still extended entry by entry in CSR order.
+      const u32 c0 = A.concurrent ? wib : 0;
+      const u32 cs = A.concurrent ? BIG_THREADS / 32 : 1;
+      for (u32 c = c0; c < nch; c += cs) {
+        u32 e = c * 32 + lane;
+        u32 key2 = s_key[e];
+        bool mine = key2 != NONE32 &&
+                    (A.concurrent || (hash32(key2) >> 29) == wib);  // 8 warps, top 3 bits
+        u32 grp = __match_any_sync(0xffffffffu, mine ? (unsigned long long)key2
+                                                     : ((1ull << 32) | lane));
+        if (mine && lane == (u32)(__ffs(grp) - 1)) {
+          u32 pos = (u32)(b0 - o0) + e;
+          u64 slot = hash32(key2) & mask;
+          u32 prev;
+          while (true) {
+            prev = atomicCAS(&tk[slot], NONE32, key2);
+            if (prev == NONE32 || prev == key2) break;
+            slot = (slot + 1) & mask;
+          }
+          if (A.concurrent) {
+            double sum = 0.0;
+            for (u32 m = grp; m; m &= m - 1) sum += s_w[c * 32 + __ffs(m) - 1];
+            atomicAdd(&tv[slot], sum);
+            atomicMin(&tp[slot], pos);
+          } else {
+            double acc = prev == NONE32 ? 0.0 : tv[slot];
+            for (u32 m = grp; m; m &= m - 1) acc = __dadd_rn(acc, s_w[c * 32 + __ffs(m) - 1]);
+            tv[slot] = acc;
+            if (prev == NONE32) tp[slot] = pos;
+          }
+        }
+        __syncwarp();
+      }
+      __syncthreads();
+    }
+    // w(v, cur) and the argmax over the table.
+    if (threadIdx.x == 0) s_wcur = 0.0;
+    __syncthreads();
+    for (u64 x = threadIdx.x; x < cap; x += BIG_THREADS)
+      if (tk[x] == cur) s_wcur = tv[x];
+    __syncthreads();
+    const double wcur = s_wcur;
+    double g = -1.0;
+    u32 p = NONE32, kk = cur;
+    if (A.tw != 0.0) {
+      for (u64 x = threadIdx.x; x < cap; x += BIG_THREADS) {
+        u32 key = tk[x];
+        if (key == NONE32 || key == cur) continue;
+        if (KIND == EVAL_REFINE && A.blocked[key]) continue;
+        double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
+        ++ncand;
+        u32 pp = tp[x];
+        if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+          g = gn;
+          p = pp;
+          kk = key;
+        }
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      double og = __shfl_xor_sync(0xffffffffu, g, o);
+      u32 op = __shfl_xor_sync(0xffffffffu, p, o);
+      u32 ok = __shfl_xor_sync(0xffffffffu, kk, o);
+      if (op != NONE32 && (p == NONE32 || og > g || (og == g && op < p))) {
+        g = og;
+        p = op;
+        kk = ok;
+      }
+    }
+    if (lane == 0) {
+      r_g[wib] = g;
+      r_p[wib] = p;
+      r_k[wib] = kk;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (u32 x = 1; x < BIG_THREADS / 32; ++x) {
+        if (r_p[x] != NONE32 && (p == NONE32 || r_g[x] > g || (r_g[x] == g && r_p[x] < p))) {
+          g = r_g[x];
+          p = r_p[x];
+          kk = r_k[x];
+        }
+      }
+      finish<KIND>(A, i, v, cur, kv, wcur, g, kk, p != NONE32);
+    }
+    __syncthreads();
+  }
+  block_count(A, trav, ncand);
+}
+
+// ---------------------------------------------------------------------------
+// Host side: bin the list by degree and launch the three kernels.
+// ---------------------------------------------------------------------------
+__global__ void k_bin(const u32* verts, u32 nv, const u64* off, u32* bin, u32* idx,
+                      u32* counts) {
+  __shared__ u32 sc[6];
+  if (threadIdx.x < 6) sc[threadIdx.x] = 0;
+  __syncthreads();
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < nv; i += (u64)gridDim.x * blockDim.x) {
+    u32 v = verts[i];
+    u64 deg = off[v + 1] - off[v];
+    u32 b = deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= MID_MAX ? 3
+          : 2 * deg <= BIG1_TAB ? 4 : 5;
+    bin[i] = b;
+    idx[i] = (u32)i;
+    atomicAdd(&sc[b], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 6 && sc[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sc[threadIdx.x]);
+}
+
+__global__ void k_big_caps2(const u32* verts, const u32* idx, u32 nb, const u64* off, u64* cap) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < nb; t += (u64)gridDim.x * blockDim.x) {
+    u32 v = verts[idx[t]];
+    u64 deg = off[v + 1] - off[v];
+    u64 c = 0;
+    if (2 * deg > BIG_TAB) {
+      c = 2;
+      while (c < 2 * deg) c <<= 1;
+    }
+    cap[t] = c;
+  }
+}
+
+static bool g_big_attr_set[64] = {false};
+
+template <u32 TAB>
+static size_t big_smem() {
+  return (size_t)TAB * (4 + 4 + 8) + (size_t)BIG_THREADS * (4 + 8);
+}
+
+void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
+              const double* d, const u8* blocked, bool allow_empty, u32* out_to, double* out_gain,
+              unsigned long long* counters) {
+  if (!nv) return;
+  cudaStream_t st = E.stream;
+  Scratch& S = E.sc;
+  S.order.ensure(E.mem, nv);
+  S.order2.ensure(E.mem, nv);
+  S.used.ensure(E.mem, nv);
+  S.rank.ensure(E.mem, nv);
+  S.cnt.ensure(E.mem, 16);
+  u32* cnt = S.cnt.p + 2;  // six bin counters (cnt[2..7])
+  HL_CUDA(cudaMemsetAsync(cnt, 0, 6 * sizeof(u32), st));
+  ++E.nlaunch, k_bin<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.used.p, S.order.p, cnt);
+  HL_LAUNCH_CHECK();
+  u32* ki = S.used.p;
+  u32* ko = S.rank.p;
+  u32* vi = S.order.p;
+  u32* vo = S.order2.p;
+  cub_run(E, [&](void* t, size_t& b) {
+    return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)nv, 0, 3, st);
+  });
+  u32 c[6];
+  HL_CUDA(cudaMemcpyAsync(E.hs.p, cnt, 6 * sizeof(u32), cudaMemcpyDeviceToHost, st));
+  E.sync();
+  std::memcpy(c, E.hs.p, sizeof(c));
+  u32 start[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < 6; ++b) start[b + 1] = start[b] + c[b];
+  // Global tables for vertices above the largest shared table.
+  DBuf<u32> tk, tp;
+  DBuf<double> tv;
+  u64* tab_off = nullptr;
+  if (c[5]) {
+    S.gkey.ensure(E.mem, (size_t)c[5] + 1);
+    S.gkey2.ensure(E.mem, (size_t)c[5] + 1);
+    ++E.nlaunch, k_big_caps2<<<grid_for(c[5]), 256, 0, st>>>(verts, vo + start[5], c[5], L.g.off.p,
+                                                             S.gkey.p);
+    HL_CUDA(cudaMemsetAsync(S.gkey.p + c[5], 0, sizeof(u64), st));
+    HL_LAUNCH_CHECK();
+    u64* ci = S.gkey.p;
+    u64* co = S.gkey2.p;
+    cub_run(E, [&](void* t, size_t& b) {
+      return cub::DeviceScan::ExclusiveSum(t, b, ci, co, (int64_t)c[5] + 1, st);
+    });
+    u64 total = E.read_u64(co + c[5]);
+    if (total) {
+      tk.ensure(E.mem, total);
+      tp.ensure(E.mem, total);
+      tv.ensure(E.mem, total);
+    }
+    tab_off = co;
+  }
+  int dev = E.device;
+  if (dev >= 0 && dev < 64 && !g_big_attr_set[dev]) {
+    HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_MOVE, BIG_TAB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)big_smem<BIG_TAB>()));
+    HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_REFINE, BIG_TAB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)big_smem<BIG_TAB>()));
+    g_big_attr_set[dev] = true;
+  }
+
+  EvalArgs A;
+  A.verts = verts;
+  A.off = L.g.off.p;
+  A.col = L.g.col.p;
+  A.w = L.g.w.p;
+  A.f = L.f.p;
+  A.s = s;
+  A.d = d;
+  A.kdeg = L.k.p;
+  A.blocked = blocked;
+  A.tw = L.tw;
+  A.gamma = E.cfg.resolution;
+  A.n = L.g.n;
+  A.allow_empty = allow_empty;
+  A.concurrent = E.integral;
+  A.out_to = out_to;
+  A.out_gain = out_gain;
+  A.counters = counters;
+  A.tab_off = nullptr;
+  A.tkey = nullptr;
+  A.tpos = nullptr;
+  A.tval = nullptr;
+
+  cudaEvent_t ev = E.kt_begin();
+  auto launch_small = [&](int b) {
+    if (!c[b]) return;
+    EvalArgs a = A;
+    a.idx = vo + start[b];
+    a.nidx = c[b];
+    u32 G = b == 0 ? 8 : b == 1 ? 16 : 32;
+    u64 threads = (u64)c[b] * G;
+    u32 blocks = grid_for(threads, 256);
+    if (kind == EVAL_MOVE) {
+      if (G == 8) ++E.nlaunch, k_eval_small<EVAL_MOVE, 8><<<blocks, 256, 0, st>>>(a);
+      else if (G == 16) ++E.nlaunch, k_eval_small<EVAL_MOVE, 16><<<blocks, 256, 0, st>>>(a);
+      else ++E.nlaunch, k_eval_small<EVAL_MOVE, 32><<<blocks, 256, 0, st>>>(a);
+    } else {
+      if (G == 8) ++E.nlaunch, k_eval_small<EVAL_REFINE, 8><<<blocks, 256, 0, st>>>(a);
+      else if (G == 16) ++E.nlaunch, k_eval_small<EVAL_REFINE, 16><<<blocks, 256, 0, st>>>(a);
+      else ++E.nlaunch, k_eval_small<EVAL_REFINE, 32><<<blocks, 256, 0, st>>>(a);
+    }
+  };
+  launch_small(0);
+  launch_small(1);
+  launch_small(2);
+  if (c[3]) {
+    EvalArgs a = A;
+    a.idx = vo + start[3];
+    a.nidx = c[3];
+    u32 blocks = grid_for((u64)c[3] * 32, MID_WARPS * 32);
+    if (kind == EVAL_MOVE)
+      ++E.nlaunch, k_eval_mid<EVAL_MOVE><<<blocks, MID_WARPS * 32, 0, st>>>(a);
+    else
+      ++E.nlaunch, k_eval_mid<EVAL_REFINE><<<blocks, MID_WARPS * 32, 0, st>>>(a);
+  }
+  HL_LAUNCH_CHECK();
+  auto launch_big = [&](int b) {
+    if (!c[b]) return;
+    EvalArgs a = A;
+    a.idx = vo + start[b];
+    a.nidx = c[b];
+    a.tab_off = b == 5 ? tab_off : nullptr;
+    a.tkey = tk.p;
+    a.tpos = tp.p;
+    a.tval = tv.p;
+    if (b == 4) {
+      u32 blocks = c[b] < 148u * 8u ? c[b] : 148u * 8u;
+      size_t sm = big_smem<BIG1_TAB>();
+      if (kind == EVAL_MOVE)
+        ++E.nlaunch, k_eval_big<EVAL_MOVE, BIG1_TAB><<<blocks, BIG_THREADS, sm, st>>>(a);
+      else
+        ++E.nlaunch, k_eval_big<EVAL_REFINE, BIG1_TAB><<<blocks, BIG_THREADS, sm, st>>>(a);
+    } else {
+      u32 blocks = c[b] < 148u * 2u ? c[b] : 148u * 2u;
+      size_t sm = big_smem<BIG_TAB>();
+      if (kind == EVAL_MOVE)
+        ++E.nlaunch, k_eval_big<EVAL_MOVE, BIG_TAB><<<blocks, BIG_THREADS, sm, st>>>(a);
+      else
+        ++E.nlaunch, k_eval_big<EVAL_REFINE, BIG_TAB><<<blocks, BIG_THREADS, sm, st>>>(a);
+    }
+    HL_LAUNCH_CHECK();
+  };
+  launch_big(4);
+  launch_big(5);
+  E.kt_end(kind == EVAL_MOVE ? KT_MOVE_EVAL : KT_REFINE_EVAL, ev);
+}
+
+}  // namespace hl

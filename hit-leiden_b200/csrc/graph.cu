@@ -347,15 +347,18 @@ __global__ void k_merge_rows(u32 n, const u64* off, const u32* col, const double
   }
 }
 
-// Row sums in CSR order (hit_leiden.rs:1063).  Serial per row: the exact
-// left-to-right rounding of the reference for any weights.
+// Row sums in CSR order (hit_leiden.rs:1063), left to right: the exact
+// rounding of the reference for any weights (warp per row, ordered fold).
 __global__ void k_row_sum_serial(const u32* rows, u32 nr, const u64* off, const double* w,
                                  double* k) {
-  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < nr; i += (u64)gridDim.x * blockDim.x) {
-    u32 v = rows[i];
-    double s = 0.0;
-    for (u64 p = off[v]; p < off[v + 1]; ++p) s = __dadd_rn(s, w[p]);
-    k[v] = s;
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 i = warp; i < nr; i += nwarps) {
+    u32 v = rows ? rows[i] : (u32)i;
+    double s = warp_ordered_sum(off[v], off[v + 1], 0.0, [&](u64 p) { return w[p]; },
+                                [](u64) { return true; });
+    if (lane == 0) k[v] = s;
   }
 }
 
@@ -375,13 +378,6 @@ __global__ void k_row_sum_warp(const u32* rows, u32 nr, const u64* off, const do
   }
 }
 
-__global__ void k_row_sum_serial_all(u32 n, const u64* off, const double* w, double* k) {
-  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (u64 p = off[v]; p < off[v + 1]; ++p) s = __dadd_rn(s, w[p]);
-    k[v] = s;
-  }
-}
 
 // Fixed-shape pairwise sum: tiles of 1024 (+0.0 padded) folded by stride
 // halving; repeated on the tile sums until one value remains.
@@ -427,7 +423,8 @@ static void recompute_rows(Engine& E, Level& L, const u32* rows, u32 nr) {
     ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p,
                                                                   L.k.p);
   else
-    ++E.nlaunch, k_row_sum_serial<<<grid_for(nr), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p, L.k.p);
+    ++E.nlaunch, k_row_sum_serial<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p,
+                                                                               L.g.w.p, L.k.p);
   HL_LAUNCH_CHECK();
 }
 
@@ -438,7 +435,8 @@ void recompute_all_degrees(Engine& E, Level& L) {
       ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(nullptr, n, L.g.off.p, L.g.w.p,
                                                                    L.k.p);
     else
-      ++E.nlaunch, k_row_sum_serial_all<<<grid_for(n), 256, 0, E.stream>>>(n, L.g.off.p, L.g.w.p, L.k.p);
+      ++E.nlaunch, k_row_sum_serial<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(nullptr, n, L.g.off.p,
+                                                                                 L.g.w.p, L.k.p);
     HL_LAUNCH_CHECK();
   }
   L.tw = tree_sum(E, L.k.p, n);

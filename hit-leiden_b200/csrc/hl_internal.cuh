@@ -167,6 +167,29 @@ __device__ __forceinline__ double remove_gain(double w_sc, double tw, double gam
   return __dadd_rn(a, __ddiv_rn(b, __dmul_rn(tw, tw)));
 }
 
+// Left-to-right sum acc + x[a] + x[a+1] + ... + x[b-1] with every addition
+// rounded in that order (the reference's sequential f64 sums), computed by a
+// whole warp: lanes load 32 consecutive values at once and the sum is then
+// extended in lane order through shuffles.  All lanes must call it with the
+// same arguments; all lanes return the same result.  `val(t)` returns the
+// t-th value; `take(t)` says whether it is part of the sum.
+template <typename V, typename P>
+__device__ __forceinline__ double warp_ordered_sum(u64 a, u64 b, double acc, V val, P take) {
+  const u32 lane = threadIdx.x & 31;
+  for (u64 base = a; base < b; base += 32) {
+    u64 t = base + lane;
+    bool ok = t < b && take(t);
+    double x = ok ? val(t) : 0.0;
+    u32 m = __ballot_sync(0xffffffffu, ok);
+    while (m) {
+      int j = __ffs(m) - 1;
+      acc = __dadd_rn(acc, __shfl_sync(0xffffffffu, x, j));
+      m &= m - 1;
+    }
+  }
+  return acc;
+}
+
 // Total order on doubles as unsigned keys (ascending).
 __device__ __forceinline__ u64 double_key(double x) {
   u64 b = (u64)__double_as_longlong(x);

@@ -72,11 +72,14 @@ __global__ void k_comm_deg_atomic(u32 n, const u32* part, const double* k, doubl
 // sums its members' degrees in ascending node order.
 __global__ void k_comm_deg_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 n,
                                    const u32* sorted_nodes, const double* k, double* d) {
-  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < nu; j += (u64)gridDim.x * blockDim.x) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 j = warp; j < nu; j += nwarps) {
     u32 a = ustart[j], b = (j + 1 < nu) ? ustart[j + 1] : n;
-    double s = 0.0;
-    for (u32 t = a; t < b; ++t) s = __dadd_rn(s, k[sorted_nodes[t]]);
-    d[ukeys[j]] = s;
+    double s = warp_ordered_sum(a, b, 0.0, [&](u64 t) { return k[sorted_nodes[t]]; },
+                                [](u64) { return true; });
+    if (lane == 0) d[ukeys[j]] = s;
   }
 }
 
@@ -137,7 +140,8 @@ void recompute_comm_degrees(Engine& E, Level& L, const u32* part, u32 ncomm_cap,
   });
   u32 nu = E.read_u32(sid + n - 1) + E.read_u32(h + n - 1);
   ++E.nlaunch, k_seg_compact<<<grid_for(n), 256, 0, st>>>(h, sid, kout, n, S.used.p, S.sel_node.p);
-  ++E.nlaunch, k_comm_deg_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.used.p, S.sel_node.p, n, vout, L.k.p, d);
+  ++E.nlaunch, k_comm_deg_ordered<<<grid_for((u64)nu * 32), 256, 0, st>>>(nu, S.used.p, S.sel_node.p, n,
+                                                                           vout, L.k.p, d);
   HL_LAUNCH_CHECK();
 }
 
@@ -193,338 +197,7 @@ void compact_labels_if_needed(Engine& E, u32* labels, u32 n, u32 limit) {
   rank_compact(E, labels, n, mx);
 }
 
-// ----------------------------------------------------------------------------
-// Best-move evaluation (shared with refinement).
-// ----------------------------------------------------------------------------
 enum EvalKind { EVAL_MOVE = 0, EVAL_REFINE = 1 };
-
-struct EvalArgs {
-  const u32* verts;    // vertices to evaluate
-  u32 nv;
-  const u64* off;
-  const u32* col;
-  const double* w;
-  const u32* f;        // communities
-  const u32* s;        // sub-communities (refine keys)
-  const double* d;     // degrees of the key sets (d(C) or d(S))
-  const double* kdeg;  // vertex degrees
-  const u8* blocked;   // refine: T-filter blocked sub-communities
-  double tw, gamma;
-  u32 n;               // graph size (empty-community id = n + v)
-  bool allow_empty;
-  u32* out_to;
-  double* out_gain;
-  // global hash tables for high-degree vertices
-  const u64* tab_off;  // per vertex index (0 if not big)
-  u32* tkey;
-  u32* tpos;
-  double* tval;
-  unsigned long long* traversed;  // [0] adjacency entries scanned, [1] candidates evaluated
-};
-
-constexpr u32 WARP_TAB = 512;  // entries per warp table in shared memory
-constexpr u32 WARPS_PER_BLOCK = 4;
-constexpr u32 SMALL_DEG = 32;
-constexpr u32 MID_DEG = WARP_TAB / 2;
-
-__device__ __forceinline__ u32 hash32(u32 x) {
-  x ^= x >> 16;
-  x *= 0x7feb352du;
-  x ^= x >> 15;
-  x *= 0x846ca68bu;
-  x ^= x >> 16;
-  return x;
-}
-
-// Warp-argmax key: larger gain wins; on equal gains the smaller CSR position.
-__device__ __forceinline__ void warp_best(double& g, u32& pos, u32& key) {
-  for (int o = 16; o; o >>= 1) {
-    double og = __shfl_xor_sync(0xffffffffu, g, o);
-    u32 op = __shfl_xor_sync(0xffffffffu, pos, o);
-    u32 ok = __shfl_xor_sync(0xffffffffu, key, o);
-    if (og > g || (og == g && op < pos)) {
-      g = og;
-      pos = op;
-      key = ok;
-    }
-  }
-}
-
-template <int KIND>
-__device__ __forceinline__ bool entry_key(const EvalArgs& A, u32 v, u32 nb, u32 fv, u32& key) {
-  if (KIND == EVAL_MOVE) {
-    if (nb == v) return false;  // self-loops skipped (parallel_frontier.rs:164-166)
-    key = A.f[nb];
-    return true;
-  } else {
-    if (A.f[nb] != fv) return false;  // same community only (throughput.rs:308-311)
-    key = A.s[nb];
-    return true;
-  }
-}
-
-template <int KIND>
-__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_eval(EvalArgs A) {
-  __shared__ u32 s_key[WARPS_PER_BLOCK][WARP_TAB];
-  __shared__ u32 s_pos[WARPS_PER_BLOCK][WARP_TAB];
-  __shared__ double s_val[WARPS_PER_BLOCK][WARP_TAB];
-  __shared__ double s_w[WARPS_PER_BLOCK][32];
-  __shared__ unsigned long long s_trav, s_cand;
-  const u32 lane = threadIdx.x & 31;
-  const u32 wib = threadIdx.x >> 5;
-  if (threadIdx.x == 0) {
-    s_trav = 0;
-    s_cand = 0;
-  }
-  __syncthreads();
-  unsigned long long my_trav = 0, my_cand = 0;
-  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
-  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
-  for (u64 i = warp; i < A.nv; i += nwarps) {
-    const u32 v = A.verts[i];
-    const u64 o0 = A.off[v], o1 = A.off[v + 1];
-    const u64 deg = o1 - o0;
-    const u32 fv = A.f[v];
-    const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
-    const double kv = A.kdeg[v];
-    if (lane == 0) my_trav += deg;
-    double wcur = 0.0;
-    double best_g = 0.0;
-    u32 best_pos = NONE32, best_key = cur;
-    if (deg <= SMALL_DEG) {
-      // One chunk: groups of lanes with equal key; the lowest lane is the
-      // first CSR occurrence, and the leader sums its group in lane order.
-      u32 key = NONE32;
-      double wv = 0.0;
-      bool has = false;
-      if (lane < deg) {
-        u32 nb = A.col[o0 + lane];
-        wv = A.w[o0 + lane];
-        has = entry_key<KIND>(A, v, nb, fv, key);
-        if (!has) key = NONE32;
-      }
-      s_w[wib][lane] = wv;
-      __syncwarp();
-      u32 grp = __match_any_sync(0xffffffffu, key);
-      bool leader = has && lane == (u32)(__ffs(grp) - 1);
-      double sum = 0.0;
-      if (leader)
-        for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, s_w[wib][__ffs(m) - 1]);
-      u32 cl = __ballot_sync(0xffffffffu, leader && key == cur);
-      if (cl) wcur = __shfl_sync(0xffffffffu, sum, __ffs(cl) - 1);
-      double g = -1.0;
-      u32 p = NONE32;
-      if (leader && key != cur && A.tw != 0.0) {
-        bool blk = (KIND == EVAL_REFINE) && A.blocked[key];
-        if (!blk) {
-          g = move_gain(sum, wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
-          p = lane;
-          ++my_cand;
-        }
-      }
-      u32 kk = key;
-      if (p == NONE32) g = -1.0;
-      warp_best(g, p, kk);
-      if (p != NONE32 && g > 0.0) {
-        best_g = g;
-        best_key = kk;
-        best_pos = p;
-      }
-      __syncwarp();
-    } else {
-      // Hash table: shared memory for mid degrees, a private global region
-      // for high-degree vertices.  Chunks are processed in CSR order and each
-      // key's sum is extended serially, preserving the reference's rounding.
-      u32* tk;
-      u32* tp;
-      double* tv;
-      u32 cap;
-      if (deg <= MID_DEG) {
-        tk = s_key[wib];
-        tp = s_pos[wib];
-        tv = s_val[wib];
-        cap = WARP_TAB;
-      } else {
-        u64 base = A.tab_off[i];
-        tk = A.tkey + base;
-        tp = A.tpos + base;
-        tv = A.tval + base;
-        cap = 2;
-        while (cap < 2 * deg) cap <<= 1;
-      }
-      const u32 mask = cap - 1;
-      for (u32 t = lane; t < cap; t += 32) tk[t] = NONE32;
-      __syncwarp();
-      for (u64 base = o0; base < o1; base += 32) {
-        u64 q = base + lane;
-        u32 key = NONE32;
-        double wv = 0.0;
-        bool has = false;
-        if (q < o1) {
-          u32 nb = A.col[q];
-          wv = A.w[q];
-          has = entry_key<KIND>(A, v, nb, fv, key);
-          if (!has) key = NONE32;
-        }
-        s_w[wib][lane] = wv;
-        __syncwarp();
-        u32 grp = __match_any_sync(0xffffffffu, key);
-        if (has && lane == (u32)(__ffs(grp) - 1)) {
-          u32 slot = hash32(key) & mask;
-          while (true) {
-            u32 prev = atomicCAS(&tk[slot], NONE32, key);
-            if (prev == NONE32) {
-              tp[slot] = (u32)(q - o0);
-              double sum = 0.0;
-              for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, s_w[wib][__ffs(m) - 1]);
-              tv[slot] = sum;
-              break;
-            }
-            if (prev == key) {
-              double sum = tv[slot];
-              for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, s_w[wib][__ffs(m) - 1]);
-              tv[slot] = sum;
-              break;
-            }
-            slot = (slot + 1) & mask;
-          }
-        }
-        __syncwarp();
-      }
-      // w(v, cur)
-      for (u32 t = lane; t < cap; t += 32)
-        if (tk[t] == cur) wcur = tv[t];
-      for (int o = 16; o; o >>= 1) {
-        double x = __shfl_xor_sync(0xffffffffu, wcur, o);
-        if (x != 0.0) wcur = x;
-      }
-      double g = -1.0;
-      u32 p = NONE32, kk = cur;
-      if (A.tw != 0.0) {
-        for (u32 t = lane; t < cap; t += 32) {
-          u32 key = tk[t];
-          if (key == NONE32 || key == cur) continue;
-          if (KIND == EVAL_REFINE && A.blocked[key]) continue;
-          double gn = move_gain(tv[t], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
-          ++my_cand;
-          u32 pp = tp[t];
-          if (p == NONE32 || gn > g || (gn == g && pp < p)) {
-            g = gn;
-            p = pp;
-            kk = key;
-          }
-        }
-      }
-      if (p == NONE32) g = -1.0;
-      warp_best(g, p, kk);
-      if (p != NONE32 && g > 0.0) {
-        best_g = g;
-        best_key = kk;
-        best_pos = p;
-      }
-      __syncwarp();
-    }
-    if (lane == 0) {
-      u32 to = best_key;
-      double g = best_g;
-      if (KIND == EVAL_MOVE && A.allow_empty && A.tw != 0.0) {
-        double eg = empty_gain(wcur, A.tw, A.gamma, kv, A.d[cur]);
-        if (eg > g) {
-          g = eg;
-          to = A.n + v;
-        }
-      }
-      (void)best_pos;
-      A.out_to[i] = to;
-      A.out_gain[i] = g;
-    }
-  }
-  if (A.traversed) {
-    if (lane == 0 && my_trav) atomicAdd(&s_trav, my_trav);
-    if (my_cand) atomicAdd(&s_cand, my_cand);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      if (s_trav) atomicAdd(&A.traversed[0], s_trav);
-      if (s_cand) atomicAdd(&A.traversed[1], s_cand);
-    }
-  }
-}
-
-__global__ void k_big_caps(const u32* verts, u32 nv, const u64* off, u64* cap) {
-  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < nv; i += (u64)gridDim.x * blockDim.x) {
-    u32 v = verts[i];
-    u64 deg = off[v + 1] - off[v];
-    u64 c = 0;
-    if (deg > MID_DEG) {
-      c = 2;
-      while (c < 2 * deg) c <<= 1;
-    }
-    cap[i] = c;
-  }
-}
-
-// Runs the evaluation kernel over `verts`; fills out_to / out_gain.
-void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
-              const double* d, const u8* blocked, bool allow_empty, u32* out_to, double* out_gain,
-              unsigned long long* traversed) {
-  if (!nv) return;
-  cudaStream_t st = E.stream;
-  Scratch& S = E.sc;
-  S.gkey.ensure(E.mem, (size_t)nv + 1);
-  ++E.nlaunch, k_big_caps<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.gkey.p);
-  HL_CUDA(cudaMemsetAsync(S.gkey.p + nv, 0, sizeof(u64), st));
-  HL_LAUNCH_CHECK();
-  u64* a = S.gkey.p;
-  S.gkey2.ensure(E.mem, (size_t)nv + 1);
-  u64* o = S.gkey2.p;
-  cub_run(E, [&](void* t, size_t& b) {
-    return cub::DeviceScan::ExclusiveSum(t, b, a, o, (int64_t)nv + 1, st);
-  });
-  u64 total = E.read_u64(o + nv);
-  DBuf<u32> tk, tp;
-  DBuf<double> tv;
-  if (total) {
-    S.res.ensure(E.mem, 1);
-    tk.ensure(E.mem, total);
-    tp.ensure(E.mem, total);
-    tv.ensure(E.mem, total);
-  }
-  EvalArgs A;
-  A.verts = verts;
-  A.nv = nv;
-  A.off = L.g.off.p;
-  A.col = L.g.col.p;
-  A.w = L.g.w.p;
-  A.f = L.f.p;
-  A.s = s;
-  A.d = d;
-  A.kdeg = L.k.p;
-  A.blocked = blocked;
-  A.tw = L.tw;
-  A.gamma = E.cfg.resolution;
-  A.n = L.g.n;
-  A.allow_empty = allow_empty;
-  A.out_to = out_to;
-  A.out_gain = out_gain;
-  A.tab_off = o;
-  A.tkey = tk.p;
-  A.tpos = tp.p;
-  A.tval = tv.p;
-  A.traversed = traversed;
-  u32 blocks = grid_for((u64)nv * 32, WARPS_PER_BLOCK * 32);
-  cudaEvent_t ev = E.kt_begin();
-  if (kind == EVAL_MOVE)
-    ++E.nlaunch, k_eval<EVAL_MOVE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(A);
-  else
-    ++E.nlaunch, k_eval<EVAL_REFINE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(A);
-  HL_LAUNCH_CHECK();
-  E.kt_end(kind == EVAL_MOVE ? KT_MOVE_EVAL : KT_REFINE_EVAL, ev);
-  if (total) {
-    tk.release();
-    tp.release();
-    tv.release();
-  }
-}
 
 // ----------------------------------------------------------------------------
 // Decoupled selection (throughput.rs:204-236) by deterministic reservations.
@@ -661,20 +334,25 @@ __global__ void k_dops(u32 M, const u8* status, const u32* sel_from, const u32* 
   }
 }
 
+// d[c] - k1 + k2 ... in selected order (a - b is a + (-b) exactly).
 __global__ void k_apply_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 total,
                                 const u32* ops, const u32* sel_node, const double* kdeg,
                                 double* d) {
-  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < nu; j += (u64)gridDim.x * blockDim.x) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 j = warp; j < nu; j += nwarps) {
     u32 c = ukeys[j];
     if (c == NONE32) continue;
     u32 a = ustart[j], b = (j + 1 < nu) ? ustart[j + 1] : total;
-    double x = d[c];
-    for (u32 t = a; t < b; ++t) {
-      u32 op = ops[t];
-      double kv = kdeg[sel_node[op >> 1]];
-      x = (op & 1) ? __dadd_rn(x, kv) : __dsub_rn(x, kv);
-    }
-    d[c] = x;
+    double x = warp_ordered_sum(a, b, d[c],
+                                [&](u64 t) {
+                                  u32 op = ops[t];
+                                  double kv = kdeg[sel_node[op >> 1]];
+                                  return (op & 1) ? kv : -kv;
+                                },
+                                [](u64) { return true; });
+    if (lane == 0) d[c] = x;
   }
 }
 
@@ -866,7 +544,7 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
       });
       u32 nu = E.read_u32(sid + M2 - 1) + E.read_u32(h + M2 - 1);
       ++E.nlaunch, k_seg_compact<<<grid_for(M2), 256, 0, st>>>(h, sid, ko, M2, S.rowlist.p, S.seg_start.p);
-      ++E.nlaunch, k_apply_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, M2, vo,
+      ++E.nlaunch, k_apply_ordered<<<grid_for((u64)nu * 32), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, M2, vo,
                                                     S.sel_node.p, L.k.p, S.d.p);
       HL_LAUNCH_CHECK();
     }

@@ -191,17 +191,20 @@ __global__ void k_wsp_atomic(u32 n, const u64* off, const u32* col, const double
 __global__ void k_wsp_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 total,
                               const u32* members, const u64* off, const u32* col, const double* w,
                               const u32* f, const u32* minmem, double* wsp) {
-  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < nu; j += (u64)gridDim.x * blockDim.x) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 j = warp; j < nu; j += nwarps) {
     u32 S = ukeys[j];
     u32 a = ustart[j], b = (j + 1 < nu) ? ustart[j + 1] : total;
     u32 parent = f[minmem[S]];
     double x = 0.0;
     for (u32 t = a; t < b; ++t) {
       u32 v = members[t];
-      for (u64 p = off[v]; p < off[v + 1]; ++p)
-        if (f[col[p]] == parent) x = __dadd_rn(x, w[p]);
+      x = warp_ordered_sum(off[v], off[v + 1], x, [&](u64 p) { return w[p]; },
+                           [&](u64 p) { return f[col[p]] == parent; });
     }
-    wsp[S] = x;
+    if (lane == 0) wsp[S] = x;
   }
 }
 
@@ -426,7 +429,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
       });
       u32 nu = E.read_u32(sid + nm - 1) + E.read_u32(h + nm - 1);
       ++E.nlaunch, k_seg_compact_b<<<grid_for(nm), 256, 0, st>>>(h, sid, ko, nm, S.rowlist.p, S.seg_start.p);
-      ++E.nlaunch, k_wsp_ordered<<<grid_for(nu), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, nm, vo,
+      ++E.nlaunch, k_wsp_ordered<<<grid_for((u64)nu * 32), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, nm, vo,
                                                   L.g.off.p, L.g.col.p, L.g.w.p, L.f.p,
                                                   S.minmem.p, S.wsp.p);
       HL_LAUNCH_CHECK();

@@ -280,3 +280,47 @@ def test_canonicalize_gpu():
     assert hl.canonicalize_community_ids([5, 5, 3, 3, 7]).tolist() == [0, 0, 1, 1, 2]
     x = np.random.default_rng(1).integers(0, 1000, 100000)
     assert np.array_equal(hl.canonicalize_community_ids(x), O.canonicalize(x))
+
+
+# ---- very high degree vertices (block kernel, shared and global tables) -----
+@pytest.mark.parametrize("integral", [True, False])
+@pytest.mark.parametrize("hub_deg", [300, 3000, 6000])
+def test_move_eval_hubs_bit_exact(integral, hub_deg):
+    rng = np.random.default_rng(hub_deg)
+    n = 9000
+    src, dst, w = gh.random_graph(rng, n, 20000, integral)
+    hs = np.zeros(hub_deg, np.uint32)
+    hd = rng.choice(np.arange(1, n), hub_deg, replace=False).astype(np.uint32)
+    hw = rng.integers(1, 3, hub_deg).astype(float) if integral else rng.uniform(0.5, 2, hub_deg)
+    g = O.Graph.from_edges(n, np.concatenate([src, hs]), np.concatenate([dst, hd]),
+                           np.concatenate([w, hw])).apply_delta([], [], [], keep_self_loops=True)
+    k = g.degrees()
+    tw = O.tree_sum(k)
+    for ncomm in [5, 400, 4000]:
+        f = gh.random_partition(rng, n, ncomm)
+        d = np.zeros(2 * n + 2)
+        np.add.at(d, f, k)
+        verts = np.arange(0, n, 7, dtype=np.uint32)
+        to_o, g_o = O.move_eval(g, f, d, k, tw, 1.0, verts)
+        to_g, g_g = gh.move_eval(g, f, d, k, tw, 1.0, verts)
+        assert gh.same_bits(g_o, g_g)
+        pos = g_o > 0
+        assert np.array_equal(to_o[pos], to_g[pos])
+
+
+@pytest.mark.parametrize("integral", [True, False])
+def test_inc_refinement_hub_bit_exact(integral):
+    rng = np.random.default_rng(7)
+    n = 7000
+    src, dst, w = gh.random_graph(rng, n, 15000, integral)
+    hd = rng.choice(np.arange(1, n), 5000, replace=False).astype(np.uint32)
+    hw = np.ones(5000) if integral else rng.uniform(0.5, 2, 5000)
+    g = O.Graph.from_edges(n, np.concatenate([src, np.zeros(5000, np.uint32)]),
+                           np.concatenate([dst, hd]), np.concatenate([w, hw])
+                           ).apply_delta([], [], [], keep_self_loops=True)
+    f = gh.random_partition(rng, n, 3)
+    s0 = np.arange(n, dtype=np.uint32)
+    aff = np.ones(n, bool)
+    ref_s, ref_r = O.inc_refinement(g, f, s0, aff, 1.0, O.MODE_THROUGHPUT)
+    gs, gr = gh.inc_refinement(g, f, s0, aff, 1.0)
+    assert np.array_equal(ref_s, gs) and np.array_equal(ref_r, gr)
