@@ -328,11 +328,12 @@ def main():
         tot_ms = float(t.item())
     value = world * K * k / (tot_ms / 1000.0)
 
-    kst = (L.KernelStat * 8)()
+    kst = (L.KernelStat * 32)()
     cnt = C.c_uint32()
-    L.check(L.lib.hl_kernel_stats(h, kst, 8, C.byref(cnt)))
+    L.check(L.lib.hl_kernel_stats(h, kst, 32, C.byref(cnt)))
     kernels = {kst[i].name.decode(): {"launches": kst[i].launches, "ms": kst[i].total_ms,
-                                      "bytes": kst[i].bytes} for i in range(cnt.value)}
+                                      "bytes": kst[i].bytes, "items": kst[i].items}
+               for i in range(cnt.value)}
 
     # end to end through the host API
     e2e_s = []

@@ -32,7 +32,7 @@ HL_FLAG_KERNEL_TIMING = 1 << 2
 
 class KernelStat(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint64), ("total_ms", C.c_double),
-                ("bytes", C.c_uint64)]
+                ("bytes", C.c_uint64), ("items", C.c_uint64)]
 
 
 class Config(C.Structure):

@@ -198,10 +198,16 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
   u32 cur_n = E.levels[0].g.n;
   for (u32 p = 0; p < P; ++p) {
     Level& L = E.levels[p];
+    cudaEvent_t e0 = E.kt_begin();
     apply_delta(E, L, cur, cur_n > L.g.n ? cur_n : L.g.n, true);
+    E.kt_end(KT_STAGE_APPLY, e0);
+    e0 = E.kt_begin();
     MoveOut mo = inc_movement(E, L, cur, cur.k == 0, true);
+    E.kt_end(KT_STAGE_MOVE, e0);
     if (p == 0) st.changed = count_flags(E, E.sc.changed.p, L.g.n);
+    e0 = E.kt_begin();
     RefineOut ro = inc_refinement(E, L, true);
+    E.kt_end(KT_STAGE_REFINE, e0);
     st.iterations += mo.iterations;
     st.moves += mo.moves;
     st.candidates += mo.candidates;
@@ -231,7 +237,9 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
       continue;
     }
     u32 nn = 0;
+    e0 = E.kt_begin();
     u64 cnt = inc_aggregation(E, L, cur, &nn, true, true);
+    E.kt_end(KT_STAGE_AGGREGATE, e0);
     int slot = (p + 1) & 1;
     B.bb.xu[slot].ensure(E.mem, cnt ? cnt : 1);
     B.bb.xv[slot].ensure(E.mem, cnt ? cnt : 1);
@@ -436,8 +444,11 @@ hl_status hl_apply_batch_device(hl_graph* g, const uint32_t* src, const uint32_t
   HL_TRY(apply_impl(g, src, dst, w, k, true, stats));
 }
 
-static const char* kernel_names[KT_COUNT] = {"move_eval", "refine_eval", "select_decoupled",
-                                             "csr_merge_rows", "aggregate_compress"};
+static const char* kernel_names[KT_COUNT] = {
+    "move_eval",   "refine_eval", "select_decoupled", "csr_merge_rows", "aggregate_compress",
+    "eval_small",  "eval_mid",    "eval_big",         "comm_degrees",   "apply_and_mark",
+    "refine_cc",   "t_filter",    "row_sums",         "delta_resolve",  "stage_apply",
+    "stage_move",  "stage_refine", "stage_aggregate"};
 
 hl_status hl_kernel_stats(const hl_graph* g, hl_kernel_stat* out, uint32_t cap, uint32_t* count) {
   HL_TRY(require(g && count, "NULL argument"); Engine& E = *const_cast<EngineBox*>(box(g))->E;
@@ -447,6 +458,7 @@ hl_status hl_kernel_stats(const hl_graph* g, hl_kernel_stat* out, uint32_t cap, 
            out[i].launches = E.kagg[i].launches;
            out[i].total_ms = E.kagg[i].ms;
            out[i].bytes = E.kagg[i].bytes;
+           out[i].items = E.kagg[i].items;
          });
 }
 

@@ -307,6 +307,121 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
 }
 
 // ---------------------------------------------------------------------------
+// Wide degrees (MID_MAX < deg <= WIDE_MAX): a warp per vertex.  The warp
+// issues the loads of up to 8 chunks (256 entries) at once, then folds the
+// chunks in CSR order into a table kept in a per-warp global region (hot in
+// L2).  The scan that picks the best key also resets every used slot, so a
+// region is clean for the warp's next vertex without a clearing pass.
+// ---------------------------------------------------------------------------
+constexpr u32 WIDE_MAX = 4096;
+constexpr u32 WIDE_TAB = 2 * WIDE_MAX;  // entries of one warp's region
+constexpr u32 WIDE_WARPS = 8;
+constexpr u32 WIDE_BATCH = 8;  // chunks loaded before folding
+
+template <int KIND>
+__global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
+  __shared__ double s_w[WIDE_WARPS][WIDE_BATCH * 32];
+  const u32 lane = threadIdx.x & 31;
+  const u32 wib = threadIdx.x >> 5;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  unsigned long long trav = 0, ncand = 0;
+  u32* tk = A.tkey + warp * (u64)WIDE_TAB;
+  u32* tp = A.tpos + warp * (u64)WIDE_TAB;
+  double* tv = A.tval + warp * (u64)WIDE_TAB;
+  double* sw = s_w[wib];
+  for (u64 t = warp; t < A.nidx; t += nwarps) {
+    const u32 i = A.idx[t];
+    const u32 v = A.verts[i];
+    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u64 deg = o1 - o0;
+    const u32 fv = A.f[v];
+    const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+    const double kv = A.kdeg[v];
+    if (lane == 0) trav += deg;
+    u32 cap = 64;
+    while (cap < 2 * deg) cap <<= 1;
+    const u32 mask = cap - 1;
+    for (u64 b0 = o0; b0 < o1; b0 += WIDE_BATCH * 32) {
+      u32 key[WIDE_BATCH];
+#pragma unroll
+      for (u32 j = 0; j < WIDE_BATCH; ++j) {
+        u64 q = b0 + j * 32 + lane;
+        key[j] = NONE32;
+        double wv = 0.0;
+        if (q < o1) {
+          u32 nb = A.col[q];
+          wv = A.w[q];
+          if (!entry_key<KIND>(A, v, nb, fv, key[j])) key[j] = NONE32;
+        }
+        sw[j * 32 + lane] = wv;
+      }
+      __syncwarp();
+#pragma unroll
+      for (u32 j = 0; j < WIDE_BATCH; ++j) {
+        if (b0 + j * 32 >= o1) break;
+        u32 grp = __match_any_sync(0xffffffffu, key[j]);
+        if (key[j] != NONE32 && lane == (u32)(__ffs(grp) - 1)) {
+          u32 slot = hash32(key[j]) & mask;
+          u32 prev;
+          while (true) {
+            prev = atomicCAS(&tk[slot], NONE32, key[j]);
+            if (prev == NONE32 || prev == key[j]) break;
+            slot = (slot + 1) & mask;
+          }
+          double acc = prev == NONE32 ? 0.0 : tv[slot];
+          for (u32 m = grp; m; m &= m - 1) acc = __dadd_rn(acc, sw[j * 32 + __ffs(m) - 1]);
+          tv[slot] = acc;
+          if (prev == NONE32) tp[slot] = (u32)(b0 + j * 32 + lane - o0);
+        }
+        __syncwarp();
+      }
+    }
+    // w(v, cur), then the argmax; every used slot is reset on the way.
+    double wcur = 0.0;
+    bool found = false;
+    for (u32 x = lane; x < cap; x += 32)
+      if (tk[x] == cur) {
+        wcur = tv[x];
+        found = true;
+      }
+    u32 fm = __ballot_sync(0xffffffffu, found);
+    wcur = __shfl_sync(0xffffffffu, wcur, fm ? __ffs(fm) - 1 : 0);
+    if (!fm) wcur = 0.0;
+    double g = -1.0;
+    u32 p = NONE32, kk = cur;
+    for (u32 x = lane; x < cap; x += 32) {
+      u32 key = tk[x];
+      if (key == NONE32) continue;
+      tk[x] = NONE32;
+      if (key == cur || A.tw == 0.0) continue;
+      if (KIND == EVAL_REFINE && A.blocked[key]) continue;
+      double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
+      ++ncand;
+      u32 pp = tp[x];
+      if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+        g = gn;
+        p = pp;
+        kk = key;
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      double og = __shfl_xor_sync(0xffffffffu, g, o);
+      u32 op = __shfl_xor_sync(0xffffffffu, p, o);
+      u32 ok = __shfl_xor_sync(0xffffffffu, kk, o);
+      if (op != NONE32 && (p == NONE32 || og > g || (og == g && op < p))) {
+        g = og;
+        p = op;
+        kk = ok;
+      }
+    }
+    if (lane == 0) finish<KIND>(A, i, v, cur, kv, wcur, g, kk, p != NONE32);
+    __syncwarp();
+  }
+  block_count(A, trav, ncand);
+}
+
+// ---------------------------------------------------------------------------
 // Large degrees: a block per vertex, adjacency staged in shared tiles.
 // ---------------------------------------------------------------------------
 template <int KIND, u32 TAB>
@@ -473,7 +588,7 @@ __global__ void k_bin(const u32* verts, u32 nv, const u64* off, u32* bin, u32* i
     u32 v = verts[i];
     u64 deg = off[v + 1] - off[v];
     u32 b = deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= MID_MAX ? 3
-          : 2 * deg <= BIG1_TAB ? 4 : 5;
+          : deg <= WIDE_MAX ? 4 : 5;
     bin[i] = b;
     idx[i] = (u32)i;
     atomicAdd(&sc[b], 1u);
@@ -607,9 +722,15 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
       else ++E.nlaunch, k_eval_small<EVAL_REFINE, 32><<<blocks, 256, 0, st>>>(a);
     }
   };
+  cudaEvent_t e_s = E.kt_begin();
   launch_small(0);
   launch_small(1);
   launch_small(2);
+  E.kt_end(KT_EVAL_SMALL, e_s);
+  E.kagg[KT_EVAL_SMALL].items += (u64)c[0] + c[1] + c[2];
+  E.kagg[KT_EVAL_MID].items += c[3];
+  E.kagg[KT_EVAL_BIG].items += (u64)c[4] + c[5];
+  cudaEvent_t e_m = E.kt_begin();
   if (c[3]) {
     EvalArgs a = A;
     a.idx = vo + start[3];
@@ -621,6 +742,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
       ++E.nlaunch, k_eval_mid<EVAL_REFINE><<<blocks, MID_WARPS * 32, 0, st>>>(a);
   }
   HL_LAUNCH_CHECK();
+  E.kt_end(KT_EVAL_MID, e_m);
   auto launch_big = [&](int b) {
     if (!c[b]) return;
     EvalArgs a = A;
@@ -647,8 +769,32 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
     }
     HL_LAUNCH_CHECK();
   };
-  launch_big(4);
+  cudaEvent_t e_b = E.kt_begin();
+  if (c[4]) {
+    EvalArgs a = A;
+    a.idx = vo + start[4];
+    a.nidx = c[4];
+    u32 blocks = grid_for((u64)c[4] * 32, WIDE_WARPS * 32);
+    if (blocks > 148u * 4u) blocks = 148u * 4u;
+    const u64 warps = (u64)blocks * WIDE_WARPS;
+    const size_t need = warps * (size_t)WIDE_TAB;
+    if (S.wide_key.cap < need) {
+      S.wide_key.ensure(E.mem, need);
+      S.wide_pos.ensure(E.mem, need);
+      S.wide_val.ensure(E.mem, need);
+      HL_CUDA(cudaMemsetAsync(S.wide_key.p, 0xFF, sizeof(u32) * S.wide_key.cap, st));
+    }
+    a.tkey = S.wide_key.p;
+    a.tpos = S.wide_pos.p;
+    a.tval = S.wide_val.p;
+    if (kind == EVAL_MOVE)
+      ++E.nlaunch, k_eval_wide<EVAL_MOVE><<<blocks, WIDE_WARPS * 32, 0, st>>>(a);
+    else
+      ++E.nlaunch, k_eval_wide<EVAL_REFINE><<<blocks, WIDE_WARPS * 32, 0, st>>>(a);
+    HL_LAUNCH_CHECK();
+  }
   launch_big(5);
+  E.kt_end(KT_EVAL_BIG, e_b);
   E.kt_end(kind == EVAL_MOVE ? KT_MOVE_EVAL : KT_REFINE_EVAL, ev);
 }
 

@@ -419,6 +419,7 @@ double tree_sum(Engine& E, const double* x, u64 n) {
 
 static void recompute_rows(Engine& E, Level& L, const u32* rows, u32 nr) {
   if (!nr) return;
+  cudaEvent_t ev = E.kt_begin();
   if (E.integral)
     ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p,
                                                                   L.k.p);
@@ -426,6 +427,7 @@ static void recompute_rows(Engine& E, Level& L, const u32* rows, u32 nr) {
     ++E.nlaunch, k_row_sum_serial<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p,
                                                                                L.g.w.p, L.k.p);
   HL_LAUNCH_CHECK();
+  E.kt_end(KT_ROW_SUMS, ev);
 }
 
 void recompute_all_degrees(Engine& E, Level& L) {
@@ -462,6 +464,7 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   HL_CUDA(cudaMemsetAsync(S.cnt.p, 0, 16 * sizeof(u32), st));  // [0] ins loops [1] del loops [2] drops
 
   u32 U = 0;
+  cudaEvent_t ev_ds = E.kt_begin();
   if (k) {
     S.keys.ensure(E.mem, k);
     S.keys2.ensure(E.mem, k);
@@ -515,6 +518,7 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
       return cub::DeviceScan::ExclusiveSum(t, bytes, ni, pi, (int64_t)U + 1, st);
     });
   }
+  E.kt_end(KT_DELTA_SORT, ev_ds);
   u64 n_del_keys = U ? E.read_u32(S.pos_del.p + U) : 0;
   u64 n_ins = U ? E.read_u32(S.pos_ins.p + U) : 0;
 

@@ -75,6 +75,9 @@ struct Scratch {
   DBuf<double> red, red2;
   DBuf<u64> red64;
   DBuf<u32> origin;
+  // per-warp hash regions of the wide evaluation kernel (kept clean by it)
+  DBuf<u32> wide_key, wide_pos;
+  DBuf<double> wide_val;
 };
 
 // Per-kernel device timing (CUDA events on the engine's stream), enabled by
@@ -83,6 +86,7 @@ struct KernelAgg {
   u64 launches = 0;
   double ms = 0.0;
   u64 bytes = 0;
+  u64 items = 0;  // vertices / records processed, where meaningful
 };
 enum KernelId : int {
   KT_MOVE_EVAL = 0,
@@ -90,6 +94,19 @@ enum KernelId : int {
   KT_SELECT,
   KT_MERGE_ROWS,
   KT_AGGREGATE,
+  KT_EVAL_SMALL,   // sub-warp bins (both evaluation kinds)
+  KT_EVAL_MID,     // warp-per-vertex bin
+  KT_EVAL_BIG,     // block-per-vertex bins
+  KT_COMM_DEG,     // per-community / per-sub-community degree sums
+  KT_MARK_NEXT,    // accepted-move application and frontier marking
+  KT_REFINE_CC,    // connected components of affected sub-communities
+  KT_TFILTER,      // T-filter sums and decisions
+  KT_ROW_SUMS,     // vertex degrees of touched rows
+  KT_DELTA_SORT,   // batch key sort and resolution in apply_delta
+  KT_STAGE_APPLY,  // whole stages of the level loop (including host waits)
+  KT_STAGE_MOVE,
+  KT_STAGE_REFINE,
+  KT_STAGE_AGGREGATE,
   KT_COUNT
 };
 

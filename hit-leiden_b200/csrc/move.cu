@@ -103,7 +103,17 @@ __global__ void k_seg_compact(const u32* head, const u32* segid, const u32* sk, 
 }
 
 // d[c] for every c in [0, ncomm_cap): zeroed, then filled from `part`.
+static void recompute_comm_degrees_impl(Engine& E, Level& L, const u32* part, u32 ncomm_cap,
+                                        double* d);
+
 void recompute_comm_degrees(Engine& E, Level& L, const u32* part, u32 ncomm_cap, double* d) {
+  cudaEvent_t ev = E.kt_begin();
+  recompute_comm_degrees_impl(E, L, part, ncomm_cap, d);
+  E.kt_end(KT_COMM_DEG, ev);
+}
+
+static void recompute_comm_degrees_impl(Engine& E, Level& L, const u32* part, u32 ncomm_cap,
+                                        double* d) {
   cudaStream_t st = E.stream;
   u32 n = L.g.n;
   HL_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * (size_t)ncomm_cap, st));
@@ -509,6 +519,7 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
                                               S.sel_node.p, S.sel_from.p, S.sel_to.p);
     HL_LAUNCH_CHECK();
     select_decoupled_dev(E, M);
+    cudaEvent_t ev_mark = E.kt_begin();
     HL_CUDA(cudaMemsetAsync(cnt + 7, 0, sizeof(u32), st));
     ++E.nlaunch, k_apply_moves<<<grid_for(M), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_from.p,
                                                S.sel_to.p, L.f.p, L.k.p, S.d.p, E.integral,
@@ -556,6 +567,7 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
                                                         L.g.off.p, L.g.col.p, L.f.p, L.s_cur.p,
                                                         S.next.p, S.affected.p);
     HL_LAUNCH_CHECK();
+    E.kt_end(KT_MARK_NEXT, ev_mark);
     S.active.swap(S.next);
   }
   out.iterations = it;

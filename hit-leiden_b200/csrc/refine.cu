@@ -289,6 +289,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   u32* s = L.s_cur.p;
 
   // ---- 1. connected-component split of affected sub-communities ----------
+  cudaEvent_t ev_cc = E.kt_begin();
   u32 smax = reduce_max_u32(E, s, n, cnt + 12);
   out.smax_before = smax;
   const size_t scap = (size_t)smax + 2 + n;
@@ -341,6 +342,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
     for (u32 i = 0; i < m_new; ++i) E.new_ids[i] = {a[i], b[i]};
   }
   out.splits = m_new;
+  E.kt_end(KT_REFINE_CC, ev_cc);
 
   // is_initial (hit_leiden.rs:1333-1339): s is the identity ⇒ R = all.
   HL_CUDA(cudaMemsetAsync(cnt + 5, 0, sizeof(u32), st));
@@ -381,6 +383,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   u32* single = S.cand_idx.p;
 
   // ---- 4. T-filter --------------------------------------------------------
+  cudaEvent_t ev_tf = E.kt_begin();
   S.cand_sc.ensure(E.mem, s2cap);
   S.blocked.ensure(E.mem, s2cap);
   S.minmem.ensure(E.mem, s2cap);
@@ -439,6 +442,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
                                              L.f.p, S.dcomm.p, L.tw, E.cfg.resolution,
                                              S.blocked.p);
   HL_LAUNCH_CHECK();
+  E.kt_end(KT_TFILTER, ev_tf);
 
   // ---- 5. Jacobi singleton merge -------------------------------------------
   S.cand_to.ensure(E.mem, ns);

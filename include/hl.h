@@ -104,7 +104,8 @@ typedef struct {
   char name[32];
   uint64_t launches;
   double total_ms;
-  uint64_t bytes;
+  uint64_t bytes;   /* algorithmic bytes, where counted            */
+  uint64_t items;   /* vertices / records processed, where counted */
 } hl_kernel_stat;
 
 typedef struct hl_graph hl_graph;

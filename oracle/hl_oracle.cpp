@@ -34,6 +34,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -1102,6 +1104,16 @@ static u32 hit_leiden_ml(State& st, const std::vector<Edge>& delta, double gamma
         for (uint8_t c : mo.changed) stats->changed += c;
         for (uint8_t c : ro.refined) stats->refined += c;
       }
+    }
+    if (std::getenv("HL_ORACLE_TRACE")) {
+      u64 nr = 0;
+      for (uint8_t c : ro.refined) nr += c;
+      std::fprintf(stderr, "level %u n=%u nnz=%llu delta=%zu rounds=%u moves=%llu traversed=%llu "
+                   "splits=%llu merges=%llu refined=%llu\n", p, st.sg[p].n,
+                   (unsigned long long)st.sg[p].col.size(), cur.size(), mo.iterations,
+                   (unsigned long long)mo.rounds_moves, (unsigned long long)mo.traversed,
+                   (unsigned long long)ro.splits, (unsigned long long)ro.merges,
+                   (unsigned long long)nr);
     }
     if (p + 1 >= P) break;
     // M6: new level-(p+1) nodes inherit the state of the node they split from.
