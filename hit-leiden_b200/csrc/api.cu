@@ -446,7 +446,8 @@ hl_status hl_apply_batch_device(hl_graph* g, const uint32_t* src, const uint32_t
 
 static const char* kernel_names[KT_COUNT] = {
     "move_eval",   "refine_eval", "select_decoupled", "csr_merge_rows", "aggregate_compress",
-    "eval_small",  "eval_mid",    "eval_big",         "comm_degrees",   "apply_and_mark",
+    "eval_small",  "eval_mid",    "eval_wide",        "eval_huge",      "comm_degrees",
+    "apply_and_mark",
     "refine_cc",   "t_filter",    "row_sums",         "delta_resolve",  "stage_apply",
     "stage_move",  "stage_refine", "stage_aggregate"};
 

@@ -646,8 +646,9 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   u32 start[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int b = 0; b < 6; ++b) start[b + 1] = start[b] + c[b];
   // Global tables for vertices above the largest shared table.
-  DBuf<u32> tk, tp;
-  DBuf<double> tv;
+  DBuf<u32>& tk = S.huge_key;
+  DBuf<u32>& tp = S.huge_pos;
+  DBuf<double>& tv = S.huge_val;
   u64* tab_off = nullptr;
   if (c[5]) {
     S.gkey.ensure(E.mem, (size_t)c[5] + 1);
@@ -707,6 +708,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   auto launch_small = [&](int b) {
     if (!c[b]) return;
     EvalArgs a = A;
+    a.counters = counters ? counters : nullptr;
     a.idx = vo + start[b];
     a.nidx = c[b];
     u32 G = b == 0 ? 8 : b == 1 ? 16 : 32;
@@ -729,10 +731,12 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   E.kt_end(KT_EVAL_SMALL, e_s);
   E.kagg[KT_EVAL_SMALL].items += (u64)c[0] + c[1] + c[2];
   E.kagg[KT_EVAL_MID].items += c[3];
-  E.kagg[KT_EVAL_BIG].items += (u64)c[4] + c[5];
+  E.kagg[KT_EVAL_BIG].items += c[4];
+  E.kagg[KT_EVAL_HUGE].items += c[5];
   cudaEvent_t e_m = E.kt_begin();
   if (c[3]) {
     EvalArgs a = A;
+    a.counters = counters ? counters + 2 : nullptr;
     a.idx = vo + start[3];
     a.nidx = c[3];
     u32 blocks = grid_for((u64)c[3] * 32, MID_WARPS * 32);
@@ -746,6 +750,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   auto launch_big = [&](int b) {
     if (!c[b]) return;
     EvalArgs a = A;
+    a.counters = counters ? counters + 6 : nullptr;
     a.idx = vo + start[b];
     a.nidx = c[b];
     a.tab_off = b == 5 ? tab_off : nullptr;
@@ -772,12 +777,13 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   cudaEvent_t e_b = E.kt_begin();
   if (c[4]) {
     EvalArgs a = A;
+    a.counters = counters ? counters + 4 : nullptr;
     a.idx = vo + start[4];
     a.nidx = c[4];
     u32 blocks = grid_for((u64)c[4] * 32, WIDE_WARPS * 32);
     if (blocks > 148u * 4u) blocks = 148u * 4u;
-    const u64 warps = (u64)blocks * WIDE_WARPS;
-    const size_t need = warps * (size_t)WIDE_TAB;
+    // regions for the largest grid, allocated once
+    const size_t need = (size_t)148u * 4u * WIDE_WARPS * WIDE_TAB;
     if (S.wide_key.cap < need) {
       S.wide_key.ensure(E.mem, need);
       S.wide_pos.ensure(E.mem, need);
@@ -793,8 +799,10 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
       ++E.nlaunch, k_eval_wide<EVAL_REFINE><<<blocks, WIDE_WARPS * 32, 0, st>>>(a);
     HL_LAUNCH_CHECK();
   }
-  launch_big(5);
   E.kt_end(KT_EVAL_BIG, e_b);
+  cudaEvent_t e_h = E.kt_begin();
+  launch_big(5);
+  E.kt_end(KT_EVAL_HUGE, e_h);
   E.kt_end(kind == EVAL_MOVE ? KT_MOVE_EVAL : KT_REFINE_EVAL, ev);
 }
 

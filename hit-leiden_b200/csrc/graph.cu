@@ -612,8 +612,8 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   }
   u64 nnz_new = E.read_u64(S.newoff.p + n);
   DevGraph& G = L.g;
-  DBuf<u32> ncol;
-  DBuf<double> nw;
+  DBuf<u32>& ncol = G.col2;
+  DBuf<double>& nw = G.w2;
   ncol.ensure(E.mem, nnz_new ? nnz_new : 1);
   nw.ensure(E.mem, nnz_new ? nnz_new : 1);
   cudaEvent_t kev = E.kt_begin();
@@ -632,8 +632,6 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   G.w.swap(nw);
   G.off.swap(S.newoff);
   G.nnz = nnz_new;
-  ncol.release();
-  nw.release();
   {
     u32 ins_loops = E.read_u32(S.cnt.p + 0);
     u32 del_loops = E.read_u32(S.cnt.p + 1);

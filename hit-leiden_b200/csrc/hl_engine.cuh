@@ -15,6 +15,8 @@ struct DevGraph {
   DBuf<u64> off;  // n+1
   DBuf<u32> col;
   DBuf<double> w;
+  DBuf<u32> col2;  // the other half of the double buffer used by apply_delta
+  DBuf<double> w2;
 };
 
 // One hierarchy level (state.rs:19-32): supergraph G^p and its maps.
@@ -78,6 +80,9 @@ struct Scratch {
   // per-warp hash regions of the wide evaluation kernel (kept clean by it)
   DBuf<u32> wide_key, wide_pos;
   DBuf<double> wide_val;
+  // global tables of the block-per-vertex kernel (degrees above 4096)
+  DBuf<u32> huge_key, huge_pos;
+  DBuf<double> huge_val;
 };
 
 // Per-kernel device timing (CUDA events on the engine's stream), enabled by
@@ -96,7 +101,8 @@ enum KernelId : int {
   KT_AGGREGATE,
   KT_EVAL_SMALL,   // sub-warp bins (both evaluation kinds)
   KT_EVAL_MID,     // warp-per-vertex bin
-  KT_EVAL_BIG,     // block-per-vertex bins
+  KT_EVAL_BIG,     // warp-per-vertex wide bin (129..4096)
+  KT_EVAL_HUGE,    // block-per-vertex bin (> 4096)
   KT_COMM_DEG,     // per-community / per-sub-community degree sums
   KT_MARK_NEXT,    // accepted-move application and frontier marking
   KT_REFINE_CC,    // connected components of affected sub-communities

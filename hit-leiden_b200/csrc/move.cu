@@ -12,6 +12,8 @@
 //      every endpoint community whose role is still open;
 //   4. accepted moves are applied, d(C) updated in selected order, and the
 //      next frontier / K set marked.
+#include <cstring>
+
 #include "hl_engine.cuh"
 
 namespace hl {
@@ -474,8 +476,8 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   S.gkey.ensure(E.mem, n);
   S.gkey2.ensure(E.mem, n);
   S.cnt.ensure(E.mem, 16);
-  S.red64.ensure(E.mem, 4);
-  HL_CUDA(cudaMemsetAsync(S.red64.p, 0, 2 * sizeof(u64), st));
+  S.red64.ensure(E.mem, 8);
+  HL_CUDA(cudaMemsetAsync(S.red64.p, 0, 8 * sizeof(u64), st));
   u64 sum_nv = 0;
   u32* cnt = S.cnt.p;
 
@@ -571,12 +573,18 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     S.active.swap(S.next);
   }
   out.iterations = it;
-  out.traversed = E.read_u64(S.red64.p);
+  u64 cnt8[8];
+  HL_CUDA(cudaMemcpyAsync(E.hs.p, S.red64.p, 8 * sizeof(u64), cudaMemcpyDeviceToHost, st));
+  E.sync();
+  std::memcpy(cnt8, E.hs.p, sizeof(cnt8));
+  out.traversed = cnt8[0] + cnt8[2] + cnt8[4] + cnt8[6];
+  u64 ncand = cnt8[1] + cnt8[3] + cnt8[5] + cnt8[7];
   // Algorithmic bytes of the evaluation kernel: per active vertex its list
   // entry, offsets, f, k, d(f) and outputs; per adjacency entry the neighbour,
   // weight and neighbour community; per evaluated candidate its d(C).
-  u64 ncand = E.read_u64(S.red64.p + 1);
   E.kagg[KT_MOVE_EVAL].bytes += 52ull * sum_nv + 16ull * out.traversed + 8ull * ncand;
+  const int bins[4] = {KT_EVAL_SMALL, KT_EVAL_MID, KT_EVAL_BIG, KT_EVAL_HUGE};
+  for (int b = 0; b < 4; ++b) E.kagg[bins[b]].bytes += 16ull * cnt8[2 * b] + 8ull * cnt8[2 * b + 1];
   return out;
 }
 
