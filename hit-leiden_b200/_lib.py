@@ -28,6 +28,7 @@ HL_MAP_COMMUNITY, HL_MAP_REFINED, HL_MAP_SUB_PREVIOUS, HL_MAP_SUB_CURRENT = 0, 1
 HL_FLAG_KEEP_SELF_LOOPS = 1 << 0
 HL_FLAG_BATCH_MODULARITY = 1 << 1
 HL_FLAG_KERNEL_TIMING = 1 << 2
+HL_NOALLOC_MAX_ELEMS = 1 << 28
 
 
 class KernelStat(C.Structure):
@@ -108,6 +109,7 @@ def _load():
                                         C.c_uint64, vp, vp, vp, C.c_int32, C.c_int32, vp, p32, vp,
                                         vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]),
         "hl_dbg_tree_sum": (st, [C.c_int32, vp, C.c_uint64, C.POINTER(C.c_double)]),
+        "hl_tree_sum_noalloc": (st, [vp, C.c_uint64, vp, vp]),
         "hl_dbg_modularity": (st, [C.c_int32, C.c_uint32, vp, vp, vp, vp,
                                    C.POINTER(C.c_double)]),
     }

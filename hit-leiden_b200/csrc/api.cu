@@ -12,6 +12,8 @@ using namespace hl;
 
 static thread_local std::string g_err;
 
+void hl_set_error_message(const std::string& m) { g_err = m; }
+
 
 namespace hl {
 

@@ -180,6 +180,22 @@ HL_API const char* hl_last_error(void);
 /* Version string of the library build. */
 HL_API const char* hl_version(void);
 
+/* The canonical 2m reduction (fixed-shape pairwise sum: tiles of 1024 values
+ * padded with +0.0, each folded by stride halving, the tile sums folded again)
+ * of n doubles at device address d_x, written to the device address d_out, on
+ * `stream` (a cudaStream_t; NULL = default stream) of the current device.
+ * No counterpart in the reference: it exists for callers that must not
+ * allocate device memory (an embedding runtime that owns all device memory, a
+ * caller in a region where cudaMalloc is forbidden).  It allocates nothing:
+ * its tile sums live in a fixed ~2 MB array compiled into the library, which
+ * every GPU that loads the library keeps until exit.  n must not exceed
+ * HL_NOALLOC_MAX_ELEMS (HL_ERR_INVALID_INPUT otherwise).  All calls on one GPU
+ * share that array: calls whose work overlaps on the GPU race and must be
+ * ordered by the caller.  The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress); make it before any stream capture. */
+#define HL_NOALLOC_MAX_ELEMS (1ull << 28)
+HL_API hl_status hl_tree_sum_noalloc(const double* d_x, uint64_t n, double* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
