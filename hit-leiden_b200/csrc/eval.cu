@@ -57,6 +57,8 @@ struct EvalArgs {
   u32* tkey;
   u32* tpos;
   double* tval;
+  u32* tlist;    // per-warp / per-block insertion lists of used slots
+  u64 region;    // table entries per block region (block kernel)
   unsigned long long* counters;  // [0] entries scanned, [1] candidates evaluated
 };
 
@@ -64,8 +66,7 @@ constexpr u32 MID_MAX = 128;
 constexpr u32 MID_TAB = 256;  // per-warp table entries (>= 2 * MID_MAX)
 constexpr u32 MID_WARPS = 8;
 constexpr u32 BIG_THREADS = 256;
-constexpr u32 BIG1_TAB = 2048;  // shared table of the block kernel, degrees up to 1024
-constexpr u32 BIG_TAB = 8192;   // shared table for larger degrees (global above 4096)
+
 
 __device__ __forceinline__ u32 hash32(u32 x) {
   x ^= x >> 16;
@@ -310,10 +311,11 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
 // Wide degrees (MID_MAX < deg <= WIDE_MAX): a warp per vertex.  The warp
 // issues the loads of up to 8 chunks (256 entries) at once, then folds the
 // chunks in CSR order into a table kept in a per-warp global region (hot in
-// L2).  The scan that picks the best key also resets every used slot, so a
-// region is clean for the warp's next vertex without a clearing pass.
+// L2).  Every new key's slot is appended to a per-warp list, so the argmax
+// scan visits only used slots and resets them: the region is clean again for
+// the warp's next vertex without a clearing pass.
 // ---------------------------------------------------------------------------
-constexpr u32 WIDE_MAX = 4096;
+constexpr u32 WIDE_MAX = 512;
 constexpr u32 WIDE_TAB = 2 * WIDE_MAX;  // entries of one warp's region
 constexpr u32 WIDE_WARPS = 8;
 constexpr u32 WIDE_BATCH = 8;  // chunks loaded before folding
@@ -321,6 +323,7 @@ constexpr u32 WIDE_BATCH = 8;  // chunks loaded before folding
 template <int KIND>
 __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
   __shared__ double s_w[WIDE_WARPS][WIDE_BATCH * 32];
+  __shared__ u32 s_cnt[WIDE_WARPS];
   const u32 lane = threadIdx.x & 31;
   const u32 wib = threadIdx.x >> 5;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
@@ -329,6 +332,7 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
   u32* tk = A.tkey + warp * (u64)WIDE_TAB;
   u32* tp = A.tpos + warp * (u64)WIDE_TAB;
   double* tv = A.tval + warp * (u64)WIDE_TAB;
+  u32* list = A.tlist + warp * (u64)WIDE_MAX;
   double* sw = s_w[wib];
   for (u64 t = warp; t < A.nidx; t += nwarps) {
     const u32 i = A.idx[t];
@@ -338,10 +342,15 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
     const u32 fv = A.f[v];
     const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
     const double kv = A.kdeg[v];
-    if (lane == 0) trav += deg;
+    const double dcur = A.d[cur];
+    if (lane == 0) {
+      trav += deg;
+      s_cnt[wib] = 0;
+    }
     u32 cap = 64;
     while (cap < 2 * deg) cap <<= 1;
     const u32 mask = cap - 1;
+    __syncwarp();
     for (u64 b0 = o0; b0 < o1; b0 += WIDE_BATCH * 32) {
       u32 key[WIDE_BATCH];
 #pragma unroll
@@ -372,33 +381,41 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
           double acc = prev == NONE32 ? 0.0 : tv[slot];
           for (u32 m = grp; m; m &= m - 1) acc = __dadd_rn(acc, sw[j * 32 + __ffs(m) - 1]);
           tv[slot] = acc;
-          if (prev == NONE32) tp[slot] = (u32)(b0 + j * 32 + lane - o0);
+          if (prev == NONE32) {
+            tp[slot] = (u32)(b0 + j * 32 + lane - o0);
+            list[atomicAdd(&s_cnt[wib], 1u)] = slot;
+          }
         }
         __syncwarp();
       }
     }
-    // w(v, cur), then the argmax; every used slot is reset on the way.
+    const u32 used = s_cnt[wib];
+    // w(v, cur), then the argmax over the used slots, resetting them.
     double wcur = 0.0;
     bool found = false;
-    for (u32 x = lane; x < cap; x += 32)
-      if (tk[x] == cur) {
-        wcur = tv[x];
+    for (u32 x = lane; x < used; x += 32) {
+      u32 sl = list[x];
+      if (tk[sl] == cur) {
+        wcur = tv[sl];
         found = true;
       }
+    }
     u32 fm = __ballot_sync(0xffffffffu, found);
     wcur = __shfl_sync(0xffffffffu, wcur, fm ? __ffs(fm) - 1 : 0);
     if (!fm) wcur = 0.0;
+    __syncwarp();
     double g = -1.0;
     u32 p = NONE32, kk = cur;
-    for (u32 x = lane; x < cap; x += 32) {
-      u32 key = tk[x];
-      if (key == NONE32) continue;
-      tk[x] = NONE32;
+    for (u32 x = lane; x < used; x += 32) {
+      u32 sl = list[x];
+      u32 key = tk[sl];
+      double val = tv[sl];
+      u32 pp = tp[sl];
+      tk[sl] = NONE32;
       if (key == cur || A.tw == 0.0) continue;
       if (KIND == EVAL_REFINE && A.blocked[key]) continue;
-      double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
+      double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, A.d[key]);
       ++ncand;
-      u32 pp = tp[x];
       if (p == NONE32 || gn > g || (gn == g && pp < p)) {
         g = gn;
         p = pp;
@@ -422,22 +439,34 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-// Large degrees: a block per vertex, adjacency staged in shared tiles.
+// Large degrees (> WIDE_MAX): a block per vertex.  The row is staged in
+// shared memory 256 entries at a time; the next tile's neighbours and weights
+// are loaded into registers while the current tile is folded, and their keys
+// gathered right after, so the row streams through with a tile of loads in
+// flight.  Keys are folded into a shared table (cap <= BIG_TAB) or, above
+// that, into the block's global region with an insertion list.
 // ---------------------------------------------------------------------------
-template <int KIND, u32 TAB>
+constexpr u32 BIG_TAB = 4096;  // shared table entries (degrees up to 2048)
+
+template <int KIND>
 __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
   extern __shared__ unsigned char smem_raw[];
-  u32* s_tk = reinterpret_cast<u32*>(smem_raw);                       // TAB
-  u32* s_tp = s_tk + TAB;                                              // TAB
-  double* s_tv = reinterpret_cast<double*>(s_tp + TAB);                // TAB
-  u32* s_key = reinterpret_cast<u32*>(s_tv + TAB);                     // BIG_THREADS
+  u32* s_tk = reinterpret_cast<u32*>(smem_raw);                       // BIG_TAB
+  u32* s_tp = s_tk + BIG_TAB;                                          // BIG_TAB
+  double* s_tv = reinterpret_cast<double*>(s_tp + BIG_TAB);            // BIG_TAB
+  u32* s_key = reinterpret_cast<u32*>(s_tv + BIG_TAB);                 // BIG_THREADS
   double* s_w = reinterpret_cast<double*>(s_key + BIG_THREADS);        // BIG_THREADS
   __shared__ double r_g[BIG_THREADS / 32];
   __shared__ u32 r_p[BIG_THREADS / 32], r_k[BIG_THREADS / 32];
   __shared__ double s_wcur;
+  __shared__ u32 s_used;
   const u32 lane = threadIdx.x & 31;
   const u32 wib = threadIdx.x >> 5;
   unsigned long long trav = 0, ncand = 0;
+  u32* g_tk = A.tkey ? A.tkey + (u64)blockIdx.x * A.region : nullptr;
+  u32* g_tp = A.tpos ? A.tpos + (u64)blockIdx.x * A.region : nullptr;
+  double* g_tv = A.tval ? A.tval + (u64)blockIdx.x * A.region : nullptr;
+  u32* g_list = A.tlist ? A.tlist + (u64)blockIdx.x * (A.region / 2) : nullptr;
   for (u64 t = blockIdx.x; t < A.nidx; t += gridDim.x) {
     const u32 i = A.idx[t];
     const u32 v = A.verts[i];
@@ -446,54 +475,67 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
     const u32 fv = A.f[v];
     const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
     const double kv = A.kdeg[v];
-    if (threadIdx.x == 0) trav += deg;
-    u32* tk;
-    u32* tp;
-    double* tv;
-    u64 cap = 2;
-    while (cap < 2 * deg) cap <<= 1;
-    if (2 * deg <= TAB) {
-      tk = s_tk;
-      tp = s_tp;
-      tv = s_tv;
-    } else {
-      u64 gb = A.tab_off[t];
-      tk = A.tkey + gb;
-      tp = A.tpos + gb;
-      tv = A.tval + gb;
+    if (threadIdx.x == 0) {
+      trav += deg;
+      s_used = 0;
     }
+    u64 cap = 64;
+    while (cap < 2 * deg) cap <<= 1;
+    const bool shared_tab = cap <= BIG_TAB;
+    u32* tk = shared_tab ? s_tk : g_tk;
+    u32* tp = shared_tab ? s_tp : g_tp;
+    double* tv = shared_tab ? s_tv : g_tv;
     const u64 mask = cap - 1;
-    for (u64 x = threadIdx.x; x < cap; x += BIG_THREADS) {
-      tk[x] = NONE32;
-      tp[x] = NONE32;
-      tv[x] = 0.0;
+    // Free slots always hold (NONE, value 0, no position): cleared here for the
+    // shared table, restored by the final scan for a global one.
+    if (shared_tab)
+      for (u64 x = threadIdx.x; x < cap; x += BIG_THREADS) {
+        tk[x] = NONE32;
+        tv[x] = 0.0;
+        tp[x] = NONE32;
+      }
+    // first tile's loads
+    u32 nb_next = 0;
+    double w_next = 0.0;
+    bool have_next = false;
+    {
+      u64 q = o0 + threadIdx.x;
+      if (q < o1) {
+        nb_next = A.col[q];
+        w_next = A.w[q];
+        have_next = true;
+      }
     }
     __syncthreads();
     for (u64 b0 = o0; b0 < o1; b0 += BIG_THREADS) {
-      u64 q = b0 + threadIdx.x;
+      // stage the current tile (keys gathered now), then prefetch the next
       u32 key = NONE32;
-      double wv = 0.0;
-      if (q < o1) {
-        u32 nb = A.col[q];
-        wv = A.w[q];
-        if (!entry_key<KIND>(A, v, nb, fv, key)) key = NONE32;
-      }
+      if (have_next && !entry_key<KIND>(A, v, nb_next, fv, key)) key = NONE32;
+      if (!have_next) key = NONE32;
       s_key[threadIdx.x] = key;
-      s_w[threadIdx.x] = wv;
+      s_w[threadIdx.x] = w_next;
+      {
+        u64 q = b0 + BIG_THREADS + threadIdx.x;
+        have_next = q < o1;
+        if (have_next) {
+          nb_next = A.col[q];
+          w_next = A.w[q];
+        } else {
+          w_next = 0.0;
+        }
+      }
       __syncthreads();
       const u32 nch = (u32)((o1 - b0 + 31) / 32 < BIG_THREADS / 32 ? (o1 - b0 + 31) / 32
                                                                    : BIG_THREADS / 32);
-      // Integral weights: every warp inserts its own chunk at once (atomic,
-      // exact in any order).  Otherwise each warp owns the keys whose hash
-      // falls in its partition and folds the tile's chunks in CSR order, so
-      // every key's sum is still extended entry by entry in CSR order.
+      // Integral weights: each warp inserts its own chunk (atomics, exact in
+      // any order).  Otherwise each warp owns a hash partition of the keys and
+      // folds the tile's chunks in CSR order, keeping every key's rounding.
       const u32 c0 = A.concurrent ? wib : 0;
       const u32 cs = A.concurrent ? BIG_THREADS / 32 : 1;
       for (u32 c = c0; c < nch; c += cs) {
         u32 e = c * 32 + lane;
         u32 key2 = s_key[e];
-        bool mine = key2 != NONE32 &&
-                    (A.concurrent || (hash32(key2) >> 29) == wib);  // 8 warps, top 3 bits
+        bool mine = key2 != NONE32 && (A.concurrent || (hash32(key2) >> 29) == wib);
         u32 grp = __match_any_sync(0xffffffffu, mine ? (unsigned long long)key2
                                                      : ((1ull << 32) | lane));
         if (mine && lane == (u32)(__ffs(grp) - 1)) {
@@ -505,13 +547,14 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
             if (prev == NONE32 || prev == key2) break;
             slot = (slot + 1) & mask;
           }
+          if (prev == NONE32 && !shared_tab) g_list[atomicAdd(&s_used, 1u)] = (u32)slot;
           if (A.concurrent) {
             double sum = 0.0;
             for (u32 m = grp; m; m &= m - 1) sum += s_w[c * 32 + __ffs(m) - 1];
             atomicAdd(&tv[slot], sum);
             atomicMin(&tp[slot], pos);
           } else {
-            double acc = prev == NONE32 ? 0.0 : tv[slot];
+            double acc = tv[slot];
             for (u32 m = grp; m; m &= m - 1) acc = __dadd_rn(acc, s_w[c * 32 + __ffs(m) - 1]);
             tv[slot] = acc;
             if (prev == NONE32) tp[slot] = pos;
@@ -521,28 +564,38 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
       }
       __syncthreads();
     }
-    // w(v, cur) and the argmax over the table.
+    // w(v, cur) and the argmax over the table (resetting a global table).
     if (threadIdx.x == 0) s_wcur = 0.0;
     __syncthreads();
-    for (u64 x = threadIdx.x; x < cap; x += BIG_THREADS)
-      if (tk[x] == cur) s_wcur = tv[x];
+    const u64 nscan = shared_tab ? cap : s_used;
+    for (u64 x = threadIdx.x; x < nscan; x += BIG_THREADS) {
+      u64 sl = shared_tab ? x : g_list[x];
+      if (tk[sl] == cur) s_wcur = tv[sl];
+    }
     __syncthreads();
     const double wcur = s_wcur;
+    const double dcur = A.d[cur];
     double g = -1.0;
     u32 p = NONE32, kk = cur;
-    if (A.tw != 0.0) {
-      for (u64 x = threadIdx.x; x < cap; x += BIG_THREADS) {
-        u32 key = tk[x];
-        if (key == NONE32 || key == cur) continue;
-        if (KIND == EVAL_REFINE && A.blocked[key]) continue;
-        double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
-        ++ncand;
-        u32 pp = tp[x];
-        if (p == NONE32 || gn > g || (gn == g && pp < p)) {
-          g = gn;
-          p = pp;
-          kk = key;
-        }
+    for (u64 x = threadIdx.x; x < nscan; x += BIG_THREADS) {
+      u64 sl = shared_tab ? x : g_list[x];
+      u32 key = tk[sl];
+      if (key == NONE32) continue;
+      const double val = tv[sl];
+      const u32 pp = tp[sl];
+      if (!shared_tab) {
+        tk[sl] = NONE32;
+        tv[sl] = 0.0;
+        tp[sl] = NONE32;
+      }
+      if (key == cur || A.tw == 0.0) continue;
+      if (KIND == EVAL_REFINE && A.blocked[key]) continue;
+      double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, A.d[key]);
+      ++ncand;
+      if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+        g = gn;
+        p = pp;
+        kk = key;
       }
     }
     for (int o = 16; o; o >>= 1) {
@@ -601,21 +654,25 @@ __global__ void k_big_caps2(const u32* verts, const u32* idx, u32 nb, const u64*
   for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < nb; t += (u64)gridDim.x * blockDim.x) {
     u32 v = verts[idx[t]];
     u64 deg = off[v + 1] - off[v];
-    u64 c = 0;
-    if (2 * deg > BIG_TAB) {
-      c = 2;
-      while (c < 2 * deg) c <<= 1;
-    }
-    cap[t] = c;
+    u64 c = 64;
+    while (c < 2 * deg) c <<= 1;
+    cap[t] = c > BIG_TAB ? c : 0;
   }
+}
+
+__global__ void k_fill_u32(u32* p, u32 v, u64 n) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+static size_t big_smem() {
+  return (size_t)BIG_TAB * (4 + 4 + 8) + (size_t)BIG_THREADS * (4 + 8);
 }
 
 static bool g_big_attr_set[64] = {false};
 
-template <u32 TAB>
-static size_t big_smem() {
-  return (size_t)TAB * (4 + 4 + 8) + (size_t)BIG_THREADS * (4 + 8);
-}
+constexpr u32 WIDE_MAX_BLOCKS = 148u * 4u;
+constexpr u32 BIG_MAX_BLOCKS = 148u * 3u;
 
 void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
               const double* d, const u8* blocked, bool allow_empty, u32* out_to, double* out_gain,
@@ -645,39 +702,52 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   std::memcpy(c, E.hs.p, sizeof(c));
   u32 start[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int b = 0; b < 6; ++b) start[b + 1] = start[b] + c[b];
-  // Global tables for vertices above the largest shared table.
-  DBuf<u32>& tk = S.huge_key;
-  DBuf<u32>& tp = S.huge_pos;
-  DBuf<double>& tv = S.huge_val;
-  u64* tab_off = nullptr;
+
+  // Per-warp regions of the wide kernel, allocated once for its largest grid.
+  if (c[4] && S.wide_key.cap < (size_t)WIDE_MAX_BLOCKS * WIDE_WARPS * WIDE_TAB) {
+    const size_t need = (size_t)WIDE_MAX_BLOCKS * WIDE_WARPS * WIDE_TAB;
+    S.wide_key.ensure(E.mem, need);
+    S.wide_pos.ensure(E.mem, need);
+    S.wide_val.ensure(E.mem, need);
+    S.wide_list.ensure(E.mem, (size_t)WIDE_MAX_BLOCKS * WIDE_WARPS * WIDE_MAX);
+    ++E.nlaunch, k_fill_u32<<<grid_for(need), 256, 0, st>>>(S.wide_key.p, NONE32, S.wide_key.cap);
+    HL_LAUNCH_CHECK();
+  }
+  // Per-block global regions of the block kernel, sized for its largest row.
+  u64 region = 0;
   if (c[5]) {
     S.gkey.ensure(E.mem, (size_t)c[5] + 1);
-    S.gkey2.ensure(E.mem, (size_t)c[5] + 1);
     ++E.nlaunch, k_big_caps2<<<grid_for(c[5]), 256, 0, st>>>(verts, vo + start[5], c[5], L.g.off.p,
                                                              S.gkey.p);
-    HL_CUDA(cudaMemsetAsync(S.gkey.p + c[5], 0, sizeof(u64), st));
     HL_LAUNCH_CHECK();
     u64* ci = S.gkey.p;
     u64* co = S.gkey2.p;
+    S.gkey2.ensure(E.mem, 2);
+    co = S.gkey2.p;
     cub_run(E, [&](void* t, size_t& b) {
-      return cub::DeviceScan::ExclusiveSum(t, b, ci, co, (int64_t)c[5] + 1, st);
+      return cub::DeviceReduce::Max(t, b, ci, co, (int64_t)c[5], st);
     });
-    u64 total = E.read_u64(co + c[5]);
-    if (total) {
-      tk.ensure(E.mem, total);
-      tp.ensure(E.mem, total);
-      tv.ensure(E.mem, total);
+    region = E.read_u64(co);
+    if (region) {
+      const size_t need = (size_t)BIG_MAX_BLOCKS * region;
+      if (S.huge_key.cap < need) {
+        S.huge_key.ensure(E.mem, need);
+        S.huge_pos.ensure(E.mem, need);
+        S.huge_val.ensure(E.mem, need);
+        S.huge_list.ensure(E.mem, need / 2 + 1);
+        ++E.nlaunch, k_fill_u32<<<grid_for(need), 256, 0, st>>>(S.huge_key.p, NONE32, S.huge_key.cap);
+        ++E.nlaunch, k_fill_u32<<<grid_for(need), 256, 0, st>>>(S.huge_pos.p, NONE32, S.huge_pos.cap);
+        HL_CUDA(cudaMemsetAsync(S.huge_val.p, 0, sizeof(double) * S.huge_val.cap, st));
+        HL_LAUNCH_CHECK();
+      }
     }
-    tab_off = co;
   }
   int dev = E.device;
   if (dev >= 0 && dev < 64 && !g_big_attr_set[dev]) {
-    HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_MOVE, BIG_TAB>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)big_smem<BIG_TAB>()));
-    HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_REFINE, BIG_TAB>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)big_smem<BIG_TAB>()));
+    HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)big_smem()));
+    HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_REFINE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem()));
     g_big_attr_set[dev] = true;
   }
 
@@ -698,22 +768,23 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   A.concurrent = E.integral;
   A.out_to = out_to;
   A.out_gain = out_gain;
-  A.counters = counters;
   A.tab_off = nullptr;
   A.tkey = nullptr;
   A.tpos = nullptr;
   A.tval = nullptr;
+  A.tlist = nullptr;
+  A.region = 0;
 
   cudaEvent_t ev = E.kt_begin();
-  auto launch_small = [&](int b) {
-    if (!c[b]) return;
+  cudaEvent_t e_s = E.kt_begin();
+  for (int b = 0; b < 3; ++b) {
+    if (!c[b]) continue;
     EvalArgs a = A;
-    a.counters = counters ? counters : nullptr;
+    a.counters = counters;
     a.idx = vo + start[b];
     a.nidx = c[b];
     u32 G = b == 0 ? 8 : b == 1 ? 16 : 32;
-    u64 threads = (u64)c[b] * G;
-    u32 blocks = grid_for(threads, 256);
+    u32 blocks = grid_for((u64)c[b] * G, 256);
     if (kind == EVAL_MOVE) {
       if (G == 8) ++E.nlaunch, k_eval_small<EVAL_MOVE, 8><<<blocks, 256, 0, st>>>(a);
       else if (G == 16) ++E.nlaunch, k_eval_small<EVAL_MOVE, 16><<<blocks, 256, 0, st>>>(a);
@@ -723,11 +794,8 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
       else if (G == 16) ++E.nlaunch, k_eval_small<EVAL_REFINE, 16><<<blocks, 256, 0, st>>>(a);
       else ++E.nlaunch, k_eval_small<EVAL_REFINE, 32><<<blocks, 256, 0, st>>>(a);
     }
-  };
-  cudaEvent_t e_s = E.kt_begin();
-  launch_small(0);
-  launch_small(1);
-  launch_small(2);
+  }
+  HL_LAUNCH_CHECK();
   E.kt_end(KT_EVAL_SMALL, e_s);
   E.kagg[KT_EVAL_SMALL].items += (u64)c[0] + c[1] + c[2];
   E.kagg[KT_EVAL_MID].items += c[3];
@@ -747,52 +815,18 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   }
   HL_LAUNCH_CHECK();
   E.kt_end(KT_EVAL_MID, e_m);
-  auto launch_big = [&](int b) {
-    if (!c[b]) return;
-    EvalArgs a = A;
-    a.counters = counters ? counters + 6 : nullptr;
-    a.idx = vo + start[b];
-    a.nidx = c[b];
-    a.tab_off = b == 5 ? tab_off : nullptr;
-    a.tkey = tk.p;
-    a.tpos = tp.p;
-    a.tval = tv.p;
-    if (b == 4) {
-      u32 blocks = c[b] < 148u * 8u ? c[b] : 148u * 8u;
-      size_t sm = big_smem<BIG1_TAB>();
-      if (kind == EVAL_MOVE)
-        ++E.nlaunch, k_eval_big<EVAL_MOVE, BIG1_TAB><<<blocks, BIG_THREADS, sm, st>>>(a);
-      else
-        ++E.nlaunch, k_eval_big<EVAL_REFINE, BIG1_TAB><<<blocks, BIG_THREADS, sm, st>>>(a);
-    } else {
-      u32 blocks = c[b] < 148u * 2u ? c[b] : 148u * 2u;
-      size_t sm = big_smem<BIG_TAB>();
-      if (kind == EVAL_MOVE)
-        ++E.nlaunch, k_eval_big<EVAL_MOVE, BIG_TAB><<<blocks, BIG_THREADS, sm, st>>>(a);
-      else
-        ++E.nlaunch, k_eval_big<EVAL_REFINE, BIG_TAB><<<blocks, BIG_THREADS, sm, st>>>(a);
-    }
-    HL_LAUNCH_CHECK();
-  };
   cudaEvent_t e_b = E.kt_begin();
   if (c[4]) {
     EvalArgs a = A;
     a.counters = counters ? counters + 4 : nullptr;
     a.idx = vo + start[4];
     a.nidx = c[4];
-    u32 blocks = grid_for((u64)c[4] * 32, WIDE_WARPS * 32);
-    if (blocks > 148u * 4u) blocks = 148u * 4u;
-    // regions for the largest grid, allocated once
-    const size_t need = (size_t)148u * 4u * WIDE_WARPS * WIDE_TAB;
-    if (S.wide_key.cap < need) {
-      S.wide_key.ensure(E.mem, need);
-      S.wide_pos.ensure(E.mem, need);
-      S.wide_val.ensure(E.mem, need);
-      HL_CUDA(cudaMemsetAsync(S.wide_key.p, 0xFF, sizeof(u32) * S.wide_key.cap, st));
-    }
     a.tkey = S.wide_key.p;
     a.tpos = S.wide_pos.p;
     a.tval = S.wide_val.p;
+    a.tlist = S.wide_list.p;
+    u32 blocks = grid_for((u64)c[4] * 32, WIDE_WARPS * 32);
+    if (blocks > WIDE_MAX_BLOCKS) blocks = WIDE_MAX_BLOCKS;
     if (kind == EVAL_MOVE)
       ++E.nlaunch, k_eval_wide<EVAL_MOVE><<<blocks, WIDE_WARPS * 32, 0, st>>>(a);
     else
@@ -801,7 +835,25 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   }
   E.kt_end(KT_EVAL_BIG, e_b);
   cudaEvent_t e_h = E.kt_begin();
-  launch_big(5);
+  if (c[5]) {
+    EvalArgs a = A;
+    a.counters = counters ? counters + 6 : nullptr;
+    a.idx = vo + start[5];
+    a.nidx = c[5];
+    if (region) {
+      a.tkey = S.huge_key.p;
+      a.tpos = S.huge_pos.p;
+      a.tval = S.huge_val.p;
+      a.tlist = S.huge_list.p;
+      a.region = region;
+    }
+    u32 blocks = c[5] < BIG_MAX_BLOCKS ? c[5] : BIG_MAX_BLOCKS;
+    if (kind == EVAL_MOVE)
+      ++E.nlaunch, k_eval_big<EVAL_MOVE><<<blocks, BIG_THREADS, big_smem(), st>>>(a);
+    else
+      ++E.nlaunch, k_eval_big<EVAL_REFINE><<<blocks, BIG_THREADS, big_smem(), st>>>(a);
+    HL_LAUNCH_CHECK();
+  }
   E.kt_end(KT_EVAL_HUGE, e_h);
   E.kt_end(kind == EVAL_MOVE ? KT_MOVE_EVAL : KT_REFINE_EVAL, ev);
 }

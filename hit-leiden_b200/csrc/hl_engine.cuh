@@ -78,10 +78,10 @@ struct Scratch {
   DBuf<u64> red64;
   DBuf<u32> origin;
   // per-warp hash regions of the wide evaluation kernel (kept clean by it)
-  DBuf<u32> wide_key, wide_pos;
+  DBuf<u32> wide_key, wide_pos, wide_list;
   DBuf<double> wide_val;
   // global tables of the block-per-vertex kernel (degrees above 4096)
-  DBuf<u32> huge_key, huge_pos;
+  DBuf<u32> huge_key, huge_pos, huge_list;
   DBuf<double> huge_val;
 };
 
