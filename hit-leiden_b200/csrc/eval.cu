@@ -13,14 +13,13 @@
 // vertex waits on a table far larger than it needs:
 //   deg <= 8, 16, 32    sub-warp groups of 8 / 16 / 32 lanes, one chunk, no table;
 //   33 .. MID_MAX       a warp per vertex, shared-memory table sized 2·deg;
-//   larger              a block per vertex: 256-entry adjacency tiles staged in
-//                       shared memory by all warps, keys accumulated in a
-//                       shared table (2048 entries up to degree 1024, 8192 up
-//                       to 4096, a global table above).  With integral weights
-//                       every warp inserts its chunk at once (exact in any
-//                       order); otherwise each warp owns a hash partition of the
-//                       keys and folds the tile in CSR order, so every key's
-//                       sum keeps the reference's rounding.
+//   MID_MAX .. WIDE_MAX a warp per vertex, a per-warp global table;
+//   larger              a block per vertex: 256-entry adjacency tiles bucketed
+//                       by a hash partition of their keys, one partition per
+//                       warp, each warp folding its own keys in CSR order into
+//                       a shared table of 4096 slots (a global one only for
+//                       rows with more than 2048 distinct keys), so every
+//                       key's sum keeps the reference's rounding.
 #include <cstring>
 
 #include "hl_engine.cuh"
@@ -439,29 +438,70 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-// Large degrees (> WIDE_MAX): a block per vertex.  The row is staged in
-// shared memory 256 entries at a time; the next tile's neighbours and weights
-// are loaded into registers while the current tile is folded, and their keys
-// gathered right after, so the row streams through with a tile of loads in
-// flight.  Keys are folded into a shared table (cap <= BIG_TAB) or, above
-// that, into the block's global region with an insertion list.
+// Large degrees (> WIDE_MAX): a block per vertex.
+//
+// The row streams through in tiles of BIG_THREADS entries with a two-stage
+// software pipeline: while tile t is folded, the keys of tile t+1 are being
+// gathered and the neighbours and weights of tile t+2 loaded.  Each tile is
+// bucketed (stable) by a hash partition of its keys, one partition per warp,
+// so a warp folds exactly the entries of its own keys, in CSR order, and no
+// key is touched by two warps: every key's sum is extended in the reference's
+// order and rounding with no atomics on values.  Inside a warp the lanes that
+// share a key are grouped with match_any; all group leaders fold their groups
+// at once in one unrolled pass over the chunk.
+//
+// The table lives in shared memory (BIG_TAB slots).  Hubs have long rows but
+// few distinct neighbour keys, so a row only moves its table to the block's
+// global region when it passes BIG_TAB / 2 distinct keys.
 // ---------------------------------------------------------------------------
-constexpr u32 BIG_TAB = 4096;  // shared table entries (degrees up to 2048)
+constexpr u32 BIG_TAB = 4096;
+constexpr u32 BIG_WARPS = BIG_THREADS / 32;
+constexpr u32 BIG_PART_BITS = 3;  // log2(BIG_WARPS)
+static_assert((1u << BIG_PART_BITS) == BIG_WARPS, "one key partition per warp");
+
+template <int KIND>
+__device__ __forceinline__ u32 tile_key(const EvalArgs& A, u32 v, u32 fv, bool ok, u32 nb) {
+  u32 key = NONE32;
+  if (ok && !entry_key<KIND>(A, v, nb, fv, key)) key = NONE32;
+  return key;
+}
+
+// Find or claim the slot of `key` (linear probing; free slots hold NONE32).
+__device__ __forceinline__ u64 claim_slot(u32* tk, u64 mask, u32 key, bool& fresh) {
+  u64 slot = hash32(key) & mask;
+  while (true) {
+    u32 prev = atomicCAS(&tk[slot], NONE32, key);
+    if (prev == NONE32) {
+      fresh = true;
+      return slot;
+    }
+    if (prev == key) {
+      fresh = false;
+      return slot;
+    }
+    slot = (slot + 1) & mask;
+  }
+}
 
 template <int KIND>
 __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
-  extern __shared__ unsigned char smem_raw[];
-  u32* s_tk = reinterpret_cast<u32*>(smem_raw);                       // BIG_TAB
-  u32* s_tp = s_tk + BIG_TAB;                                          // BIG_TAB
-  double* s_tv = reinterpret_cast<double*>(s_tp + BIG_TAB);            // BIG_TAB
-  u32* s_key = reinterpret_cast<u32*>(s_tv + BIG_TAB);                 // BIG_THREADS
-  double* s_w = reinterpret_cast<double*>(s_key + BIG_THREADS);        // BIG_THREADS
-  __shared__ double r_g[BIG_THREADS / 32];
-  __shared__ u32 r_p[BIG_THREADS / 32], r_k[BIG_THREADS / 32];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s_tv = reinterpret_cast<double*>(smem_raw);        // BIG_TAB values
+  u32* s_tk = reinterpret_cast<u32*>(s_tv + BIG_TAB);        // BIG_TAB keys
+  u32* s_tp = s_tk + BIG_TAB;                                // BIG_TAB first positions
+  double* b_w = reinterpret_cast<double*>(s_tp + BIG_TAB);   // bucketed tile: weights
+  u32* b_key = reinterpret_cast<u32*>(b_w + BIG_THREADS);    // keys
+  u32* b_pos = b_key + BIG_THREADS;                          // positions in the row
+  __shared__ u32 s_cnt[BIG_WARPS * BIG_WARPS];               // [partition][warp]
+  __shared__ u32 s_off[BIG_WARPS * BIG_WARPS + 1];
+  __shared__ double r_g[BIG_WARPS];
+  __shared__ u32 r_p[BIG_WARPS], r_k[BIG_WARPS];
   __shared__ double s_wcur;
-  __shared__ u32 s_used;
-  const u32 lane = threadIdx.x & 31;
-  const u32 wib = threadIdx.x >> 5;
+  __shared__ u32 s_used, s_gused;
+  const u32 tid = threadIdx.x;
+  const u32 lane = tid & 31;
+  const u32 wib = tid >> 5;
+  const u32 lt_mask = (1u << lane) - 1u;
   unsigned long long trav = 0, ncand = 0;
   u32* g_tk = A.tkey ? A.tkey + (u64)blockIdx.x * A.region : nullptr;
   u32* g_tp = A.tpos ? A.tpos + (u64)blockIdx.x * A.region : nullptr;
@@ -475,122 +515,180 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
     const u32 fv = A.f[v];
     const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
     const double kv = A.kdeg[v];
-    if (threadIdx.x == 0) {
+    u64 gcap = 64;
+    while (gcap < 2 * deg) gcap <<= 1;
+    const u32 cap = gcap < BIG_TAB ? (u32)gcap : BIG_TAB;
+    if (tid == 0) {
       trav += deg;
       s_used = 0;
+      s_gused = 0;
     }
-    u64 cap = 64;
-    while (cap < 2 * deg) cap <<= 1;
-    const bool shared_tab = cap <= BIG_TAB;
-    u32* tk = shared_tab ? s_tk : g_tk;
-    u32* tp = shared_tab ? s_tp : g_tp;
-    double* tv = shared_tab ? s_tv : g_tv;
-    const u64 mask = cap - 1;
-    // Free slots always hold (NONE, value 0, no position): cleared here for the
-    // shared table, restored by the final scan for a global one.
-    if (shared_tab)
-      for (u64 x = threadIdx.x; x < cap; x += BIG_THREADS) {
-        tk[x] = NONE32;
-        tv[x] = 0.0;
-        tp[x] = NONE32;
-      }
-    // first tile's loads
-    u32 nb_next = 0;
-    double w_next = 0.0;
-    bool have_next = false;
+    for (u32 x = tid; x < cap; x += BIG_THREADS) {
+      s_tk[x] = NONE32;
+      s_tv[x] = 0.0;
+      s_tp[x] = NONE32;
+    }
+    // pipeline prologue: keys of tile 0, neighbours of tile 1
+    u32 key1;
+    double w1 = 0.0;
     {
-      u64 q = o0 + threadIdx.x;
-      if (q < o1) {
-        nb_next = A.col[q];
-        w_next = A.w[q];
-        have_next = true;
+      const u64 q = o0 + tid;
+      const bool ok = q < o1;
+      const u32 nb = ok ? A.col[q] : 0u;
+      w1 = ok ? A.w[q] : 0.0;
+      key1 = tile_key<KIND>(A, v, fv, ok, nb);
+    }
+    u32 nb2 = 0;
+    double w2 = 0.0;
+    bool ok2;
+    {
+      const u64 q = o0 + BIG_THREADS + tid;
+      ok2 = q < o1;
+      if (ok2) {
+        nb2 = A.col[q];
+        w2 = A.w[q];
       }
     }
+    bool global = false;
+    u32* tk = s_tk;
+    u32* tp = s_tp;
+    double* tv = s_tv;
+    u64 mask = cap - 1;
     __syncthreads();
     for (u64 b0 = o0; b0 < o1; b0 += BIG_THREADS) {
-      // stage the current tile (keys gathered now), then prefetch the next
-      u32 key = NONE32;
-      if (have_next && !entry_key<KIND>(A, v, nb_next, fv, key)) key = NONE32;
-      if (!have_next) key = NONE32;
-      s_key[threadIdx.x] = key;
-      s_w[threadIdx.x] = w_next;
+      const u32 key = key1;
+      const double wv = w1;
+      const u32 pos = (u32)(b0 - o0) + tid;
+      // advance the pipeline: gather tile t+1's keys, load tile t+2's entries
+      key1 = tile_key<KIND>(A, v, fv, ok2, nb2);
+      w1 = w2;
       {
-        u64 q = b0 + BIG_THREADS + threadIdx.x;
-        have_next = q < o1;
-        if (have_next) {
-          nb_next = A.col[q];
-          w_next = A.w[q];
-        } else {
-          w_next = 0.0;
+        const u64 q = b0 + 2 * BIG_THREADS + tid;
+        ok2 = q < o1;
+        nb2 = ok2 ? A.col[q] : 0u;
+        w2 = ok2 ? A.w[q] : 0.0;
+      }
+      // stable bucketing of the tile by key partition
+      const u32 part = key == NONE32 ? NONE32 : hash32(key) >> (32 - BIG_PART_BITS);
+      u32 rank = 0, mycnt = 0;
+#pragma unroll
+      for (u32 q = 0; q < BIG_WARPS; ++q) {
+        const u32 bq = __ballot_sync(0xffffffffu, part == q);
+        if (lane == q) mycnt = __popc(bq);
+        if (part == q) rank = __popc(bq & lt_mask);
+      }
+      if (lane < BIG_WARPS) s_cnt[lane * BIG_WARPS + wib] = mycnt;
+      __syncthreads();
+      // The previous tile's folds are complete here and s_used is stable: a row
+      // with too many distinct keys moves its table to the global region (its
+      // degree is then above BIG_TAB / 2, so the region exists).
+      if (!global && s_used > BIG_TAB / 2 && g_tk) {
+        const u64 gmask = gcap - 1;
+        for (u32 x = tid; x < BIG_TAB; x += BIG_THREADS) {
+          const u32 k = s_tk[x];
+          if (k == NONE32) continue;
+          bool fresh;
+          const u64 sl = claim_slot(g_tk, gmask, k, fresh);
+          g_tv[sl] = s_tv[x];
+          g_tp[sl] = s_tp[x];
+          g_list[atomicAdd(&s_gused, 1u)] = (u32)sl;
         }
+        global = true;
+        tk = g_tk;
+        tp = g_tp;
+        tv = g_tv;
+        mask = gmask;
+      }
+      if (wib == 0) {
+        // exclusive scan of the 64 counts in (partition, warp) order
+        const u32 a0 = s_cnt[2 * lane], a1 = s_cnt[2 * lane + 1];
+        u32 inc = a0 + a1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const u32 y = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= (u32)o) inc += y;
+        }
+        const u32 ex = inc - a0 - a1;
+        s_off[2 * lane] = ex;
+        s_off[2 * lane + 1] = ex + a0;
+        if (lane == 31) s_off[BIG_WARPS * BIG_WARPS] = inc;
       }
       __syncthreads();
-      const u32 nch = (u32)((o1 - b0 + 31) / 32 < BIG_THREADS / 32 ? (o1 - b0 + 31) / 32
-                                                                   : BIG_THREADS / 32);
-      // Integral weights: each warp inserts its own chunk (atomics, exact in
-      // any order).  Otherwise each warp owns a hash partition of the keys and
-      // folds the tile's chunks in CSR order, keeping every key's rounding.
-      const u32 c0 = A.concurrent ? wib : 0;
-      const u32 cs = A.concurrent ? BIG_THREADS / 32 : 1;
-      for (u32 c = c0; c < nch; c += cs) {
-        u32 e = c * 32 + lane;
-        u32 key2 = s_key[e];
-        bool mine = key2 != NONE32 && (A.concurrent || (hash32(key2) >> 29) == wib);
-        u32 grp = __match_any_sync(0xffffffffu, mine ? (unsigned long long)key2
-                                                     : ((1ull << 32) | lane));
-        if (mine && lane == (u32)(__ffs(grp) - 1)) {
-          u32 pos = (u32)(b0 - o0) + e;
-          u64 slot = hash32(key2) & mask;
-          u32 prev;
-          while (true) {
-            prev = atomicCAS(&tk[slot], NONE32, key2);
-            if (prev == NONE32 || prev == key2) break;
-            slot = (slot + 1) & mask;
+      if (part != NONE32) {
+        const u32 dst = s_off[part * BIG_WARPS + wib] + rank;
+        b_key[dst] = key;
+        b_w[dst] = wv;
+        b_pos[dst] = pos;
+      }
+      const u32 beg = s_off[wib * BIG_WARPS];
+      const u32 end = s_off[(wib + 1) * BIG_WARPS];
+      __syncthreads();
+      // this warp's keys, in CSR order
+      for (u32 c = beg; c < end; c += 32) {
+        const u32 e = c + lane;
+        const bool ok = e < end;
+        const u32 k = ok ? b_key[e] : NONE32;
+        const u32 grp = __match_any_sync(0xffffffffu, ok ? (unsigned long long)k
+                                                         : ((1ull << 32) | lane));
+        const bool leader = ok && lane == (u32)(__ffs(grp) - 1);
+        u64 slot = 0;
+        double acc = 0.0;
+        if (leader) {
+          bool fresh;
+          slot = claim_slot(tk, mask, k, fresh);
+          if (fresh) {
+            tp[slot] = b_pos[e];
+            if (global) g_list[atomicAdd(&s_gused, 1u)] = (u32)slot;
+            else atomicAdd(&s_used, 1u);
           }
-          if (prev == NONE32 && !shared_tab) g_list[atomicAdd(&s_used, 1u)] = (u32)slot;
-          if (A.concurrent) {
-            double sum = 0.0;
-            for (u32 m = grp; m; m &= m - 1) sum += s_w[c * 32 + __ffs(m) - 1];
-            atomicAdd(&tv[slot], sum);
-            atomicMin(&tp[slot], pos);
-          } else {
-            double acc = tv[slot];
-            for (u32 m = grp; m; m &= m - 1) acc = __dadd_rn(acc, s_w[c * 32 + __ffs(m) - 1]);
-            tv[slot] = acc;
-            if (prev == NONE32) tp[slot] = pos;
+          acc = tv[slot];
+        }
+        const u32 nhere = end - c < 32 ? end - c : 32;
+#pragma unroll
+        for (u32 j = 0; j < 32; ++j) {
+          if (j < nhere) {
+            const double y = b_w[c + j];
+            if (leader && ((grp >> j) & 1u)) acc = __dadd_rn(acc, y);
           }
         }
+        if (leader) tv[slot] = acc;
         __syncwarp();
       }
-      __syncthreads();
     }
-    // w(v, cur) and the argmax over the table (resetting a global table).
-    if (threadIdx.x == 0) s_wcur = 0.0;
     __syncthreads();
-    const u64 nscan = shared_tab ? cap : s_used;
-    for (u64 x = threadIdx.x; x < nscan; x += BIG_THREADS) {
-      u64 sl = shared_tab ? x : g_list[x];
-      if (tk[sl] == cur) s_wcur = tv[sl];
+    // w(v, cur), then the argmax over the table (resetting a global table).
+    if (tid == 0) {
+      double wc = 0.0;
+      u64 sl = hash32(cur) & mask;
+      while (tk[sl] != NONE32) {
+        if (tk[sl] == cur) {
+          wc = tv[sl];
+          break;
+        }
+        sl = (sl + 1) & mask;
+      }
+      s_wcur = wc;
     }
     __syncthreads();
     const double wcur = s_wcur;
     const double dcur = A.d[cur];
+    const u32 nscan = global ? s_gused : cap;
     double g = -1.0;
     u32 p = NONE32, kk = cur;
-    for (u64 x = threadIdx.x; x < nscan; x += BIG_THREADS) {
-      u64 sl = shared_tab ? x : g_list[x];
-      u32 key = tk[sl];
+    for (u32 x = tid; x < nscan; x += BIG_THREADS) {
+      const u64 sl = global ? g_list[x] : x;
+      const u32 key = tk[sl];
       if (key == NONE32) continue;
       const double val = tv[sl];
       const u32 pp = tp[sl];
-      if (!shared_tab) {
+      if (global) {
         tk[sl] = NONE32;
         tv[sl] = 0.0;
         tp[sl] = NONE32;
       }
       if (key == cur || A.tw == 0.0) continue;
       if (KIND == EVAL_REFINE && A.blocked[key]) continue;
-      double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, A.d[key]);
+      const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, A.d[key]);
       ++ncand;
       if (p == NONE32 || gn > g || (gn == g && pp < p)) {
         g = gn;
@@ -599,9 +697,9 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
       }
     }
     for (int o = 16; o; o >>= 1) {
-      double og = __shfl_xor_sync(0xffffffffu, g, o);
-      u32 op = __shfl_xor_sync(0xffffffffu, p, o);
-      u32 ok = __shfl_xor_sync(0xffffffffu, kk, o);
+      const double og = __shfl_xor_sync(0xffffffffu, g, o);
+      const u32 op = __shfl_xor_sync(0xffffffffu, p, o);
+      const u32 ok = __shfl_xor_sync(0xffffffffu, kk, o);
       if (op != NONE32 && (p == NONE32 || og > g || (og == g && op < p))) {
         g = og;
         p = op;
@@ -614,8 +712,8 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
       r_k[wib] = kk;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      for (u32 x = 1; x < BIG_THREADS / 32; ++x) {
+    if (tid == 0) {
+      for (u32 x = 1; x < BIG_WARPS; ++x) {
         if (r_p[x] != NONE32 && (p == NONE32 || r_g[x] > g || (r_g[x] == g && r_p[x] < p))) {
           g = r_g[x];
           p = r_p[x];
@@ -666,7 +764,7 @@ __global__ void k_fill_u32(u32* p, u32 v, u64 n) {
 }
 
 static size_t big_smem() {
-  return (size_t)BIG_TAB * (4 + 4 + 8) + (size_t)BIG_THREADS * (4 + 8);
+  return (size_t)BIG_TAB * (8 + 4 + 4) + (size_t)BIG_THREADS * (8 + 4 + 4);
 }
 
 static bool g_big_attr_set[64] = {false};

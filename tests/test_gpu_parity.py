@@ -284,10 +284,10 @@ def test_canonicalize_gpu():
 
 # ---- very high degree vertices (block kernel, shared and global tables) -----
 @pytest.mark.parametrize("integral", [True, False])
-@pytest.mark.parametrize("hub_deg", [300, 3000, 6000])
+@pytest.mark.parametrize("hub_deg", [300, 3000, 6000, 20000])
 def test_move_eval_hubs_bit_exact(integral, hub_deg):
     rng = np.random.default_rng(hub_deg)
-    n = 9000
+    n = max(9000, hub_deg + 1000)
     src, dst, w = gh.random_graph(rng, n, 20000, integral)
     hs = np.zeros(hub_deg, np.uint32)
     hd = rng.choice(np.arange(1, n), hub_deg, replace=False).astype(np.uint32)
@@ -309,7 +309,8 @@ def test_move_eval_hubs_bit_exact(integral, hub_deg):
 
 
 @pytest.mark.parametrize("integral", [True, False])
-def test_inc_refinement_hub_bit_exact(integral):
+@pytest.mark.parametrize("ncomm", [1, 3])
+def test_inc_refinement_hub_bit_exact(integral, ncomm):
     rng = np.random.default_rng(7)
     n = 7000
     src, dst, w = gh.random_graph(rng, n, 15000, integral)
@@ -318,7 +319,8 @@ def test_inc_refinement_hub_bit_exact(integral):
     g = O.Graph.from_edges(n, np.concatenate([src, np.zeros(5000, np.uint32)]),
                            np.concatenate([dst, hd]), np.concatenate([w, hw])
                            ).apply_delta([], [], [], keep_self_loops=True)
-    f = gh.random_partition(rng, n, 3)
+    # one community: the hub sees ~5000 distinct sub-communities (global table)
+    f = gh.random_partition(rng, n, ncomm)
     s0 = np.arange(n, dtype=np.uint32)
     aff = np.ones(n, bool)
     ref_s, ref_r = O.inc_refinement(g, f, s0, aff, 1.0, O.MODE_THROUGHPUT)
