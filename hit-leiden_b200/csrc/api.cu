@@ -810,6 +810,11 @@ hl_status hl_dbg_inc_refinement(int32_t device, uint32_t n, const uint64_t* off,
   });
 }
 
+hl_status hl_dbg_set_exact_tfilter(int32_t on) {
+  g_exact_tfilter.store(on ? 1 : 0);
+  return HL_OK;
+}
+
 hl_status hl_dbg_inc_aggregation(int32_t device, uint32_t n, const uint64_t* off,
                                  const uint32_t* col, const double* w, const uint32_t* dsrc,
                                  const uint32_t* ddst, const double* dw, uint64_t dk,

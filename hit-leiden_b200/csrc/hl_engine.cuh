@@ -1,5 +1,6 @@
 // hl_engine.cuh — device state of one graph handle and the stage entry points.
 #pragma once
+#include <atomic>
 #include <cub/cub.cuh>
 
 #include "hl_internal.cuh"
@@ -72,6 +73,9 @@ struct Scratch {
   DBuf<u8> affsc, cand_sc, blocked;
   DBuf<u32> sizes;
   DBuf<double> dS, wsp, dcomm;
+  DBuf<u64> wcnt;       // T-filter: terms of each any-order sum
+  DBuf<u8> amb;         // T-filter: S whose decision needs the ordered sum
+  DBuf<u32> longrows;   // T-filter: member rows summed by a whole block
   DBuf<u32> upd_node, upd_to;
   // reductions
   DBuf<double> red, red2;
@@ -187,9 +191,13 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
 // refine.cu
 struct RefineOut {
   u64 splits = 0, merges = 0, refined = 0;
+  u64 tfilter_exact = 0;  // candidates decided from the ordered sum
   u32 smax_before = 0;
 };
 RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community);
+
+// Test switch: decide every T-filter candidate from the ordered sum.
+extern std::atomic<int> g_exact_tfilter;
 
 // aggregate.cu
 u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n,

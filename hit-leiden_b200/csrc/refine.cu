@@ -168,21 +168,94 @@ __global__ void k_min_member(u32 n, const u32* s, const u8* cand, u32* minmem) {
     if (cand[s[v]]) atomicMin(&minmem[s[v]], (u32)v);
 }
 
-// w(S, C_parent) with integral weights: per-member partial sums, any order.
-__global__ void k_wsp_atomic(u32 n, const u64* off, const u32* col, const double* w, const u32* f,
-                             const u32* s, const u8* cand, const u32* minmem, double* wsp) {
+// w(S, C_parent) summed in any order, with the number of terms.  The T-filter
+// only needs the side of its threshold on which the ordered sum falls, and
+// the any-order sum plus a rounding-error bound decides that for almost every
+// S (k_blocked_bounds).  A warp per member row; rows longer than LONG_ROW go to
+// a list that k_wsp_any_long covers with a whole block per row.
+constexpr u32 LONG_ROW = 4096;
+
+__device__ __forceinline__ void wsp_row_part(u64 a, u64 b, u64 step, const u32* col,
+                                             const double* w, const u32* f, u32 parent,
+                                             double& x, unsigned long long& c) {
+  u64 p = a;
+  for (; p + 3 * step < b; p += 4 * step) {
+    const u32 c0 = col[p], c1 = col[p + step], c2 = col[p + 2 * step], c3 = col[p + 3 * step];
+    const double w0 = w[p], w1 = w[p + step], w2 = w[p + 2 * step], w3 = w[p + 3 * step];
+    const u32 f0 = f[c0], f1 = f[c1], f2 = f[c2], f3 = f[c3];
+    if (f0 == parent) x += w0, ++c;
+    if (f1 == parent) x += w1, ++c;
+    if (f2 == parent) x += w2, ++c;
+    if (f3 == parent) x += w3, ++c;
+  }
+  for (; p < b; p += step)
+    if (f[col[p]] == parent) x += w[p], ++c;
+}
+
+__global__ void k_wsp_any(u32 n, const u64* off, const u32* col, const double* w, const u32* f,
+                          const u32* s, const u8* cand, const u32* minmem, double* wsp,
+                          unsigned long long* wcnt, u32* longrows, u32* nlong) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 v = warp; v < n; v += nwarps) {
-    u32 S = s[v];
+    const u32 S = s[v];
     if (!cand[S]) continue;
-    u32 parent = f[minmem[S]];
+    const u64 o0 = off[v], o1 = off[v + 1];
+    if (o1 - o0 > LONG_ROW) {
+      if (lane == 0) longrows[atomicAdd(nlong, 1u)] = (u32)v;
+      continue;
+    }
+    const u32 parent = f[minmem[S]];
     double x = 0.0;
-    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32)
-      if (f[col[p]] == parent) x += w[p];
-    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0 && x != 0.0) atomicAdd(&wsp[S], x);
+    unsigned long long c = 0;
+    wsp_row_part(o0 + lane, o1, 32, col, w, f, parent, x, c);
+    for (int o = 16; o; o >>= 1) {
+      x += __shfl_xor_sync(0xffffffffu, x, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0 && c) {
+      atomicAdd(&wsp[S], x);
+      atomicAdd(&wcnt[S], c);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_wsp_any_long(const u32* longrows, const u32* nlong,
+                                                      const u64* off, const u32* col,
+                                                      const double* w, const u32* f, const u32* s,
+                                                      const u32* minmem, double* wsp,
+                                                      unsigned long long* wcnt) {
+  __shared__ double sx[8];
+  __shared__ unsigned long long sc[8];
+  const u32 lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const u32 nl = *nlong;
+  for (u32 t = blockIdx.x; t < nl; t += gridDim.x) {
+    const u32 v = longrows[t];
+    const u32 S = s[v];
+    const u32 parent = f[minmem[S]];
+    double x = 0.0;
+    unsigned long long c = 0;
+    wsp_row_part(off[v] + threadIdx.x, off[v + 1], 256, col, w, f, parent, x, c);
+    for (int o = 16; o; o >>= 1) {
+      x += __shfl_xor_sync(0xffffffffu, x, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
+      sx[wib] = x;
+      sc[wib] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tx = 0.0;
+      unsigned long long tc = 0;
+      for (int j = 0; j < 8; ++j) tx += sx[j], tc += sc[j];
+      if (tc) {
+        atomicAdd(&wsp[S], tx);
+        atomicAdd(&wcnt[S], tc);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -208,20 +281,58 @@ __global__ void k_wsp_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 t
   }
 }
 
-__global__ void k_blocked(u32 ns, const u8* cand, const double* dS, const double* wsp,
-                          const u32* minmem, const u32* f, const double* dcomm, double tw,
-                          double gamma, u8* blocked) {
+// T-filter decision from the any-order sum x of N positive terms.  The ordered
+// sum the reference computes and x are both within γ_{N-1}·Σ of the exact sum
+// (any summation tree of N terms), so they differ by at most
+// 2γ_{N-1}/(1-γ_{N-1})·x < 2.0001·N·u·x (u = 2^-53); the window used here is
+// 8·N·u·x, which also covers the rounding of the window itself.  ΔQ(S→∅) is
+// non-increasing in w(S, C) (every rounding step is monotone), so the decision
+// is certain when both ends of the window agree; otherwise S is flagged for
+// the exact ordered sum.  With integral weights (exact in any order) or N <= 1
+// the window is empty.
+__global__ void k_blocked_bounds(u32 ns, const u8* cand, const double* dS, const double* wsp,
+                                 const unsigned long long* wcnt, const u32* minmem,
+                                 const u32* f, const double* dcomm, double tw, double gamma,
+                                 bool exact_sums, bool force_exact, u8* blocked, u8* amb,
+                                 u32* namb) {
+  u32 local = 0;
   for (u64 S = blockIdx.x * (u64)blockDim.x + threadIdx.x; S < ns; S += (u64)gridDim.x * blockDim.x) {
-    u8 b = 0;
+    u8 b = 0, a = 0;
     if (cand[S]) {
-      double ds = dS[S];
+      const double ds = dS[S];
       if (ds > 0.0) {
-        double dpar = dcomm[f[minmem[S]]];
-        double dq = remove_gain(wsp[S], tw, gamma, ds, dpar);
-        b = dq > 1e-9 ? 1 : 0;
+        const double dpar = dcomm[f[minmem[S]]];
+        const double x = wsp[S];
+        const unsigned long long N = wcnt[S];
+        if (force_exact && N > 1) {
+          a = 1;
+        } else if (exact_sums || N <= 1) {
+          b = remove_gain(x, tw, gamma, ds, dpar) > 1e-9 ? 1 : 0;
+        } else {
+          const double err = __dmul_rn(__dmul_rn(x, (double)N), 0x1p-50);
+          const double lo = fmax(__dsub_rn(x, err), 0.0);
+          const double hi = __dadd_rn(x, err);
+          if (remove_gain(hi, tw, gamma, ds, dpar) > 1e-9) b = 1;
+          else if (!(remove_gain(lo, tw, gamma, ds, dpar) > 1e-9)) b = 0;
+          else a = 1;
+        }
       }
     }
     blocked[S] = b;
+    amb[S] = a;
+    local += a;
+  }
+  if (local) atomicAdd(namb, local);
+}
+
+// Exact decision for the flagged S, from the ordered sum.
+__global__ void k_blocked_exact(u32 ns, const u8* amb, const double* dS, const double* wsp,
+                                const u32* minmem, const u32* f, const double* dcomm, double tw,
+                                double gamma, u8* blocked) {
+  for (u64 S = blockIdx.x * (u64)blockDim.x + threadIdx.x; S < ns; S += (u64)gridDim.x * blockDim.x) {
+    if (!amb[S]) continue;
+    const double dpar = dcomm[f[minmem[S]]];
+    blocked[S] = remove_gain(wsp[S], tw, gamma, dS[S], dpar) > 1e-9 ? 1 : 0;
   }
 }
 
@@ -274,6 +385,8 @@ static u32 select_flagged(Engine& E, const u8* flags, u32 n, u32* out, u32* cnt)
   });
   return E.read_u32(cnt);
 }
+
+std::atomic<int> g_exact_tfilter{0};
 
 RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   RefineOut out;
@@ -391,18 +504,33 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   HL_CUDA(cudaMemsetAsync(S.cand_sc.p, 0, s2cap, st));
   HL_CUDA(cudaMemsetAsync(S.minmem.p, 0xFF, sizeof(u32) * s2cap, st));
   HL_CUDA(cudaMemsetAsync(S.wsp.p, 0, sizeof(double) * s2cap, st));
+  S.wcnt.ensure(E.mem, s2cap);
+  S.amb.ensure(E.mem, s2cap);
+  HL_CUDA(cudaMemsetAsync(S.wcnt.p, 0, sizeof(u64) * s2cap, st));
+  HL_CUDA(cudaMemsetAsync(cnt + 10, 0, 2 * sizeof(u32), st));
   ++E.nlaunch, k_t_candidates<<<grid_for((u64)ns * 32), 256, 0, st>>>(single, ns, L.g.off.p, L.g.col.p, L.f.p,
                                                          s, S.cand_sc.p);
   ++E.nlaunch, k_min_member<<<grid_for(n), 256, 0, st>>>(n, s, S.cand_sc.p, S.minmem.p);
   HL_LAUNCH_CHECK();
-  if (E.integral) {
-    ++E.nlaunch, k_wsp_atomic<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, L.f.p, s,
-                                                         S.cand_sc.p, S.minmem.p, S.wsp.p);
-    HL_LAUNCH_CHECK();
-  } else {
-    // Members of candidate sub-communities, sorted by (S, v).
+  // any-order w(S, C_parent) and term counts
+  S.longrows.ensure(E.mem, n);
+  unsigned long long* wcnt = reinterpret_cast<unsigned long long*>(S.wcnt.p);
+  ++E.nlaunch, k_wsp_any<<<grid_for((u64)n * 32), 256, 0, st>>>(
+      n, L.g.off.p, L.g.col.p, L.g.w.p, L.f.p, s, S.cand_sc.p, S.minmem.p, S.wsp.p, wcnt,
+      S.longrows.p, cnt + 11);
+  ++E.nlaunch, k_wsp_any_long<<<148 * 4, 256, 0, st>>>(S.longrows.p, cnt + 11, L.g.off.p, L.g.col.p,
+                                                        L.g.w.p, L.f.p, s, S.minmem.p, S.wsp.p,
+                                                        wcnt);
+  ++E.nlaunch, k_blocked_bounds<<<grid_for(s2cap), 256, 0, st>>>(
+      (u32)s2cap, S.cand_sc.p, S.dS.p, S.wsp.p, wcnt, S.minmem.p, L.f.p, S.dcomm.p, L.tw,
+      E.cfg.resolution, E.integral, g_exact_tfilter.load() != 0, S.blocked.p, S.amb.p, cnt + 10);
+  HL_LAUNCH_CHECK();
+  const u32 namb = E.read_u32(cnt + 10);
+  out.tfilter_exact = namb;
+  if (namb) {
+    // Ordered w(S, C_parent) for the undecided S: members sorted by (S, v).
     S.next.ensure(E.mem, n);
-    ++E.nlaunch, k_member_keys<<<grid_for(n), 256, 0, st>>>(n, s, S.cand_sc.p, S.next.p);
+    ++E.nlaunch, k_member_keys<<<grid_for(n), 256, 0, st>>>(n, s, S.amb.p, S.next.p);
     HL_LAUNCH_CHECK();
     S.order.ensure(E.mem, n);
     u32 nm = select_flagged(E, S.next.p, n, S.order.p, cnt + 8);
@@ -437,11 +565,11 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
                                                   S.minmem.p, S.wsp.p);
       HL_LAUNCH_CHECK();
     }
+    ++E.nlaunch, k_blocked_exact<<<grid_for(s2cap), 256, 0, st>>>(
+        (u32)s2cap, S.amb.p, S.dS.p, S.wsp.p, S.minmem.p, L.f.p, S.dcomm.p, L.tw,
+        E.cfg.resolution, S.blocked.p);
+    HL_LAUNCH_CHECK();
   }
-  ++E.nlaunch, k_blocked<<<grid_for(s2cap), 256, 0, st>>>((u32)s2cap, S.cand_sc.p, S.dS.p, S.wsp.p, S.minmem.p,
-                                             L.f.p, S.dcomm.p, L.tw, E.cfg.resolution,
-                                             S.blocked.p);
-  HL_LAUNCH_CHECK();
   E.kt_end(KT_TFILTER, ev_tf);
 
   // ---- 5. Jacobi singleton merge -------------------------------------------

@@ -66,6 +66,13 @@ HL_API hl_status hl_dbg_inc_aggregation(int32_t device, uint32_t n, const uint64
 /* The fixed-shape pairwise sum used for 2m (tiles of 1024, stride halving). */
 HL_API hl_status hl_dbg_tree_sum(int32_t device, const double* x, uint64_t n, double* out);
 
+/* Test switch, process-wide: nonzero makes the refinement's T-filter decide
+ * every candidate from the ordered sum w(S, C) (hit_leiden.rs:1618-1625)
+ * instead of the any-order sum with its rounding window.  Results are the same
+ * either way; the switch lets tests cover the ordered path.  No reference
+ * counterpart. */
+HL_API hl_status hl_dbg_set_exact_tfilter(int32_t on);
+
 /* Modularity of `part` on the CSR (hit_leiden.rs:121-161). */
 HL_API hl_status hl_dbg_modularity(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
                             const double* w, const uint32_t* part, double* q);

@@ -2,6 +2,7 @@
 and shared generators for the GPU parity tests."""
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import importlib
 
@@ -67,6 +68,16 @@ def inc_movement(g: O.Graph, dsrc, ddst, dw, f, s, gamma, max_rounds=20, mark_mo
                                       max_rounds, int(mark_moved), L.ptr(ch), L.ptr(af),
                                       C.byref(it)))
     return f, ch.astype(bool), af.astype(bool), it.value
+
+
+@contextlib.contextmanager
+def exact_tfilter(on=True):
+    """Make the T-filter decide every candidate from the ordered sum."""
+    L.check(L.lib.hl_dbg_set_exact_tfilter(int(on)))
+    try:
+        yield
+    finally:
+        L.check(L.lib.hl_dbg_set_exact_tfilter(0))
 
 
 def inc_refinement(g: O.Graph, f, s, affected, gamma, cc_same_community=False):

@@ -12,6 +12,7 @@ import pytest
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
+gh = pytest.importorskip("tests.gpu_helpers")
 
 hl = importlib.import_module("hit-leiden_b200")
 W = importlib.import_module("hit-leiden_b200.workloads")
@@ -74,7 +75,13 @@ def test_e2e_unit_weights_inserts(levels, seed):
 
 @pytest.mark.parametrize("levels", [1, 10])
 @pytest.mark.parametrize("seed", [0, 1])
-def test_e2e_f64_weights_mixed(levels, seed):
+@pytest.mark.parametrize("exact", [False, True])
+def test_e2e_f64_weights_mixed(levels, seed, exact):
+    with gh.exact_tfilter(exact):
+        _f64_weights_mixed(levels, seed)
+
+
+def _f64_weights_mixed(levels, seed):
     n, s, d, w = small_planted(seed, weights=(0.5, 2.0))
     cfg = hl.RunConfig(max_iterations=levels)
     gs = hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w), cfg)

@@ -173,7 +173,8 @@ def test_gpu_kat_intra_deletion_activates():
 @pytest.mark.parametrize("seed", SEEDS)
 @pytest.mark.parametrize("integral", [True, False])
 @pytest.mark.parametrize("same_f", [False, True])
-def test_inc_refinement_bit_exact(seed, integral, same_f):
+@pytest.mark.parametrize("exact", [False, True])
+def test_inc_refinement_bit_exact(seed, integral, same_f, exact):
     rng, g = _graph(seed, n=400, m=1200, integral=integral)
     g = g.apply_delta([], [], [], keep_self_loops=True)
     n = g.n
@@ -183,7 +184,8 @@ def test_inc_refinement_bit_exact(seed, integral, same_f):
         aff = rng.random(n) < 0.3
         so = s0.copy()
         ref_s, ref_r = _oracle_refine(g, f, so, aff, same_f)
-        gs, gr = gh.inc_refinement(g, f, s0, aff, 1.0, same_f)
+        with gh.exact_tfilter(exact):
+            gs, gr = gh.inc_refinement(g, f, s0, aff, 1.0, same_f)
         assert np.array_equal(ref_s, gs)
         assert np.array_equal(ref_r, gr)
 
@@ -310,7 +312,8 @@ def test_move_eval_hubs_bit_exact(integral, hub_deg):
 
 @pytest.mark.parametrize("integral", [True, False])
 @pytest.mark.parametrize("ncomm", [1, 3])
-def test_inc_refinement_hub_bit_exact(integral, ncomm):
+@pytest.mark.parametrize("exact", [False, True])
+def test_inc_refinement_hub_bit_exact(integral, ncomm, exact):
     rng = np.random.default_rng(7)
     n = 7000
     src, dst, w = gh.random_graph(rng, n, 15000, integral)
@@ -324,5 +327,6 @@ def test_inc_refinement_hub_bit_exact(integral, ncomm):
     s0 = np.arange(n, dtype=np.uint32)
     aff = np.ones(n, bool)
     ref_s, ref_r = O.inc_refinement(g, f, s0, aff, 1.0, O.MODE_THROUGHPUT)
-    gs, gr = gh.inc_refinement(g, f, s0, aff, 1.0)
+    with gh.exact_tfilter(exact):
+        gs, gr = gh.inc_refinement(g, f, s0, aff, 1.0)
     assert np.array_equal(ref_s, gs) and np.array_equal(ref_r, gr)
