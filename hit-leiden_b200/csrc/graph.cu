@@ -270,14 +270,6 @@ __global__ void k_emit_loop_drops(u32 n, const u64* off, const u32* col, u64* rk
   }
 }
 
-__global__ void k_rowop_flags(const u32* rvals, u64 R, u32* isdel, u32* isins) {
-  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < R; t += (u64)gridDim.x * blockDim.x) {
-    bool d = rvals[t] == DEL_MARK;
-    isdel[t] = d ? 1u : 0u;
-    isins[t] = d ? 0u : 1u;
-  }
-}
-
 __global__ void k_rowop_deg(const u64* rkeys, const u32* rvals, u64 R, int* ddeg, u8* touched) {
   for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < R; t += (u64)gridDim.x * blockDim.x) {
     u32 r = (u32)(rkeys[t] >> 32);
@@ -291,58 +283,219 @@ __global__ void k_new_degrees(u32 n, const u64* off, const int* ddeg, u64* nd) {
     nd[v] = v < n ? (u64)((long long)(off[v + 1] - off[v]) + ddeg[v]) : 0ull;
 }
 
-// Warp per row: untouched rows are copied; touched rows are merged with their
-// sorted row-operations (deleted entries skipped, inserted entries placed by
-// rank), so the output row is again sorted by neighbour id.
+// Untouched rows of the new CSR, copied by output position: each block takes
+// COPY_CH consecutive output entries, finds the rows they span with one
+// search, stages those rows' new offsets in shared memory and maps every
+// entry to its row there.  Reads and writes stream; entries of touched rows
+// are left to k_merge_rows.
+constexpr u32 COPY_CH = 4096;
+constexpr u32 COPY_ROWS = 1024;
+
+// Largest i in [lo, hi) with a[i] <= x, given a[lo] <= x (a ascending).
+__device__ __forceinline__ u64 last_le_u64(const u64* a, u64 lo, u64 hi, u64 x) {
+  while (hi - lo > 1) {
+    const u64 mid = lo + (hi - lo) / 2;
+    if (a[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_copy_untouched(u32 n, const u64* off, const u32* col,
+                                                        const double* w, const u64* noff,
+                                                        u32* ncol, double* nw, const u8* touched,
+                                                        u64 nnz_new) {
+  __shared__ u64 s_noff[COPY_ROWS + 1];
+  __shared__ u32 s_rb, s_re;
+  for (u64 q0 = (u64)blockIdx.x * COPY_CH; q0 < nnz_new; q0 += (u64)gridDim.x * COPY_CH) {
+    const u64 q1 = q0 + COPY_CH < nnz_new ? q0 + COPY_CH : nnz_new;
+    if (threadIdx.x == 0) {
+      // rows r with noff[r] <= q < noff[r + 1]; noff[0] = 0 <= q0, noff[n] = nnz_new > q
+      const u64 rb = last_le_u64(noff, 0, (u64)n + 1, q0);
+      const u64 re = last_le_u64(noff, rb, (u64)n + 1, q1 - 1);
+      s_rb = (u32)rb;
+      s_re = (u32)re;
+    }
+    __syncthreads();
+    const u32 rb = s_rb;
+    const u32 nrow = s_re - rb + 1;
+    const bool staged = nrow <= COPY_ROWS;
+    if (staged)
+      for (u32 x = threadIdx.x; x <= nrow; x += blockDim.x) s_noff[x] = noff[rb + x];
+    __syncthreads();
+    for (u64 q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+      u32 r;
+      u64 nq;
+      if (staged) {
+        u32 lo = 0, hi = nrow;
+        while (hi - lo > 1) {
+          const u32 mid = (lo + hi) >> 1;
+          if (s_noff[mid] <= q) lo = mid;
+          else hi = mid;
+        }
+        r = rb + lo;
+        nq = s_noff[lo];
+      } else {
+        r = (u32)last_le_u64(noff, rb, (u64)rb + nrow, q);
+        nq = noff[r];
+      }
+      if (touched[r]) continue;
+      const u64 src = off[r] + (q - nq);
+      ncol[q] = col[src];
+      nw[q] = w[src];
+    }
+    __syncthreads();
+  }
+}
+
+// Row-operation range [rstart[r], rend[r]) of every row that has operations
+// (row-operations sorted by (row, neighbour)).
+__global__ void k_row_ranges(const u64* rkeys, u64 R, u32* rstart, u32* rend) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < R; t += (u64)gridDim.x * blockDim.x) {
+    const u32 r = (u32)(rkeys[t] >> 32);
+    if (t == 0 || (u32)(rkeys[t - 1] >> 32) != r) rstart[r] = (u32)t;
+    if (t + 1 == R || (u32)(rkeys[t + 1] >> 32) != r) rend[r] = (u32)(t + 1);
+  }
+}
+
+// Touched rows, merged with their sorted row-operations, so the output row is
+// again sorted by neighbour id: deleted entries are skipped, every surviving
+// entry moves by (inserts before it) - (deletes before it), and an insert
+// lands at its lower bound in the old row, after the earlier inserts and
+// before the entries it precedes.  A warp per row walks the old row in
+// chunks of 32 and consumes, per chunk, the operations whose neighbour is not
+// above the chunk's last one (all of them in the last chunk), 32 operations at
+// a time with bisections over lanes, so the row and its operations are each
+// read once and no step is serial in the number of operations.  A self-loop is stored twice in its row
+// and its operations come in pairs; operations on one neighbour come deletes
+// first (a dropped self-loop replaced by an inserted one).
 __global__ void k_merge_rows(u32 n, const u64* off, const u32* col, const double* w,
                              const u64* noff, u32* ncol, double* nw, const u8* touched,
-                             const u64* rkeys, const u32* rvals, u64 R, const u32* delpre,
-                             const u32* inspre, const double* neww, u64 nnz_new, u32* err) {
+                             const u64* rkeys, const u32* rvals, const u32* rstart,
+                             const u32* rend, const double* neww, u64 nnz_new, u32* err) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 r = warp; r < n; r += nwarps) {
-    u64 o0 = off[r], o1 = off[r + 1], no = noff[r];
-    if (!touched[r]) {
-      if (no + (o1 - o0) > nnz_new) {
-        if (lane == 0) atomicAdd(err, 1u);
-        continue;
-      }
-      for (u64 q = o0 + lane; q < o1; q += 32) {
-        ncol[no + (q - o0)] = col[q];
-        nw[no + (q - o0)] = w[q];
-      }
-      continue;
+    if (!touched[r]) continue;
+    const u64 o0 = off[r], o1 = off[r + 1], no = noff[r];
+    const u32 b = rend[r];
+    u32 p = rstart[r];
+    u32 drun = 0, irun = 0;       // deletes / inserts consumed so far
+    u32 del_key = NONE32;         // neighbour of the last consumed delete
+    u32 del_same = 0;             // consumed deletes on that neighbour
+    // operation tile [tb, tb + 32) in registers: neighbour, value (DEL_MARK
+    // for a delete, else the index of the inserted weight)
+    u32 tb = p;
+    u32 tk = NONE32, tv = 0;
+    if (tb + lane < b) {
+      tk = (u32)rkeys[tb + lane];
+      tv = rvals[tb + lane];
     }
-    u64 a = lower_bound_u64(rkeys, 0, R, (u64)r << 32);
-    u64 b = lower_bound_u64(rkeys, a, R, ((u64)r + 1) << 32);
-    u32 dbase = delpre[a], ibase = inspre[a];
-    for (u64 q = o0 + lane; q < o1; q += 32) {
-      u32 c = col[q];
-      u64 key = ((u64)r << 32) | c;
-      u64 lb = lower_bound_u64(rkeys, a, b, key);
-      bool deleted = lb < b && rkeys[lb] == key && rvals[lb] == DEL_MARK;
-      if (deleted) continue;
-      u64 out = no + (q - o0) - (delpre[lb] - dbase) + (inspre[lb] - ibase);
-      if (out >= nnz_new) {
-        atomicAdd(err, 1u);
-        continue;
+    // entry chunk prefetched one ahead
+    u32 c_n = o0 + lane < o1 ? col[o0 + lane] : NONE32;
+    double w_n = o0 + lane < o1 ? w[o0 + lane] : 0.0;
+    for (u64 base = o0;; base += 32) {
+      const bool last = base + 32 >= o1;
+      const u64 q = base + lane;
+      const bool valid = q < o1;
+      const u32 c = c_n;
+      const double wv = w_n;
+      if (!last) {
+        const u64 qn = q + 32;
+        c_n = qn < o1 ? col[qn] : NONE32;
+        w_n = qn < o1 ? w[qn] : 0.0;
       }
-      ncol[out] = c;
-      nw[out] = w[q];
-    }
-    for (u64 t = a + lane; t < b; t += 32) {
-      if (rvals[t] == DEL_MARK) continue;
-      u32 c = (u32)rkeys[t];
-      u64 lb = lower_bound_u64(rkeys, a, b, ((u64)r << 32) | c);
-      u64 qc = lower_bound_u32(col, o0, o1, c);
-      u64 out = no + (qc - o0) - (delpre[lb] - dbase) + (inspre[t] - ibase);
-      if (out >= nnz_new) {
-        atomicAdd(err, 1u);
-        continue;
+      const u32 vmask = __ballot_sync(0xffffffffu, valid);
+      const u32 c_last = vmask ? __shfl_sync(0xffffffffu, c, 31 - __clz(vmask)) : 0u;
+      const u32 d0 = drun, i0 = irun;
+      u32 dl = 0, il = 0;
+      // the two copies of a deleted self-loop may straddle two chunks: the
+      // earlier chunk consumed their deletes
+      bool deleted = valid && del_key != NONE32 && c == del_key;
+      while (p < b) {
+        const u32 o = p - tb;  // first unconsumed lane of the tile
+        const bool ok = tb + lane < b && lane >= o;
+        const u32 m = __ballot_sync(0xffffffffu, ok && (last || tk <= c_last));
+        const u32 cnt = __popc(m);  // lanes o .. o+cnt-1 (operations are sorted)
+        if (cnt) {
+          const u32 hiL = o + cnt;
+          const u32 delm = __ballot_sync(0xffffffffu, tv == DEL_MARK) & m;
+          // Entries: the consumed operations below c (lower bound of c among
+          // the tile's keys) and whether c itself is deleted.
+          u32 lo = o, hi = hiL;
+#pragma unroll
+          for (int it = 0; it < 6; ++it) {
+            const u32 mid = (lo + hi) >> 1;
+            const u32 km = __shfl_sync(0xffffffffu, tk, mid & 31);
+            if (lo < hi) {
+              if (km < c) lo = mid + 1;
+              else hi = mid;
+            }
+          }
+          const u32 ltm = m & (lo >= 32 ? 0xffffffffu : ((1u << lo) - 1u));
+          dl += __popc(ltm & delm);
+          il += __popc(ltm & ~delm);
+          const u32 kp = __shfl_sync(0xffffffffu, tk, lo & 31);
+          const u32 vp = __shfl_sync(0xffffffffu, tv, lo & 31);
+          if (valid && lo < hiL && kp == c && vp == DEL_MARK) deleted = true;
+          // Inserts: lower bound among the chunk's entries (padded with
+          // NONE32), earlier deletes below the key and earlier inserts.
+          u32 lo2 = 0, hi2 = 32;
+#pragma unroll
+          for (int it = 0; it < 6; ++it) {
+            const u32 mid = (lo2 + hi2) >> 1;
+            const u32 cm = __shfl_sync(0xffffffffu, c, mid & 31);
+            if (lo2 < hi2) {
+              if (cm < tk) lo2 = mid + 1;
+              else hi2 = mid;
+            }
+          }
+          const u32 grp = __match_any_sync(0xffffffffu, tk) & m;
+          const u32 before = (1u << lane) - 1u;
+          const bool ins = ((m >> lane) & 1u) && tv != DEL_MARK;
+          if (ins) {
+            const u32 dlt = drun + __popc(delm & before) - __popc(grp & delm & before) -
+                            (del_key == tk ? del_same : 0u);
+            const u64 out = no + (base + lo2 - o0) - dlt + irun + __popc(m & ~delm & before);
+            if (out >= nnz_new) {
+              atomicAdd(err, 1u);
+            } else {
+              ncol[out] = tk;
+              nw[out] = neww[tv];
+            }
+          }
+          if (delm) {
+            const u32 ld = 31 - __clz(delm);
+            const u32 kd = __shfl_sync(0xffffffffu, tk, ld);
+            const u32 same = __popc(__shfl_sync(0xffffffffu, grp, ld) & delm);
+            del_same = (del_key == kd) ? del_same + same : same;
+            del_key = kd;
+          }
+          drun += __popc(delm);
+          irun += cnt - __popc(delm);
+        }
+        p += cnt;
+        if (o + cnt < 32 || p >= b) break;
+        // the whole tile was consumed: load the next one
+        tb = p;
+        tk = NONE32;
+        tv = 0;
+        if (tb + lane < b) {
+          tk = (u32)rkeys[tb + lane];
+          tv = rvals[tb + lane];
+        }
       }
-      ncol[out] = c;
-      nw[out] = neww[rvals[t]];
+      if (valid && !deleted) {
+        const u64 out = no + (q - o0) - (d0 + dl) + (i0 + il);
+        if (out >= nnz_new) {
+          atomicAdd(err, 1u);
+        } else {
+          ncol[out] = c;
+          nw[out] = wv;
+        }
+      }
+      if (last) break;
     }
   }
 }
@@ -573,29 +726,12 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
       return cub::DeviceRadixSort::SortPairs(t, bytes, kin, kout, vin, vout, (int64_t)R, 0, 64, st);
     });
   }
-  S.delpre.ensure(E.mem, R + 1);
-  S.inspre.ensure(E.mem, R + 1);
-  // reuse: flags in segid/rowlist-sized temporaries
-  DBuf<u32>& fdel = S.cand_idx;
-  DBuf<u32>& fins = S.cand_to;
-  fdel.ensure(E.mem, R + 1);
-  fins.ensure(E.mem, R + 1);
-  ++E.nlaunch, k_rowop_flags<<<grid_for(R), 256, 0, st>>>(S.rvals2.p, R, fdel.p, fins.p);
+  require(R < 0xFFFFFFFFull, "too many row operations in one batch");
+  // row-operation range of every row that has operations
+  S.delpre.ensure(E.mem, n ? n : 1);
+  S.inspre.ensure(E.mem, n ? n : 1);
+  ++E.nlaunch, k_row_ranges<<<grid_for(R), 256, 0, st>>>(S.rkeys2.p, R, S.delpre.p, S.inspre.p);
   HL_LAUNCH_CHECK();
-  HL_CUDA(cudaMemsetAsync(fdel.p + R, 0, sizeof(u32), st));
-  HL_CUDA(cudaMemsetAsync(fins.p + R, 0, sizeof(u32), st));
-  {
-    u32* a = fdel.p;
-    u32* o = S.delpre.p;
-    cub_run(E, [&](void* t, size_t& bytes) {
-      return cub::DeviceScan::ExclusiveSum(t, bytes, a, o, (int64_t)R + 1, st);
-    });
-    u32* a2 = fins.p;
-    u32* o2 = S.inspre.p;
-    cub_run(E, [&](void* t, size_t& bytes) {
-      return cub::DeviceScan::ExclusiveSum(t, bytes, a2, o2, (int64_t)R + 1, st);
-    });
-  }
   S.ddeg.ensure(E.mem, n ? n : 1);
   S.touched.ensure(E.mem, n ? n : 1);
   HL_CUDA(cudaMemsetAsync(S.ddeg.p, 0, sizeof(int) * (n ? n : 1), st));
@@ -617,10 +753,13 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   ncol.ensure(E.mem, nnz_new ? nnz_new : 1);
   nw.ensure(E.mem, nnz_new ? nnz_new : 1);
   cudaEvent_t kev = E.kt_begin();
+  if (nnz_new)
+    ++E.nlaunch, k_copy_untouched<<<grid_for((nnz_new + COPY_CH - 1) / COPY_CH * 256), 256, 0, st>>>(
+        n, G.off.p, G.col.p, G.w.p, S.newoff.p, ncol.p, nw.p, S.touched.p, nnz_new);
   if (n)
     ++E.nlaunch, k_merge_rows<<<grid_for((u64)n * 32), 256, 0, st>>>(n, G.off.p, G.col.p, G.w.p, S.newoff.p,
                                                          ncol.p, nw.p, S.touched.p, S.rkeys2.p,
-                                                         S.rvals2.p, R, S.delpre.p, S.inspre.p,
+                                                         S.rvals2.p, S.delpre.p, S.inspre.p,
                                                          S.neww.p, nnz_new, S.cnt.p + 4);
   HL_LAUNCH_CHECK();
   E.kt_end(KT_MERGE_ROWS, kev);

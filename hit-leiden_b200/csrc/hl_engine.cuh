@@ -51,7 +51,7 @@ struct Scratch {
   DBuf<u8> op, touched, ktouched, isdel, isins;
   DBuf<double> neww;
   DBuf<u32> nops_del, nops_ins, pos_del, pos_ins;
-  DBuf<u32> delpre, inspre;
+  DBuf<u32> delpre, inspre;  // per-row operation ranges (start, end) of apply_delta
   DBuf<int> ddeg;
   DBuf<u64> newoff;
   DBuf<u32> rowlist;

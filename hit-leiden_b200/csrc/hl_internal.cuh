@@ -173,19 +173,38 @@ __device__ __forceinline__ double remove_gain(double w_sc, double tw, double gam
 // extended in lane order through shuffles.  All lanes must call it with the
 // same arguments; all lanes return the same result.  `val(t)` returns the
 // t-th value; `take(t)` says whether it is part of the sum.
+//
+// The next chunk is loaded while the current one is folded.  A chunk with
+// many taken values is folded by an unrolled pass (the 32 shuffles do not
+// depend on the running sum, so only the additions form the chain); a sparse
+// one walks its set lanes.
 template <typename V, typename P>
 __device__ __forceinline__ double warp_ordered_sum(u64 a, u64 b, double acc, V val, P take) {
   const u32 lane = threadIdx.x & 31;
+  if (a >= b) return acc;
+  u64 t = a + lane;
+  bool ok = t < b && take(t);
+  double x = ok ? val(t) : 0.0;
   for (u64 base = a; base < b; base += 32) {
-    u64 t = base + lane;
-    bool ok = t < b && take(t);
-    double x = ok ? val(t) : 0.0;
+    const u64 tn = base + 32 + lane;
+    const bool okn = tn < b && take(tn);
+    const double xn = okn ? val(tn) : 0.0;
     u32 m = __ballot_sync(0xffffffffu, ok);
-    while (m) {
-      int j = __ffs(m) - 1;
-      acc = __dadd_rn(acc, __shfl_sync(0xffffffffu, x, j));
-      m &= m - 1;
+    if (__popc(m) > 8) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const double y = __shfl_sync(0xffffffffu, x, j);
+        if ((m >> j) & 1u) acc = __dadd_rn(acc, y);
+      }
+    } else {
+      while (m) {
+        int j = __ffs(m) - 1;
+        acc = __dadd_rn(acc, __shfl_sync(0xffffffffu, x, j));
+        m &= m - 1;
+      }
     }
+    x = xn;
+    ok = okn;
   }
   return acc;
 }

@@ -51,6 +51,33 @@ def test_apply_delta_bit_exact(seed, integral, keep_loops):
     assert gh.same_bits(go, ro) and gh.same_bits(gc, rc) and gh.same_bits(gw, rw)
 
 
+@pytest.mark.parametrize("before", [30, 31, 32, 63])
+@pytest.mark.parametrize("keep_loops", [False, True])
+def test_apply_delta_self_loop_across_chunks(before, keep_loops):
+    # The self-loop of vertex v is stored twice in its row, at positions
+    # `before` and `before + 1`: the warp merge reads rows 32 entries at a time,
+    # so the two copies sit in one chunk or straddle two.
+    n = 200
+    v = 150
+    nb = list(range(before)) + list(range(v + 1, v + 11))
+    src = [v] * len(nb) + [v]
+    dst = nb + [v]
+    w = [1.0 + 0.25 * (i % 5) for i in range(len(nb))] + [4.0]
+    g = O.Graph.from_edges(n, src, dst, w).apply_delta([], [], [], keep_self_loops=True)
+    off, col, _ = g.csr()
+    row = col[off[v]:off[v + 1]].tolist()
+    assert row[before] == v and row[before + 1] == v
+    cases = [([v], [v], [-4.0]),                        # delete the loop
+             ([v, v, 3], [v, v + 20, 4], [-4.0, 2.0, 1.0]),  # delete it, insert around it
+             ([v, 0], [v, v], [1.5, -1.0]),             # reweight it, delete an edge before it
+             ([v, 7], [v + 30, 8], [1.0, 1.0])]         # untouched loop in a touched row
+    for ds, dd, dw in cases:
+        ref = g.apply_delta(ds, dd, dw, keep_self_loops=keep_loops)
+        go, gc, gw = gh.apply_delta(g, ds, dd, dw, keep_loops)
+        ro, rc, rw = ref.csr()
+        assert gh.same_bits(go, ro) and gh.same_bits(gc, rc) and gh.same_bits(gw, rw)
+
+
 def test_apply_delta_drops_existing_self_loops():
     g = O.Graph.from_edges(3, [0, 0], [0, 1], [5.0, 1.0])
     off, col, w = gh.apply_delta(g, [2], [2], [3.0], keep_loops=False)
