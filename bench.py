@@ -263,20 +263,12 @@ def main():
             run_reference(args, cfg)
         return
     import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    R = importlib.import_module("hit-leiden_b200.replicas")
+    rep = R.Replicas("nccl")
     torch.cuda.set_device(local)
     hl = importlib.import_module("hit-leiden_b200")
     L = importlib.import_module("hit-leiden_b200._lib")
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    barrier = rep.barrier
 
     n, s, d, w, wts, ins, pref = make_graph(args.config, args.seed, args.ncu_small)
     k = cfg["batch"]
@@ -321,12 +313,8 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    tot_ms = float(sum(dev_ms))
-    if dist is not None:
-        t = torch.tensor([tot_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = world * K * k / (tot_ms / 1000.0)
+    tot_ms = rep.max_over_ranks(float(sum(dev_ms)))
+    value = rep.whole_job_rate(K, k, tot_ms / 1000.0)
 
     kst = (L.KernelStat * 32)()
     cnt = C.c_uint32()
@@ -347,12 +335,8 @@ def main():
         e2e_s.append(time.perf_counter() - t1)
     torch.cuda.synchronize()
     barrier()
-    tot_e2e = float(sum(e2e_s))
-    if dist is not None:
-        t = torch.tensor([tot_e2e], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_e2e = float(t.item())
-    e2e_val = world * K * k / tot_e2e
+    tot_e2e = rep.max_over_ranks(float(sum(e2e_s)))
+    e2e_val = rep.whole_job_rate(K, k, tot_e2e)
     lat = sorted(1000.0 * x for x in e2e_s)
 
     ev = kernels.get("move_eval", {})
@@ -405,8 +389,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     st.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
