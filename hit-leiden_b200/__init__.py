@@ -6,8 +6,9 @@ reference crate's API.  Importing it fails loudly if the library is missing.
 """
 from ._lib import HitLeidenError, BatchStats  # noqa: F401  (loads libhl.so)
 from .api import (GraphInput, PartitionResult, PartitionState, RunConfig, RunMode,  # noqa: F401
-                  RunOutcome, canonicalize_community_ids, compute_modularity, hit_leiden, run)
+                  RunOutcome, Server, apply_batches, canonicalize_community_ids,
+                  compute_modularity, hit_leiden, run)
 
 __all__ = ["GraphInput", "PartitionResult", "PartitionState", "RunConfig", "RunMode", "RunOutcome",
            "HitLeidenError", "BatchStats", "canonicalize_community_ids", "compute_modularity",
-           "hit_leiden", "run"]
+           "hit_leiden", "run", "apply_batches", "Server"]

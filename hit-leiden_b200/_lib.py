@@ -53,6 +53,18 @@ class BatchStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class RequestDone(C.Structure):
+    """hl_request_done: completion record of one served request."""
+    _fields_ = [("request_id", C.c_uint64), ("batch_id", C.c_uint64), ("batch_seq", C.c_uint64),
+                ("edges", C.c_uint64), ("batch_edges", C.c_uint64), ("changed", C.c_uint64),
+                ("modularity", C.c_double), ("queue_ms", C.c_double), ("service_ms", C.c_double),
+                ("latency_ms", C.c_double), ("graph", C.c_uint32), ("batch_requests", C.c_uint32),
+                ("status", C.c_int32), ("pad_", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+
 class HitLeidenError(RuntimeError):
     """Error raised by the library; ``kind`` mirrors HitLeidenError's variants
     (src/core/error.rs:19-27) plus the device-side statuses."""
@@ -92,6 +104,17 @@ def _load():
         "hl_modularity_of": (st, [vp, vp, C.POINTER(C.c_double)]),
         "hl_canonicalize": (st, [C.c_int32, vp, C.c_uint64]),
         "hl_destroy": (None, [vp]),
+        "hl_device_bytes": (st, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "hl_apply_batches": (st, [vp, vp, vp, vp, vp, C.c_uint32, C.c_uint32, vp,
+                                  C.POINTER(BatchStats)]),
+        "hl_server_create": (st, [C.c_uint32, C.c_uint64, C.POINTER(vp)]),
+        "hl_server_add_graph": (st, [vp, vp, p32]),
+        "hl_server_set_edge_estimate": (st, [vp, C.c_uint64]),
+        "hl_server_submit": (st, [vp, C.c_uint32, vp, vp, vp, C.c_uint64,
+                                  C.POINTER(C.c_uint64)]),
+        "hl_server_poll": (st, [vp, C.POINTER(RequestDone), C.c_uint32, p32, C.c_int32]),
+        "hl_server_drain": (st, [vp]),
+        "hl_server_destroy": (None, [vp]),
         "hl_last_error": (C.c_char_p, []),
         "hl_version": (C.c_char_p, []),
         "hl_dbg_move_eval": (st, [C.c_int32, C.c_uint32, vp, vp, vp, vp, vp, C.c_uint64, vp,

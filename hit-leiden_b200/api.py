@@ -264,6 +264,98 @@ def hit_leiden(state: PartitionState, delta_g: GraphInput, gamma: float = 1.0,
     return state.apply_batch(src, dst, w).iterations
 
 
+# ---------------------------------------------------------------------------
+# Many graphs on one GPU (no reference counterpart): batching and serving.
+# ---------------------------------------------------------------------------
+def apply_batches(states: Sequence[PartitionState], batches, workers: int = 16):
+    """Batching form: apply batches[i] = (src, dst, w or None) to states[i] for
+    every i at once (hl_apply_batches).  Each state ends exactly as
+    ``states[i].apply_batch(*batches[i])`` would leave it; graphs run
+    concurrently on their own streams.  Returns the per-graph BatchStats."""
+    n = len(states)
+    if len(batches) != n:
+        raise HitLeidenError(L.HL_ERR_INVALID_INPUT, "one batch per state is required")
+    keep = []
+    hs = (C.c_void_p * n)()
+    ps = (C.c_void_p * n)()
+    pd = (C.c_void_p * n)()
+    pw = (C.c_void_p * n)()
+    ks = (C.c_uint64 * n)()
+    for i, (st, b) in enumerate(zip(states, batches)):
+        src, dst = L.u32(b[0]), L.u32(b[1])
+        w = L.f64(b[2]) if len(b) > 2 else None
+        keep.append((src, dst, w))
+        hs[i] = st._h.value if isinstance(st._h, C.c_void_p) else st._h
+        ps[i] = src.ctypes.data if len(src) else None
+        pd[i] = dst.ctypes.data if len(dst) else None
+        pw[i] = w.ctypes.data if (w is not None and len(w)) else None
+        ks[i] = len(src)
+    stats = (L.BatchStats * n)()
+    statuses = (C.c_int * n)()
+    vp = C.c_void_p
+    L.check(L.lib.hl_apply_batches(C.cast(hs, vp), C.cast(ps, vp), C.cast(pd, vp), C.cast(pw, vp),
+                                   C.cast(ks, vp), n, int(workers), C.cast(statuses, vp), stats))
+    for st, s_ in zip(states, stats):
+        st.last_stats = s_
+    return list(stats)
+
+
+class Server:
+    """Serving form (hl_server_*): a request loop over resident graphs.
+
+    Requests are admitted against ``hbm_budget`` bytes (0 = unlimited); the
+    requests a graph receives while it is being updated are coalesced, in
+    arrival order, into its next batch; ``workers`` threads update different
+    graphs concurrently.  The server does not own the states: close it first."""
+
+    def __init__(self, workers: int = 8, hbm_budget: int = 0):
+        self._s = C.c_void_p()
+        L.check(L.lib.hl_server_create(int(workers), int(hbm_budget), C.byref(self._s)))
+        self._states = []
+
+    def add(self, state: PartitionState) -> int:
+        gid = C.c_uint32()
+        L.check(L.lib.hl_server_add_graph(self._s, state._h, C.byref(gid)))
+        self._states.append(state)
+        return gid.value
+
+    def set_edge_estimate(self, bytes_per_edge: int) -> None:
+        L.check(L.lib.hl_server_set_edge_estimate(self._s, int(bytes_per_edge)))
+
+    def submit(self, graph_id: int, src, dst, w=None) -> int:
+        src, dst, w = L.u32(src), L.u32(dst), L.f64(w)
+        rid = C.c_uint64()
+        L.check(L.lib.hl_server_submit(self._s, int(graph_id), L.ptr(src), L.ptr(dst), L.ptr(w),
+                                       len(src), C.byref(rid)))
+        return rid.value
+
+    def poll(self, cap: int = 4096, wait_ms: int = 0):
+        out = (L.RequestDone * cap)()
+        cnt = C.c_uint32()
+        L.check(L.lib.hl_server_poll(self._s, out, cap, C.byref(cnt), int(wait_ms)))
+        return [out[i].as_dict() for i in range(cnt.value)]
+
+    def drain(self) -> None:
+        L.check(L.lib.hl_server_drain(self._s))
+
+    def close(self) -> None:
+        if self._s:
+            L.lib.hl_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def compute_modularity(graph: GraphInput, node_to_community) -> float:
     """compute_modularity (hit_leiden.rs:121-161) on the GPU."""
     src, dst, w = graph.arrays()

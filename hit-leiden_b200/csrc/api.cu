@@ -408,6 +408,31 @@ static void apply_impl(hl_graph* g, const uint32_t* src, const uint32_t* dst, co
   finish_stats(B, stats);
 }
 
+namespace hl {
+
+// Entry points for the multi-graph executors (multi.cu): one batch on one
+// handle, with the error captured for the calling thread; device bytes held.
+hl_status apply_on_handle(hl_graph* g, const uint32_t* src, const uint32_t* dst, const double* w,
+                          uint64_t k, hl_batch_stats* stats, std::string* err) {
+  try {
+    apply_impl(g, src, dst, w, k, false, stats);
+    return HL_OK;
+  } catch (const Error& e) {
+    if (err) *err = e.what();
+    return e.status;
+  } catch (const std::exception& e) {
+    if (err) *err = e.what();
+    return HL_ERR_CUDA;
+  } catch (...) {
+    if (err) *err = "unknown error";
+    return HL_ERR_CUDA;
+  }
+}
+
+u64 handle_device_bytes(const hl_graph* g) { return box(g)->E->mem.used; }
+
+}  // namespace hl
+
 extern "C" {
 
 hl_status hl_config_default(hl_config* cfg) {
@@ -576,6 +601,11 @@ hl_status hl_modularity(const hl_graph* g, double* q) { HL_TRY(modularity_impl(g
 
 hl_status hl_modularity_of(const hl_graph* g, const uint32_t* part, double* q) {
   HL_TRY(require(part != nullptr, "part is NULL"); modularity_impl(g, part, q));
+}
+
+hl_status hl_device_bytes(const hl_graph* g, uint64_t* used, uint64_t* peak) {
+  HL_TRY(require(g != nullptr, "graph handle is NULL"); const Engine& E = *box(g)->E;
+         if (used) *used = E.mem.used; if (peak) *peak = E.mem.peak);
 }
 
 void hl_destroy(hl_graph* g) {

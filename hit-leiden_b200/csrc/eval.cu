@@ -767,7 +767,7 @@ static size_t big_smem() {
   return (size_t)BIG_TAB * (8 + 4 + 4) + (size_t)BIG_THREADS * (8 + 4 + 4);
 }
 
-static bool g_big_attr_set[64] = {false};
+static std::atomic<bool> g_big_attr_set[64];
 
 constexpr u32 WIDE_MAX_BLOCKS = 148u * 4u;
 constexpr u32 BIG_MAX_BLOCKS = 148u * 3u;

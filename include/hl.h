@@ -174,6 +174,70 @@ HL_API hl_status hl_canonicalize(int32_t device, uint32_t* labels, uint64_t n);
 
 HL_API void hl_destroy(hl_graph* g);
 
+/* Device bytes the handle holds now and at most since creation. */
+HL_API hl_status hl_device_bytes(const hl_graph* g, uint64_t* used, uint64_t* peak);
+
+/* ---- Many graphs on one GPU (no reference counterpart: the reference
+ * updates one PartitionState per call) ------------------------------------
+ *
+ * Batching form.  Apply batch i (src[i], dst[i], w[i] — w may be NULL, or
+ * w[i] NULL for all-ones — of k[i] edges, host arrays) to graphs[i], for all
+ * i at once: up to `workers` host threads (0 = 16) each drive one graph at a
+ * time on that graph's own stream, so the graphs' kernels and round trips
+ * overlap on the GPU.  Each graph ends exactly as hl_apply_batch would leave
+ * it.  A handle may appear once per call.  statuses (may be NULL) receives
+ * each graph's status, stats (may be NULL) each graph's batch statistics;
+ * the return value is the first failing status (HL_OK if none). */
+HL_API hl_status hl_apply_batches(hl_graph* const* graphs, const uint32_t* const* src,
+                                  const uint32_t* const* dst, const double* const* w,
+                                  const uint64_t* k, uint32_t count, uint32_t workers,
+                                  hl_status* statuses, hl_batch_stats* stats);
+
+/* Serving form: a request loop over resident graphs.
+ *   - A request (edges for one registered graph, host arrays, copied at
+ *     submit) is admitted when the graphs' device bytes plus the estimates of
+ *     admitted, unfinished requests (bytes_per_edge × edges, default 512)
+ *     stay within hbm_budget (0 = no limit); a request that cannot fit even
+ *     with nothing in flight completes with HL_ERR_OUT_OF_MEMORY.
+ *   - `workers` threads update different graphs concurrently.  All requests
+ *     admitted for a graph while it is busy are coalesced into its next batch,
+ *     in arrival order; a graph's batches are applied one after another.
+ *   - Each request completes with an hl_request_done record (hl_server_poll).
+ * The server does not own the graph handles: destroy it before them. */
+typedef struct hl_server hl_server;
+typedef struct {
+  uint64_t request_id;
+  uint64_t batch_id;       /* server-wide batch number                          */
+  uint64_t batch_seq;      /* this graph's batch number, 1, 2, ... in order     */
+  uint64_t edges;          /* edges of this request                             */
+  uint64_t batch_edges;    /* edges of the coalesced batch it was applied in    */
+  uint64_t changed;        /* |B^1| of that batch                               */
+  double modularity;       /* NaN unless the graph has HL_FLAG_BATCH_MODULARITY */
+  double queue_ms;         /* submit -> its batch started                       */
+  double service_ms;       /* its batch started -> finished                     */
+  double latency_ms;       /* submit -> finished                                */
+  uint32_t graph;          /* graph id from hl_server_add_graph                 */
+  uint32_t batch_requests; /* requests coalesced into that batch                */
+  int32_t status;          /* hl_status of the batch                            */
+  uint32_t pad_;
+} hl_request_done;
+
+HL_API hl_status hl_server_create(uint32_t workers, uint64_t hbm_budget, hl_server** out);
+HL_API hl_status hl_server_add_graph(hl_server* s, hl_graph* g, uint32_t* graph_id);
+HL_API hl_status hl_server_set_edge_estimate(hl_server* s, uint64_t bytes_per_edge);
+HL_API hl_status hl_server_submit(hl_server* s, uint32_t graph_id, const uint32_t* src,
+                                  const uint32_t* dst, const double* w, uint64_t k,
+                                  uint64_t* request_id);
+/* Up to cap completed requests (oldest first) into out; *count receives how
+ * many.  wait_ms: 0 = do not wait, < 0 = wait until one completes or nothing
+ * is outstanding, > 0 = wait at most that long. */
+HL_API hl_status hl_server_poll(hl_server* s, hl_request_done* out, uint32_t cap, uint32_t* count,
+                                int32_t wait_ms);
+/* Wait until every submitted request has completed. */
+HL_API hl_status hl_server_drain(hl_server* s);
+/* Waits for outstanding requests, then stops the workers. */
+HL_API void hl_server_destroy(hl_server* s);
+
 /* Message for the last error on this thread (empty string if none). */
 HL_API const char* hl_last_error(void);
 
