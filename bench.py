@@ -50,6 +50,19 @@ CONFIGS = {
                     "batches of 10k updates (90% degree-preferential inserts, 10% deletes)",
         "batch": 10000,
     },
+    "batch256": {
+        "workload": "batching form: 256 independent planted graphs, vertices log-uniform "
+                    "[1k, 200k], mu log-uniform [0.1, 0.4], target mean degree U[4, 32], unit "
+                    "weights; per graph a batch of 1-5% of its edges (80% inserts, 20% deletes)",
+        "batch": 0,
+    },
+    "serve32": {
+        "workload": "serving form: 32 resident planted graphs, vertices log-uniform [100k, 5M] "
+                    "(x scale), mu 0.25, target mean degree 16; Poisson request arrivals at "
+                    "100 / 1,000 / 10,000 req/s, request sizes log-uniform [10, 100k] edges "
+                    "(85% inserts, 15% deletes), 120 GB admission budget",
+        "batch": 0,
+    },
     "ca_hepth": {
         "workload": "planted graph shaped like ca-HepTh: 9,877 vertices / ~21.8k unit edges, "
                     "mu 0.15, triangle closure; batches of 1,000 uniform inserts",
@@ -70,7 +83,13 @@ def parse():
     ap.add_argument("--cpu-sample-batches", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncu-small", action="store_true",
-                    help="small case for ncu captures (100k vertices, 2 warm-up steps)")
+                    help="small case for ncu captures (200k vertices)")
+    ap.add_argument("--workers", type=int, default=16,
+                    help="host worker threads of the batching / serving forms")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="vertex-count scale of the serving form's graphs")
+    ap.add_argument("--requests", type=int, default=400,
+                    help="requests per arrival rate in the serving form")
     return ap.parse_args()
 
 
@@ -252,15 +271,199 @@ def run_reference(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def _load_many(hl, graphs, levels, device, threads=16):
+    """Load and bootstrap many graphs concurrently (each on its own stream)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(g):
+        n, s, d, w = g
+        return hl.PartitionState.load(hl.GraphInput.from_arrays("g", n, s, d, w),
+                                      hl.RunConfig(max_iterations=levels, device=device))
+    with ThreadPoolExecutor(threads) as ex:
+        return list(ex.map(one, graphs))
+
+
+def run_batching(args, cfg):
+    """Batching form: every step applies one batch to each of 256 graphs, once
+    through hl_apply_batches (graphs concurrent) and once through the plain
+    per-graph path (a loop of hl_apply_batch) on an identical copy; both from
+    host arrays, host clock with the device synchronised on both sides."""
+    import torch
+    R = importlib.import_module("hit-leiden_b200.replicas")
+    W = importlib.import_module("hit-leiden_b200.workloads")
+    rep = R.Replicas("nccl")
+    torch.cuda.set_device(rep.local)
+    hl = importlib.import_module("hit-leiden_b200")
+    graphs = W.config4(args.seed + rep.rank)
+    rng = np.random.default_rng(args.seed + 7)
+    fracs = rng.uniform(0.01, 0.05, len(graphs))
+    A = _load_many(hl, graphs, args.levels, rep.local)
+    B = _load_many(hl, graphs, args.levels, rep.local)
+
+    def batches(step):
+        out = []
+        for i, (n, s, d, w) in enumerate(graphs):
+            k = max(1, int(fracs[i] * len(s)))
+            out.append(W.fast_batch(n, s, d, k, 0.8, (step + 1) * 1_000_003 + i))
+        return out
+    K, Wm = args.steps, args.warmup
+    t_plain = t_batch = 0.0
+    edges = 0
+    launches = 0
+    for step in range(Wm + K):
+        bs = batches(step)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for st, b in zip(B, bs):
+            st.apply_batch(*b)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        stats = hl.apply_batches(A, bs, workers=args.workers)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if step >= Wm:
+            t_plain += t1 - t0
+            t_batch += t2 - t1
+            edges += sum(len(b[0]) for b in bs)
+            launches += sum(x.launches for x in stats)
+    same = all(np.array_equal(a.community_mapping_per_level[0], b.community_mapping_per_level[0])
+               for a, b in zip(A, B))
+    t_batch = rep.max_over_ranks(t_batch)
+    t_plain = rep.max_over_ranks(t_plain)
+    value = rep.world * edges / t_batch
+    plain = rep.world * edges / t_plain
+    if rep.rank == 0:
+        line = {
+            "metric": "edge_updates_per_s", "value": value, "unit": "edge-updates/s",
+            "n_gpus": rep.world, "steps": K, "warmup": Wm, "ms_per_step": 1000.0 * t_batch / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": cfg["workload"], "graphs": len(graphs),
+                       "vertices": int(sum(g[0] for g in graphs)),
+                       "edges": int(sum(len(g[1]) for g in graphs)),
+                       "edges_per_step": edges // K, "workers": args.workers,
+                       "parallelism": f"replicas{rep.world}",
+                       "timing": "host clock, device synchronised on both sides",
+                       "plain_gpu_edge_updates_per_s": plain, "batched_over_plain": value / plain,
+                       "batched_equals_plain_bit_exact": bool(same)},
+            "e2e": {"value": value, "unit": "edge-updates/s",
+                    "h2d_bytes_per_step": int(16 * edges // K), "d2h_bytes_per_step": 0},
+            "gpu_launches": int(launches), "roofline": None, "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    for st in A + B:
+        st.close()
+    rep.close()
+
+
+def _serve(hl, states, reqs, arrivals, workers, coalesce, budget):
+    """Submit reqs[i] = (graph, u, v, w) at arrivals[i] seconds; return the
+    completion records and the wall time from the first submit to the last
+    completion."""
+    srv = hl.Server(workers=workers, hbm_budget=budget)
+    if coalesce is not None:
+        srv.set_coalescing(coalesce)
+    ids = [srv.add(s) for s in states]
+    t0 = time.perf_counter()
+    for (g, u, v, w), ta in zip(reqs, arrivals):
+        while True:
+            dt = ta - (time.perf_counter() - t0)
+            if dt <= 0:
+                break
+            if dt > 0.002:
+                time.sleep(dt - 0.001)
+        srv.submit(ids[g], u, v, w)
+    srv.drain()
+    t1 = time.perf_counter()
+    done = []
+    while True:
+        part = srv.poll(cap=4096)
+        if not part:
+            break
+        done += part
+    srv.close()
+    return done, t1 - t0
+
+
+def run_serving(args, cfg):
+    """Serving form at several arrival rates: the server (coalescing, several
+    workers, admission against 120 GB) against the plain per-request GPU path
+    (one request per batch, one at a time), on identical graph copies."""
+    import torch
+    W = importlib.import_module("hit-leiden_b200.workloads")
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    hl = importlib.import_module("hit-leiden_b200")
+    graphs = W.config5(args.seed + rank, scale=args.scale)
+    A = _load_many(hl, graphs, args.levels, local)
+    B = _load_many(hl, graphs, args.levels, local)
+    rng = np.random.default_rng(args.seed + 99)
+    rates = [100.0, 1000.0, 10000.0]
+    per_rate = []
+    for ri, rate in enumerate(rates):
+        nreq = args.requests
+        gsel = rng.integers(0, len(graphs), nreq)
+        sizes = np.exp(rng.uniform(np.log(10), np.log(100_000), nreq)).astype(np.int64)
+        reqs = []
+        for j in range(nreq):
+            n, s, d, w = graphs[gsel[j]]
+            u, v, ww = W.fast_batch(n, s, d, int(sizes[j]), 0.85, 17 + 1000 * ri + j)
+            reqs.append((int(gsel[j]), u, v, ww))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+        res = {}
+        for name, states, workers, coalesce in (("served", A, args.workers, None),
+                                                ("plain", B, 1, 1)):
+            done, wall = _serve(hl, states, reqs, arrivals, workers, coalesce, 120 * 10**9)
+            ok = [d for d in done if d["status"] == 0]
+            lat = sorted(d["latency_ms"] for d in ok)
+            e = sum(d["edges"] for d in ok)
+            res[name] = {"edge_updates_per_s": e / wall, "p50_ms": lat[len(lat) // 2],
+                         "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                         "batches": len({d["batch_id"] for d in ok}), "requests": len(ok),
+                         "rejected": len(done) - len(ok)}
+        per_rate.append({"rate_req_s": rate, **{f"{k}_{m}": v for k, r in res.items()
+                                                for m, v in r.items()}})
+    top = per_rate[-1]
+    if rank == 0:
+        line = {
+            "metric": "edge_updates_per_s", "value": top["served_edge_updates_per_s"],
+            "unit": "edge-updates/s", "n_gpus": 1, "steps": len(rates), "warmup": 0,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "scale": args.scale, "graphs": len(graphs),
+                       "vertices": int(sum(g[0] for g in graphs)),
+                       "edges": int(sum(len(g[1]) for g in graphs)), "workers": args.workers,
+                       "requests_per_rate": args.requests,
+                       "timing": "host clock, first submit to last completion",
+                       "rates": per_rate},
+            "e2e": {"value": top["served_edge_updates_per_s"], "unit": "edge-updates/s",
+                    "p50_ms": top["served_p50_ms"], "p99_ms": top["served_p99_ms"]},
+            "roofline": None, "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    for st in A + B:
+        st.close()
+
+
 def main():
     args = parse()
     cfg = CONFIGS[args.config]
+    if args.impl == "ours" and args.config == "batch256":
+        return run_batching(args, cfg)
+    if args.impl == "ours" and args.config == "serve32":
+        return run_serving(args, cfg)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         if rank == 0:
-            run_reference(args, cfg)
+            if args.config in ("batch256", "serve32"):
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference updates one graph per call; its per-graph path "
+                                  "is the lfr1m / ca_hepth reference arm"}), flush=True)
+            else:
+                run_reference(args, cfg)
         return
     import torch
     R = importlib.import_module("hit-leiden_b200.replicas")

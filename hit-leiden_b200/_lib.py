@@ -110,6 +110,7 @@ def _load():
         "hl_server_create": (st, [C.c_uint32, C.c_uint64, C.POINTER(vp)]),
         "hl_server_add_graph": (st, [vp, vp, p32]),
         "hl_server_set_edge_estimate": (st, [vp, C.c_uint64]),
+        "hl_server_set_coalescing": (st, [vp, C.c_uint32]),
         "hl_server_submit": (st, [vp, C.c_uint32, vp, vp, vp, C.c_uint64,
                                   C.POINTER(C.c_uint64)]),
         "hl_server_poll": (st, [vp, C.POINTER(RequestDone), C.c_uint32, p32, C.c_int32]),

@@ -322,6 +322,10 @@ class Server:
     def set_edge_estimate(self, bytes_per_edge: int) -> None:
         L.check(L.lib.hl_server_set_edge_estimate(self._s, int(bytes_per_edge)))
 
+    def set_coalescing(self, max_requests: int) -> None:
+        """At most ``max_requests`` per batch (0 = all pending; 1 = none)."""
+        L.check(L.lib.hl_server_set_coalescing(self._s, int(max_requests)))
+
     def submit(self, graph_id: int, src, dst, w=None) -> int:
         src, dst, w = L.u32(src), L.u32(dst), L.f64(w)
         rid = C.c_uint64()

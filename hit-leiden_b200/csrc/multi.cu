@@ -85,6 +85,7 @@ struct hl_server {
   uint64_t next_batch = 1;
   uint64_t outstanding = 0;         // submitted, not completed
   uint64_t bytes_per_edge = 512;
+  uint32_t max_coalesce = 0;        // requests per batch at most (0 = all pending)
   bool stop = false;
 
   uint64_t resident_bytes() const {
@@ -149,7 +150,8 @@ struct hl_server {
         GraphSlot& gs = graphs[gid];
         gs.queued = false;
         gs.busy = true;
-        while (!gs.pending.empty()) {  // coalesce everything admitted so far
+        while (!gs.pending.empty() &&  // coalesce what was admitted so far
+               (max_coalesce == 0 || batch.size() < max_coalesce)) {
           batch.push_back(std::move(gs.pending.front()));
           gs.pending.pop_front();
         }
@@ -304,6 +306,11 @@ HL_API hl_status hl_server_add_graph(hl_server* S, hl_graph* g, uint32_t* graph_
 HL_API hl_status hl_server_set_edge_estimate(hl_server* S, uint64_t bytes_per_edge) {
   HLM_TRY(need(S != nullptr, "NULL argument"); std::lock_guard<std::mutex> lk(S->mu);
           S->bytes_per_edge = bytes_per_edge);
+}
+
+HL_API hl_status hl_server_set_coalescing(hl_server* S, uint32_t max_requests) {
+  HLM_TRY(need(S != nullptr, "NULL argument"); std::lock_guard<std::mutex> lk(S->mu);
+          S->max_coalesce = max_requests);
 }
 
 HL_API hl_status hl_server_submit(hl_server* S, uint32_t graph_id, const uint32_t* src,

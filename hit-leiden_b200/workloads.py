@@ -298,3 +298,56 @@ def rmat_torch(scale, edge_factor, seed, a=0.57, b=0.19, c=0.19, device="cuda"):
         del src, dst, lo, hi
     key = torch.unique(torch.cat(keys))
     return n, (key // n).to(torch.int32), (key % n).to(torch.int32)
+
+
+def _loguniform_int(rng, lo, hi, size):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), size)).astype(np.int64)
+
+
+def config4(seed=0, count=256):
+    """Batching form: `count` independent graphs, vertex counts log-uniform in
+    [1k, 200k], planted power-law communities with mu log-uniform in
+    [0.1, 0.4], target mean degree uniform in [4, 32], unit weights."""
+    rng = np.random.default_rng(seed)
+    ns = _loguniform_int(rng, 1000, 200_000, count)
+    mus = np.exp(rng.uniform(np.log(0.1), np.log(0.4), count))
+    degs = rng.uniform(4.0, 32.0, count)
+    out = []
+    for i in range(count):
+        n, s, d, w, _ = planted(int(ns[i]), float(degs[i]), float(mus[i]), seed * 100_000 + i,
+                                comm_min=5, comm_max=400)
+        out.append((n, s, d, w))
+    return out
+
+
+def fast_batch(n, src, dst, k, insert_frac, seed):
+    """k unit updates: insert_frac uniform random new pairs (u != v; a pair
+    that already exists is strengthened) and the rest deletes of base edges
+    drawn uniformly (weight -1; deleting an edge an earlier batch already
+    removed is a no-op).  Vectorised, for large request streams."""
+    rng = np.random.default_rng(seed)
+    ki = int(round(k * insert_frac))
+    kd = k - ki
+    a = rng.integers(0, n, size=ki, dtype=np.int64)
+    b = rng.integers(0, n - 1, size=ki, dtype=np.int64)
+    b = b + (b >= a)  # b != a
+    di = rng.integers(0, len(src), size=kd) if len(src) else np.zeros(0, np.int64)
+    u = np.concatenate([np.minimum(a, b), src[di].astype(np.int64)]).astype(np.uint32)
+    v = np.concatenate([np.maximum(a, b), dst[di].astype(np.int64)]).astype(np.uint32)
+    w = np.concatenate([np.ones(ki), -np.ones(kd)])
+    return u, v, w
+
+
+def config5(seed=0, count=32, scale=1.0):
+    """Serving form: `count` resident graphs, vertex counts log-uniform in
+    [100k, 5M] (times `scale`), planted communities, mu 0.25, target mean
+    degree 16, unit weights."""
+    rng = np.random.default_rng(seed)
+    ns = _loguniform_int(rng, max(1000, int(100_000 * scale)), max(2000, int(5_000_000 * scale)),
+                         count)
+    out = []
+    for i in range(count):
+        n, s, d, w, _ = planted(int(ns[i]), 16.0, 0.25, seed * 100_000 + 50_000 + i,
+                                comm_min=5, comm_max=2000)
+        out.append((n, s, d, w))
+    return out

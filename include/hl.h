@@ -225,6 +225,9 @@ typedef struct {
 HL_API hl_status hl_server_create(uint32_t workers, uint64_t hbm_budget, hl_server** out);
 HL_API hl_status hl_server_add_graph(hl_server* s, hl_graph* g, uint32_t* graph_id);
 HL_API hl_status hl_server_set_edge_estimate(hl_server* s, uint64_t bytes_per_edge);
+/* At most max_requests requests per coalesced batch (0 = all pending, the
+ * default; 1 = every request is its own batch). */
+HL_API hl_status hl_server_set_coalescing(hl_server* s, uint32_t max_requests);
 HL_API hl_status hl_server_submit(hl_server* s, uint32_t graph_id, const uint32_t* src,
                                   const uint32_t* dst, const double* w, uint64_t k,
                                   uint64_t* request_id);
