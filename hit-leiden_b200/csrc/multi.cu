@@ -261,11 +261,16 @@ HL_API hl_status hl_apply_batches(hl_graph* const* graphs, const uint32_t* const
   if (workers > count) workers = count;
   std::vector<hl_status> rc(count, HL_OK);
   std::vector<std::string> msg(count);
+  // largest batches first, so that the longest graphs do not start last
+  std::vector<uint32_t> order(count);
+  for (uint32_t i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return k[a] > k[b]; });
   std::atomic<uint32_t> next{0};
   auto run = [&] {
     for (;;) {
-      const uint32_t i = next.fetch_add(1);
-      if (i >= count) return;
+      const uint32_t t = next.fetch_add(1);
+      if (t >= count) return;
+      const uint32_t i = order[t];
       rc[i] = hl::apply_on_handle(graphs[i], src[i], dst[i], w ? w[i] : nullptr, k[i],
                                   stats ? &stats[i] : nullptr, &msg[i]);
     }
