@@ -63,6 +63,13 @@ CONFIGS = {
                     "(85% inserts, 15% deletes), 120 GB admission budget",
         "batch": 0,
     },
+    "rmat25": {
+        "workload": "R-MAT scale 25 (33.5M vertices), edge factor 16, (a,b,c,d) = "
+                    "(.57,.19,.19,.05), symmetrised, duplicates and self-loops removed; unit "
+                    "weights summed in FP64; batches of 1M updates (90% R-MAT inserts, 10% "
+                    "uniform deletes)",
+        "batch": 1_000_000,
+    },
     "ca_hepth": {
         "workload": "planted graph shaped like ca-HepTh: 9,877 vertices / ~21.8k unit edges, "
                     "mu 0.15, triangle closure; batches of 1,000 uniform inserts",
@@ -446,9 +453,147 @@ def run_serving(args, cfg):
         st.close()
 
 
+def _roof(kernels, key, label, peak, peak_kind):
+    ev = kernels.get(key, {})
+    if not ev.get("launches") or not ev.get("ms"):
+        return None
+    achieved = ev["bytes"] / (ev["ms"] / 1000.0) / 1e9
+    return {"kernel": label, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind,
+            "bytes_per_launch": ev["bytes"] / ev["launches"],
+            "avg_launch_ms": ev["ms"] / ev["launches"], "traffic": None}
+
+
+def _device_bytes(L, h):
+    used, peak = C.c_uint64(), C.c_uint64()
+    L.check(L.lib.hl_device_bytes(h, C.byref(used), C.byref(peak)))
+    return {"used": used.value, "peak": peak.value}
+
+
+def run_rmat(args, cfg):
+    """R-MAT scale 25: graph and batches generated on the GPU (torch, input
+    plumbing only), loaded with hl_create_device; value from device-resident
+    batches (CUDA events), e2e through hl_apply_batch with host arrays."""
+    import torch
+    R = importlib.import_module("hit-leiden_b200.replicas")
+    W = importlib.import_module("hit-leiden_b200.workloads")
+    rep = R.Replicas("nccl")
+    local = rep.local
+    torch.cuda.set_device(local)
+    hl = importlib.import_module("hit-leiden_b200")
+    L = importlib.import_module("hit-leiden_b200._lib")
+    scale = 25 if not args.ncu_small else 20
+    n, bs, bd = W.rmat_torch(scale, 16, args.seed + rep.rank, device=f"cuda:{local}")
+    m = bs.numel()
+    torch.cuda.empty_cache()  # hand the generator's cached blocks back before the load
+    free_b, total_b = torch.cuda.mem_get_info()
+    print(f"# R-MAT scale {scale}: {n} vertices, {m} edges; device free {free_b} of {total_b}",
+          file=sys.stderr, flush=True)
+    k = cfg["batch"] if not args.ncu_small else 50_000
+    rc = hl.RunConfig(max_iterations=args.levels, device=local)
+    c = rc.to_c()
+    c.flags |= L.HL_FLAG_KERNEL_TIMING
+    h = C.c_void_p()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.check(L.lib.hl_create_device(C.byref(c), n, C.c_void_p(bs.data_ptr()),
+                                   C.c_void_p(bd.data_ptr()), None, m, C.byref(h)))
+    boot_s = time.perf_counter() - t0
+    st = hl.PartitionState(h, n, rc)
+    K, Wm = args.steps, args.warmup
+    seeds = iter(range(10_000, 20_000))
+    for _ in range(Wm):
+        u, v, w = W.rmat_batch_torch(scale, bs, bd, k, 0.9, next(seeds))
+        L.check(L.lib.hl_apply_batch_device(h, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
+                                            C.c_void_p(w.data_ptr()), k, None))
+    dev = [W.rmat_batch_torch(scale, bs, bd, k, 0.9, next(seeds)) for _ in range(K)]
+    torch.cuda.synchronize()
+    L.check(L.lib.hl_reset_kernel_stats(h))
+    clocks = Clocks(local)
+    clocks.start()
+    rep.barrier()
+    torch.cuda.synchronize()
+    dev_ms, launches, traversed = [], 0, 0
+    stats = L.BatchStats()
+    torch.cuda.nvtx.range_push("hl_timed")
+    for (u, v, w) in dev:
+        L.check(L.lib.hl_apply_batch_device(h, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
+                                            C.c_void_p(w.data_ptr()), k, C.byref(stats)))
+        dev_ms.append(stats.device_ms)
+        launches += stats.launches
+        traversed += stats.traversed
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    rep.barrier()
+    clk = clocks.stop()
+    tot_ms = rep.max_over_ranks(float(sum(dev_ms)))
+    value = rep.whole_job_rate(K, k, tot_ms / 1000.0)
+    kst = (L.KernelStat * 32)()
+    cnt = C.c_uint32()
+    L.check(L.lib.hl_kernel_stats(h, kst, 32, C.byref(cnt)))
+    kernels = {kst[i].name.decode(): {"launches": kst[i].launches, "ms": kst[i].total_ms,
+                                      "bytes": kst[i].bytes, "items": kst[i].items}
+               for i in range(cnt.value)}
+    del dev
+    # end to end: host arrays in, level-0 map out
+    host = []
+    for _ in range(K):
+        u, v, w = W.rmat_batch_torch(scale, bs, bd, k, 0.9, next(seeds))
+        host.append((u.cpu().numpy().view(np.uint32), v.cpu().numpy().view(np.uint32),
+                     w.cpu().numpy()))
+    comm = np.zeros(n, np.uint32)
+    rep.barrier()
+    torch.cuda.synchronize()
+    e2e_s = []
+    for (u, v, w) in host:
+        t1 = time.perf_counter()
+        st.apply_batch(u, v, w)
+        L.check(L.lib.hl_get_map(h, 0, L.HL_MAP_COMMUNITY, L.ptr(comm)))
+        e2e_s.append(time.perf_counter() - t1)
+    tot_e2e = rep.max_over_ranks(float(sum(e2e_s)))
+    e2e_val = rep.whole_job_rate(K, k, tot_e2e)
+    lat = sorted(1000.0 * x for x in e2e_s)
+    peak, peak_kind = measured_peak()
+    mv = kernels.get("stage_move", {})
+    if rep.rank == 0:
+        line = {
+            "metric": "edge_updates_per_s", "value": value, "unit": "edge-updates/s",
+            "n_gpus": rep.world, "steps": K, "warmup": Wm, "ms_per_step": tot_ms / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": cfg["workload"], "scale": scale, "vertices": n,
+                       "edges": int(m), "batch_edges": k, "levels": st.levels,
+                       "parallelism": f"replicas{rep.world}",
+                       "l2": "inputs larger than L2 (resident CSR > 126 MB)",
+                       "bootstrap_s": boot_s},
+            "e2e": {"value": e2e_val, "unit": "edge-updates/s",
+                    "h2d_bytes_per_step": int(k * 16), "d2h_bytes_per_step": int(n * 4),
+                    "p50_ms": lat[len(lat) // 2],
+                    "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "gpu_launches": int(launches),
+            "traversed_edges_per_s": traversed / (mv["ms"] / 1000.0) if mv.get("ms") else None,
+            "roofline": _roof(kernels, "move_eval",
+                              "k_eval<EVAL_MOVE> (inc-movement best-move evaluation)", peak,
+                              peak_kind),
+            "roofline_aggregation": _roof(kernels, "aggregate_compress",
+                                          "inc-aggregation (emission + compression)", peak,
+                                          peak_kind),
+            "cpu_baseline": None,
+            "cpu_baseline_note": "the CPU port is not run at 500M edges (a single batch "
+                                 "would take hours on one core)",
+            "clocks": clk, "modularity": st.modularity(), "kernels": kernels,
+            "device_bytes": _device_bytes(L, h),
+        }
+        print(json.dumps(line), flush=True)
+    st.close()
+    rep.close()
+
+
 def main():
     args = parse()
     cfg = CONFIGS[args.config]
+    if args.impl == "ours" and args.config == "rmat25":
+        return run_rmat(args, cfg)
     if args.impl == "ours" and args.config == "batch256":
         return run_batching(args, cfg)
     if args.impl == "ours" and args.config == "serve32":
@@ -458,10 +603,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         if rank == 0:
-            if args.config in ("batch256", "serve32"):
+            if args.config in ("batch256", "serve32", "rmat25"):
                 print(json.dumps({"impl": "reference", "unavailable":
-                                  "the reference updates one graph per call; its per-graph path "
-                                  "is the lfr1m / ca_hepth reference arm"}), flush=True)
+                                  "not run for this configuration: the CPU port's per-graph "
+                                  "path is the lfr1m / ca_hepth reference arm"}), flush=True)
             else:
                 run_reference(args, cfg)
         return

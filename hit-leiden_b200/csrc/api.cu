@@ -383,6 +383,10 @@ static void create_impl(const hl_config* cfg, uint32_t n, const uint32_t* src, c
   bootstrap(*B, n, G);
   if (E.levels[0].tw >= 4503599627370496.0) E.integral = false;  // 2^52
   finish_stats(*B, nullptr);
+  // The bootstrap's scratch (sorts over the whole edge list) is far larger
+  // than an update batch needs: hand it back; batches regrow what they use.
+  E.sc = Scratch();
+  E.sync();
   *out = reinterpret_cast<hl_graph*>(B.release());
 }
 

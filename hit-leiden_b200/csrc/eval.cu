@@ -59,6 +59,8 @@ struct EvalArgs {
   u32* tlist;    // per-warp / per-block insertion lists of used slots
   u64 region;    // table entries per block region (block kernel)
   unsigned long long* counters;  // [0] entries scanned, [1] candidates evaluated
+  u32* ovf_list;   // block kernel without global regions: rows deferred because
+  u32* ovf_count;  // they passed BIG_TAB / 2 distinct keys (idx values)
 };
 
 constexpr u32 MID_MAX = 128;
@@ -519,7 +521,6 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
     while (gcap < 2 * deg) gcap <<= 1;
     const u32 cap = gcap < BIG_TAB ? (u32)gcap : BIG_TAB;
     if (tid == 0) {
-      trav += deg;
       s_used = 0;
       s_gused = 0;
     }
@@ -550,6 +551,7 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
       }
     }
     bool global = false;
+    bool deferred = false;
     u32* tk = s_tk;
     u32* tp = s_tp;
     double* tv = s_tv;
@@ -579,10 +581,15 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
       }
       if (lane < BIG_WARPS) s_cnt[lane * BIG_WARPS + wib] = mycnt;
       __syncthreads();
-      // The previous tile's folds are complete here and s_used is stable: a row
-      // with too many distinct keys moves its table to the global region (its
-      // degree is then above BIG_TAB / 2, so the region exists).
-      if (!global && s_used > BIG_TAB / 2 && g_tk) {
+      // The previous tile's folds are complete here and s_used is stable.  A
+      // row with too many distinct keys moves its table to the block's global
+      // region; a launch without regions defers the row to its overflow list
+      // instead (a later launch with regions takes it from the start).
+      if (!global && s_used > BIG_TAB / 2 && !g_tk) {
+        deferred = true;
+        break;
+      }
+      if (!global && s_used > BIG_TAB / 2) {
         const u64 gmask = gcap - 1;
         for (u32 x = tid; x < BIG_TAB; x += BIG_THREADS) {
           const u32 k = s_tk[x];
@@ -655,6 +662,11 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         __syncwarp();
       }
     }
+    if (deferred) {
+      if (tid == 0) A.ovf_list[atomicAdd(A.ovf_count, 1u)] = i;
+      __syncthreads();
+      continue;
+    }
     __syncthreads();
     // w(v, cur), then the argmax over the table (resetting a global table).
     if (tid == 0) {
@@ -720,6 +732,7 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
           kk = r_k[x];
         }
       }
+      trav += deg;
       finish<KIND>(A, i, v, cur, kv, wcur, g, kk, p != NONE32);
     }
     __syncthreads();
@@ -771,6 +784,8 @@ static std::atomic<bool> g_big_attr_set[64];
 
 constexpr u32 WIDE_MAX_BLOCKS = 148u * 4u;
 constexpr u32 BIG_MAX_BLOCKS = 148u * 3u;
+constexpr u32 OVF_BLOCKS = 32;  // least blocks (global regions) for rows deferred by pass 1
+constexpr u64 OVF_TABLE_BYTES = 4ull << 30;  // table bytes pass 2 may spread over its blocks
 
 void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
               const double* d, const u8* blocked, bool allow_empty, u32* out_to, double* out_gain,
@@ -811,35 +826,6 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
     ++E.nlaunch, k_fill_u32<<<grid_for(need), 256, 0, st>>>(S.wide_key.p, NONE32, S.wide_key.cap);
     HL_LAUNCH_CHECK();
   }
-  // Per-block global regions of the block kernel, sized for its largest row.
-  u64 region = 0;
-  if (c[5]) {
-    S.gkey.ensure(E.mem, (size_t)c[5] + 1);
-    ++E.nlaunch, k_big_caps2<<<grid_for(c[5]), 256, 0, st>>>(verts, vo + start[5], c[5], L.g.off.p,
-                                                             S.gkey.p);
-    HL_LAUNCH_CHECK();
-    u64* ci = S.gkey.p;
-    u64* co = S.gkey2.p;
-    S.gkey2.ensure(E.mem, 2);
-    co = S.gkey2.p;
-    cub_run(E, [&](void* t, size_t& b) {
-      return cub::DeviceReduce::Max(t, b, ci, co, (int64_t)c[5], st);
-    });
-    region = E.read_u64(co);
-    if (region) {
-      const size_t need = (size_t)BIG_MAX_BLOCKS * region;
-      if (S.huge_key.cap < need) {
-        S.huge_key.ensure(E.mem, need);
-        S.huge_pos.ensure(E.mem, need);
-        S.huge_val.ensure(E.mem, need);
-        S.huge_list.ensure(E.mem, need / 2 + 1);
-        ++E.nlaunch, k_fill_u32<<<grid_for(need), 256, 0, st>>>(S.huge_key.p, NONE32, S.huge_key.cap);
-        ++E.nlaunch, k_fill_u32<<<grid_for(need), 256, 0, st>>>(S.huge_pos.p, NONE32, S.huge_pos.cap);
-        HL_CUDA(cudaMemsetAsync(S.huge_val.p, 0, sizeof(double) * S.huge_val.cap, st));
-        HL_LAUNCH_CHECK();
-      }
-    }
-  }
   int dev = E.device;
   if (dev >= 0 && dev < 64 && !g_big_attr_set[dev]) {
     HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -872,6 +858,8 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   A.tval = nullptr;
   A.tlist = nullptr;
   A.region = 0;
+  A.ovf_list = nullptr;
+  A.ovf_count = nullptr;
 
   cudaEvent_t ev = E.kt_begin();
   cudaEvent_t e_s = E.kt_begin();
@@ -934,23 +922,70 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   E.kt_end(KT_EVAL_BIG, e_b);
   cudaEvent_t e_h = E.kt_begin();
   if (c[5]) {
+    // Pass 1: shared tables only; rows with more than BIG_TAB / 2 distinct keys
+    // are deferred to an overflow list.
     EvalArgs a = A;
     a.counters = counters ? counters + 6 : nullptr;
     a.idx = vo + start[5];
     a.nidx = c[5];
-    if (region) {
-      a.tkey = S.huge_key.p;
-      a.tpos = S.huge_pos.p;
-      a.tval = S.huge_val.p;
-      a.tlist = S.huge_list.p;
-      a.region = region;
-    }
+    S.ovf.ensure(E.mem, c[5]);
+    a.ovf_list = S.ovf.p;
+    S.ovf_cnt.ensure(E.mem, 1);
+    a.ovf_count = S.ovf_cnt.p;
+    HL_CUDA(cudaMemsetAsync(a.ovf_count, 0, sizeof(u32), st));
     u32 blocks = c[5] < BIG_MAX_BLOCKS ? c[5] : BIG_MAX_BLOCKS;
     if (kind == EVAL_MOVE)
       ++E.nlaunch, k_eval_big<EVAL_MOVE><<<blocks, BIG_THREADS, big_smem(), st>>>(a);
     else
       ++E.nlaunch, k_eval_big<EVAL_REFINE><<<blocks, BIG_THREADS, big_smem(), st>>>(a);
     HL_LAUNCH_CHECK();
+    const u32 novf = E.read_u32(a.ovf_count);
+    if (novf) {
+      // Pass 2: the deferred rows on at most OVF_BLOCKS blocks, each with a
+      // global region sized for the largest of them.
+      S.gkey.ensure(E.mem, (size_t)novf + 1);
+      S.gkey2.ensure(E.mem, 2);
+      ++E.nlaunch, k_big_caps2<<<grid_for(novf), 256, 0, st>>>(verts, S.ovf.p, novf, L.g.off.p,
+                                                               S.gkey.p);
+      HL_LAUNCH_CHECK();
+      u64* ci = S.gkey.p;
+      u64* co = S.gkey2.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceReduce::Max(t, b, ci, co, (int64_t)novf, st);
+      });
+      const u64 region = E.read_u64(co);
+      // as many blocks as OVF_TABLE_BYTES of tables allow, within [32, 444]
+      u64 fit = OVF_TABLE_BYTES / (region * 18);
+      if (fit < OVF_BLOCKS) fit = OVF_BLOCKS;
+      if (fit > BIG_MAX_BLOCKS) fit = BIG_MAX_BLOCKS;
+      const u32 pb = novf < fit ? novf : (u32)fit;
+      const size_t need = (size_t)pb * region;
+      if (S.huge_key.cap < need) {
+        S.huge_key.ensure(E.mem, need);
+        S.huge_pos.ensure(E.mem, need);
+        S.huge_val.ensure(E.mem, need);
+        S.huge_list.ensure(E.mem, need / 2 + 1);
+        ++E.nlaunch, k_fill_u32<<<grid_for(S.huge_key.cap), 256, 0, st>>>(S.huge_key.p, NONE32,
+                                                                           S.huge_key.cap);
+        ++E.nlaunch, k_fill_u32<<<grid_for(S.huge_pos.cap), 256, 0, st>>>(S.huge_pos.p, NONE32,
+                                                                           S.huge_pos.cap);
+        HL_CUDA(cudaMemsetAsync(S.huge_val.p, 0, sizeof(double) * S.huge_val.cap, st));
+        HL_LAUNCH_CHECK();
+      }
+      EvalArgs a2 = a;
+      a2.idx = S.ovf.p;
+      a2.nidx = novf;
+      a2.tkey = S.huge_key.p;
+      a2.tpos = S.huge_pos.p;
+      a2.tval = S.huge_val.p;
+      a2.tlist = S.huge_list.p;
+      a2.region = region;
+      if (kind == EVAL_MOVE)
+        ++E.nlaunch, k_eval_big<EVAL_MOVE><<<pb, BIG_THREADS, big_smem(), st>>>(a2);
+      else
+        ++E.nlaunch, k_eval_big<EVAL_REFINE><<<pb, BIG_THREADS, big_smem(), st>>>(a2);
+      HL_LAUNCH_CHECK();
+    }
   }
   E.kt_end(KT_EVAL_HUGE, e_h);
   E.kt_end(kind == EVAL_MOVE ? KT_MOVE_EVAL : KT_REFINE_EVAL, ev);

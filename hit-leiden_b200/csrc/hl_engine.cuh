@@ -86,6 +86,7 @@ struct Scratch {
   DBuf<double> wide_val;
   // global tables of the block-per-vertex kernel (degrees above 4096)
   DBuf<u32> huge_key, huge_pos, huge_list;
+  DBuf<u32> ovf, ovf_cnt;  // block kernel: rows deferred to the pass with global regions
   DBuf<double> huge_val;
 };
 

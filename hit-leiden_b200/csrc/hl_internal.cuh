@@ -96,8 +96,11 @@ struct DBuf {
   void ensure(MemCtx& c, size_t n, bool keep = false) {
     ctx = &c;
     if (n <= cap) return;
-    size_t ncap = cap ? cap : 1;
-    while (ncap < n) ncap = ncap < (1u << 20) ? ncap * 4 : ncap + ncap / 2;
+    // a first allocation is the request plus a small fixed pad; a buffer that
+    // has to grow again grows by at least half, so repeated growth stays
+    // amortised
+    size_t ncap = n + 256;
+    if (cap && ncap < cap + cap / 2) ncap = cap + cap / 2;
     u64 bytes = (u64)ncap * sizeof(T);
     if (c.budget && c.used - (u64)cap * sizeof(T) + bytes > c.budget)
       throw Error(HL_ERR_OUT_OF_MEMORY, "HBM budget exceeded (" + std::to_string(c.used + bytes) +
@@ -106,9 +109,13 @@ struct DBuf {
     cudaError_t e = cudaMallocAsync((void**)&np, bytes, c.stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
-      throw Error(HL_ERR_OUT_OF_MEMORY, std::string("device allocation of ") +
-                                            std::to_string(bytes) + " bytes failed: " +
-                                            cudaGetErrorString(e));
+      size_t fr = 0, tot = 0;
+      cudaMemGetInfo(&fr, &tot);
+      throw Error(HL_ERR_OUT_OF_MEMORY,
+                  std::string("device allocation of ") + std::to_string(bytes) +
+                      " bytes failed: " + cudaGetErrorString(e) + " (this handle holds " +
+                      std::to_string(c.used) + " bytes; device free " + std::to_string(fr) +
+                      " of " + std::to_string(tot) + ")");
     }
     if (keep && p && cap) HL_CUDA(cudaMemcpyAsync(np, p, cap * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
     if (p) {

@@ -300,6 +300,37 @@ def rmat_torch(scale, edge_factor, seed, a=0.57, b=0.19, c=0.19, device="cuda"):
     return n, (key // n).to(torch.int32), (key % n).to(torch.int32)
 
 
+def rmat_batch_torch(scale, base_src, base_dst, k, insert_frac, seed, a=0.57, b=0.19, c=0.19):
+    """k unit updates on the GPU: insert_frac R-MAT-sampled pairs (self-loops
+    redrawn as the pair's next sample is not needed: they are dropped and the
+    batch is topped up with uniform pairs) and the rest deletes of base edges
+    drawn uniformly (weight -1; deleting an edge that is already gone is a
+    no-op).  Returns int32 device tensors (src, dst) and an f64 tensor w."""
+    import torch
+    dev = base_src.device
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    n = 1 << scale
+    ki = int(round(k * insert_frac))
+    kd = k - ki
+    src = torch.zeros(ki, dtype=torch.int64, device=dev)
+    dst = torch.zeros(ki, dtype=torch.int64, device=dev)
+    for lvl in range(scale):
+        r = torch.rand(ki, generator=g, device=dev)
+        src |= (r >= a + b).to(torch.int64) << lvl
+        dst |= (((r >= a) & (r < a + b)) | (r >= a + b + c)).to(torch.int64) << lvl
+    loop = src == dst
+    if bool(loop.any()):
+        fix = torch.randint(0, n - 1, (int(loop.sum()),), generator=g, device=dev)
+        dst[loop] = fix + (fix >= src[loop]).to(torch.int64)
+    di = torch.randint(0, base_src.numel(), (kd,), generator=g, device=dev)
+    u = torch.cat([torch.minimum(src, dst).to(torch.int32), base_src[di]])
+    v = torch.cat([torch.maximum(src, dst).to(torch.int32), base_dst[di]])
+    w = torch.cat([torch.ones(ki, dtype=torch.float64, device=dev),
+                   -torch.ones(kd, dtype=torch.float64, device=dev)])
+    return u.contiguous(), v.contiguous(), w.contiguous()
+
+
 def _loguniform_int(rng, lo, hi, size):
     return np.exp(rng.uniform(np.log(lo), np.log(hi), size)).astype(np.int64)
 

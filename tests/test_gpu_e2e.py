@@ -174,3 +174,28 @@ def test_empty_and_tiny_graphs():
             src, dst, w = g.arrays()
             os_ = oracle_state(n, src, dst, w, lv)
             compare(st, os_)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_e2e_rmat_integral_hubs(seed):
+    """Skewed R-MAT degrees with unit weights (the large plain configuration's
+    shape, scale 12): GPU state bit-exact with the oracle after the bootstrap
+    and after mixed batches of R-MAT inserts and deletes."""
+    import torch
+    n, bs, bd = W.rmat_torch(12, 16, seed, device="cuda:0")
+    s = bs.cpu().numpy().view(np.uint32)
+    d = bd.cpu().numpy().view(np.uint32)
+    w = np.ones(len(s))
+    gs = hl.PartitionState.load(hl.GraphInput.from_arrays("rmat", n, s, d, None),
+                                hl.RunConfig(max_iterations=10))
+    os_ = oracle_state(n, s, d, w, 10)
+    compare(gs, os_)
+    for b in range(3):
+        u, v, ww = W.rmat_batch_torch(12, bs, bd, 2000, 0.9, 100 * seed + b)
+        u = u.cpu().numpy().view(np.uint32)
+        v = v.cpu().numpy().view(np.uint32)
+        ww = ww.cpu().numpy()
+        gs.apply_batch(u, v, ww)
+        os_.hit_leiden(u, v, ww)
+        compare(gs, os_)
+    del torch
