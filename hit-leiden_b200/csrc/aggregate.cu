@@ -84,8 +84,12 @@ __global__ void k_agg_rows(u32 n, const u64* off, const u32* col, const double* 
       o += 2ull * __popc(m);
       c += 2ull * __popc(m);
     }
-    double slw = warp_ordered_sum(o0, o1, 0.0, [&](u64 p) { return w[p]; },
-                                  [&](u64 p) { return col[p] == (u32)v; });
+    // The self-loop's entries (stored twice) sit together at the lower bound
+    // of v in the sorted row; their sum in CSR order is the row-order sum of
+    // the entries whose neighbour is v.
+    double slw = 0.0;
+    for (u64 p = lower_bound_u32(col, o0, o1, (u32)v); p < o1 && col[p] == (u32)v; ++p)
+      slw = __dadd_rn(slw, w[p]);
     if (edge_weight_loops) slw = slw / 2.0;
     bool loop = fabs(slw) > 1e-12;
     if (lane == 0) {

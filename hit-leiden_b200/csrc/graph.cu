@@ -90,17 +90,6 @@ void graph_grow_nodes(Engine& E, Level& L, u32 n) {
   HL_LAUNCH_CHECK();
 }
 
-__device__ __forceinline__ u64 lower_bound_u32(const u32* a, u64 lo, u64 hi, u32 x) {
-  while (lo < hi) {
-    u64 mid = (lo + hi) >> 1;
-    if (a[mid] < x)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
 __device__ __forceinline__ u64 lower_bound_u64(const u64* a, u64 lo, u64 hi, u64 x) {
   while (lo < hi) {
     u64 mid = (lo + hi) >> 1;

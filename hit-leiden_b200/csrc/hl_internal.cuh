@@ -216,6 +216,18 @@ __device__ __forceinline__ double warp_ordered_sum(u64 a, u64 b, double acc, V v
   return acc;
 }
 
+// First position in [lo, hi) of the ascending array a whose value is >= x.
+__device__ __forceinline__ u64 lower_bound_u32(const u32* a, u64 lo, u64 hi, u32 x) {
+  while (lo < hi) {
+    u64 mid = (lo + hi) >> 1;
+    if (a[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
 // Total order on doubles as unsigned keys (ascending).
 __device__ __forceinline__ u64 double_key(double x) {
   u64 b = (u64)__double_as_longlong(x);

@@ -380,13 +380,27 @@ __global__ void k_mark_next(u32 M, const u8* status, const u32* sel_node, const 
     u32 v = sel_node[r], to = sel_to[r];
     u32 sv = s[v];
     bool any_same = false;
-    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32) {
-      u32 nb = col[p];
-      if (f[nb] != to) next[nb] = 1;
-      if (s[nb] == sv) {
-        affected[nb] = 1;
-        any_same = true;
-      }
+    const u64 o1 = off[v + 1];
+    // four entries per lane in flight: their neighbours, then their labels
+    for (u64 p0 = off[v] + lane; p0 < o1; p0 += 128) {
+      u32 nb[4], fn[4], sn[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) nb[j] = p0 + 32 * j < o1 ? col[p0 + 32 * j] : NONE32;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (nb[j] != NONE32) {
+          fn[j] = f[nb[j]];
+          sn[j] = s[nb[j]];
+        }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (nb[j] != NONE32) {
+          if (fn[j] != to) next[nb[j]] = 1;
+          if (sn[j] == sv) {
+            affected[nb[j]] = 1;
+            any_same = true;
+          }
+        }
     }
     if (__any_sync(0xffffffffu, any_same) && lane == 0) affected[v] = 1;
   }

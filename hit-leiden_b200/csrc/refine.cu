@@ -64,12 +64,22 @@ __global__ void k_uf_edges(u32 n, const u64* off, const u32* col, const u32* s, 
     u32 sv = s[v];
     if (!affsc[sv]) continue;
     u32 fv = f[v];
-    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32) {
-      u32 nb = col[p];
-      if (nb <= v) continue;  // each undirected edge once (self-loops irrelevant)
-      if (s[nb] != sv) continue;
-      if (same_f && f[nb] != fv) continue;
-      uf_unite(par, (u32)v, nb);
+    const u64 o1 = off[v + 1];
+    // each undirected edge once (self-loops irrelevant): neighbours above v,
+    // four entries per lane in flight
+    for (u64 p0 = lower_bound_u32(col, off[v], o1, (u32)v + 1) + lane; p0 < o1; p0 += 128) {
+      u32 nb[4], sn[4], fn[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) nb[j] = p0 + 32 * j < o1 ? col[p0 + 32 * j] : NONE32;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (nb[j] != NONE32) {
+          sn[j] = s[nb[j]];
+          fn[j] = same_f ? f[nb[j]] : fv;
+        }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (nb[j] != NONE32 && sn[j] == sv && fn[j] == fv) uf_unite(par, (u32)v, nb[j]);
     }
   }
 }
@@ -154,11 +164,20 @@ __global__ void k_t_candidates(const u32* single, u32 ns, const u64* off, const 
   for (u64 i = warp; i < ns; i += nwarps) {
     u32 v = single[i];
     u32 fv = f[v], sv = s[v];
-    for (u64 p = off[v] + lane; p < off[v + 1]; p += 32) {
-      u32 nb = col[p];
-      if (f[nb] != fv) continue;
-      u32 x = s[nb];
-      if (x != sv) cand[x] = 1;
+    const u64 o1 = off[v + 1];
+    for (u64 p0 = off[v] + lane; p0 < o1; p0 += 128) {
+      u32 nb[4], fn[4], sn[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) nb[j] = p0 + 32 * j < o1 ? col[p0 + 32 * j] : NONE32;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (nb[j] != NONE32) {
+          fn[j] = f[nb[j]];
+          sn[j] = s[nb[j]];
+        }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (nb[j] != NONE32 && fn[j] == fv && sn[j] != sv) cand[sn[j]] = 1;
     }
   }
 }
