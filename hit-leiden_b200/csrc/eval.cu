@@ -61,6 +61,7 @@ struct EvalArgs {
   unsigned long long* counters;  // [0] entries scanned, [1] candidates evaluated
   u32* ovf_list;   // block kernel without global regions: rows deferred because
   u32* ovf_count;  // they passed BIG_TAB / 2 distinct keys (idx values)
+  const u32* nidx_dev;  // if set, the number of idx entries is read here
 };
 
 constexpr u32 MID_MAX = 128;
@@ -509,7 +510,8 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
   u32* g_tp = A.tpos ? A.tpos + (u64)blockIdx.x * A.region : nullptr;
   double* g_tv = A.tval ? A.tval + (u64)blockIdx.x * A.region : nullptr;
   u32* g_list = A.tlist ? A.tlist + (u64)blockIdx.x * (A.region / 2) : nullptr;
-  for (u64 t = blockIdx.x; t < A.nidx; t += gridDim.x) {
+  const u32 nidx = A.nidx_dev ? *A.nidx_dev : A.nidx;
+  for (u64 t = blockIdx.x; t < nidx; t += gridDim.x) {
     const u32 i = A.idx[t];
     const u32 v = A.verts[i];
     const u64 o0 = A.off[v], o1 = A.off[v + 1];
@@ -744,7 +746,7 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
 // Host side: bin the list by degree and launch the three kernels.
 // ---------------------------------------------------------------------------
 __global__ void k_bin(const u32* verts, u32 nv, const u64* off, u32* bin, u32* idx,
-                      u32* counts) {
+                      u32* counts, unsigned long long* maxdeg) {
   __shared__ u32 sc[6];
   if (threadIdx.x < 6) sc[threadIdx.x] = 0;
   __syncthreads();
@@ -756,6 +758,7 @@ __global__ void k_bin(const u32* verts, u32 nv, const u64* off, u32* bin, u32* i
     bin[i] = b;
     idx[i] = (u32)i;
     atomicAdd(&sc[b], 1u);
+    if (b == 5) atomicMax(maxdeg, (unsigned long long)deg);
   }
   __syncthreads();
   if (threadIdx.x < 6 && sc[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sc[threadIdx.x]);
@@ -800,7 +803,11 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   S.cnt.ensure(E.mem, 16);
   u32* cnt = S.cnt.p + 2;  // six bin counters (cnt[2..7])
   HL_CUDA(cudaMemsetAsync(cnt, 0, 6 * sizeof(u32), st));
-  ++E.nlaunch, k_bin<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.used.p, S.order.p, cnt);
+  S.ovf_cnt.ensure(E.mem, 4);  // [0] deferred rows, [2..3] largest degree of the block bin
+  unsigned long long* maxdeg = reinterpret_cast<unsigned long long*>(S.ovf_cnt.p + 2);
+  HL_CUDA(cudaMemsetAsync(S.ovf_cnt.p, 0, 4 * sizeof(u32), st));
+  ++E.nlaunch, k_bin<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.used.p, S.order.p, cnt,
+                                                    maxdeg);
   HL_LAUNCH_CHECK();
   u32* ki = S.used.p;
   u32* ko = S.rank.p;
@@ -811,8 +818,10 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   });
   u32 c[6];
   HL_CUDA(cudaMemcpyAsync(E.hs.p, cnt, 6 * sizeof(u32), cudaMemcpyDeviceToHost, st));
+  HL_CUDA(cudaMemcpyAsync(E.hs.p + 4, maxdeg, sizeof(u64), cudaMemcpyDeviceToHost, st));
   E.sync();
   std::memcpy(c, E.hs.p, sizeof(c));
+  const u64 big_maxdeg = E.hs.p[4];
   u32 start[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int b = 0; b < 6; ++b) start[b + 1] = start[b] + c[b];
 
@@ -860,6 +869,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   A.region = 0;
   A.ovf_list = nullptr;
   A.ovf_count = nullptr;
+  A.nidx_dev = nullptr;
 
   cudaEvent_t ev = E.kt_begin();
   cudaEvent_t e_s = E.kt_begin();
@@ -930,35 +940,23 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
     a.nidx = c[5];
     S.ovf.ensure(E.mem, c[5]);
     a.ovf_list = S.ovf.p;
-    S.ovf_cnt.ensure(E.mem, 1);
-    a.ovf_count = S.ovf_cnt.p;
-    HL_CUDA(cudaMemsetAsync(a.ovf_count, 0, sizeof(u32), st));
+    a.ovf_count = S.ovf_cnt.p;  // zeroed with the bin counters
     u32 blocks = c[5] < BIG_MAX_BLOCKS ? c[5] : BIG_MAX_BLOCKS;
     if (kind == EVAL_MOVE)
       ++E.nlaunch, k_eval_big<EVAL_MOVE><<<blocks, BIG_THREADS, big_smem(), st>>>(a);
     else
       ++E.nlaunch, k_eval_big<EVAL_REFINE><<<blocks, BIG_THREADS, big_smem(), st>>>(a);
     HL_LAUNCH_CHECK();
-    const u32 novf = E.read_u32(a.ovf_count);
-    if (novf) {
-      // Pass 2: the deferred rows on at most OVF_BLOCKS blocks, each with a
-      // global region sized for the largest of them.
-      S.gkey.ensure(E.mem, (size_t)novf + 1);
-      S.gkey2.ensure(E.mem, 2);
-      ++E.nlaunch, k_big_caps2<<<grid_for(novf), 256, 0, st>>>(verts, S.ovf.p, novf, L.g.off.p,
-                                                               S.gkey.p);
-      HL_LAUNCH_CHECK();
-      u64* ci = S.gkey.p;
-      u64* co = S.gkey2.p;
-      cub_run(E, [&](void* t, size_t& b) {
-        return cub::DeviceReduce::Max(t, b, ci, co, (int64_t)novf, st);
-      });
-      const u64 region = E.read_u64(co);
-      // as many blocks as OVF_TABLE_BYTES of tables allow, within [32, 444]
+    if (big_maxdeg > BIG_TAB / 2) {
+      // Pass 2: the deferred rows (their number is read on the device), on as
+      // many blocks as OVF_TABLE_BYTES of global regions allow, each region
+      // sized for the largest row of the bin.
+      u64 region = 64;
+      while (region < 2 * big_maxdeg) region <<= 1;
       u64 fit = OVF_TABLE_BYTES / (region * 18);
       if (fit < OVF_BLOCKS) fit = OVF_BLOCKS;
       if (fit > BIG_MAX_BLOCKS) fit = BIG_MAX_BLOCKS;
-      const u32 pb = novf < fit ? novf : (u32)fit;
+      const u32 pb = (u32)fit;
       const size_t need = (size_t)pb * region;
       if (S.huge_key.cap < need) {
         S.huge_key.ensure(E.mem, need);
@@ -974,7 +972,8 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
       }
       EvalArgs a2 = a;
       a2.idx = S.ovf.p;
-      a2.nidx = novf;
+      a2.nidx = 0;
+      a2.nidx_dev = S.ovf_cnt.p;
       a2.tkey = S.huge_key.p;
       a2.tpos = S.huge_pos.p;
       a2.tval = S.huge_val.p;
