@@ -171,7 +171,9 @@ static u64 compress_records(Engine& E, u64 R, double threshold) {
   cub_run(E, [&](void* t, size_t& b) {
     return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)R, st);
   });
-  u32 U = E.read_u32(sid + R - 1) + E.read_u32(h + R - 1);
+  u32 uh[2];
+  E.read_u32s({sid + R - 1, h + R - 1}, uh);
+  const u32 U = uh[0] + uh[1];
   ++E.nlaunch, k_seg_start64<<<grid_for(R), 256, 0, st>>>(h, sid, R, S.seg_start.p);
   S.eu.ensure(E.mem, U);
   S.ev.ensure(E.mem, U);
@@ -219,11 +221,13 @@ u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n, boo
       cub_run(E, [&](void* t, size_t& b) {
         return cub::DeviceReduce::Max(t, b, sp, o, (int64_t)n, st);
       });
-      m1 = E.read_u32(o);
       cub_run(E, [&](void* t, size_t& b) {
-        return cub::DeviceReduce::Max(t, b, sc, o, (int64_t)n, st);
+        return cub::DeviceReduce::Max(t, b, sc, o + 1, (int64_t)n, st);
       });
-      m2 = E.read_u32(o);
+      u32 mm[2];
+      E.read_u32s({o, o + 1}, mm);
+      m1 = mm[0];
+      m2 = mm[1];
     }
     *next_n = (m1 > m2 ? m1 : m2) + 1;
   }

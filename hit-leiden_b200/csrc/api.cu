@@ -18,23 +18,40 @@ void hl_set_error_message(const std::string& m) { g_err = m; }
 namespace hl {
 
 u64 Engine::read_u64(const u64* d) {
+  if (ktiming) ++kagg[KT_HOST_SYNC].launches;
   HL_CUDA(cudaMemcpyAsync(hs.p, d, sizeof(u64), cudaMemcpyDeviceToHost, stream));
   HL_CUDA(cudaStreamSynchronize(stream));
   return hs.p[0];
 }
 u32 Engine::read_u32(const u32* d) {
+  if (ktiming) ++kagg[KT_HOST_SYNC].launches;
   HL_CUDA(cudaMemcpyAsync(hs.p, d, sizeof(u32), cudaMemcpyDeviceToHost, stream));
   HL_CUDA(cudaStreamSynchronize(stream));
   return (u32)(hs.p[0] & 0xFFFFFFFFull);
 }
+void Engine::read_u32s(std::initializer_list<const u32*> ptrs, u32* out) {
+  if (ktiming) ++kagg[KT_HOST_SYNC].launches;
+  require(ptrs.size() <= 16, "too many scalars in one read");
+  u32* h = reinterpret_cast<u32*>(hs.p + 32);  // slots 32..39 of the pinned staging
+  int i = 0;
+  for (const u32* d : ptrs)
+    HL_CUDA(cudaMemcpyAsync(h + i++, d, sizeof(u32), cudaMemcpyDeviceToHost, stream));
+  HL_CUDA(cudaStreamSynchronize(stream));
+  for (int j = 0; j < i; ++j) out[j] = h[j];
+}
+
 double Engine::read_f64(const double* d) {
+  if (ktiming) ++kagg[KT_HOST_SYNC].launches;
   HL_CUDA(cudaMemcpyAsync(hs.p, d, sizeof(double), cudaMemcpyDeviceToHost, stream));
   HL_CUDA(cudaStreamSynchronize(stream));
   double x;
   std::memcpy(&x, hs.p, sizeof(double));
   return x;
 }
-void Engine::sync() { HL_CUDA(cudaStreamSynchronize(stream)); }
+void Engine::sync() {
+  if (ktiming) ++kagg[KT_HOST_SYNC].launches;
+  HL_CUDA(cudaStreamSynchronize(stream));
+}
 
 static cudaEvent_t pool_get(std::vector<cudaEvent_t>& pool) {
   if (!pool.empty()) {
@@ -480,7 +497,7 @@ static const char* kernel_names[KT_COUNT] = {
     "eval_small",  "eval_mid",    "eval_wide",        "eval_huge",      "comm_degrees",
     "apply_and_mark",
     "refine_cc",   "t_filter",    "row_sums",         "delta_resolve",  "stage_apply",
-    "stage_move",  "stage_refine", "stage_aggregate"};
+    "stage_move",  "stage_refine", "stage_aggregate", "host_syncs"};
 
 hl_status hl_kernel_stats(const hl_graph* g, hl_kernel_stat* out, uint32_t cap, uint32_t* count) {
   HL_TRY(require(g && count, "NULL argument"); Engine& E = *const_cast<EngineBox*>(box(g))->E;

@@ -491,13 +491,15 @@ __global__ void k_merge_rows(u32 n, const u64* off, const u32* col, const double
 
 // Row sums in CSR order (hit_leiden.rs:1063), left to right: the exact
 // rounding of the reference for any weights (warp per row, ordered fold).
+// `flags` (if set) restricts the rows to those flagged.
 __global__ void k_row_sum_serial(const u32* rows, u32 nr, const u64* off, const double* w,
-                                 double* k) {
+                                 double* k, const u8* flags = nullptr) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 i = warp; i < nr; i += nwarps) {
     u32 v = rows ? rows[i] : (u32)i;
+    if (flags && !flags[v]) continue;
     double s = warp_ordered_sum(off[v], off[v + 1], 0.0, [&](u64 p) { return w[p]; },
                                 [](u64) { return true; });
     if (lane == 0) k[v] = s;
@@ -507,12 +509,13 @@ __global__ void k_row_sum_serial(const u32* rows, u32 nr, const u64* off, const 
 // Warp-parallel row sums; only used when every weight is integral, where any
 // summation order gives the same bits.
 __global__ void k_row_sum_warp(const u32* rows, u32 nr, const u64* off, const double* w,
-                               double* k) {
+                               double* k, const u8* flags = nullptr) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 i = warp; i < nr; i += nwarps) {
     u32 v = rows ? rows[i] : (u32)i;
+    if (flags && !flags[v]) continue;
     double s = 0.0;
     for (u64 p = off[v] + lane; p < off[v + 1]; p += 32) s += w[p];
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -559,15 +562,17 @@ double tree_sum(Engine& E, const double* x, u64 n) {
   return E.read_f64(a);
 }
 
-static void recompute_rows(Engine& E, Level& L, const u32* rows, u32 nr) {
-  if (!nr) return;
+// Rows whose flag is set (no list, so no count to read back first).
+static void recompute_flagged_rows(Engine& E, Level& L, const u8* flags) {
+  const u32 n = L.g.n;
+  if (!n) return;
   cudaEvent_t ev = E.kt_begin();
   if (E.integral)
-    ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p, L.g.w.p,
-                                                                  L.k.p);
+    ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(
+        nullptr, n, L.g.off.p, L.g.w.p, L.k.p, flags);
   else
-    ++E.nlaunch, k_row_sum_serial<<<grid_for((u64)nr * 32), 256, 0, E.stream>>>(rows, nr, L.g.off.p,
-                                                                               L.g.w.p, L.k.p);
+    ++E.nlaunch, k_row_sum_serial<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(
+        nullptr, n, L.g.off.p, L.g.w.p, L.k.p, flags);
   HL_LAUNCH_CHECK();
   E.kt_end(KT_ROW_SUMS, ev);
 }
@@ -633,9 +638,9 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
     });
     ++E.nlaunch, k_seg_start<<<grid_for(k), 256, 0, st>>>(head, segid, k, S.seg_start.p);
     HL_LAUNCH_CHECK();
-    u32 last_seg = E.read_u32(segid + (k - 1));
-    u32 last_head = E.read_u32(head + (k - 1));
-    U = last_seg + last_head;
+    u32 lh[2];
+    E.read_u32s({segid + (k - 1), head + (k - 1)}, lh);
+    U = lh[0] + lh[1];
 
     S.op.ensure(E.mem, U);
     S.neww.ensure(E.mem, U);
@@ -661,8 +666,13 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
     });
   }
   E.kt_end(KT_DELTA_SORT, ev_ds);
-  u64 n_del_keys = U ? E.read_u32(S.pos_del.p + U) : 0;
-  u64 n_ins = U ? E.read_u32(S.pos_ins.p + U) : 0;
+  u64 n_del_keys = 0, n_ins = 0;
+  if (U) {
+    u32 di[2];
+    E.read_u32s({S.pos_del.p + U, S.pos_ins.p + U}, di);
+    n_del_keys = di[0];
+    n_ins = di[1];
+  }
 
   // Existing self-loops to drop (reference behaviour) — counted first.
   u64 n_drop = 0;
@@ -677,17 +687,7 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   if (R == 0) {
     // Weight updates only: no structural change.
     if (U) {
-      u32* rows = S.rowlist.p;
-      S.cnt.ensure(E.mem, 16);
-      u32* cnt = S.cnt.p + 8;
-      S.act.ensure(E.mem, n ? n : 1);
-      cub_run(E, [&](void* t, size_t& bytes) {
-        return cub::DeviceSelect::Flagged(t, bytes, cub::CountingInputIterator<u32>(0),
-                                          S.ktouched.p, S.act.p, cnt, (int64_t)n, st);
-      });
-      u32 nr = E.read_u32(cnt);
-      (void)rows;
-      recompute_rows(E, L, S.act.p, nr);
+      recompute_flagged_rows(E, L, S.ktouched.p);
       L.tw = tree_sum(E, L.k.p, n);
     }
     return;
@@ -754,32 +754,25 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   E.kt_end(KT_MERGE_ROWS, kev);
   // old and new offsets, touched flags, old and new (col, w) entries
   E.kagg[KT_MERGE_ROWS].bytes += 16ull * ((u64)n + 1) + n + 12ull * (G.nnz + nnz_new);
-  if (E.read_u32(S.cnt.p + 4) != 0)
+  u32 ce[3];  // merge errors, inserted and deleted self-loops
+  E.read_u32s({S.cnt.p + 4, S.cnt.p + 0, S.cnt.p + 1}, ce);
+  if (ce[0] != 0)
     throw Error(HL_ERR_CUDA, "internal error: CSR merge produced an out-of-range position");
   G.col.swap(ncol);
   G.w.swap(nw);
   G.off.swap(S.newoff);
   G.nnz = nnz_new;
   {
-    u32 ins_loops = E.read_u32(S.cnt.p + 0);
-    u32 del_loops = E.read_u32(S.cnt.p + 1);
+    u32 ins_loops = ce[1];
+    u32 del_loops = ce[2];
     if (drop_loops)
       G.self_loop_entries = 2ull * ins_loops;
     else
       G.self_loop_entries = G.self_loop_entries + 2ull * ins_loops - 2ull * del_loops;
   }
   // Degrees of every row whose weights changed, then 2m.
-  {
-    u32* cnt = S.cnt.p + 8;
-    S.act.ensure(E.mem, n ? n : 1);
-    cub_run(E, [&](void* t, size_t& bytes) {
-      return cub::DeviceSelect::Flagged(t, bytes, cub::CountingInputIterator<u32>(0), S.ktouched.p,
-                                        S.act.p, cnt, (int64_t)n, st);
-    });
-    u32 nr = E.read_u32(cnt);
-    recompute_rows(E, L, S.act.p, nr);
-    L.tw = tree_sum(E, L.k.p, n);
-  }
+  recompute_flagged_rows(E, L, S.ktouched.p);
+  L.tw = tree_sum(E, L.k.p, n);
 }
 
 }  // namespace hl

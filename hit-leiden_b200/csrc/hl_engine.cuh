@@ -1,6 +1,7 @@
 // hl_engine.cuh — device state of one graph handle and the stage entry points.
 #pragma once
 #include <atomic>
+#include <initializer_list>
 #include <cub/cub.cuh>
 
 #include "hl_internal.cuh"
@@ -87,6 +88,7 @@ struct Scratch {
   // global tables of the block-per-vertex kernel (degrees above 4096)
   DBuf<u32> huge_key, huge_pos, huge_list;
   DBuf<u32> ovf, ovf_cnt;  // block kernel: rows deferred to the pass with global regions
+  DBuf<u32> acc_cnt;       // inc-movement: accepted moves over all rounds
   DBuf<double> huge_val;
 };
 
@@ -106,8 +108,8 @@ enum KernelId : int {
   KT_AGGREGATE,
   KT_EVAL_SMALL,   // sub-warp bins (both evaluation kinds)
   KT_EVAL_MID,     // warp-per-vertex bin
-  KT_EVAL_BIG,     // warp-per-vertex wide bin (129..4096)
-  KT_EVAL_HUGE,    // block-per-vertex bin (> 4096)
+  KT_EVAL_BIG,     // warp-per-vertex wide bin (129..512)
+  KT_EVAL_HUGE,    // block-per-vertex bin (> 512), both passes
   KT_COMM_DEG,     // per-community / per-sub-community degree sums
   KT_MARK_NEXT,    // accepted-move application and frontier marking
   KT_REFINE_CC,    // connected components of affected sub-communities
@@ -118,6 +120,7 @@ enum KernelId : int {
   KT_STAGE_MOVE,
   KT_STAGE_REFINE,
   KT_STAGE_AGGREGATE,
+  KT_HOST_SYNC,    // host waits on the stream (launches = count; no time)
   KT_COUNT
 };
 
@@ -151,6 +154,8 @@ struct Engine {
 
   u64 read_u64(const u64* dptr);
   u32 read_u32(const u32* dptr);
+  // Several device scalars with one wait: out[i] = *ptrs[i] (at most 16).
+  void read_u32s(std::initializer_list<const u32*> ptrs, u32* out);
   double read_f64(const double* dptr);
   void sync();
 };

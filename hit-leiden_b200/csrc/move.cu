@@ -72,11 +72,15 @@ __global__ void k_comm_deg_atomic(u32 n, const u32* part, const double* k, doubl
 
 // Ordered variant: nodes sorted by (community, node); one thread per community
 // sums its members' degrees in ascending node order.
-__global__ void k_comm_deg_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 n,
-                                   const u32* sorted_nodes, const double* k, double* d) {
+// The number of communities is read on the device (exclusive scan of the
+// segment heads at the last position plus the last head).
+__global__ void k_comm_deg_ordered(const u32* seg_last, const u32* head_last, const u32* ukeys,
+                                   const u32* ustart, u32 n, const u32* sorted_nodes,
+                                   const double* k, double* d) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  const u32 nu = *seg_last + *head_last;
   for (u64 j = warp; j < nu; j += nwarps) {
     u32 a = ustart[j], b = (j + 1 < nu) ? ustart[j + 1] : n;
     double s = warp_ordered_sum(a, b, 0.0, [&](u64 t) { return k[sorted_nodes[t]]; },
@@ -150,10 +154,9 @@ static void recompute_comm_degrees_impl(Engine& E, Level& L, const u32* part, u3
   cub_run(E, [&](void* t, size_t& b) {
     return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)n, st);
   });
-  u32 nu = E.read_u32(sid + n - 1) + E.read_u32(h + n - 1);
   ++E.nlaunch, k_seg_compact<<<grid_for(n), 256, 0, st>>>(h, sid, kout, n, S.used.p, S.sel_node.p);
-  ++E.nlaunch, k_comm_deg_ordered<<<grid_for((u64)nu * 32), 256, 0, st>>>(nu, S.used.p, S.sel_node.p, n,
-                                                                           vout, L.k.p, d);
+  ++E.nlaunch, k_comm_deg_ordered<<<grid_for((u64)n * 32), 256, 0, st>>>(
+      sid + n - 1, h + n - 1, S.used.p, S.sel_node.p, n, vout, L.k.p, d);
   HL_LAUNCH_CHECK();
 }
 
@@ -347,12 +350,15 @@ __global__ void k_dops(u32 M, const u8* status, const u32* sel_from, const u32* 
 }
 
 // d[c] - k1 + k2 ... in selected order (a - b is a + (-b) exactly).
-__global__ void k_apply_ordered(u32 nu, const u32* ukeys, const u32* ustart, u32 total,
-                                const u32* ops, const u32* sel_node, const double* kdeg,
-                                double* d) {
+// The number of segments is read on the device: the exclusive scan of the
+// segment heads plus the last head.
+__global__ void k_apply_ordered(const u32* seg_last, const u32* head_last, const u32* ukeys,
+                                const u32* ustart, u32 total, const u32* ops,
+                                const u32* sel_node, const double* kdeg, double* d) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  const u32 nu = *seg_last + *head_last;
   for (u64 j = warp; j < nu; j += nwarps) {
     u32 c = ukeys[j];
     if (c == NONE32) continue;
@@ -497,6 +503,8 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
 
   const u32 max_rounds = E.cfg.max_rounds ? E.cfg.max_rounds : 20;
   u32 it = 0;
+  S.acc_cnt.ensure(E.mem, 1);
+  HL_CUDA(cudaMemsetAsync(S.acc_cnt.p, 0, sizeof(u32), st));  // accepted moves, all rounds
   while (it < max_rounds) {
     // Active list, ascending (iter_ones order).
     cub_run(E, [&](void* t, size_t& b) {
@@ -536,10 +544,9 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     HL_LAUNCH_CHECK();
     select_decoupled_dev(E, M);
     cudaEvent_t ev_mark = E.kt_begin();
-    HL_CUDA(cudaMemsetAsync(cnt + 7, 0, sizeof(u32), st));
     ++E.nlaunch, k_apply_moves<<<grid_for(M), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_from.p,
                                                S.sel_to.p, L.f.p, L.k.p, S.d.p, E.integral,
-                                               S.changed.p, S.affected.p, mark_moved, cnt + 7);
+                                               S.changed.p, S.affected.p, mark_moved, S.acc_cnt.p);
     HL_LAUNCH_CHECK();
     if (!E.integral) {
       // Replay d(C) -= k / += k in selected order, per community.
@@ -569,15 +576,14 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
       cub_run(E, [&](void* t, size_t& b) {
         return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)M2, st);
       });
-      u32 nu = E.read_u32(sid + M2 - 1) + E.read_u32(h + M2 - 1);
       ++E.nlaunch, k_seg_compact<<<grid_for(M2), 256, 0, st>>>(h, sid, ko, M2, S.rowlist.p, S.seg_start.p);
-      ++E.nlaunch, k_apply_ordered<<<grid_for((u64)nu * 32), 256, 0, st>>>(nu, S.rowlist.p, S.seg_start.p, M2, vo,
-                                                    S.sel_node.p, L.k.p, S.d.p);
+      ++E.nlaunch, k_apply_ordered<<<grid_for((u64)M2 * 32), 256, 0, st>>>(
+          sid + M2 - 1, h + M2 - 1, S.rowlist.p, S.seg_start.p, M2, vo, S.sel_node.p, L.k.p, S.d.p);
       HL_LAUNCH_CHECK();
     }
-    u32 acc = E.read_u32(cnt + 7);
-    out.moves += acc;
-    if (!acc) break;
+    // No early exit on zero accepted moves (it would cost a read-back every
+    // round): such a round marks nothing, so the next frontier is empty and
+    // the loop ends on it with the same iteration count.
     HL_CUDA(cudaMemsetAsync(S.next.p, 0, n, st));
     ++E.nlaunch, k_mark_next<<<grid_for((u64)M * 32), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_to.p,
                                                         L.g.off.p, L.g.col.p, L.f.p, L.s_cur.p,
@@ -589,8 +595,10 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   out.iterations = it;
   u64 cnt8[8];
   HL_CUDA(cudaMemcpyAsync(E.hs.p, S.red64.p, 8 * sizeof(u64), cudaMemcpyDeviceToHost, st));
+  HL_CUDA(cudaMemcpyAsync(E.hs.p + 8, S.acc_cnt.p, sizeof(u32), cudaMemcpyDeviceToHost, st));
   E.sync();
   std::memcpy(cnt8, E.hs.p, sizeof(cnt8));
+  out.moves = (u32)(E.hs.p[8] & 0xFFFFFFFFull);
   out.traversed = cnt8[0] + cnt8[2] + cnt8[4] + cnt8[6];
   u64 ncand = cnt8[1] + cnt8[3] + cnt8[5] + cnt8[7];
   // Algorithmic bytes of the evaluation kernel: per active vertex its list

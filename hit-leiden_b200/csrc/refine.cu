@@ -145,6 +145,12 @@ __global__ void k_not_identity(u32 n, const u32* s, u32* bad) {
   if (local) atomicAdd(bad, local);
 }
 
+__global__ void k_refine_all_if_identity(u32 n, const u32* not_identity, u8* refined) {
+  if (*not_identity) return;
+  for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x)
+    refined[v] = 1;
+}
+
 __global__ void k_sizes(u32 n, const u32* s, u32* sizes) {
   for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x)
     atomicAdd(&sizes[s[v]], 1u);
@@ -476,11 +482,12 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   out.splits = m_new;
   E.kt_end(KT_REFINE_CC, ev_cc);
 
-  // is_initial (hit_leiden.rs:1333-1339): s is the identity ⇒ R = all.
+  // is_initial (hit_leiden.rs:1333-1339): s is the identity ⇒ R = all
+  // (decided on the device: no read-back).
   HL_CUDA(cudaMemsetAsync(cnt + 5, 0, sizeof(u32), st));
   ++E.nlaunch, k_not_identity<<<grid_for(n), 256, 0, st>>>(n, s, cnt + 5);
+  ++E.nlaunch, k_refine_all_if_identity<<<grid_for(n), 256, 0, st>>>(n, cnt + 5, S.refined.p);
   HL_LAUNCH_CHECK();
-  if (E.read_u32(cnt + 5) == 0) HL_CUDA(cudaMemsetAsync(S.refined.p, 1, n, st));
 
   // ---- 2. sizes, d_S, d_C -----------------------------------------------
   u32 smax2 = m_new ? smax + m_new : smax;
