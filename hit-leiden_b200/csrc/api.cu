@@ -497,7 +497,8 @@ static const char* kernel_names[KT_COUNT] = {
     "eval_small",  "eval_mid",    "eval_wide",        "eval_huge",      "comm_degrees",
     "apply_and_mark",
     "refine_cc",   "t_filter",    "row_sums",         "delta_resolve",  "stage_apply",
-    "stage_move",  "stage_refine", "stage_aggregate", "host_syncs"};
+    "stage_move",  "stage_refine", "stage_aggregate", "host_syncs",
+    "csr_copy_untouched"};
 
 hl_status hl_kernel_stats(const hl_graph* g, hl_kernel_stat* out, uint32_t cap, uint32_t* count) {
   HL_TRY(require(g && count, "NULL argument"); Engine& E = *const_cast<EngineBox*>(box(g))->E;

@@ -358,134 +358,221 @@ __global__ void k_row_ranges(const u64* rkeys, u64 R, u32* rstart, u32* rend) {
 // read once and no step is serial in the number of operations.  A self-loop is stored twice in its row
 // and its operations come in pairs; operations on one neighbour come deletes
 // first (a dropped self-loop replaced by an inserted one).
+// Merge of the row slice [s0, s1) (chunks of 32 from the row start o0) of a
+// touched row, by one warp.  The state on entry is that of the operations
+// consumed before the slice: p = first operation not consumed, drun / irun =
+// deletes / inserts consumed, del_key / del_same = neighbour of the last
+// consumed delete and the consumed deletes on it.  `row_end` marks the row's
+// last slice, whose last chunk takes every remaining operation.
+__device__ __forceinline__ void merge_slice(u64 o0, u64 s0, u64 s1, bool row_end, u64 no, u32 p,
+                                            u32 b, u32 drun, u32 irun, u32 del_key,
+                                            u32 del_same, const u32* col, const double* w,
+                                            u32* ncol, double* nw, const u64* rkeys,
+                                            const u32* rvals, const double* neww, u64 nnz_new,
+                                            u32* err) {
+  const u32 lane = threadIdx.x & 31;
+  // operation tile [tb, tb + 32) in registers: neighbour, value (DEL_MARK
+  // for a delete, else the index of the inserted weight)
+  u32 tb = p;
+  u32 tk = NONE32, tv = 0;
+  if (tb + lane < b) {
+    tk = (u32)rkeys[tb + lane];
+    tv = rvals[tb + lane];
+  }
+  // entry chunk prefetched one ahead
+  u32 c_n = s0 + lane < s1 ? col[s0 + lane] : NONE32;
+  double w_n = s0 + lane < s1 ? w[s0 + lane] : 0.0;
+  for (u64 base = s0;; base += 32) {
+    const bool chunk_last = base + 32 >= s1;
+    const bool last = chunk_last && row_end;  // the row's last chunk takes every remaining op
+    const u64 q = base + lane;
+    const bool valid = q < s1;
+    const u32 c = c_n;
+    const double wv = w_n;
+    if (!chunk_last) {
+      const u64 qn = q + 32;
+      c_n = qn < s1 ? col[qn] : NONE32;
+      w_n = qn < s1 ? w[qn] : 0.0;
+    }
+    const u32 vmask = __ballot_sync(0xffffffffu, valid);
+    const u32 c_last = vmask ? __shfl_sync(0xffffffffu, c, 31 - __clz(vmask)) : 0u;
+    const u32 d0 = drun, i0 = irun;
+    u32 dl = 0, il = 0;
+    // the two copies of a deleted self-loop may straddle two chunks: the
+    // earlier chunk consumed their deletes
+    bool deleted = valid && del_key != NONE32 && c == del_key;
+    while (p < b) {
+      const u32 o = p - tb;  // first unconsumed lane of the tile
+      const bool ok = tb + lane < b && lane >= o;
+      const u32 m = __ballot_sync(0xffffffffu, ok && (last || tk <= c_last));
+      const u32 cnt = __popc(m);  // lanes o .. o+cnt-1 (operations are sorted)
+      if (cnt) {
+        const u32 hiL = o + cnt;
+        const u32 delm = __ballot_sync(0xffffffffu, tv == DEL_MARK) & m;
+        // Entries: the consumed operations below c (lower bound of c among
+        // the tile's keys) and whether c itself is deleted.
+        u32 lo = o, hi = hiL;
+#pragma unroll
+        for (int it = 0; it < 6; ++it) {
+          const u32 mid = (lo + hi) >> 1;
+          const u32 km = __shfl_sync(0xffffffffu, tk, mid & 31);
+          if (lo < hi) {
+            if (km < c) lo = mid + 1;
+            else hi = mid;
+          }
+        }
+        const u32 ltm = m & (lo >= 32 ? 0xffffffffu : ((1u << lo) - 1u));
+        dl += __popc(ltm & delm);
+        il += __popc(ltm & ~delm);
+        const u32 kp = __shfl_sync(0xffffffffu, tk, lo & 31);
+        const u32 vp = __shfl_sync(0xffffffffu, tv, lo & 31);
+        if (valid && lo < hiL && kp == c && vp == DEL_MARK) deleted = true;
+        // Inserts: lower bound among the chunk's entries (padded with
+        // NONE32), earlier deletes below the key and earlier inserts.
+        u32 lo2 = 0, hi2 = 32;
+#pragma unroll
+        for (int it = 0; it < 6; ++it) {
+          const u32 mid = (lo2 + hi2) >> 1;
+          const u32 cm = __shfl_sync(0xffffffffu, c, mid & 31);
+          if (lo2 < hi2) {
+            if (cm < tk) lo2 = mid + 1;
+            else hi2 = mid;
+          }
+        }
+        const u32 grp = __match_any_sync(0xffffffffu, tk) & m;
+        const u32 before = (1u << lane) - 1u;
+        const bool ins = ((m >> lane) & 1u) && tv != DEL_MARK;
+        if (ins) {
+          const u32 dlt = drun + __popc(delm & before) - __popc(grp & delm & before) -
+                          (del_key == tk ? del_same : 0u);
+          const u64 out = no + (base + lo2 - o0) - dlt + irun + __popc(m & ~delm & before);
+          if (out >= nnz_new) {
+            atomicAdd(err, 1u);
+          } else {
+            ncol[out] = tk;
+            nw[out] = neww[tv];
+          }
+        }
+        if (delm) {
+          const u32 ld = 31 - __clz(delm);
+          const u32 kd = __shfl_sync(0xffffffffu, tk, ld);
+          const u32 same = __popc(__shfl_sync(0xffffffffu, grp, ld) & delm);
+          del_same = (del_key == kd) ? del_same + same : same;
+          del_key = kd;
+        }
+        drun += __popc(delm);
+        irun += cnt - __popc(delm);
+      }
+      p += cnt;
+      if (o + cnt < 32 || p >= b) break;
+      // the whole tile was consumed: load the next one
+      tb = p;
+      tk = NONE32;
+      tv = 0;
+      if (tb + lane < b) {
+        tk = (u32)rkeys[tb + lane];
+        tv = rvals[tb + lane];
+      }
+    }
+    if (valid && !deleted) {
+      const u64 out = no + (q - o0) - (d0 + dl) + (i0 + il);
+      if (out >= nnz_new) {
+        atomicAdd(err, 1u);
+      } else {
+        ncol[out] = c;
+        nw[out] = wv;
+      }
+    }
+    if (chunk_last) break;
+  }
+}
+
+// Touched rows, merged with their sorted row-operations, so the output row is
+// again sorted by neighbour id: deleted entries are skipped, every surviving
+// entry moves by (inserts before it) - (deletes before it), and an insert
+// lands at its lower bound in the old row, after the earlier inserts and
+// before the entries it precedes.  A warp walks the row in chunks of 32 and
+// consumes, per chunk, the operations whose neighbour is not above the
+// chunk's last one (all of them in the row's last chunk), 32 operations at a
+// time with bisections over lanes.  A self-loop is stored twice in its row and
+// its operations come in pairs; operations on one neighbour come deletes
+// first (a dropped self-loop replaced by an inserted one).
+//
+// Rows longer than MERGE_LONG go to `long_rows` for k_merge_long.
+constexpr u64 MERGE_LONG = 2048;
+
 __global__ void k_merge_rows(u32 n, const u64* off, const u32* col, const double* w,
                              const u64* noff, u32* ncol, double* nw, const u8* touched,
                              const u64* rkeys, const u32* rvals, const u32* rstart,
-                             const u32* rend, const double* neww, u64 nnz_new, u32* err) {
+                             const u32* rend, const double* neww, u64 nnz_new, u32* err,
+                             u32* long_rows, u32* nlong) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 r = warp; r < n; r += nwarps) {
     if (!touched[r]) continue;
-    const u64 o0 = off[r], o1 = off[r + 1], no = noff[r];
-    const u32 b = rend[r];
-    u32 p = rstart[r];
-    u32 drun = 0, irun = 0;       // deletes / inserts consumed so far
-    u32 del_key = NONE32;         // neighbour of the last consumed delete
-    u32 del_same = 0;             // consumed deletes on that neighbour
-    // operation tile [tb, tb + 32) in registers: neighbour, value (DEL_MARK
-    // for a delete, else the index of the inserted weight)
-    u32 tb = p;
-    u32 tk = NONE32, tv = 0;
-    if (tb + lane < b) {
-      tk = (u32)rkeys[tb + lane];
-      tv = rvals[tb + lane];
+    const u64 o0 = off[r], o1 = off[r + 1];
+    if (o1 - o0 > MERGE_LONG) {
+      if (lane == 0) long_rows[atomicAdd(nlong, 1u)] = (u32)r;
+      continue;
     }
-    // entry chunk prefetched one ahead
-    u32 c_n = o0 + lane < o1 ? col[o0 + lane] : NONE32;
-    double w_n = o0 + lane < o1 ? w[o0 + lane] : 0.0;
-    for (u64 base = o0;; base += 32) {
-      const bool last = base + 32 >= o1;
-      const u64 q = base + lane;
-      const bool valid = q < o1;
-      const u32 c = c_n;
-      const double wv = w_n;
-      if (!last) {
-        const u64 qn = q + 32;
-        c_n = qn < o1 ? col[qn] : NONE32;
-        w_n = qn < o1 ? w[qn] : 0.0;
+    merge_slice(o0, o0, o1, true, noff[r], rstart[r], rend[r], 0, 0, NONE32, 0, col, w, ncol, nw,
+                rkeys, rvals, neww, nnz_new, err);
+  }
+}
+
+// Long touched rows: a block per row, its warps on consecutive slices of
+// whole chunks.  A warp rebuilds the state at its slice start from the
+// operations whose neighbour is not above the entry before the slice.
+__global__ void __launch_bounds__(256) k_merge_long(const u32* long_rows, const u32* nlong,
+                                                    const u64* off, const u32* col,
+                                                    const double* w, const u64* noff, u32* ncol,
+                                                    double* nw, const u64* rkeys,
+                                                    const u32* rvals, const u32* rstart,
+                                                    const u32* rend, const double* neww,
+                                                    u64 nnz_new, u32* err) {
+  const u32 lane = threadIdx.x & 31;
+  const u32 wib = threadIdx.x >> 5;
+  const u32 nw_ = blockDim.x >> 5;
+  const u32 cnt = *nlong;
+  for (u32 t = blockIdx.x; t < cnt; t += gridDim.x) {
+    const u32 r = long_rows[t];
+    const u64 o0 = off[r], o1 = off[r + 1];
+    const u64 chunks = (o1 - o0 + 31) / 32;  // > MERGE_LONG / 32 >= warps per block
+    const u64 c0 = chunks * wib / nw_, c1 = chunks * (wib + 1) / nw_;
+    const u64 s0 = o0 + 32 * c0;
+    const u64 s1 = (o0 + 32 * c1 < o1) ? o0 + 32 * c1 : o1;
+    const u32 a = rstart[r], b = rend[r];
+    u32 p = a, drun = 0, irun = 0, del_key = NONE32, del_same = 0;
+    if (s0 > o0) {
+      // operations consumed before the slice: neighbour <= col[s0 - 1]
+      const u32 cprev = col[s0 - 1];
+      u32 lo = a, hi = b;
+      while (lo < hi) {
+        const u32 mid = (lo + hi) >> 1;
+        if ((u32)rkeys[mid] <= cprev) lo = mid + 1;
+        else hi = mid;
       }
-      const u32 vmask = __ballot_sync(0xffffffffu, valid);
-      const u32 c_last = vmask ? __shfl_sync(0xffffffffu, c, 31 - __clz(vmask)) : 0u;
-      const u32 d0 = drun, i0 = irun;
-      u32 dl = 0, il = 0;
-      // the two copies of a deleted self-loop may straddle two chunks: the
-      // earlier chunk consumed their deletes
-      bool deleted = valid && del_key != NONE32 && c == del_key;
-      while (p < b) {
-        const u32 o = p - tb;  // first unconsumed lane of the tile
-        const bool ok = tb + lane < b && lane >= o;
-        const u32 m = __ballot_sync(0xffffffffu, ok && (last || tk <= c_last));
-        const u32 cnt = __popc(m);  // lanes o .. o+cnt-1 (operations are sorted)
-        if (cnt) {
-          const u32 hiL = o + cnt;
-          const u32 delm = __ballot_sync(0xffffffffu, tv == DEL_MARK) & m;
-          // Entries: the consumed operations below c (lower bound of c among
-          // the tile's keys) and whether c itself is deleted.
-          u32 lo = o, hi = hiL;
-#pragma unroll
-          for (int it = 0; it < 6; ++it) {
-            const u32 mid = (lo + hi) >> 1;
-            const u32 km = __shfl_sync(0xffffffffu, tk, mid & 31);
-            if (lo < hi) {
-              if (km < c) lo = mid + 1;
-              else hi = mid;
-            }
-          }
-          const u32 ltm = m & (lo >= 32 ? 0xffffffffu : ((1u << lo) - 1u));
-          dl += __popc(ltm & delm);
-          il += __popc(ltm & ~delm);
-          const u32 kp = __shfl_sync(0xffffffffu, tk, lo & 31);
-          const u32 vp = __shfl_sync(0xffffffffu, tv, lo & 31);
-          if (valid && lo < hiL && kp == c && vp == DEL_MARK) deleted = true;
-          // Inserts: lower bound among the chunk's entries (padded with
-          // NONE32), earlier deletes below the key and earlier inserts.
-          u32 lo2 = 0, hi2 = 32;
-#pragma unroll
-          for (int it = 0; it < 6; ++it) {
-            const u32 mid = (lo2 + hi2) >> 1;
-            const u32 cm = __shfl_sync(0xffffffffu, c, mid & 31);
-            if (lo2 < hi2) {
-              if (cm < tk) lo2 = mid + 1;
-              else hi2 = mid;
-            }
-          }
-          const u32 grp = __match_any_sync(0xffffffffu, tk) & m;
-          const u32 before = (1u << lane) - 1u;
-          const bool ins = ((m >> lane) & 1u) && tv != DEL_MARK;
-          if (ins) {
-            const u32 dlt = drun + __popc(delm & before) - __popc(grp & delm & before) -
-                            (del_key == tk ? del_same : 0u);
-            const u64 out = no + (base + lo2 - o0) - dlt + irun + __popc(m & ~delm & before);
-            if (out >= nnz_new) {
-              atomicAdd(err, 1u);
-            } else {
-              ncol[out] = tk;
-              nw[out] = neww[tv];
-            }
-          }
-          if (delm) {
-            const u32 ld = 31 - __clz(delm);
-            const u32 kd = __shfl_sync(0xffffffffu, tk, ld);
-            const u32 same = __popc(__shfl_sync(0xffffffffu, grp, ld) & delm);
-            del_same = (del_key == kd) ? del_same + same : same;
-            del_key = kd;
-          }
-          drun += __popc(delm);
-          irun += cnt - __popc(delm);
-        }
-        p += cnt;
-        if (o + cnt < 32 || p >= b) break;
-        // the whole tile was consumed: load the next one
-        tb = p;
-        tk = NONE32;
-        tv = 0;
-        if (tb + lane < b) {
-          tk = (u32)rkeys[tb + lane];
-          tv = rvals[tb + lane];
-        }
+      p = lo;
+      // deletes among them, and the last one (warp-uniform)
+      u32 last_del = NONE32;
+      for (u32 x0 = a; x0 < p; x0 += 32) {
+        const bool d = x0 + lane < p && rvals[x0 + lane] == DEL_MARK;
+        const u32 m = __ballot_sync(0xffffffffu, d);
+        drun += __popc(m);
+        if (m) last_del = x0 + 31 - __clz(m);
       }
-      if (valid && !deleted) {
-        const u64 out = no + (q - o0) - (d0 + dl) + (i0 + il);
-        if (out >= nnz_new) {
-          atomicAdd(err, 1u);
-        } else {
-          ncol[out] = c;
-          nw[out] = wv;
-        }
+      irun = (p - a) - drun;
+      if (last_del != NONE32) {
+        // the deletes on that neighbour are consecutive and end at last_del
+        del_key = (u32)rkeys[last_del];
+        u32 x = last_del;
+        while (x > a && rvals[x - 1] == DEL_MARK && (u32)rkeys[x - 1] == del_key) --x;
+        del_same = last_del - x + 1;
       }
-      if (last) break;
     }
+    merge_slice(o0, s0, s1, c1 == chunks, noff[r], p, b, drun, irun, del_key, del_same, col, w,
+                ncol, nw, rkeys, rvals, neww, nnz_new, err);
   }
 }
 
@@ -741,15 +828,23 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   DBuf<double>& nw = G.w2;
   ncol.ensure(E.mem, nnz_new ? nnz_new : 1);
   nw.ensure(E.mem, nnz_new ? nnz_new : 1);
-  cudaEvent_t kev = E.kt_begin();
+  cudaEvent_t cev = E.kt_begin();
   if (nnz_new)
     ++E.nlaunch, k_copy_untouched<<<grid_for((nnz_new + COPY_CH - 1) / COPY_CH * 256), 256, 0, st>>>(
         n, G.off.p, G.col.p, G.w.p, S.newoff.p, ncol.p, nw.p, S.touched.p, nnz_new);
-  if (n)
-    ++E.nlaunch, k_merge_rows<<<grid_for((u64)n * 32), 256, 0, st>>>(n, G.off.p, G.col.p, G.w.p, S.newoff.p,
-                                                         ncol.p, nw.p, S.touched.p, S.rkeys2.p,
-                                                         S.rvals2.p, S.delpre.p, S.inspre.p,
-                                                         S.neww.p, nnz_new, S.cnt.p + 4);
+  E.kt_end(KT_COPY_ROWS, cev);
+  cudaEvent_t kev = E.kt_begin();
+  if (n) {
+    S.ovf.ensure(E.mem, n);
+    S.ovf_cnt.ensure(E.mem, 4);
+    HL_CUDA(cudaMemsetAsync(S.ovf_cnt.p, 0, sizeof(u32), st));
+    ++E.nlaunch, k_merge_rows<<<grid_for((u64)n * 32), 256, 0, st>>>(
+        n, G.off.p, G.col.p, G.w.p, S.newoff.p, ncol.p, nw.p, S.touched.p, S.rkeys2.p, S.rvals2.p,
+        S.delpre.p, S.inspre.p, S.neww.p, nnz_new, S.cnt.p + 4, S.ovf.p, S.ovf_cnt.p);
+    ++E.nlaunch, k_merge_long<<<148 * 2, 256, 0, st>>>(
+        S.ovf.p, S.ovf_cnt.p, G.off.p, G.col.p, G.w.p, S.newoff.p, ncol.p, nw.p, S.rkeys2.p,
+        S.rvals2.p, S.delpre.p, S.inspre.p, S.neww.p, nnz_new, S.cnt.p + 4);
+  }
   HL_LAUNCH_CHECK();
   E.kt_end(KT_MERGE_ROWS, kev);
   // old and new offsets, touched flags, old and new (col, w) entries

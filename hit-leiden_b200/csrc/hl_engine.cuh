@@ -121,6 +121,7 @@ enum KernelId : int {
   KT_STAGE_REFINE,
   KT_STAGE_AGGREGATE,
   KT_HOST_SYNC,    // host waits on the stream (launches = count; no time)
+  KT_COPY_ROWS,    // untouched CSR rows copied into the new buffer
   KT_COUNT
 };
 

@@ -78,6 +78,38 @@ def test_apply_delta_self_loop_across_chunks(before, keep_loops):
         assert gh.same_bits(go, ro) and gh.same_bits(gc, rc) and gh.same_bits(gw, rw)
 
 
+@pytest.mark.parametrize("before", [2558, 2559, 2560])
+@pytest.mark.parametrize("keep_loops", [False, True])
+def test_apply_delta_long_rows_split_across_warps(before, keep_loops):
+    # A row above 2048 entries is merged by a whole block, its warps on
+    # consecutive slices of 32-entry chunks.  With 2560 + 2560 neighbours
+    # and a self-loop the row has 161 chunks, so a slice starts at entry 2560:
+    # the loop's two copies sit just before, across, or just after it.
+    rng = np.random.default_rng(before)
+    n = 9000
+    v = 4000
+    nb = list(range(before)) + list(range(v + 1, v + 1 + 5120 - before))
+    src = [v] * len(nb) + [v]
+    dst = nb + [v]
+    w = list(rng.uniform(0.5, 2.0, len(nb))) + [3.0]
+    g = O.Graph.from_edges(n, src, dst, w).apply_delta([], [], [], keep_self_loops=True)
+    off, col, ww = g.csr()
+    row = col[off[v]:off[v + 1]]
+    assert row[before] == v and row[before + 1] == v
+    # deletes of existing row entries, inserts of new neighbours on both sides
+    # of the loop, the loop itself deleted or reweighted
+    dels = rng.choice(len(nb), 400, replace=False)
+    new_nb = rng.choice(np.setdiff1d(np.arange(n), np.array(nb + [v])), 400, replace=False)
+    for loop_w in (-3.0, 1.25):
+        ds = [v] * (len(dels) + len(new_nb)) + [v]
+        dd = [nb[i] for i in dels] + new_nb.tolist() + [v]
+        dw = [-w[i] for i in dels] + rng.uniform(0.5, 2.0, len(new_nb)).tolist() + [loop_w]
+        ref = g.apply_delta(ds, dd, dw, keep_self_loops=keep_loops)
+        go, gc, gw = gh.apply_delta(g, ds, dd, dw, keep_loops)
+        ro, rc, rw = ref.csr()
+        assert gh.same_bits(go, ro) and gh.same_bits(gc, rc) and gh.same_bits(gw, rw)
+
+
 def test_apply_delta_drops_existing_self_loops():
     g = O.Graph.from_edges(3, [0, 0], [0, 1], [5.0, 1.0])
     off, col, w = gh.apply_delta(g, [2], [2], [3.0], keep_loops=False)
