@@ -61,28 +61,44 @@ __global__ void k_agg_rows(u32 n, const u64* off, const u32* col, const double* 
     const u32 sp = s_pre[v], sc = s_cur[v];
     u64 o = pos ? base + pos[v] : 0;
     u64 c = 0;
-    for (u64 b0 = o0; b0 < o1; b0 += 32) {
-      u64 p = b0 + lane;
-      bool emit = false;
-      u32 nb = 0;
-      double x = 0.0;
-      if (p < o1) {
-        nb = col[p];
-        x = w[p];
-        emit = nb != (u32)v && agg_emit((u32)v, nb, refined, s_pre, s_cur, changed_only);
+    // Four chunks per step: their neighbours, then their labels, are loaded
+    // before any is decided, so a long row keeps several gathers in flight;
+    // the chunks' records are then placed in CSR order.
+    for (u64 b0 = o0; b0 < o1; b0 += 128) {
+      u32 nb[4], np_[4], nc[4];
+      u8 rf[4];
+      double x[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const u64 p = b0 + 32 * j + lane;
+        nb[j] = p < o1 ? col[p] : NONE32;
+        x[j] = p < o1 ? w[p] : 0.0;
       }
-      u32 m = __ballot_sync(0xffffffffu, emit);
-      if (pos && emit) {
-        u64 at = o + 2ull * __popc(m & ((1u << lane) - 1u));
-        keys[at] = pair_key(sp, s_pre[nb]);
-        vals[at] = -x;
-        seq[at] = (u32)at;
-        keys[at + 1] = pair_key(sc, s_cur[nb]);
-        vals[at + 1] = x;
-        seq[at + 1] = (u32)(at + 1);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (nb[j] != NONE32) {
+          np_[j] = s_pre[nb[j]];
+          nc[j] = s_cur[nb[j]];
+          rf[j] = refined[nb[j]];
+        }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        // agg_emit on the gathered labels
+        const bool emit = nb[j] != NONE32 && nb[j] != (u32)v &&
+                          (nc[j] == np_[j] || (u32)v < nb[j] || (changed_only && !rf[j]));
+        const u32 m = __ballot_sync(0xffffffffu, emit);
+        if (pos && emit) {
+          const u64 at = o + 2ull * __popc(m & ((1u << lane) - 1u));
+          keys[at] = pair_key(sp, np_[j]);
+          vals[at] = -x[j];
+          seq[at] = (u32)at;
+          keys[at + 1] = pair_key(sc, nc[j]);
+          vals[at + 1] = x[j];
+          seq[at + 1] = (u32)(at + 1);
+        }
+        o += 2ull * __popc(m);
+        c += 2ull * __popc(m);
       }
-      o += 2ull * __popc(m);
-      c += 2ull * __popc(m);
     }
     // The self-loop's entries (stored twice) sit together at the lower bound
     // of v in the sorted row; their sum in CSR order is the row-order sum of

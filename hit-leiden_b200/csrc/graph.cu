@@ -259,6 +259,11 @@ __global__ void k_emit_loop_drops(u32 n, const u64* off, const u32* col, u64* rk
   }
 }
 
+__global__ void k_del_flags(const u32* rvals, u64 R, u32* flag) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t <= R; t += (u64)gridDim.x * blockDim.x)
+    flag[t] = (t < R && rvals[t] == DEL_MARK) ? 1u : 0u;
+}
+
 __global__ void k_rowop_deg(const u64* rkeys, const u32* rvals, u64 R, int* ddeg, u8* touched) {
   for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < R; t += (u64)gridDim.x * blockDim.x) {
     u32 r = (u32)(rkeys[t] >> 32);
@@ -499,7 +504,7 @@ __device__ __forceinline__ void merge_slice(u64 o0, u64 s0, u64 s1, bool row_end
 // first (a dropped self-loop replaced by an inserted one).
 //
 // Rows longer than MERGE_LONG go to `long_rows` for k_merge_long.
-constexpr u64 MERGE_LONG = 2048;
+constexpr u64 MERGE_LONG = 512;
 
 __global__ void k_merge_rows(u32 n, const u64* off, const u32* col, const double* w,
                              const u64* noff, u32* ncol, double* nw, const u8* touched,
@@ -523,14 +528,15 @@ __global__ void k_merge_rows(u32 n, const u64* off, const u32* col, const double
 
 // Long touched rows: a block per row, its warps on consecutive slices of
 // whole chunks.  A warp rebuilds the state at its slice start from the
-// operations whose neighbour is not above the entry before the slice.
+// operations whose neighbour is not above the entry before the slice (a
+// bisection, and the delete prefix of the sorted operations).
 __global__ void __launch_bounds__(256) k_merge_long(const u32* long_rows, const u32* nlong,
                                                     const u64* off, const u32* col,
                                                     const double* w, const u64* noff, u32* ncol,
                                                     double* nw, const u64* rkeys,
                                                     const u32* rvals, const u32* rstart,
-                                                    const u32* rend, const double* neww,
-                                                    u64 nnz_new, u32* err) {
+                                                    const u32* rend, const u32* delpre,
+                                                    const double* neww, u64 nnz_new, u32* err) {
   const u32 lane = threadIdx.x & 31;
   const u32 wib = threadIdx.x >> 5;
   const u32 nw_ = blockDim.x >> 5;
@@ -545,7 +551,7 @@ __global__ void __launch_bounds__(256) k_merge_long(const u32* long_rows, const 
     const u32 a = rstart[r], b = rend[r];
     u32 p = a, drun = 0, irun = 0, del_key = NONE32, del_same = 0;
     if (s0 > o0) {
-      // operations consumed before the slice: neighbour <= col[s0 - 1]
+      // operations consumed before the slice: neighbour <= cprev = col[s0 - 1]
       const u32 cprev = col[s0 - 1];
       u32 lo = a, hi = b;
       while (lo < hi) {
@@ -554,22 +560,16 @@ __global__ void __launch_bounds__(256) k_merge_long(const u32* long_rows, const 
         else hi = mid;
       }
       p = lo;
-      // deletes among them, and the last one (warp-uniform)
-      u32 last_del = NONE32;
-      for (u32 x0 = a; x0 < p; x0 += 32) {
-        const bool d = x0 + lane < p && rvals[x0 + lane] == DEL_MARK;
-        const u32 m = __ballot_sync(0xffffffffu, d);
-        drun += __popc(m);
-        if (m) last_del = x0 + 31 - __clz(m);
-      }
+      drun = delpre[p] - delpre[a];
       irun = (p - a) - drun;
-      if (last_del != NONE32) {
-        // the deletes on that neighbour are consecutive and end at last_del
-        del_key = (u32)rkeys[last_del];
-        u32 x = last_del;
-        while (x > a && rvals[x - 1] == DEL_MARK && (u32)rkeys[x - 1] == del_key) --x;
-        del_same = last_del - x + 1;
-      }
+      // Only deletes on cprev itself matter from here on (a self-loop whose
+      // two copies the slice boundary separates): entries of this slice and
+      // the operations still to come are all >= cprev.
+      u32 x = p;
+      while (x > a && (u32)rkeys[x - 1] == cprev) --x;
+      for (; x < p; ++x)
+        if (rvals[x] == DEL_MARK) ++del_same;
+      if (del_same) del_key = cprev;
     }
     merge_slice(o0, s0, s1, c1 == chunks, noff[r], p, b, drun, irun, del_key, del_same, col, w,
                 ncol, nw, rkeys, rvals, neww, nnz_new, err);
@@ -807,7 +807,18 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
   S.delpre.ensure(E.mem, n ? n : 1);
   S.inspre.ensure(E.mem, n ? n : 1);
   ++E.nlaunch, k_row_ranges<<<grid_for(R), 256, 0, st>>>(S.rkeys2.p, R, S.delpre.p, S.inspre.p);
+  // deletes before every operation (for the long-row merge's slice starts)
+  S.opdel.ensure(E.mem, R + 1);
+  S.opdelpre.ensure(E.mem, R + 1);
+  ++E.nlaunch, k_del_flags<<<grid_for(R + 1), 256, 0, st>>>(S.rvals2.p, R, S.opdel.p);
   HL_LAUNCH_CHECK();
+  {
+    u32* a = S.opdel.p;
+    u32* o = S.opdelpre.p;
+    cub_run(E, [&](void* t, size_t& bytes) {
+      return cub::DeviceScan::ExclusiveSum(t, bytes, a, o, (int64_t)R + 1, st);
+    });
+  }
   S.ddeg.ensure(E.mem, n ? n : 1);
   S.touched.ensure(E.mem, n ? n : 1);
   HL_CUDA(cudaMemsetAsync(S.ddeg.p, 0, sizeof(int) * (n ? n : 1), st));
@@ -843,7 +854,7 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
         S.delpre.p, S.inspre.p, S.neww.p, nnz_new, S.cnt.p + 4, S.ovf.p, S.ovf_cnt.p);
     ++E.nlaunch, k_merge_long<<<148 * 2, 256, 0, st>>>(
         S.ovf.p, S.ovf_cnt.p, G.off.p, G.col.p, G.w.p, S.newoff.p, ncol.p, nw.p, S.rkeys2.p,
-        S.rvals2.p, S.delpre.p, S.inspre.p, S.neww.p, nnz_new, S.cnt.p + 4);
+        S.rvals2.p, S.delpre.p, S.inspre.p, S.opdelpre.p, S.neww.p, nnz_new, S.cnt.p + 4);
   }
   HL_LAUNCH_CHECK();
   E.kt_end(KT_MERGE_ROWS, kev);

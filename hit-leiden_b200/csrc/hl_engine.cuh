@@ -53,6 +53,7 @@ struct Scratch {
   DBuf<double> neww;
   DBuf<u32> nops_del, nops_ins, pos_del, pos_ins;
   DBuf<u32> delpre, inspre;  // per-row operation ranges (start, end) of apply_delta
+  DBuf<u32> opdel, opdelpre;  // apply_delta: delete flags of the sorted operations, their scan
   DBuf<int> ddeg;
   DBuf<u64> newoff;
   DBuf<u32> rowlist;

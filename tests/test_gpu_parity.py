@@ -78,17 +78,19 @@ def test_apply_delta_self_loop_across_chunks(before, keep_loops):
         assert gh.same_bits(go, ro) and gh.same_bits(gc, rc) and gh.same_bits(gw, rw)
 
 
-@pytest.mark.parametrize("before", [2558, 2559, 2560])
+@pytest.mark.parametrize("total,before", [(5120, 2558), (5120, 2559), (5120, 2560),
+                                          (600, 222), (600, 223), (600, 224)])
 @pytest.mark.parametrize("keep_loops", [False, True])
-def test_apply_delta_long_rows_split_across_warps(before, keep_loops):
-    # A row above 2048 entries is merged by a whole block, its warps on
-    # consecutive slices of 32-entry chunks.  With 2560 + 2560 neighbours
-    # and a self-loop the row has 161 chunks, so a slice starts at entry 2560:
-    # the loop's two copies sit just before, across, or just after it.
+def test_apply_delta_long_rows_split_across_warps(total, before, keep_loops):
+    # A row above 512 entries is merged by a whole block, its 8 warps on
+    # consecutive slices of 32-entry chunks.  With 5120 neighbours and a
+    # self-loop the row has 161 chunks and a slice starts at entry 2560; with
+    # 600 it has 19 chunks and a slice starts at entry 224.  The loop's two
+    # copies sit just before, across, or just after that boundary.
     rng = np.random.default_rng(before)
     n = 9000
     v = 4000
-    nb = list(range(before)) + list(range(v + 1, v + 1 + 5120 - before))
+    nb = list(range(before)) + list(range(v + 1, v + 1 + total - before))
     src = [v] * len(nb) + [v]
     dst = nb + [v]
     w = list(rng.uniform(0.5, 2.0, len(nb))) + [3.0]
@@ -98,8 +100,9 @@ def test_apply_delta_long_rows_split_across_warps(before, keep_loops):
     assert row[before] == v and row[before + 1] == v
     # deletes of existing row entries, inserts of new neighbours on both sides
     # of the loop, the loop itself deleted or reweighted
-    dels = rng.choice(len(nb), 400, replace=False)
-    new_nb = rng.choice(np.setdiff1d(np.arange(n), np.array(nb + [v])), 400, replace=False)
+    k = min(400, total // 4)
+    dels = rng.choice(len(nb), k, replace=False)
+    new_nb = rng.choice(np.setdiff1d(np.arange(n), np.array(nb + [v])), k, replace=False)
     for loop_w in (-3.0, 1.25):
         ds = [v] * (len(dels) + len(new_nb)) + [v]
         dd = [nb[i] for i in dels] + new_nb.tolist() + [v]
