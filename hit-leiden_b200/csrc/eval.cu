@@ -62,6 +62,7 @@ struct EvalArgs {
   u32* ovf_list;   // block kernel without global regions: rows deferred because
   u32* ovf_count;  // they passed BIG_TAB / 2 distinct keys (idx values)
   const u32* nidx_dev;  // if set, the number of idx entries is read here
+  u32* work;            // block kernel: next idx position to take (zeroed per launch)
 };
 
 constexpr u32 MID_MAX = 128;
@@ -500,7 +501,7 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
   __shared__ double r_g[BIG_WARPS];
   __shared__ u32 r_p[BIG_WARPS], r_k[BIG_WARPS];
   __shared__ double s_wcur;
-  __shared__ u32 s_used, s_gused;
+  __shared__ u32 s_used, s_gused, s_next;
   const u32 tid = threadIdx.x;
   const u32 lane = tid & 31;
   const u32 wib = tid >> 5;
@@ -511,7 +512,14 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
   double* g_tv = A.tval ? A.tval + (u64)blockIdx.x * A.region : nullptr;
   u32* g_list = A.tlist ? A.tlist + (u64)blockIdx.x * (A.region / 2) : nullptr;
   const u32 nidx = A.nidx_dev ? *A.nidx_dev : A.nidx;
-  for (u64 t = blockIdx.x; t < nidx; t += gridDim.x) {
+  // Vertices are taken from a shared counter (the list is ordered by degree,
+  // largest first), so the longest rows start first and no block queues
+  // several of them behind each other.
+  for (;;) {
+    if (tid == 0) s_next = atomicAdd(A.work, 1u);
+    __syncthreads();
+    const u32 t = s_next;
+    if (t >= nidx) break;
     const u32 i = A.idx[t];
     const u32 v = A.verts[i];
     const u64 o0 = A.off[v], o1 = A.off[v + 1];
@@ -764,6 +772,15 @@ __global__ void k_bin(const u32* verts, u32 nv, const u64* off, u32* bin, u32* i
   if (threadIdx.x < 6 && sc[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sc[threadIdx.x]);
 }
 
+// Sort keys that order vertices by degree, largest first.
+__global__ void k_degree_keys(const u32* verts, const u32* idx, u32 nb, const u64* off, u32* key) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < nb; t += (u64)gridDim.x * blockDim.x) {
+    const u32 v = verts[idx[t]];
+    const u64 deg = off[v + 1] - off[v];
+    key[t] = 0xFFFFFFFFu - (u32)(deg < 0xFFFFFFFFull ? deg : 0xFFFFFFFFull);
+  }
+}
+
 __global__ void k_big_caps2(const u32* verts, const u32* idx, u32 nb, const u64* off, u64* cap) {
   for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < nb; t += (u64)gridDim.x * blockDim.x) {
     u32 v = verts[idx[t]];
@@ -803,9 +820,11 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   S.cnt.ensure(E.mem, 16);
   u32* cnt = S.cnt.p + 2;  // six bin counters (cnt[2..7])
   HL_CUDA(cudaMemsetAsync(cnt, 0, 6 * sizeof(u32), st));
-  S.ovf_cnt.ensure(E.mem, 4);  // [0] deferred rows, [2..3] largest degree of the block bin
+  // [0] deferred rows, [2..3] largest degree of the block bin, [4..5] work
+  // counters of the block kernel's two passes
+  S.ovf_cnt.ensure(E.mem, 6);
   unsigned long long* maxdeg = reinterpret_cast<unsigned long long*>(S.ovf_cnt.p + 2);
-  HL_CUDA(cudaMemsetAsync(S.ovf_cnt.p, 0, 4 * sizeof(u32), st));
+  HL_CUDA(cudaMemsetAsync(S.ovf_cnt.p, 0, 6 * sizeof(u32), st));
   ++E.nlaunch, k_bin<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.used.p, S.order.p, cnt,
                                                     maxdeg);
   HL_LAUNCH_CHECK();
@@ -870,6 +889,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   A.ovf_list = nullptr;
   A.ovf_count = nullptr;
   A.nidx_dev = nullptr;
+  A.work = nullptr;
 
   cudaEvent_t ev = E.kt_begin();
   cudaEvent_t e_s = E.kt_begin();
@@ -936,8 +956,25 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
     // are deferred to an overflow list.
     EvalArgs a = A;
     a.counters = counters ? counters + 6 : nullptr;
-    a.idx = vo + start[5];
+    // the bin's list by degree, largest first
+    S.hubk.ensure(E.mem, c[5]);
+    S.hubk2.ensure(E.mem, c[5]);
+    S.hubv.ensure(E.mem, c[5]);
+    ++E.nlaunch, k_degree_keys<<<grid_for(c[5]), 256, 0, st>>>(verts, vo + start[5], c[5],
+                                                                L.g.off.p, S.hubk.p);
+    HL_LAUNCH_CHECK();
+    {
+      u32* ki = S.hubk.p;
+      u32* ko = S.hubk2.p;
+      const u32* vi = vo + start[5];
+      u32* vv = S.hubv.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vv, (int64_t)c[5], 0, 32, st);
+      });
+    }
+    a.idx = S.hubv.p;
     a.nidx = c[5];
+    a.work = S.ovf_cnt.p + 4;
     S.ovf.ensure(E.mem, c[5]);
     a.ovf_list = S.ovf.p;
     a.ovf_count = S.ovf_cnt.p;  // zeroed with the bin counters
@@ -979,6 +1016,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
       a2.tval = S.huge_val.p;
       a2.tlist = S.huge_list.p;
       a2.region = region;
+      a2.work = S.ovf_cnt.p + 5;
       if (kind == EVAL_MOVE)
         ++E.nlaunch, k_eval_big<EVAL_MOVE><<<pb, BIG_THREADS, big_smem(), st>>>(a2);
       else

@@ -90,6 +90,7 @@ struct Scratch {
   DBuf<u32> huge_key, huge_pos, huge_list;
   DBuf<u32> ovf, ovf_cnt;  // block kernel: rows deferred to the pass with global regions
   DBuf<u32> acc_cnt;       // inc-movement: accepted moves over all rounds
+  DBuf<u32> hubk, hubk2, hubv;  // block bin ordered by degree (keys, sorted keys, list)
   DBuf<double> huge_val;
 };
 
