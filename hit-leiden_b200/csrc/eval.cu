@@ -580,16 +580,18 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         nb2 = ok2 ? A.col[q] : 0u;
         w2 = ok2 ? A.w[q] : 0.0;
       }
-      // stable bucketing of the tile by key partition
+      // stable bucketing of the tile by key partition (ordered sums only)
       const u32 part = key == NONE32 ? NONE32 : hash32(key) >> (32 - BIG_PART_BITS);
       u32 rank = 0, mycnt = 0;
+      if (!A.concurrent) {
 #pragma unroll
-      for (u32 q = 0; q < BIG_WARPS; ++q) {
-        const u32 bq = __ballot_sync(0xffffffffu, part == q);
-        if (lane == q) mycnt = __popc(bq);
-        if (part == q) rank = __popc(bq & lt_mask);
+        for (u32 q = 0; q < BIG_WARPS; ++q) {
+          const u32 bq = __ballot_sync(0xffffffffu, part == q);
+          if (lane == q) mycnt = __popc(bq);
+          if (part == q) rank = __popc(bq & lt_mask);
+        }
+        if (lane < BIG_WARPS) s_cnt[lane * BIG_WARPS + wib] = mycnt;
       }
-      if (lane < BIG_WARPS) s_cnt[lane * BIG_WARPS + wib] = mycnt;
       __syncthreads();
       // The previous tile's folds are complete here and s_used is stable.  A
       // row with too many distinct keys moves its table to the block's global
@@ -615,6 +617,30 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         tp = g_tp;
         tv = g_tv;
         mask = gmask;
+      }
+      if (A.concurrent) {
+        // Integral weights: every order of additions gives the same sums, so
+        // each warp inserts its own lanes' entries right away, lanes sharing a
+        // key combined first; the first position is the smallest one.
+        const bool okk = key != NONE32;
+        const u32 grp = __match_any_sync(0xffffffffu, okk ? (unsigned long long)key
+                                                           : ((1ull << 32) | lane));
+        b_w[tid] = wv;
+        __syncwarp();
+        if (okk && lane == (u32)(__ffs(grp) - 1)) {
+          double gsum = 0.0;
+          for (u32 m = grp; m; m &= m - 1) gsum += b_w[(tid & ~31u) + __ffs(m) - 1];
+          bool fresh;
+          const u64 slot = claim_slot(tk, mask, key, fresh);
+          if (fresh) {
+            if (global) g_list[atomicAdd(&s_gused, 1u)] = (u32)slot;
+            else atomicAdd(&s_used, 1u);
+          }
+          atomicAdd(&tv[slot], gsum);
+          atomicMin(&tp[slot], pos);
+        }
+        __syncwarp();
+        continue;
       }
       if (wib == 0) {
         // exclusive scan of the 64 counts in (partition, warp) order
