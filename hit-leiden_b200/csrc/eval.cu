@@ -313,30 +313,41 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
 // ---------------------------------------------------------------------------
 // Wide degrees (MID_MAX < deg <= WIDE_MAX): a warp per vertex.  The warp
 // issues the loads of up to 8 chunks (256 entries) at once, then folds the
-// chunks in CSR order into a table kept in a per-warp global region (hot in
-// L2).  Every new key's slot is appended to a per-warp list, so the argmax
-// scan visits only used slots and resets them: the region is clean again for
-// the warp's next vertex without a clearing pass.
+// chunks in CSR order into its own shared-memory table (1024 slots: keys,
+// 16-bit first positions, sums).  Every new key's slot is appended to a
+// per-warp list, so the argmax scan visits only used slots and resets them:
+// the table is clean again for the warp's next vertex without a clearing pass.
 // ---------------------------------------------------------------------------
 constexpr u32 WIDE_MAX = 512;
-constexpr u32 WIDE_TAB = 2 * WIDE_MAX;  // entries of one warp's region
-constexpr u32 WIDE_WARPS = 8;
+constexpr u32 WIDE_TAB = 2 * WIDE_MAX;  // slots of one warp's table
+constexpr u32 WIDE_WARPS = 4;
 constexpr u32 WIDE_BATCH = 8;  // chunks loaded before folding
+
+struct WideSmem {
+  double tv[WIDE_WARPS][WIDE_TAB];
+  double sw[WIDE_WARPS][WIDE_BATCH * 32];
+  u32 tk[WIDE_WARPS][WIDE_TAB];
+  unsigned short tp[WIDE_WARPS][WIDE_TAB];
+  unsigned short list[WIDE_WARPS][WIDE_MAX];
+  u32 cnt[WIDE_WARPS];
+};
 
 template <int KIND>
 __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
-  __shared__ double s_w[WIDE_WARPS][WIDE_BATCH * 32];
-  __shared__ u32 s_cnt[WIDE_WARPS];
+  extern __shared__ __align__(16) unsigned char wide_raw[];
+  WideSmem& W = *reinterpret_cast<WideSmem*>(wide_raw);
   const u32 lane = threadIdx.x & 31;
   const u32 wib = threadIdx.x >> 5;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   unsigned long long trav = 0, ncand = 0;
-  u32* tk = A.tkey + warp * (u64)WIDE_TAB;
-  u32* tp = A.tpos + warp * (u64)WIDE_TAB;
-  double* tv = A.tval + warp * (u64)WIDE_TAB;
-  u32* list = A.tlist + warp * (u64)WIDE_MAX;
-  double* sw = s_w[wib];
+  u32* tk = W.tk[wib];
+  unsigned short* tp = W.tp[wib];
+  double* tv = W.tv[wib];
+  unsigned short* list = W.list[wib];
+  double* sw = W.sw[wib];
+  for (u32 x = lane; x < WIDE_TAB; x += 32) tk[x] = NONE32;
+  __syncwarp();
   for (u64 t = warp; t < A.nidx; t += nwarps) {
     const u32 i = A.idx[t];
     const u32 v = A.verts[i];
@@ -348,7 +359,7 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
     const double dcur = A.d[cur];
     if (lane == 0) {
       trav += deg;
-      s_cnt[wib] = 0;
+      W.cnt[wib] = 0;
     }
     u32 cap = 64;
     while (cap < 2 * deg) cap <<= 1;
@@ -385,14 +396,14 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
           for (u32 m = grp; m; m &= m - 1) acc = __dadd_rn(acc, sw[j * 32 + __ffs(m) - 1]);
           tv[slot] = acc;
           if (prev == NONE32) {
-            tp[slot] = (u32)(b0 + j * 32 + lane - o0);
-            list[atomicAdd(&s_cnt[wib], 1u)] = slot;
+            tp[slot] = (unsigned short)(b0 + j * 32 + lane - o0);
+            list[atomicAdd(&W.cnt[wib], 1u)] = (unsigned short)slot;
           }
         }
         __syncwarp();
       }
     }
-    const u32 used = s_cnt[wib];
+    const u32 used = W.cnt[wib];
     // w(v, cur), then the argmax over the used slots, resetting them.
     double wcur = 0.0;
     bool found = false;
@@ -828,7 +839,7 @@ static size_t big_smem() {
 
 static std::atomic<bool> g_big_attr_set[64];
 
-constexpr u32 WIDE_MAX_BLOCKS = 148u * 4u;
+constexpr u32 WIDE_MAX_BLOCKS = 148u * 3u;
 constexpr u32 BIG_MAX_BLOCKS = 148u * 3u;
 constexpr u32 OVF_BLOCKS = 32;  // least blocks (global regions) for rows deferred by pass 1
 constexpr u64 OVF_TABLE_BYTES = 4ull << 30;  // table bytes pass 2 may spread over its blocks
@@ -870,22 +881,17 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   u32 start[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int b = 0; b < 6; ++b) start[b + 1] = start[b] + c[b];
 
-  // Per-warp regions of the wide kernel, allocated once for its largest grid.
-  if (c[4] && S.wide_key.cap < (size_t)WIDE_MAX_BLOCKS * WIDE_WARPS * WIDE_TAB) {
-    const size_t need = (size_t)WIDE_MAX_BLOCKS * WIDE_WARPS * WIDE_TAB;
-    S.wide_key.ensure(E.mem, need);
-    S.wide_pos.ensure(E.mem, need);
-    S.wide_val.ensure(E.mem, need);
-    S.wide_list.ensure(E.mem, (size_t)WIDE_MAX_BLOCKS * WIDE_WARPS * WIDE_MAX);
-    ++E.nlaunch, k_fill_u32<<<grid_for(need), 256, 0, st>>>(S.wide_key.p, NONE32, S.wide_key.cap);
-    HL_LAUNCH_CHECK();
-  }
   int dev = E.device;
   if (dev >= 0 && dev < 64 && !g_big_attr_set[dev]) {
     HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)big_smem()));
     HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_REFINE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem()));
+    HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(WideSmem)));
+    HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_REFINE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(WideSmem)));
     g_big_attr_set[dev] = true;
   }
 
@@ -963,16 +969,12 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
     a.counters = counters ? counters + 4 : nullptr;
     a.idx = vo + start[4];
     a.nidx = c[4];
-    a.tkey = S.wide_key.p;
-    a.tpos = S.wide_pos.p;
-    a.tval = S.wide_val.p;
-    a.tlist = S.wide_list.p;
     u32 blocks = grid_for((u64)c[4] * 32, WIDE_WARPS * 32);
     if (blocks > WIDE_MAX_BLOCKS) blocks = WIDE_MAX_BLOCKS;
     if (kind == EVAL_MOVE)
-      ++E.nlaunch, k_eval_wide<EVAL_MOVE><<<blocks, WIDE_WARPS * 32, 0, st>>>(a);
+      ++E.nlaunch, k_eval_wide<EVAL_MOVE><<<blocks, WIDE_WARPS * 32, sizeof(WideSmem), st>>>(a);
     else
-      ++E.nlaunch, k_eval_wide<EVAL_REFINE><<<blocks, WIDE_WARPS * 32, 0, st>>>(a);
+      ++E.nlaunch, k_eval_wide<EVAL_REFINE><<<blocks, WIDE_WARPS * 32, sizeof(WideSmem), st>>>(a);
     HL_LAUNCH_CHECK();
   }
   E.kt_end(KT_EVAL_BIG, e_b);

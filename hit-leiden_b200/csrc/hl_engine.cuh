@@ -83,10 +83,8 @@ struct Scratch {
   DBuf<double> red, red2;
   DBuf<u64> red64;
   DBuf<u32> origin;
-  // per-warp hash regions of the wide evaluation kernel (kept clean by it)
-  DBuf<u32> wide_key, wide_pos, wide_list;
-  DBuf<double> wide_val;
-  // global tables of the block-per-vertex kernel (degrees above 4096)
+  // global tables of the block-per-vertex kernel's second pass (rows with
+  // more than 2048 distinct keys)
   DBuf<u32> huge_key, huge_pos, huge_list;
   DBuf<u32> ovf, ovf_cnt;  // block kernel: rows deferred to the pass with global regions
   DBuf<u32> acc_cnt;       // inc-movement: accepted moves over all rounds
