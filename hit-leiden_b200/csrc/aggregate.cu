@@ -166,7 +166,8 @@ __global__ void k_set_spre(u32 n, const u8* refined, const u32* s_cur, u32* s_pr
 
 // Sort (key, seq) records, sum each key in push order, drop |w| <= threshold.
 // Output edges land in sc.eu2 / ev2 / ew2 in ascending key order.
-static u64 compress_records(Engine& E, u64 R, double threshold) {
+// Keys are pair_key(a, b) of ids below id_bound.
+static u64 compress_records(Engine& E, u64 R, double threshold, u32 id_bound) {
   Scratch& S = E.sc;
   cudaStream_t st = E.stream;
   if (!R) return 0;
@@ -175,7 +176,8 @@ static u64 compress_records(Engine& E, u64 R, double threshold) {
   u32* vi = S.idx.p;
   u32* vo = S.idx2.p;
   cub_run(E, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)R, 0, 64, st);
+    return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)R, 0,
+                                           32 + bits_for(id_bound ? id_bound - 1 : 0), st);
   });
   S.rowlist.ensure(E.mem, R);
   S.segid.ensure(E.mem, R);
@@ -275,7 +277,7 @@ u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n, boo
         edge_weight_loops, nullptr, pos, delta.k, S.keys.p, S.neww.p, S.idx.p);
     HL_LAUNCH_CHECK();
   }
-  u64 out = compress_records(E, R, 1e-9);
+  u64 out = compress_records(E, R, 1e-9, *next_n);
   ++E.nlaunch, k_set_spre<<<grid_for(n), 256, 0, st>>>(n, S.refined.p, L.s_cur.p, L.s_pre.p);
   HL_LAUNCH_CHECK();
   E.kt_end(KT_AGGREGATE, kev);
@@ -341,7 +343,7 @@ u64 aggregate_full(Engine& E, Level& L, const u32* s, u32*, u32*, double*) {
   ++E.nlaunch, k_full_emit<<<grid_for(n), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, L.g.w.p, s, pos, S.keys.p,
                                            S.neww.p, S.idx.p);
   HL_LAUNCH_CHECK();
-  return compress_records(E, R, -1.0);
+  return compress_records(E, R, -1.0, n);
 }
 
 // f^{p+1}(s^p(v)) := f^p(v); with several members the largest v writes last,

@@ -714,7 +714,9 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
     u32* vin = S.idx.p;
     u32* vout = S.idx2.p;
     cub_run(E, [&](void* t, size_t& bytes) {
-      return cub::DeviceRadixSort::SortPairs(t, bytes, kin, kout, vin, vout, (int64_t)k, 0, 64, st);
+      // keys (u << 32) | v with u, v < n
+      return cub::DeviceRadixSort::SortPairs(t, bytes, kin, kout, vin, vout, (int64_t)k, 0,
+                                             32 + bits_for(n ? n - 1 : 0), st);
     });
     ++E.nlaunch, k_heads<<<grid_for(k), 256, 0, st>>>(kout, k, S.rowlist.p);
     HL_LAUNCH_CHECK();
@@ -799,7 +801,9 @@ void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_lo
     u32* vin = S.rvals.p;
     u32* vout = S.rvals2.p;
     cub_run(E, [&](void* t, size_t& bytes) {
-      return cub::DeviceRadixSort::SortPairs(t, bytes, kin, kout, vin, vout, (int64_t)R, 0, 64, st);
+      // keys (row << 32) | neighbour with both < n
+      return cub::DeviceRadixSort::SortPairs(t, bytes, kin, kout, vin, vout, (int64_t)R, 0,
+                                             32 + bits_for(n ? n - 1 : 0), st);
     });
   }
   require(R < 0xFFFFFFFFull, "too many row operations in one batch");

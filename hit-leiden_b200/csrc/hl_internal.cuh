@@ -146,6 +146,14 @@ struct HostScalars {
 
 inline u32 div_up(u64 a, u64 b) { return (u32)((a + b - 1) / b); }
 
+// Bits that hold every value in [0, maxval] (at least 1): radix sorts of keys
+// with a known bound sort only those bits.
+inline int bits_for(u64 maxval) {
+  int b = 1;
+  while (b < 64 && (maxval >> b) != 0) ++b;
+  return b;
+}
+
 // ---------------------------------------------------------------------------
 // FP64 arithmetic that rounds exactly like the reference's Rust expressions.
 // The library is compiled with -fmad=false; the explicit _rn intrinsics make

@@ -145,7 +145,8 @@ static void recompute_comm_degrees_impl(Engine& E, Level& L, const u32* part, u3
   u32* vin = S.order.p;
   u32* vout = S.order2.p;
   cub_run(E, [&](void* t, size_t& b) {
-    return cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int64_t)n, 0, 32, st);
+    return cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int64_t)n, 0,
+                                           bits_for(ncomm_cap ? ncomm_cap - 1 : 0), st);
   });
   ++E.nlaunch, k_heads_u32<<<grid_for(n), 256, 0, st>>>(kout, n, S.cand_node.p);
   HL_LAUNCH_CHECK();

@@ -575,7 +575,8 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
       u32* vi = S.order.p;
       u32* vo = S.order2.p;
       cub_run(E, [&](void* t, size_t& b) {
-        return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)nm, 0, 32, st);
+        return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)nm, 0,
+                                               bits_for(s2cap), st);
       });
       ++E.nlaunch, k_heads_u32b<<<grid_for(nm), 256, 0, st>>>(ko, nm, S.sel_node.p);
       HL_LAUNCH_CHECK();
