@@ -70,7 +70,7 @@ struct Scratch {
   DBuf<double> d;       // community degrees (2n)
   DBuf<u32> used, rank;
   // refinement
-  DBuf<u32> par, csize, ncomp, newid, minmem;
+  DBuf<u32> par, uroot, csize, ncomp, newid, minmem;
   DBuf<u64> keep;
   DBuf<u8> affsc, cand_sc, blocked;
   DBuf<u32> sizes;

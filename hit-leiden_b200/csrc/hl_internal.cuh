@@ -206,11 +206,13 @@ __device__ __forceinline__ double warp_ordered_sum(u64 a, u64 b, double acc, V v
     const double xn = okn ? val(tn) : 0.0;
     u32 m = __ballot_sync(0xffffffffu, ok);
     if (__popc(m) > 8) {
+      // all 32 values first (independent shuffles), then the dependent chain
+      double y[32];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const double y = __shfl_sync(0xffffffffu, x, j);
-        if ((m >> j) & 1u) acc = __dadd_rn(acc, y);
-      }
+      for (int j = 0; j < 32; ++j) y[j] = __shfl_sync(0xffffffffu, x, j);
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if ((m >> j) & 1u) acc = __dadd_rn(acc, y[j]);
     } else {
       while (m) {
         int j = __ffs(m) - 1;

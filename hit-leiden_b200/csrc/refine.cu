@@ -84,11 +84,16 @@ __global__ void k_uf_edges(u32 n, const u64* off, const u32* col, const u32* s, 
   }
 }
 
-__global__ void k_uf_final(u32 n, const u32* s, const u8* affsc, u32* par, u32* csize) {
+// Every union is done: the forest no longer changes, so each vertex finds its
+// root read-only (no path compression, which would race with the other
+// threads' walks) and writes it to `root`.
+__global__ void k_uf_final(u32 n, const u32* s, const u8* affsc, const u32* par, u32* root,
+                           u32* csize) {
   for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x) {
     if (!affsc[s[v]]) continue;
-    u32 r = uf_find(par, (u32)v);
-    par[v] = r;
+    u32 r = (u32)v;
+    while (par[r] != r) r = par[r];
+    root[v] = r;
     atomicAdd(&csize[r], 1u);
   }
 }
@@ -440,15 +445,17 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   HL_CUDA(cudaMemsetAsync(S.csize.p, 0, sizeof(u32) * n, st));
   ++E.nlaunch, k_uf_edges<<<grid_for((u64)n * 32), 256, 0, st>>>(n, L.g.off.p, L.g.col.p, s, L.f.p, S.affsc.p,
                                                      cc_same_community, S.par.p);
-  ++E.nlaunch, k_uf_final<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.csize.p);
+  S.uroot.ensure(E.mem, n);
+  ++E.nlaunch, k_uf_final<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.uroot.p,
+                                                        S.csize.p);
   S.keep.ensure(E.mem, scap);
   HL_CUDA(cudaMemsetAsync(S.keep.p, 0, sizeof(u64) * scap, st));
-  ++E.nlaunch, k_keep<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.csize.p,
+  ++E.nlaunch, k_keep<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.uroot.p, S.csize.p,
                                       (unsigned long long*)S.keep.p);
   S.status.ensure(E.mem, n);
   S.gkey.ensure(E.mem, n);
   S.gkey2.ensure(E.mem, n);
-  ++E.nlaunch, k_split_roots<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p,
+  ++E.nlaunch, k_split_roots<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.uroot.p,
                                               (const unsigned long long*)S.keep.p, S.status.p,
                                               S.gkey.p);
   HL_LAUNCH_CHECK();
@@ -469,7 +476,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
     });
     ++E.nlaunch, k_assign_newid<<<grid_for(m_new), 256, 0, st>>>(ko, m_new, smax + 1, S.newid.p, S.used.p,
                                                      S.rank.p);
-    ++E.nlaunch, k_apply_split<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.par.p, S.status.p, S.newid.p,
+    ++E.nlaunch, k_apply_split<<<grid_for(n), 256, 0, st>>>(n, s, S.affsc.p, S.uroot.p, S.status.p, S.newid.p,
                                                S.refined.p);
     HL_LAUNCH_CHECK();
     std::vector<u32> a(m_new), b(m_new);
