@@ -1,0 +1,52 @@
+"""Quality of the incremental result, in the terms of the reference's own
+benchmark report (hit_leiden_incremental.rs:513-665): after the updates, the
+GPU state's level-0 partition is compared with a from-scratch multilevel Leiden
+run on the final graph (the oracle's seeded restatement of run(),
+hit_leiden.rs:30-118) by modularity, NMI, purities and largest-community
+Jaccard, and with the throughput-mode bootstrap of the final graph by
+modularity.  These are quality bounds, not parity: the incremental update and
+a fresh run are different algorithms."""
+import importlib
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+hl = importlib.import_module("hit-leiden_b200")
+W = importlib.import_module("hit-leiden_b200.workloads")
+IO = importlib.import_module("hit-leiden_b200.io")
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_incremental_quality_close_to_fresh_run(seed):
+    n, s, d, w = W.config1(seed)
+    st = hl.PartitionState.load(hl.GraphInput.from_arrays("c1", n, s, d, w), hl.RunConfig())
+    ex = set(zip(s.tolist(), d.tolist()))
+    us, vs = [s], [d]
+    for b in range(5):
+        u, v, ww = W.uniform_inserts(n, 1000, 100 * seed + b, ex)
+        st.apply_batch(u, v, ww)
+        ex.update(zip(u.tolist(), v.tolist()))
+        us.append(u)
+        vs.append(v)
+    q_inc = st.modularity()
+    part_inc = st.partition()
+    fs, fd = np.concatenate(us), np.concatenate(vs)
+    # a sequential from-scratch run (the reference's run()) ...
+    part_fresh, q_fresh, _ = O.run(n, fs, fd, None, 1.0, 10, 42 + seed)
+    # ... and the throughput-mode bootstrap of the same final graph
+    boot = O.State(n, mode=O.MODE_THROUGHPUT)
+    boot.bootstrap(fs, fd, np.ones(len(fs)), max_levels=10)
+    q_boot = boot.modularity(0)
+    rep = IO.compare_partitions(part_inc, part_fresh)
+    # Measured on these seeds: incremental 0.67-0.70, fresh bootstrap
+    # 0.64-0.66, sequential run 0.75; NMI to the run 0.80-0.82 (the reference
+    # reports NMI 0.77 between its run() and a fresh igraph Leiden).
+    assert q_inc >= q_boot - 0.01, (q_inc, q_boot)
+    assert q_fresh - q_inc <= 0.1, (q_inc, q_fresh)
+    assert rep.nmi >= 0.7, rep
+    assert rep.largest_jaccard >= 0.5, rep
+    st.close()
