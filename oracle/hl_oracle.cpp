@@ -44,11 +44,56 @@
 #include <unordered_set>
 #include <vector>
 
+#include <atomic>
+#include <thread>
+
 extern "C" {
 #include "hl_oracle.h"
 }
 
 namespace ora {
+
+// ---------------------------------------------------------------------------
+// Host threads for the throughput mode's snapshot evaluations (the reference
+// runs them on rayon's pool).  Work is taken in chunks from a shared counter;
+// each worker builds its own scratch.  Results are written by index, so they do
+// not depend on the number of threads.
+// ---------------------------------------------------------------------------
+static std::atomic<int> g_threads{0};  // 0 = hardware concurrency, at most 64
+
+static int num_threads() {
+  int t = g_threads.load();
+  if (t <= 0) {
+    t = (int)std::thread::hardware_concurrency();
+    if (t <= 0) t = 1;
+    if (t > 64) t = 64;
+  }
+  return t;
+}
+
+template <typename MakeScratch, typename Body>
+static void parallel_for(size_t count, MakeScratch make, Body body) {
+  const int nt = (int)std::min<size_t>((size_t)num_threads(), (count + 255) / 256);
+  if (nt <= 1) {
+    auto sc = make();
+    for (size_t i = 0; i < count; ++i) body(i, sc);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    auto sc = make();
+    for (;;) {
+      const size_t a = next.fetch_add(256);
+      if (a >= count) break;
+      const size_t b = std::min(count, a + 256);
+      for (size_t i = a; i < b; ++i) body(i, sc);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+  worker();
+  for (std::thread& th : pool) th.join();
+}
 
 using u32 = uint32_t;
 using u64 = uint64_t;
@@ -433,26 +478,39 @@ static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std:
   }
 
   if (mode == OR_MODE_THROUGHPUT) {
-    MoveScratch sc;
-    sc.buf.assign(d.size() + n + 1, 0.0);
     std::vector<u32> act;
     for (u32 i = 0; i < n; ++i)
       if (active[i]) act.push_back(i);
     u32 it = 0;
+    std::vector<Eval> ev;
     while (!act.empty() && it < max_rounds) {
+      // Every active vertex is evaluated on the same snapshot (the reference
+      // runs these with rayon, throughput.rs:80-202), so the evaluations run
+      // in parallel; candidates are then taken in list order.
+      ev.assign(act.size(), Eval{0, 0.0});
+      const size_t bufsize = d.size() + n + 1;
+      parallel_for(
+          act.size(),
+          [&]() {
+            MoveScratch tsc;
+            tsc.buf.assign(bufsize, 0.0);
+            return tsc;
+          },
+          [&](size_t i, MoveScratch& tsc) {
+            ev[i] = eval_move(g, act[i], f, d, k, tw, gamma, true, tsc);
+          });
       std::vector<Move> cand;
-      for (u32 v : act) {
+      for (size_t i = 0; i < act.size(); ++i) {
+        const u32 v = act[i];
         out.traversed += g.deg(v);
-        Eval e = eval_move(g, v, f, d, k, tw, gamma, true, sc);
-        if (e.gain <= 0.0) continue;
-        cand.push_back({v, f[v], e.to, k[v], e.gain});
+        if (ev[i].gain <= 0.0) continue;
+        cand.push_back({v, f[v], ev[i].to, k[v], ev[i].gain});
       }
       out.rounds_candidates += cand.size();
       std::vector<Move> sel = select_decoupled(cand);
       size_t need = 0;
       for (const Move& m : sel) need = std::max(need, (size_t)m.to + 1);
       if (need > d.size()) d.resize(need, 0.0);
-      if (sc.buf.size() < d.size()) sc.buf.resize(d.size(), 0.0);
       double total = 0.0;
       for (const Move& m : sel) total += m.gain;
       std::vector<uint8_t> next(n, 0);
@@ -812,13 +870,33 @@ static RefineOut inc_refinement(const Graph& g, const std::vector<u32>& f, std::
 
   if (mode == OR_MODE_THROUGHPUT) {
     std::vector<uint8_t> blocked = compute_blocked(g, f, s, dS, rs, sizes, k, tw, gamma, faithful);
+    // Jacobi on the snapshot (throughput.rs:239-288): evaluated in parallel,
+    // applied in list order.
+    std::vector<RefMove> mv(rs.size());
+    std::vector<uint8_t> has(rs.size(), 0);
+    struct RefScratch {
+      std::vector<double> buf;
+      std::vector<uint8_t> seen;
+      std::vector<u32> order;
+    };
+    parallel_for(
+        rs.size(),
+        [&]() {
+          RefScratch t;
+          t.buf.assign(dS.size(), 0.0);
+          t.seen.assign(dS.size(), 0);
+          return t;
+        },
+        [&](size_t i, RefScratch& t) {
+          const u32 v = rs[i];
+          if (sizes[s[v]] != 1) return;
+          if (try_refinement_move(g, v, f, s, dS, k, tw, gamma, blocked, t.buf, t.seen, t.order,
+                                  mv[i]))
+            has[i] = 1;
+        });
     std::vector<RefMove> upd;
-    for (u32 v : rs) {
-      if (sizes[s[v]] != 1) continue;
-      RefMove m;
-      if (try_refinement_move(g, v, f, s, dS, k, tw, gamma, blocked, buf, seen, order, m))
-        upd.push_back(m);
-    }
+    for (size_t i = 0; i < rs.size(); ++i)
+      if (has[i]) upd.push_back(mv[i]);
     for (const RefMove& m : upd) {
       s[m.node] = m.to;
       dS[m.from] -= m.kdeg;
@@ -1633,6 +1711,10 @@ void or_canonicalize(uint32_t* c, uint64_t n) {
   canonicalize(v);
   std::memcpy(c, v.data(), sizeof(u32) * n);
 }
+
+int or_num_threads(void) { return ora::num_threads(); }
+
+void or_set_num_threads(int t) { ora::g_threads.store(t > 0 ? t : 0); }
 
 uint64_t or_select_decoupled(const uint32_t* node, const uint32_t* from, const uint32_t* to,
                              const double* kdeg, const double* gain, uint64_t m,

@@ -92,4 +92,9 @@ double or_run(uint32_t n, const uint32_t* src, const uint32_t* dst, const double
               double gamma, uint32_t max_levels, uint64_t seed, uint32_t* out_part,
               uint32_t* out_levels);
 
+/* Host threads the throughput-mode snapshot evaluations use (default: the
+ * hardware concurrency, at most 64; 0 restores the default). */
+int or_num_threads(void);
+void or_set_num_threads(int threads);
+
 #endif

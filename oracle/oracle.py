@@ -122,8 +122,22 @@ def load():
         lib.or_run.restype = C.c_double
         lib.or_run.argtypes = [C.c_uint32, u32p, u32p, vp, C.c_uint64, C.c_double, C.c_uint32,
                                C.c_uint64, u32p, C.POINTER(C.c_uint32)]
+        lib.or_num_threads.restype = C.c_int
+        lib.or_num_threads.argtypes = []
+        lib.or_set_num_threads.restype = None
+        lib.or_set_num_threads.argtypes = [C.c_int]
         _lib = lib
         return lib
+
+
+def num_threads():
+    """Host threads of the throughput mode's snapshot evaluations."""
+    return int(load().or_num_threads())
+
+
+def set_num_threads(threads):
+    """Set them (0 = hardware concurrency, at most 64)."""
+    load().or_set_num_threads(int(threads))
 
 
 def _edges(src, dst, w):

@@ -422,3 +422,28 @@ def test_move_eval_first_encountered_wins_ties():
 def test_tree_sum_is_exact_for_integers():
     x = np.arange(5000, dtype=np.float64)
     assert O.tree_sum(x) == float(x.sum())
+
+
+def test_results_do_not_depend_on_host_threads():
+    # The throughput mode's snapshot evaluations run on host threads; the
+    # state after a bootstrap and batches must not depend on how many.
+    import importlib
+    W = importlib.import_module("hit-leiden_b200.workloads")
+    n, s, d, w, _ = W.planted(3000, 8.0, 0.25, 9, comm_min=5, comm_max=80, weights=(0.5, 2.0))
+    states = []
+    for threads in (1, 8):
+        O.set_num_threads(threads)
+        st = O.State(n, mode=O.MODE_THROUGHPUT)
+        st.bootstrap(s, d, w, max_levels=6)
+        store = W.EdgeStore(n, s, d, w)
+        for b in range(3):
+            u, v, ww = W.mixed_batch(store, 300, 0.9, 50 + b, weights=(0.5, 2.0))
+            store.apply(u, v, ww)
+            st.hit_leiden(u, v, ww)
+        states.append(st)
+    O.set_num_threads(0)
+    a, b = states
+    assert a.levels == b.levels
+    for p in range(a.levels):
+        for which in (O.MAP_F, O.MAP_G, O.MAP_S_PRE, O.MAP_S_CUR):
+            assert np.array_equal(a.get_map(p, which), b.get_map(p, which))
