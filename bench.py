@@ -15,9 +15,10 @@ datasets are not available.
 Reported:
   value   edge-updates/s with batches already on the device (hl_apply_batch_device),
           timed by CUDA events on the library's stream, summed over the K steps;
-  e2e     edge-updates/s through the public host API (hl_apply_batch with host
-          arrays, host→device copies inside) plus a device→host read of the
-          level-0 community map every step, timed on the host clock;
+  e2e     edge-updates/s through the public host API (hl_apply_batch with
+          batches in pinned host memory, host→device copies inside) plus a
+          device→host read of the level-0 community map into pinned memory
+          every step, timed on the host clock;
   roofline for the inc-movement evaluation kernel (algorithmic bytes / event time);
   cpu_baseline: the CPU oracle (a C++ port of the reference's Rust, its
           snapshot evaluations on all host threads as the reference's rayon
@@ -675,15 +676,22 @@ def main():
                                       "bytes": kst[i].bytes, "items": kst[i].items}
                for i in range(cnt.value)}
 
-    # end to end through the host API
+    # end to end through the host API: each batch is copied in from pinned host
+    # memory and the level-0 community map read back into pinned host memory
     e2e_s = []
-    comm = np.zeros(n, np.uint32)
+    pinned = [(torch.from_numpy(u.view(np.int32)).pin_memory(),
+               torch.from_numpy(v.view(np.int32)).pin_memory(),
+               torch.from_numpy(ww).pin_memory()) for (u, v, ww) in batches[Wm + K:Wm + 2 * K]]
+    comm = torch.empty(n, dtype=torch.int32).pin_memory()
+    e2e_stats = L.BatchStats()
     barrier()
     torch.cuda.synchronize()
-    for (u, v, ww) in batches[Wm + K:Wm + 2 * K]:
+    for (pu, pv, pw) in pinned:
         t1 = time.perf_counter()
-        st.apply_batch(u, v, ww)
-        L.check(L.lib.hl_get_map(h, 0, L.HL_MAP_COMMUNITY, L.ptr(comm)))
+        L.check(L.lib.hl_apply_batch(h, C.c_void_p(pu.data_ptr()), C.c_void_p(pv.data_ptr()),
+                                     C.c_void_p(pw.data_ptr()), pu.numel(),
+                                     C.byref(e2e_stats)))
+        L.check(L.lib.hl_get_map(h, 0, L.HL_MAP_COMMUNITY, C.c_void_p(comm.data_ptr())))
         e2e_s.append(time.perf_counter() - t1)
     torch.cuda.synchronize()
     barrier()
