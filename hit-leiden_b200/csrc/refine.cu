@@ -496,18 +496,13 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   ++E.nlaunch, k_refine_all_if_identity<<<grid_for(n), 256, 0, st>>>(n, cnt + 5, S.refined.p);
   HL_LAUNCH_CHECK();
 
-  // ---- 2. sizes, d_S, d_C -----------------------------------------------
+  // ---- 2. sub-community sizes ------------------------------------------------
   u32 smax2 = m_new ? smax + m_new : smax;
   const size_t s2cap = (size_t)smax2 + 1;
   S.sizes.ensure(E.mem, s2cap);
   HL_CUDA(cudaMemsetAsync(S.sizes.p, 0, sizeof(u32) * s2cap, st));
   ++E.nlaunch, k_sizes<<<grid_for(n), 256, 0, st>>>(n, s, S.sizes.p);
   HL_LAUNCH_CHECK();
-  S.dS.ensure(E.mem, s2cap);
-  recompute_comm_degrees(E, L, s, (u32)s2cap, S.dS.p);
-  const size_t fcap = 2 * (size_t)n + 2;
-  S.dcomm.ensure(E.mem, fcap);
-  recompute_comm_degrees(E, L, L.f.p, (u32)fcap, S.dcomm.p);
 
   // ---- 3. refined singletons ---------------------------------------------
   u32 nr = select_flagged(E, S.refined.p, n, S.act.p, cnt + 6);
@@ -527,6 +522,12 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   }
   if (!ns) return out;
   u32* single = S.cand_idx.p;
+  // d_S and d_C serve only the T-filter and the singleton merges below
+  S.dS.ensure(E.mem, s2cap);
+  recompute_comm_degrees(E, L, s, (u32)s2cap, S.dS.p);
+  const size_t fcap = 2 * (size_t)n + 2;
+  S.dcomm.ensure(E.mem, fcap);
+  recompute_comm_degrees(E, L, L.f.p, (u32)fcap, S.dcomm.p);
 
   // ---- 4. T-filter --------------------------------------------------------
   cudaEvent_t ev_tf = E.kt_begin();
