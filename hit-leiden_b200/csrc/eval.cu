@@ -17,9 +17,10 @@
 //   larger              a block per vertex: 256-entry adjacency tiles bucketed
 //                       by a hash partition of their keys, one partition per
 //                       warp, each warp folding its own keys in CSR order into
-//                       a shared table of 4096 slots (a global one only for
-//                       rows with more than 2048 distinct keys), so every
-//                       key's sum keeps the reference's rounding.
+//                       a shared table of 4096 slots (a second pass with
+//                       global tables takes rows with more than 2048 distinct
+//                       keys), so every key's sum keeps the reference's
+//                       rounding.
 #include <cstring>
 
 #include "hl_engine.cuh"
@@ -52,7 +53,6 @@ struct EvalArgs {
   bool concurrent;  // integral weights: order-free accumulation allowed
   u32* out_to;
   double* out_gain;
-  const u64* tab_off;  // global table offset per idx position (big vertices)
   u32* tkey;
   u32* tpos;
   double* tval;
@@ -463,11 +463,16 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
 // key is touched by two warps: every key's sum is extended in the reference's
 // order and rounding with no atomics on values.  Inside a warp the lanes that
 // share a key are grouped with match_any; all group leaders fold their groups
-// at once in one unrolled pass over the chunk.
+// at once in one unrolled pass over the chunk.  With integral weights (sums
+// exact in any order) there is no bucketing: each warp inserts its lanes'
+// entries with atomics, one barrier per tile.
 //
-// The table lives in shared memory (BIG_TAB slots).  Hubs have long rows but
-// few distinct neighbour keys, so a row only moves its table to the block's
-// global region when it passes BIG_TAB / 2 distinct keys.
+// The bin is ordered by degree and vertices are handed out largest first
+// through a work counter.  The table lives in shared memory (BIG_TAB slots):
+// hubs have long rows but few distinct neighbour keys.  A launch without
+// global regions (pass 1) defers a row that passes BIG_TAB / 2 distinct keys
+// to an overflow list; pass 2 takes those rows on blocks that own global
+// regions, moving a row's table there when it passes the same bound.
 // ---------------------------------------------------------------------------
 constexpr u32 BIG_TAB = 4096;
 constexpr u32 BIG_WARPS = BIG_THREADS / 32;
@@ -818,16 +823,6 @@ __global__ void k_degree_keys(const u32* verts, const u32* idx, u32 nb, const u6
   }
 }
 
-__global__ void k_big_caps2(const u32* verts, const u32* idx, u32 nb, const u64* off, u64* cap) {
-  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < nb; t += (u64)gridDim.x * blockDim.x) {
-    u32 v = verts[idx[t]];
-    u64 deg = off[v + 1] - off[v];
-    u64 c = 64;
-    while (c < 2 * deg) c <<= 1;
-    cap[t] = c > BIG_TAB ? c : 0;
-  }
-}
-
 __global__ void k_fill_u32(u32* p, u32 v, u64 n) {
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
     p[i] = v;
@@ -912,7 +907,6 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   A.concurrent = E.integral;
   A.out_to = out_to;
   A.out_gain = out_gain;
-  A.tab_off = nullptr;
   A.tkey = nullptr;
   A.tpos = nullptr;
   A.tval = nullptr;
