@@ -133,15 +133,32 @@ __global__ void k_seg_start64(const u32* head, const u32* segid, u64 n, u32* sta
     if (head[i]) start[segid[i]] = (u32)i;
 }
 
-// In-order segmented sum; keep |w| > threshold.
+// One compressed record: the key of segment j (starting at a), its sum x.
+__device__ __forceinline__ void compress_out(u64 j, u64 a, double x, const u64* sk,
+                                             double threshold, u32* ou, u32* ov, double* ow,
+                                             u8* keepf) {
+  if ((threadIdx.x & 31) == 0) {
+    u64 key = sk[a];
+    ou[j] = (u32)(key >> 32);
+    ov[j] = (u32)key;
+    ow[j] = x;
+    keepf[j] = fabs(x) > threshold ? 1 : 0;
+  }
+}
+
+// In-order segmented sum; keep |w| > threshold.  Segments of RUN_FOLD_MIN or
+// more terms are listed for k_compress_runs.
 __global__ void k_compress(u32 U, const u32* start, u64 total, const u64* sk, const u32* sseq,
                            const double* vals, double threshold, u32* ou, u32* ov, double* ow,
-                           u8* keepf) {
-  const u32 lane = threadIdx.x & 31;
+                           u8* keepf, u32* longl, u32* longn) {
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 j = warp; j < U; j += nwarps) {
     u64 a = start[j], b = (j + 1 < U) ? start[j + 1] : total;
+    if (b - a >= RUN_FOLD_MIN) {
+      fold_defer(longl, longn, (u32)j);
+      continue;
+    }
     double x = 0.0;
     if (b - a == 1) {
       x = vals[sseq[a]];
@@ -149,13 +166,22 @@ __global__ void k_compress(u32 U, const u32* start, u64 total, const u64* sk, co
       x = warp_ordered_sum(a, b, 0.0, [&](u64 t) { return vals[sseq[t]]; },
                            [](u64) { return true; });
     }
-    if (lane == 0) {
-      u64 key = sk[a];
-      ou[j] = (u32)(key >> 32);
-      ov[j] = (u32)key;
-      ow[j] = x;
-      keepf[j] = fabs(x) > threshold ? 1 : 0;
-    }
+    compress_out(j, a, x, sk, threshold, ou, ov, ow, keepf);
+  }
+}
+
+// The long segments listed by k_compress, folded in runs (the same bits).
+__global__ void k_compress_runs(const u32* longl, const u32* longn, u32 U, const u32* start,
+                                u64 total, const u64* sk, const u32* sseq, const double* vals,
+                                double threshold, u32* ou, u32* ov, double* ow, u8* keepf) {
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  const u32 nl = *longn;
+  for (u64 i = warp; i < nl; i += nwarps) {
+    const u32 j = longl[i];
+    u64 a = start[j], b = (j + 1 < U) ? start[j + 1] : total;
+    double x = warp_fold_runs(a, b, 0.0, [&](u64 t) { return vals[sseq[t]]; });
+    compress_out(j, a, x, sk, threshold, ou, ov, ow, keepf);
   }
 }
 
@@ -197,8 +223,13 @@ static u64 compress_records(Engine& E, u64 R, double threshold, u32 id_bound) {
   S.ev.ensure(E.mem, U);
   S.ew.ensure(E.mem, U);
   S.op.ensure(E.mem, U);
-  ++E.nlaunch, k_compress<<<grid_for((u64)U * 32), 256, 0, st>>>(U, S.seg_start.p, R, ko, vo, S.neww.p, threshold,
-                                          S.eu.p, S.ev.p, S.ew.p, S.op.p);
+  FoldList fl = fold_list(E, R, U);
+  ++E.nlaunch, k_compress<<<grid_for((u64)U * 32), 256, 0, st>>>(
+      U, S.seg_start.p, R, ko, vo, S.neww.p, threshold, S.eu.p, S.ev.p, S.ew.p, S.op.p, fl.seg,
+      fl.cnt);
+  ++E.nlaunch, k_compress_runs<<<FOLD_BLOCKS, 256, 0, st>>>(
+      fl.seg, fl.cnt, U, S.seg_start.p, R, ko, vo, S.neww.p, threshold, S.eu.p, S.ev.p, S.ew.p,
+      S.op.p);
   HL_LAUNCH_CHECK();
   S.eu2.ensure(E.mem, U);
   S.ev2.ensure(E.mem, U);

@@ -716,6 +716,28 @@ hl_status hl_dbg_tree_sum(int32_t device, const double* x, uint64_t n, double* o
   });
 }
 
+hl_status hl_dbg_seq_sums(int32_t device, uint32_t nseg, const uint64_t* off, const double* x,
+                          double init, int32_t path, double* out) {
+  HL_TRY({
+    require(nseg == 0 || (off && x && out), "NULL argument");
+    require(path >= 0 && path <= 2, "path must be 0, 1 or 2");
+    auto B = scratch_engine(device);
+    Engine& E = *B->E;
+    if (nseg) {
+      const u64 total = off[nseg];
+      for (u32 i = 0; i < nseg; ++i) require(off[i] <= off[i + 1], "offsets must ascend");
+      DBuf<u64> doff;
+      DBuf<double> dx, dout;
+      up(E, doff, off, (size_t)nseg + 1);
+      up(E, dx, x, total);
+      dout.ensure(E.mem, nseg);
+      seq_sums(E, nseg, doff.p, dx.p, init, path, dout.p);
+      down(E, out, dout.p, nseg);
+      E.sync();
+    }
+  });
+}
+
 hl_status hl_dbg_move_eval(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
                            const double* w, const uint32_t* f, const double* d, uint64_t d_len,
                            const double* k, double tw, double gamma, const uint32_t* verts,

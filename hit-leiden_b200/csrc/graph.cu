@@ -278,12 +278,14 @@ __global__ void k_new_degrees(u32 n, const u64* off, const int* ddeg, u64* nd) {
 }
 
 // Untouched rows of the new CSR, copied by output position: each block takes
-// COPY_CH consecutive output entries, finds the rows they span with one
-// search, stages those rows' new offsets in shared memory and maps every
-// entry to its row there.  Reads and writes stream; entries of touched rows
-// are left to k_merge_rows.
+// COPY_CH consecutive output entries and finds the rows they span with two
+// warp searches.  It stages those rows' new offsets, their shifts (old minus
+// new offset) and touched flags in shared memory, maps every entry to its row
+// there, and moves four entries per thread at a time.  Reads and writes
+// stream; entries of touched rows are left to k_merge_rows.
 constexpr u32 COPY_CH = 4096;
 constexpr u32 COPY_ROWS = 1024;
+constexpr u32 COPY_UNROLL = 4;
 
 // Largest i in [lo, hi) with a[i] <= x, given a[lo] <= x (a ascending).
 __device__ __forceinline__ u64 last_le_u64(const u64* a, u64 lo, u64 hi, u64 x) {
@@ -295,48 +297,98 @@ __device__ __forceinline__ u64 last_le_u64(const u64* a, u64 lo, u64 hi, u64 x) 
   return lo;
 }
 
+// The same search by a whole warp: each step probes 32 evenly spaced
+// positions lo + span·k/32 at once and keeps the interval between the last
+// probe <= x and the next, so the span shrinks 32-fold per step.
+__device__ __forceinline__ u64 warp_last_le_u64(const u64* a, u64 lo, u64 hi, u64 x) {
+  const u32 lane = threadIdx.x & 31;
+  while (hi - lo > 32) {
+    const u64 span = hi - lo;
+    const u64 p = lo + span * lane / 32;
+    const u32 m = __ballot_sync(0xffffffffu, lane == 0 || a[p] <= x);
+    const u32 j = (u32)__popc(m) - 1;  // probes 0..j are <= x
+    const u64 nlo = lo + span * j / 32;
+    hi = j == 31 ? hi : lo + span * (j + 1) / 32;
+    lo = nlo;
+  }
+  const u64 p = lo + lane;
+  const u32 m = __ballot_sync(0xffffffffu, p < hi && (lane == 0 || a[p] <= x));
+  return lo + (u32)__popc(m) - 1;
+}
+
 __global__ void __launch_bounds__(256) k_copy_untouched(u32 n, const u64* off, const u32* col,
                                                         const double* w, const u64* noff,
                                                         u32* ncol, double* nw, const u8* touched,
                                                         u64 nnz_new) {
   __shared__ u64 s_noff[COPY_ROWS + 1];
+  __shared__ u64 s_shift[COPY_ROWS];
+  __shared__ u8 s_touched[COPY_ROWS];
   __shared__ u32 s_rb, s_re;
+  const u32 wid = threadIdx.x >> 5;
   for (u64 q0 = (u64)blockIdx.x * COPY_CH; q0 < nnz_new; q0 += (u64)gridDim.x * COPY_CH) {
     const u64 q1 = q0 + COPY_CH < nnz_new ? q0 + COPY_CH : nnz_new;
-    if (threadIdx.x == 0) {
-      // rows r with noff[r] <= q < noff[r + 1]; noff[0] = 0 <= q0, noff[n] = nnz_new > q
-      const u64 rb = last_le_u64(noff, 0, (u64)n + 1, q0);
-      const u64 re = last_le_u64(noff, rb, (u64)n + 1, q1 - 1);
-      s_rb = (u32)rb;
-      s_re = (u32)re;
+    // rows r with noff[r] <= q < noff[r + 1]; noff[0] = 0 <= q0, noff[n] = nnz_new > q
+    if (wid == 0) {
+      const u64 rb = warp_last_le_u64(noff, 0, (u64)n + 1, q0);
+      if ((threadIdx.x & 31) == 0) s_rb = (u32)rb;
+    } else if (wid == 1) {
+      const u64 re = warp_last_le_u64(noff, 0, (u64)n + 1, q1 - 1);
+      if ((threadIdx.x & 31) == 0) s_re = (u32)re;
     }
     __syncthreads();
     const u32 rb = s_rb;
-    const u32 nrow = s_re - rb + 1;
+    const u32 nrow = s_re - rb + 1;  // re <= n - 1, so rb + nrow <= n
     const bool staged = nrow <= COPY_ROWS;
     if (staged)
-      for (u32 x = threadIdx.x; x <= nrow; x += blockDim.x) s_noff[x] = noff[rb + x];
-    __syncthreads();
-    for (u64 q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-      u32 r;
-      u64 nq;
-      if (staged) {
-        u32 lo = 0, hi = nrow;
-        while (hi - lo > 1) {
-          const u32 mid = (lo + hi) >> 1;
-          if (s_noff[mid] <= q) lo = mid;
-          else hi = mid;
+      for (u32 x = threadIdx.x; x <= nrow; x += blockDim.x) {
+        const u64 no = noff[rb + x];
+        s_noff[x] = no;
+        if (x < nrow) {
+          s_shift[x] = off[rb + x] - no;  // modulo 2^64: src = q + shift
+          s_touched[x] = touched[rb + x];
         }
-        r = rb + lo;
-        nq = s_noff[lo];
-      } else {
-        r = (u32)last_le_u64(noff, rb, (u64)rb + nrow, q);
-        nq = noff[r];
       }
-      if (touched[r]) continue;
-      const u64 src = off[r] + (q - nq);
-      ncol[q] = col[src];
-      nw[q] = w[src];
+    __syncthreads();
+    for (u64 qb = q0 + threadIdx.x; qb < q1; qb += COPY_UNROLL * blockDim.x) {
+      u64 src[COPY_UNROLL];
+      bool mv[COPY_UNROLL];
+#pragma unroll
+      for (u32 u = 0; u < COPY_UNROLL; ++u) {
+        const u64 q = qb + (u64)u * blockDim.x;
+        mv[u] = false;
+        src[u] = 0;
+        if (q < q1) {
+          if (staged) {
+            u32 lo = 0, hi = nrow;
+            while (hi - lo > 1) {
+              const u32 mid = (lo + hi) >> 1;
+              if (s_noff[mid] <= q) lo = mid;
+              else hi = mid;
+            }
+            mv[u] = !s_touched[lo];
+            src[u] = q + s_shift[lo];
+          } else {
+            const u32 r = (u32)last_le_u64(noff, rb, (u64)rb + nrow, q);
+            mv[u] = !touched[r];
+            src[u] = off[r] + (q - noff[r]);
+          }
+        }
+      }
+      u32 c[COPY_UNROLL];
+      double v[COPY_UNROLL];
+#pragma unroll
+      for (u32 u = 0; u < COPY_UNROLL; ++u)
+        if (mv[u]) {
+          c[u] = col[src[u]];
+          v[u] = w[src[u]];
+        }
+#pragma unroll
+      for (u32 u = 0; u < COPY_UNROLL; ++u)
+        if (mv[u]) {
+          const u64 q = qb + (u64)u * blockDim.x;
+          ncol[q] = c[u];
+          nw[q] = v[u];
+        }
     }
     __syncthreads();
   }
@@ -578,19 +630,120 @@ __global__ void __launch_bounds__(256) k_merge_long(const u32* long_rows, const 
 
 // Row sums in CSR order (hit_leiden.rs:1063), left to right: the exact
 // rounding of the reference for any weights (warp per row, ordered fold).
-// `flags` (if set) restricts the rows to those flagged.
+// `flags` (if set) restricts the rows to those flagged.  Rows of RUN_FOLD_MIN
+// or more entries are listed for k_row_sum_runs.
 __global__ void k_row_sum_serial(const u32* rows, u32 nr, const u64* off, const double* w,
-                                 double* k, const u8* flags = nullptr) {
+                                 double* k, const u8* flags, u32* longl, u32* longn) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 i = warp; i < nr; i += nwarps) {
     u32 v = rows ? rows[i] : (u32)i;
     if (flags && !flags[v]) continue;
-    double s = warp_ordered_sum(off[v], off[v + 1], 0.0, [&](u64 p) { return w[p]; },
+    const u64 a = off[v], b = off[v + 1];
+    if (b - a >= RUN_FOLD_MIN) {
+      fold_defer(longl, longn, v);
+      continue;
+    }
+    double s = warp_ordered_sum(a, b, 0.0, [&](u64 p) { return w[p]; },
                                 [](u64) { return true; });
     if (lane == 0) k[v] = s;
   }
+}
+
+// The long rows listed by k_row_sum_serial, folded in runs (the same bits).
+__global__ void k_row_sum_runs(const u32* longl, const u32* longn, const u64* off,
+                               const double* w, double* k) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  const u32 nl = *longn;
+  for (u64 j = warp; j < nl; j += nwarps) {
+    const u32 v = longl[j];
+    double s = warp_fold_runs(off[v], off[v + 1], 0.0, [&](u64 p) { return w[p]; });
+    if (lane == 0) k[v] = s;
+  }
+}
+
+// Left-to-right sums of the segments [off[i], off[i+1]) of x from `init`:
+// PATH 0 is the library's pair (short segments here, long ones listed for
+// k_seq_sums_runs), 1 folds every segment in runs, 2 none.
+template <int PATH>
+__global__ void k_seq_sums(u32 nseg, const u64* off, const double* x, double init, double* out,
+                           u32* longl, u32* longn) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 i = warp; i < nseg; i += nwarps) {
+    const u64 a = off[i], b = off[i + 1];
+    auto val = [&](u64 p) { return x[p]; };
+    double s;
+    if constexpr (PATH == 1) {
+      s = warp_fold_runs(a, b, init, val);
+    } else {
+      if (PATH == 0 && b - a >= RUN_FOLD_MIN) {
+        fold_defer(longl, longn, (u32)i);
+        continue;
+      }
+      s = warp_ordered_sum(a, b, init, val, [](u64) { return true; });
+    }
+    if (lane == 0) out[i] = s;
+  }
+}
+
+__global__ void k_seq_sums_runs(const u32* longl, const u32* longn, const u64* off,
+                                const double* x, double init, double* out) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  const u32 nl = *longn;
+  for (u64 j = warp; j < nl; j += nwarps) {
+    const u32 i = longl[j];
+    double s = warp_fold_runs(off[i], off[i + 1], init, [&](u64 p) { return x[p]; });
+    if (lane == 0) out[i] = s;
+  }
+}
+
+FoldList fold_list(Engine& E, u64 total, u32 nseg) {
+  Scratch& S = E.sc;
+  u64 cap = total / RUN_FOLD_MIN + 1;
+  if (cap > nseg) cap = nseg ? nseg : 1;
+  S.foldseg.ensure(E.mem, cap);
+  S.foldcnt.ensure(E.mem, 1);
+  HL_CUDA(cudaMemsetAsync(S.foldcnt.p, 0, sizeof(u32), E.stream));
+  return FoldList{S.foldseg.p, S.foldcnt.p};
+}
+
+void seq_sums(Engine& E, u32 nseg, const u64* off, const double* x, double init, int path,
+              double* out) {
+  if (!nseg) return;
+  const u32 grid = grid_for((u64)nseg * 32);
+  if (path == 1) {
+    ++E.nlaunch, k_seq_sums<1><<<grid, 256, 0, E.stream>>>(nseg, off, x, init, out, nullptr,
+                                                            nullptr);
+  } else if (path == 2) {
+    ++E.nlaunch, k_seq_sums<2><<<grid, 256, 0, E.stream>>>(nseg, off, x, init, out, nullptr,
+                                                            nullptr);
+  } else {
+    // the total is only known on the device: room for every segment
+    FoldList fl = fold_list(E, (u64)nseg * RUN_FOLD_MIN, nseg);
+    ++E.nlaunch, k_seq_sums<0><<<grid, 256, 0, E.stream>>>(nseg, off, x, init, out, fl.seg,
+                                                            fl.cnt);
+    ++E.nlaunch, k_seq_sums_runs<<<FOLD_BLOCKS, 256, 0, E.stream>>>(fl.seg, fl.cnt, off, x, init,
+                                                                  out);
+  }
+  HL_LAUNCH_CHECK();
+}
+
+// Ordered row sums of the flagged rows (all rows without flags): the short
+// rows in k_row_sum_serial, the long ones in k_row_sum_runs.
+static void row_sums_ordered(Engine& E, Level& L, const u8* flags) {
+  const u32 n = L.g.n;
+  FoldList fl = fold_list(E, L.g.nnz, n);
+  ++E.nlaunch, k_row_sum_serial<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(
+      nullptr, n, L.g.off.p, L.g.w.p, L.k.p, flags, fl.seg, fl.cnt);
+  ++E.nlaunch, k_row_sum_runs<<<FOLD_BLOCKS, 256, 0, E.stream>>>(fl.seg, fl.cnt, L.g.off.p,
+                                                                 L.g.w.p, L.k.p);
 }
 
 // Warp-parallel row sums; only used when every weight is integral, where any
@@ -658,8 +811,7 @@ static void recompute_flagged_rows(Engine& E, Level& L, const u8* flags) {
     ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(
         nullptr, n, L.g.off.p, L.g.w.p, L.k.p, flags);
   else
-    ++E.nlaunch, k_row_sum_serial<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(
-        nullptr, n, L.g.off.p, L.g.w.p, L.k.p, flags);
+    row_sums_ordered(E, L, flags);
   HL_LAUNCH_CHECK();
   E.kt_end(KT_ROW_SUMS, ev);
 }
@@ -671,8 +823,7 @@ void recompute_all_degrees(Engine& E, Level& L) {
       ++E.nlaunch, k_row_sum_warp<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(nullptr, n, L.g.off.p, L.g.w.p,
                                                                    L.k.p);
     else
-      ++E.nlaunch, k_row_sum_serial<<<grid_for((u64)n * 32), 256, 0, E.stream>>>(nullptr, n, L.g.off.p,
-                                                                                 L.g.w.p, L.k.p);
+      row_sums_ordered(E, L, nullptr);
     HL_LAUNCH_CHECK();
   }
   L.tw = tree_sum(E, L.k.p, n);

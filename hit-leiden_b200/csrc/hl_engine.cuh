@@ -89,6 +89,7 @@ struct Scratch {
   DBuf<u32> ovf, ovf_cnt;  // block kernel: rows deferred to the pass with global regions
   DBuf<u32> acc_cnt;       // inc-movement: accepted moves over all rounds
   DBuf<u32> hubk, hubk2, hubv;  // block bin ordered by degree (keys, sorted keys, list)
+  DBuf<u32> foldseg, foldcnt;   // ordered sums: long segments, folded in runs, and their count
   DBuf<double> huge_val;
 };
 
@@ -177,6 +178,15 @@ void graph_grow_nodes(Engine& E, Level& L, u32 n);
 void apply_delta(Engine& E, Level& L, const DevEdges& b, u32 new_n, bool keep_loops);
 void recompute_all_degrees(Engine& E, Level& L);
 double tree_sum(Engine& E, const double* x, u64 n);
+void seq_sums(Engine& E, u32 nseg, const u64* off, const double* x, double init, int path,
+              double* out);
+// List (and zeroed count) for the long segments of one ordered-sum kernel
+// pair: room for every segment of RUN_FOLD_MIN or more of `total` terms.
+struct FoldList {
+  u32* seg;
+  u32* cnt;
+};
+FoldList fold_list(Engine& E, u64 total, u32 nseg);
 bool edges_integral(Engine& E, const DevEdges& b);
 void check_endpoints(Engine& E, const DevEdges& b, u32 n);
 

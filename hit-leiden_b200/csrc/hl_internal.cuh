@@ -226,6 +226,140 @@ __device__ __forceinline__ double warp_ordered_sum(u64 a, u64 b, double acc, V v
   return acc;
 }
 
+// The same left-to-right sum as warp_ordered_sum with every value taken, the
+// same bits, computed in runs instead of one addition after another.
+//
+// Write the running sum as |s| = M·u, u = 2^(e-52), M in [2^52, 2^53).  A term
+// y with the sign of s (or a zero) is t·u.  If t is not an odd multiple of 1/2
+// and M + rnd(t) <= 2^53 - 1 (rnd: nearest integer), the exact sum stays below
+// 2^(e+1), so fl(s + y) has the sign of s and the magnitude (M + rnd(t))·u:
+// the rounding does not depend on s.  A run of such terms therefore adds the
+// exact integer prefix sums of their rnd(t).  Lane l holds the 4 consecutive
+// terms 4l..4l+3 of a 128-term tile, and one warp scan of the lanes' integer
+// totals gives every prefix.  A run ends before the first term that is a tie,
+// has the other sign, is not finite, or would carry M past 2^53 - 1.  From
+// there the terms take ordinary rounded additions to the end of that lane's
+// 4 terms (to the end of the tile when the run was shorter than 32 terms) and
+// a new run starts.  A sum that is zero, subnormal, below 2^-959, infinite or
+// NaN also takes ordinary additions, 4 terms at a time.
+//
+// Worth it from a few hundred terms on: the first terms of a sum from zero
+// cross a binade every few terms.
+constexpr u64 RUN_FOLD_MIN = 512;
+
+template <typename V>
+__device__ __forceinline__ double warp_fold_runs(u64 a, u64 b, double acc, V val) {
+  constexpr u32 PER = 4, TILE = 32 * PER;
+  constexpr u64 MAXM = (1ull << 53) - 1;
+  const u32 lane = threadIdx.x & 31;
+  if (a >= b) return acc;
+  double x[PER], xn[PER];
+#pragma unroll
+  for (u32 j = 0; j < PER; ++j) {
+    const u64 t = a + PER * lane + j;
+    x[j] = t < b ? val(t) : 0.0;
+  }
+  for (u64 base = a; base < b; base += TILE) {
+    // the next tile's terms are in flight while this one is folded
+#pragma unroll
+    for (u32 j = 0; j < PER; ++j) {
+      const u64 t = base + TILE + PER * lane + j;
+      xn[j] = t < b ? val(t) : 0.0;
+    }
+    const u32 cnt = (u32)(b - base < TILE ? b - base : TILE);
+    u32 q0 = 0;
+    while (q0 < cnt) {
+      const u64 bits = (u64)__double_as_longlong(acc);
+      const u32 bexp = (u32)(bits >> 52) & 0x7ffu;
+      u32 q = q0, e;
+      if (bexp >= 64 && bexp <= 2046) {
+        const bool neg = acc < 0.0;
+        // 1/u = 2^(52-e), a normal power of two for these exponents
+        const double scale = __longlong_as_double((long long)((u64)(2098u - bexp) << 52));
+        const u64 M = (bits & ((1ull << 52) - 1)) | (1ull << 52);
+        u64 C[PER];
+        u32 badm = 0;  // bit j: this lane's term j ends the run
+        u64 P = 0;
+#pragma unroll
+        for (u32 j = 0; j < PER; ++j) {
+          const u32 idx = PER * lane + j;
+          const bool in = idx >= q0 && idx < cnt;
+          const double y = neg ? -x[j] : x[j];
+          const double t = __dmul_rn(y, scale);  // exact, or below 2^-1022 where rnd is 0
+          const bool good = (y >= 0.0) && (t < 4503599627370496.0);  // 2^52; false for NaN
+          const double tg = good ? t : 0.0;
+          const double f = floor(tg);
+          const double fr = __dsub_rn(tg, f);  // exact
+          const bool tie = fr == 0.5;
+          P += (in && good && !tie) ? (u64)f + (fr > 0.5 ? 1ull : 0ull) : 0ull;
+          C[j] = P;
+          if (in && (!good || tie)) badm |= 1u << j;
+        }
+        u64 inc = P;
+#pragma unroll
+        for (u32 o = 1; o < 32; o <<= 1) {
+          const u64 v = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += v;
+        }
+        const u64 excl = inc - P;
+#pragma unroll
+        for (u32 j = 0; j < PER; ++j) {
+          C[j] += excl;
+          const u32 idx = PER * lane + j;
+          if (idx >= q0 && idx < cnt && M + C[j] > MAXM) badm |= 1u << j;
+        }
+        const u32 fb = badm ? (u32)(__ffs(badm) - 1) : PER;
+        const u32 ball = __ballot_sync(0xffffffffu, badm != 0);
+        q = cnt;
+        if (ball) {
+          const u32 first = (u32)(__ffs(ball) - 1);
+          q = PER * first + __shfl_sync(0xffffffffu, fb, first);
+        }
+        if (q > q0) {
+          // the prefix through term q - 1, from the lane that holds it (a
+          // masked overwrite: a select by q % 4 would index C dynamically)
+          u64 mine = excl;
+#pragma unroll
+          for (u32 j = 0; j < PER; ++j)
+            if (PER * lane + j < q) mine = C[j];
+          const u64 cr = __shfl_sync(0xffffffffu, mine, (q - 1) / PER);
+          acc = __longlong_as_double(
+              (long long)((bits & (1ull << 63)) | ((u64)bexp << 52) | (M + cr - (1ull << 52))));
+        }
+        if (q >= cnt) break;
+        e = (q - q0 < 32) ? cnt : min(cnt, (q / PER) * PER + PER);
+      } else {
+        e = min(cnt, (q0 / PER) * PER + PER);
+      }
+      // ordinary rounded additions of the terms [q, e)
+      for (u32 l = q / PER; l * PER < e; ++l) {
+#pragma unroll
+        for (u32 j = 0; j < PER; ++j) {
+          const double y = __shfl_sync(0xffffffffu, x[j], l);
+          const u32 idx = l * PER + j;
+          if (idx >= q && idx < e) acc = __dadd_rn(acc, y);
+        }
+      }
+      q0 = e;
+    }
+#pragma unroll
+    for (u32 j = 0; j < PER; ++j) x[j] = xn[j];
+  }
+  return acc;
+}
+
+// The ordered-sum kernels come in pairs.  The first, a warp per segment with
+// the few registers of warp_ordered_sum, sums the segments below RUN_FOLD_MIN
+// and lists the longer ones; the second folds the listed ones in runs, with
+// FOLD_BLOCKS blocks of 256 threads (one wave at 64 registers a thread) and
+// the count read on the device.
+constexpr u32 FOLD_BLOCKS = 148 * 4;
+
+// Appends segment i to the list of long segments (lane 0 of the calling warp).
+__device__ __forceinline__ void fold_defer(u32* list, u32* count, u32 i) {
+  if ((threadIdx.x & 31) == 0) list[atomicAdd(count, 1u)] = i;
+}
+
 // First position in [lo, hi) of the ascending array a whose value is >= x.
 __device__ __forceinline__ u64 lower_bound_u32(const u32* a, u64 lo, u64 hi, u32 x) {
   while (lo < hi) {

@@ -66,6 +66,16 @@ HL_API hl_status hl_dbg_inc_aggregation(int32_t device, uint32_t n, const uint64
 /* The fixed-shape pairwise sum used for 2m (tiles of 1024, stride halving). */
 HL_API hl_status hl_dbg_tree_sum(int32_t device, const double* x, uint64_t n, double* out);
 
+/* Left-to-right f64 sums, out[i] = init + x[off[i]] + ... + x[off[i+1]-1]
+ * with every addition rounded in that order: the fold behind the row sums
+ * (hit_leiden.rs:1063), the community degrees and the aggregation's
+ * per-super-edge sums.  path 0 is the library's own choice (runs of same-binade
+ * terms for segments of 512 or more, one addition after another below), 1
+ * always folds in runs, 2 never does; all three give the same bits.  No
+ * reference counterpart: the entry point exposes the fold to tests. */
+HL_API hl_status hl_dbg_seq_sums(int32_t device, uint32_t nseg, const uint64_t* off,
+                                 const double* x, double init, int32_t path, double* out);
+
 /* Test switch, process-wide: nonzero makes the refinement's T-filter decide
  * every candidate from the ordered sum w(S, C) (hit_leiden.rs:1618-1625)
  * instead of the any-order sum with its rounding window.  Results are the same
