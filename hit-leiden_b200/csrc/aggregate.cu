@@ -146,11 +146,12 @@ __device__ __forceinline__ void compress_out(u64 j, u64 a, double x, const u64* 
   }
 }
 
-// In-order segmented sum; keep |w| > threshold.  Segments of RUN_FOLD_MIN or
-// more terms are listed for k_compress_runs.
-__global__ void k_compress(u32 U, const u32* start, u64 total, const u64* sk, const u32* sseq,
-                           const double* vals, double threshold, u32* ou, u32* ov, double* ow,
-                           u8* keepf, u32* longl, u32* longn) {
+// In-order segmented sum over the records' weights gathered into sorted
+// order (sw); keep |w| > threshold.  Segments of RUN_FOLD_MIN or more terms
+// are listed for k_compress_runs.
+__global__ void k_compress(u32 U, const u32* start, u64 total, const u64* sk, const double* sw,
+                           double threshold, u32* ou, u32* ov, double* ow, u8* keepf, u32* longl,
+                           u32* longn) {
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 j = warp; j < U; j += nwarps) {
@@ -161,10 +162,9 @@ __global__ void k_compress(u32 U, const u32* start, u64 total, const u64* sk, co
     }
     double x = 0.0;
     if (b - a == 1) {
-      x = vals[sseq[a]];
+      x = sw[a];
     } else {
-      x = warp_ordered_sum(a, b, 0.0, [&](u64 t) { return vals[sseq[t]]; },
-                           [](u64) { return true; });
+      x = warp_ordered_sum(a, b, 0.0, [&](u64 t) { return sw[t]; }, [](u64) { return true; });
     }
     compress_out(j, a, x, sk, threshold, ou, ov, ow, keepf);
   }
@@ -172,17 +172,23 @@ __global__ void k_compress(u32 U, const u32* start, u64 total, const u64* sk, co
 
 // The long segments listed by k_compress, folded in runs (the same bits).
 __global__ void k_compress_runs(const u32* longl, const u32* longn, u32 U, const u32* start,
-                                u64 total, const u64* sk, const u32* sseq, const double* vals,
-                                double threshold, u32* ou, u32* ov, double* ow, u8* keepf) {
+                                u64 total, const u64* sk, const double* sw, double threshold,
+                                u32* ou, u32* ov, double* ow, u8* keepf) {
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   const u32 nl = *longn;
   for (u64 i = warp; i < nl; i += nwarps) {
     const u32 j = longl[i];
     u64 a = start[j], b = (j + 1 < U) ? start[j + 1] : total;
-    double x = warp_fold_runs(a, b, 0.0, [&](u64 t) { return vals[sseq[t]]; });
+    double x = warp_fold_runs(a, b, 0.0, sw);
     compress_out(j, a, x, sk, threshold, ou, ov, ow, keepf);
   }
+}
+
+// out[t] = src[idx[t]]: the weights gathered into the records' sorted order.
+__global__ void k_gather_weights(const u32* idx, const double* src, u64 n, double* out) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < n; t += (u64)gridDim.x * blockDim.x)
+    out[t] = src[idx[t]];
 }
 
 __global__ void k_set_spre(u32 n, const u8* refined, const u32* s_cur, u32* s_pre) {
@@ -223,12 +229,14 @@ static u64 compress_records(Engine& E, u64 R, double threshold, u32 id_bound) {
   S.ev.ensure(E.mem, U);
   S.ew.ensure(E.mem, U);
   S.op.ensure(E.mem, U);
+  S.fvals.ensure(E.mem, R);
+  ++E.nlaunch, k_gather_weights<<<grid_for(R), 256, 0, st>>>(vo, S.neww.p, R, S.fvals.p);
   FoldList fl = fold_list(E, R, U);
   ++E.nlaunch, k_compress<<<grid_for((u64)U * 32), 256, 0, st>>>(
-      U, S.seg_start.p, R, ko, vo, S.neww.p, threshold, S.eu.p, S.ev.p, S.ew.p, S.op.p, fl.seg,
+      U, S.seg_start.p, R, ko, S.fvals.p, threshold, S.eu.p, S.ev.p, S.ew.p, S.op.p, fl.seg,
       fl.cnt);
   ++E.nlaunch, k_compress_runs<<<FOLD_BLOCKS, 256, 0, st>>>(
-      fl.seg, fl.cnt, U, S.seg_start.p, R, ko, vo, S.neww.p, threshold, S.eu.p, S.ev.p, S.ew.p,
+      fl.seg, fl.cnt, U, S.seg_start.p, R, ko, S.fvals.p, threshold, S.eu.p, S.ev.p, S.ew.p,
       S.op.p);
   HL_LAUNCH_CHECK();
   S.eu2.ensure(E.mem, U);

@@ -660,7 +660,7 @@ __global__ void k_row_sum_runs(const u32* longl, const u32* longn, const u64* of
   const u32 nl = *longn;
   for (u64 j = warp; j < nl; j += nwarps) {
     const u32 v = longl[j];
-    double s = warp_fold_runs(off[v], off[v + 1], 0.0, [&](u64 p) { return w[p]; });
+    double s = warp_fold_runs(off[v], off[v + 1], 0.0, w);
     if (lane == 0) k[v] = s;
   }
 }
@@ -676,16 +676,15 @@ __global__ void k_seq_sums(u32 nseg, const u64* off, const double* x, double ini
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 i = warp; i < nseg; i += nwarps) {
     const u64 a = off[i], b = off[i + 1];
-    auto val = [&](u64 p) { return x[p]; };
     double s;
     if constexpr (PATH == 1) {
-      s = warp_fold_runs(a, b, init, val);
+      s = warp_fold_runs(a, b, init, x);
     } else {
       if (PATH == 0 && b - a >= RUN_FOLD_MIN) {
         fold_defer(longl, longn, (u32)i);
         continue;
       }
-      s = warp_ordered_sum(a, b, init, val, [](u64) { return true; });
+      s = warp_ordered_sum(a, b, init, [&](u64 p) { return x[p]; }, [](u64) { return true; });
     }
     if (lane == 0) out[i] = s;
   }
@@ -699,7 +698,7 @@ __global__ void k_seq_sums_runs(const u32* longl, const u32* longn, const u64* o
   const u32 nl = *longn;
   for (u64 j = warp; j < nl; j += nwarps) {
     const u32 i = longl[j];
-    double s = warp_fold_runs(off[i], off[i + 1], init, [&](u64 p) { return x[p]; });
+    double s = warp_fold_runs(off[i], off[i + 1], init, x);
     if (lane == 0) out[i] = s;
   }
 }

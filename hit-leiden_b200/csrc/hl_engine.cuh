@@ -90,6 +90,7 @@ struct Scratch {
   DBuf<u32> acc_cnt;       // inc-movement: accepted moves over all rounds
   DBuf<u32> hubk, hubk2, hubv;  // block bin ordered by degree (keys, sorted keys, list)
   DBuf<u32> foldseg, foldcnt;   // ordered sums: long segments, folded in runs, and their count
+  DBuf<double> fvals;           // ordered sums: the terms gathered into sum order
   DBuf<double> huge_val;
 };
 

@@ -247,24 +247,30 @@ __device__ __forceinline__ double warp_ordered_sum(u64 a, u64 b, double acc, V v
 // cross a binade every few terms.
 constexpr u64 RUN_FOLD_MIN = 512;
 
-template <typename V>
-__device__ __forceinline__ double warp_fold_runs(u64 a, u64 b, double acc, V val) {
+// The terms are xs[a..b), contiguous: one warp folds one long segment, so its
+// own loads must be in flight well ahead.  The tiles after the current one
+// are held in registers, and the one four tiles ahead is prefetched into L2.
+__device__ __forceinline__ double warp_fold_runs(u64 a, u64 b, double acc,
+                                                 const double* __restrict__ xs) {
   constexpr u32 PER = 4, TILE = 32 * PER;
   constexpr u64 MAXM = (1ull << 53) - 1;
   const u32 lane = threadIdx.x & 31;
   if (a >= b) return acc;
-  double x[PER], xn[PER];
-#pragma unroll
-  for (u32 j = 0; j < PER; ++j) {
-    const u64 t = a + PER * lane + j;
-    x[j] = t < b ? val(t) : 0.0;
-  }
-  for (u64 base = a; base < b; base += TILE) {
-    // the next tile's terms are in flight while this one is folded
+  double x[PER], xn[PER], xnn[PER];
+  auto load = [&](u64 base, double* dst) {
 #pragma unroll
     for (u32 j = 0; j < PER; ++j) {
-      const u64 t = base + TILE + PER * lane + j;
-      xn[j] = t < b ? val(t) : 0.0;
+      const u64 t = base + PER * lane + j;
+      dst[j] = t < b ? xs[t] : 0.0;
+    }
+  };
+  load(a, x);
+  load(a + TILE, xn);
+  for (u64 base = a; base < b; base += TILE) {
+    load(base + 2 * TILE, xnn);
+    {
+      const u64 t = base + 4 * TILE + PER * lane;
+      if (t < b) asm volatile("prefetch.global.L2 [%0];" ::"l"(xs + t));
     }
     const u32 cnt = (u32)(b - base < TILE ? b - base : TILE);
     u32 q0 = 0;
@@ -343,7 +349,10 @@ __device__ __forceinline__ double warp_fold_runs(u64 a, u64 b, double acc, V val
       q0 = e;
     }
 #pragma unroll
-    for (u32 j = 0; j < PER; ++j) x[j] = xn[j];
+    for (u32 j = 0; j < PER; ++j) {
+      x[j] = xn[j];
+      xn[j] = xnn[j];
+    }
   }
   return acc;
 }
@@ -351,9 +360,9 @@ __device__ __forceinline__ double warp_fold_runs(u64 a, u64 b, double acc, V val
 // The ordered-sum kernels come in pairs.  The first, a warp per segment with
 // the few registers of warp_ordered_sum, sums the segments below RUN_FOLD_MIN
 // and lists the longer ones; the second folds the listed ones in runs, with
-// FOLD_BLOCKS blocks of 256 threads (one wave at 64 registers a thread) and
-// the count read on the device.
-constexpr u32 FOLD_BLOCKS = 148 * 4;
+// FOLD_BLOCKS blocks of 256 threads (one wave at up to 80 registers a
+// thread) and the count read on the device.
+constexpr u32 FOLD_BLOCKS = 148 * 3;
 
 // Appends segment i to the list of long segments (lane 0 of the calling warp).
 __device__ __forceinline__ void fold_defer(u32* list, u32* count, u32 i) {

@@ -70,14 +70,15 @@ __global__ void k_comm_deg_atomic(u32 n, const u32* part, const double* k, doubl
   }
 }
 
-// Ordered variant: nodes sorted by (community, node); one warp per community
-// sums its members' degrees in ascending node order.
-// The number of communities is read on the device (exclusive scan of the
-// segment heads at the last position plus the last head).
-// Communities of RUN_FOLD_MIN or more members are listed for k_comm_deg_runs.
+// Ordered variant: nodes sorted by (community, node), their degrees gathered
+// into that order (vals); one warp per community sums its members' degrees in
+// ascending node order.  The number of communities is read on the device
+// (exclusive scan of the segment heads at the last position plus the last
+// head).  Communities of RUN_FOLD_MIN or more members are listed for
+// k_comm_deg_runs.
 __global__ void k_comm_deg_ordered(const u32* seg_last, const u32* head_last, const u32* ukeys,
-                                   const u32* ustart, u32 n, const u32* sorted_nodes,
-                                   const double* k, double* d, u32* longl, u32* longn) {
+                                   const u32* ustart, u32 n, const double* vals, double* d,
+                                   u32* longl, u32* longn) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
@@ -88,7 +89,7 @@ __global__ void k_comm_deg_ordered(const u32* seg_last, const u32* head_last, co
       fold_defer(longl, longn, (u32)j);
       continue;
     }
-    double s = warp_ordered_sum(a, b, 0.0, [&](u64 t) { return k[sorted_nodes[t]]; },
+    double s = warp_ordered_sum(a, b, 0.0, [&](u64 t) { return vals[t]; },
                                 [](u64) { return true; });
     if (lane == 0) d[ukeys[j]] = s;
   }
@@ -98,7 +99,7 @@ __global__ void k_comm_deg_ordered(const u32* seg_last, const u32* head_last, co
 // same bits).
 __global__ void k_comm_deg_runs(const u32* longl, const u32* longn, const u32* seg_last,
                                 const u32* head_last, const u32* ukeys, const u32* ustart, u32 n,
-                                const u32* sorted_nodes, const double* k, double* d) {
+                                const double* vals, double* d) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
@@ -107,9 +108,15 @@ __global__ void k_comm_deg_runs(const u32* longl, const u32* longn, const u32* s
   for (u64 i = warp; i < nl; i += nwarps) {
     const u32 j = longl[i];
     u32 a = ustart[j], b = (j + 1 < nu) ? ustart[j + 1] : n;
-    double s = warp_fold_runs(a, b, 0.0, [&](u64 t) { return k[sorted_nodes[t]]; });
+    double s = warp_fold_runs(a, b, 0.0, vals);
     if (lane == 0) d[ukeys[j]] = s;
   }
+}
+
+// out[t] = src[idx[t]]: the terms of an ordered sum gathered into sum order.
+__global__ void k_gather_f64(const u32* idx, const double* src, u64 n, double* out) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < n; t += (u64)gridDim.x * blockDim.x)
+    out[t] = src[idx[t]];
 }
 
 __global__ void k_copy_u32(const u32* a, u32* b, u64 n) {
@@ -179,11 +186,13 @@ static void recompute_comm_degrees_impl(Engine& E, Level& L, const u32* part, u3
     return cub::DeviceScan::ExclusiveSum(t, b, h, sid, (int64_t)n, st);
   });
   ++E.nlaunch, k_seg_compact<<<grid_for(n), 256, 0, st>>>(h, sid, kout, n, S.used.p, S.sel_node.p);
+  S.fvals.ensure(E.mem, n);
+  ++E.nlaunch, k_gather_f64<<<grid_for(n), 256, 0, st>>>(vout, L.k.p, n, S.fvals.p);
   FoldList fl = fold_list(E, n, n);
   ++E.nlaunch, k_comm_deg_ordered<<<grid_for((u64)n * 32), 256, 0, st>>>(
-      sid + n - 1, h + n - 1, S.used.p, S.sel_node.p, n, vout, L.k.p, d, fl.seg, fl.cnt);
+      sid + n - 1, h + n - 1, S.used.p, S.sel_node.p, n, S.fvals.p, d, fl.seg, fl.cnt);
   ++E.nlaunch, k_comm_deg_runs<<<FOLD_BLOCKS, 256, 0, st>>>(
-      fl.seg, fl.cnt, sid + n - 1, h + n - 1, S.used.p, S.sel_node.p, n, vout, L.k.p, d);
+      fl.seg, fl.cnt, sid + n - 1, h + n - 1, S.used.p, S.sel_node.p, n, S.fvals.p, d);
   HL_LAUNCH_CHECK();
 }
 
