@@ -655,6 +655,7 @@ def main():
     torch.cuda.synchronize()
     dev_ms = []
     launches = 0
+    traversed = 0
     stats = L.BatchStats()
     torch.cuda.nvtx.range_push("hl_timed")
     for (du, dv, dw) in dev:
@@ -662,6 +663,7 @@ def main():
                                             C.c_void_p(dw.data_ptr()), k, C.byref(stats)))
         dev_ms.append(stats.device_ms)
         launches += stats.launches
+        traversed += stats.traversed
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier()
@@ -743,7 +745,12 @@ def main():
                     "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1,
                                                                     int(0.99 * len(lat)))]},
             "gpu_launches": int(launches),
+            "traversed_edges_per_s": (traversed / (kernels["stage_move"]["ms"] / 1000.0)
+                                      if kernels.get("stage_move", {}).get("ms") else None),
             "roofline": roof,
+            "roofline_aggregation": _roof(kernels, "aggregate_compress",
+                                          "inc-aggregation (emission + compression)", peak,
+                                          peak_kind),
             "cpu_baseline": cpu,
             "clocks": clk,
             "modularity": q,
