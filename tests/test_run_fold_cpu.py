@@ -136,3 +136,30 @@ def test_grid_rounding_lemma():
         if m + r > MAXM:
             continue
         assert s + y == math.ldexp(float(m + r), e - 52)
+
+
+def test_oracle_degrees_are_the_sequential_fold():
+    # the oracle's k_v is the left-to-right row sum in CSR order
+    # (hit_leiden.rs:1063), hub rows included: the value the run fold must
+    # reproduce on the GPU
+    from fold_cases import seq_fold
+    from oracle import oracle as O
+    rng = np.random.default_rng(4)
+    n = 3000
+    src = [rng.integers(0, n, 6000)]
+    dst = [rng.integers(0, n, 6000)]
+    for hub, deg in ((0, 700), (1, 2500)):
+        src.append(np.full(deg, hub))
+        dst.append(rng.choice(np.arange(2, n), deg, replace=False))
+    s = np.concatenate(src).astype(np.uint32)
+    d = np.concatenate(dst).astype(np.uint32)
+    g = O.Graph.from_edges(n, s, d, rng.uniform(0.5, 2.0, len(s)))
+    off, _, w = g.csr()
+    assert np.diff(off).max() >= 2500
+    k = g.degrees()
+    for v in range(n):
+        row = w[off[v]:off[v + 1]]
+        want = seq_fold(row, 0.0)
+        assert _bits(k[v]) == _bits(want), v
+        if len(row) >= 512:
+            assert _bits(fold_runs(row, 0.0)) == _bits(want), v
