@@ -447,3 +447,37 @@ def test_results_do_not_depend_on_host_threads():
     for p in range(a.levels):
         for which in (O.MAP_F, O.MAP_G, O.MAP_S_PRE, O.MAP_S_CUR):
             assert np.array_equal(a.get_map(p, which), b.get_map(p, which))
+
+
+# --- run() integration and property tests (tests/integration/*.rs, ----------
+# --- tests/property/test_partition_invariants.rs) ---------------------------
+
+def test_run_connected_graph_not_all_singletons():
+    # test_connected_graph_not_all_singletons.rs:21-49: two triangles and a
+    # 0.05 bridge merge at least one pair
+    src, dst, w = weighted([(0, 1, 1.0), (1, 2, 1.0), (2, 0, 1.0), (3, 4, 1.0), (4, 5, 1.0),
+                            (5, 3, 1.0), (2, 3, 0.05)])
+    part, _, _ = O.run(6, src, dst, w)
+    assert len(set(part.tolist())) < 6
+    st = O.State(6, mode=O.MODE_THROUGHPUT)
+    st.bootstrap(src, dst, w, max_levels=10)
+    assert len(set(st.get_map(0, O.MAP_F).tolist())) < 6
+
+
+def test_run_deterministic_replay_identity():
+    # test_deterministic_identity.rs:19-30: two runs on the same input agree
+    src, dst, w = unit([(0, 1), (2, 3)])
+    a = O.run(4, src, dst, w)
+    b = O.run(4, src, dst, w)
+    assert np.array_equal(a[0], b[0]) and a[1] == b[1]
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 7, 31, 49])
+def test_run_partition_length_matches_node_count(n):
+    # test_partition_invariants.rs:20-32: isolated nodes, node_count in 0..50
+    part, q, _ = O.run(n, [], [], [])
+    assert len(part) == n and q == 0.0
+    if n:
+        st = O.State(n, mode=O.MODE_THROUGHPUT)
+        st.bootstrap([], [], [], max_levels=10)
+        assert len(st.get_map(0, O.MAP_F)) == n
