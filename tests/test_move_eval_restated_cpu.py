@@ -1,0 +1,72 @@
+"""The throughput best-move evaluation restated a second time, in plain Python
+straight from the reference (parallel_frontier.rs:150-230), and compared bit
+for bit with the oracle's `move_eval` on random graphs.  The GPU's evaluation
+kernels are compared with the oracle in test_gpu_parity.py, so this pins the
+two restatements to each other.
+
+Python floats are IEEE doubles and every expression keeps the reference's
+operation order, so equality is exact: neighbour weights summed per community
+in CSR order, candidates in first-encounter order, strict `>` from a best
+gain of 0.0, and the empty community n + v last."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+def best_move(off, col, w, v, f, d, k, tw, gamma, n):
+    cur = int(f[v])
+    kv = float(k[v])
+    best, bestg = cur, 0.0
+    wcur = 0.0
+    buf, dirty = {}, []
+    for p in range(int(off[v]), int(off[v + 1])):
+        nb = int(col[p])
+        if nb == v:
+            continue  # self-loops are skipped
+        c = int(f[nb])
+        if buf.get(c, 0.0) == 0.0:
+            dirty.append(c)
+        buf[c] = buf.get(c, 0.0) + float(w[p])
+        if c == cur:
+            wcur += float(w[p])
+    dcur = float(d[cur])
+    for c in dirty:
+        if c == cur:
+            continue
+        g = (buf[c] - wcur) / tw + gamma * kv * (dcur - kv - float(d[c])) / (tw * tw)
+        if g > bestg:
+            best, bestg = c, g
+    eg = -wcur / tw + gamma * kv * (dcur - kv) / (tw * tw)
+    if eg > bestg:
+        best, bestg = n + v, eg
+    return best, bestg
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("integral", [True, False])
+@pytest.mark.parametrize("gamma", [0.5, 1.0, 3.0])
+def test_move_eval_matches_restatement(seed, integral, gamma):
+    rng = np.random.default_rng(seed)
+    n, m = 300, 1500
+    s = rng.integers(0, n, m)
+    t = rng.integers(0, n, m)
+    s[:10] = t[:10]  # a few self-loops
+    w = rng.integers(1, 4, m).astype(float) if integral else rng.uniform(0.5, 2.0, m)
+    g = O.Graph.from_edges(n, s.astype(np.uint32), t.astype(np.uint32), w)
+    off, col, ww = g.csr()
+    k = g.degrees()
+    tw = g.total_weight() * 2.0
+    f = rng.integers(0, 25, n).astype(np.uint32)
+    d = np.zeros(2 * n + 2)
+    for v in range(n):
+        d[f[v]] += k[v]
+    verts = np.arange(n, dtype=np.uint32)
+    to, gain = O.move_eval(g, f, d, k, tw, gamma, verts)
+    moves = 0
+    for v in range(n):
+        bt, bg = best_move(off, col, ww, v, f, d, k, tw, gamma, n)
+        assert (int(to[v]), np.float64(gain[v]).view(np.uint64)) == \
+            (bt, np.float64(bg).view(np.uint64)), v
+        moves += bt != f[v]
+    assert moves > 0
