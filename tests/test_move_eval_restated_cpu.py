@@ -1,6 +1,7 @@
-"""The throughput best-move evaluation restated a second time, in plain Python
-straight from the reference (parallel_frontier.rs:150-230), and compared bit
-for bit with the oracle's `move_eval` on random graphs.  The GPU's evaluation
+"""The throughput best-move evaluation (parallel_frontier.rs:150-230) and the
+decoupled move selection (throughput.rs:204-236) restated a second time, in
+plain Python straight from the reference, and compared bit for bit with the
+oracle's `move_eval` and `select_decoupled` on random inputs.  The GPU's evaluation
 kernels are compared with the oracle in test_gpu_parity.py, so this pins the
 two restatements to each other.
 
@@ -70,3 +71,37 @@ def test_move_eval_matches_restatement(seed, integral, gamma):
             (bt, np.float64(bg).view(np.uint64)), v
         moves += bt != f[v]
     assert moves > 0
+
+
+def select_moves(node, frm, to, gain):
+    """throughput.rs:204-236: sort by gain descending then node ascending
+    (stable), then accept a move iff its gain is positive, its node has not
+    moved, it leaves no acceptor and enters no emitter."""
+    order = sorted(range(len(node)), key=lambda i: (-float(gain[i]), int(node[i])))
+    emitters, acceptors, moved, out = set(), set(), set(), []
+    for i in order:
+        if gain[i] <= 0.0 or node[i] in moved:
+            continue
+        if frm[i] in acceptors or to[i] in emitters:
+            continue
+        out.append(int(node[i]))
+        moved.add(node[i])
+        emitters.add(frm[i])
+        acceptors.add(to[i])
+    return out
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("ncomm", [3, 12, 200])
+def test_select_decoupled_matches_restatement(seed, ncomm):
+    rng = np.random.default_rng(100 + seed)
+    m = 400
+    node = rng.permutation(5000)[:m].astype(np.uint32)
+    frm = rng.integers(0, ncomm, m).astype(np.uint32)
+    to = rng.integers(0, ncomm, m).astype(np.uint32)
+    # coarse gains so that ties occur, a few of them not positive
+    gain = rng.integers(-2, 40, m).astype(float) / 8.0
+    got = O.select_decoupled(node, frm, to, gain).tolist()
+    want = select_moves(node.tolist(), frm.tolist(), to.tolist(), gain.tolist())
+    assert got == want
+    assert len(want) > 0
