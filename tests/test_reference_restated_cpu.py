@@ -1,7 +1,8 @@
-"""The throughput best-move evaluation (parallel_frontier.rs:150-230) and the
-decoupled move selection (throughput.rs:204-236) restated a second time, in
-plain Python straight from the reference, and compared bit for bit with the
-oracle's `move_eval` and `select_decoupled` on random inputs.  The GPU's evaluation
+"""The throughput best-move evaluation (parallel_frontier.rs:150-230), the
+decoupled move selection (throughput.rs:204-236) and apply_delta
+(in_memory.rs:103-137) restated a second time, in plain Python straight from
+the reference, and compared bit for bit with the oracle's `move_eval`,
+`select_decoupled` and `Graph.apply_delta` on random inputs.  The GPU's evaluation
 kernels are compared with the oracle in test_gpu_parity.py, so this pins the
 two restatements to each other.
 
@@ -105,3 +106,66 @@ def test_select_decoupled_matches_restatement(seed, ncomm):
     want = select_moves(node.tolist(), frm.tolist(), to.tolist(), gain.tolist())
     assert got == want
     assert len(want) > 0
+
+
+def apply_delta(off, col, w, n, ds, dd, dw, delta_n):
+    """in_memory.rs:103-137: the existing edges keyed (u, v) with u < v (so
+    existing self-loops are dropped), the batch added in batch order on
+    (min, max) keys, w > 1e-12 kept, node count the larger of the two; rows
+    then built with both directions (a self-loop twice) and, in the canonical
+    order the oracle fixes, sorted by neighbour."""
+    edges = {}
+    for u in range(n):
+        for p in range(int(off[u]), int(off[u + 1])):
+            v = int(col[p])
+            if u < v:
+                edges[(u, v)] = float(w[p])
+    for a, b, x in zip(ds, dd, dw):
+        key = (min(int(a), int(b)), max(int(a), int(b)))
+        edges[key] = edges.get(key, 0.0) + float(x)
+    nn = max(n, delta_n)
+    rows = [[] for _ in range(nn)]
+    for (u, v), x in edges.items():
+        if x > 1e-12:
+            rows[u].append((v, x))
+            rows[v].append((u, x))
+    noff = np.zeros(nn + 1, np.uint64)
+    ncol, nw = [], []
+    for u in range(nn):
+        rows[u].sort(key=lambda e: e[0])
+        ncol += [e[0] for e in rows[u]]
+        nw += [e[1] for e in rows[u]]
+        noff[u + 1] = len(ncol)
+    return noff, np.array(ncol, np.uint32), np.array(nw, np.float64)
+
+
+@pytest.mark.parametrize("seed", range(5))
+@pytest.mark.parametrize("integral", [True, False])
+def test_apply_delta_matches_restatement(seed, integral):
+    rng = np.random.default_rng(200 + seed)
+    n, m = 120, 500
+    s = rng.integers(0, n, m)
+    t = rng.integers(0, n, m)
+    s[:6] = t[:6]  # existing self-loops, which apply_delta drops
+    w = rng.integers(1, 4, m).astype(float) if integral else rng.uniform(0.5, 2.0, m)
+    g = O.Graph.from_edges(n, s.astype(np.uint32), t.astype(np.uint32), w)
+    g = g.apply_delta([], [], [], keep_self_loops=True)  # canonical, duplicates merged
+    off, col, ww = g.csr()
+    k = 150
+    ds = rng.integers(0, n + 10, k)
+    dd = rng.integers(0, n + 10, k)
+    dw = rng.integers(-3, 4, k).astype(float) if integral else rng.uniform(-2.5, 2.5, k)
+    # exact deletes of existing edges, repeated keys, a self-loop in the batch
+    for i in range(0, 30, 3):
+        u = int(rng.integers(0, n))
+        if off[u + 1] > off[u]:
+            p = int(rng.integers(off[u], off[u + 1]))
+            ds[i], dd[i], dw[i] = u, col[p], -ww[p]
+    ds[40:44], dd[40:44] = ds[39], dd[39]
+    ds[50], dd[50], dw[50] = 7, 7, 2.5
+    delta_n = n + 10
+    ref = g.apply_delta(ds.astype(np.uint32), dd.astype(np.uint32), dw, delta_n=delta_n)
+    ro, rc, rw = ref.csr()
+    eo, ec, ew = apply_delta(off, col, ww, n, ds, dd, dw, delta_n)
+    assert np.array_equal(ro, eo) and np.array_equal(rc, ec)
+    assert np.array_equal(rw.view(np.uint64), ew.view(np.uint64))
