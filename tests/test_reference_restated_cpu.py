@@ -1,8 +1,9 @@
 """The throughput best-move evaluation (parallel_frontier.rs:150-230), the
-decoupled move selection (throughput.rs:204-236) and apply_delta
-(in_memory.rs:103-137) restated a second time, in plain Python straight from
-the reference, and compared bit for bit with the oracle's `move_eval`,
-`select_decoupled` and `Graph.apply_delta` on random inputs.  The GPU's evaluation
+decoupled move selection (throughput.rs:204-236), apply_delta
+(in_memory.rs:103-137) and inc_aggregation (hit_leiden.rs:1639-1731)
+restated a second time, in plain Python straight from the reference, and
+compared bit for bit with the oracle's `move_eval`, `select_decoupled`,
+`Graph.apply_delta` and `inc_aggregation` on random inputs.  The GPU's evaluation
 kernels are compared with the oracle in test_gpu_parity.py, so this pins the
 two restatements to each other.
 
@@ -169,3 +170,66 @@ def test_apply_delta_matches_restatement(seed, integral):
     eo, ec, ew = apply_delta(off, col, ww, n, ds, dd, dw, delta_n)
     assert np.array_equal(ro, eo) and np.array_equal(rc, ec)
     assert np.array_equal(rw.view(np.uint64), ew.view(np.uint64))
+
+
+def inc_aggregation(off, col, w, ds, dd, dw, s_pre, s_cur, refined):
+    """hit_leiden.rs:1639-1731: ΔG lifted through s_pre; for each refined v
+    (ascending) every neighbour j != v with s_cur(j) = s_pre(j) or v < j moves
+    its weight from (s_pre v, s_pre j) to (s_cur v, s_cur j); v's self-loop
+    weight (both stored copies) moves likewise if above 1e-12; s_pre <- s_cur
+    on the refined nodes; records summed per (min, max) key in push order and
+    kept if |w| > 1e-9; node count max(s_cur, s_pre) + 1."""
+    recs = [(int(s_pre[a]), int(s_pre[b]), float(x)) for a, b, x in zip(ds, dd, dw)]
+    for v in np.flatnonzero(refined):
+        v = int(v)
+        loop = 0.0
+        for p in range(int(off[v]), int(off[v + 1])):
+            j = int(col[p])
+            if j == v:
+                loop += float(w[p])
+                continue
+            if s_cur[j] == s_pre[j] or v < j:
+                recs.append((int(s_pre[v]), int(s_pre[j]), -float(w[p])))
+                recs.append((int(s_cur[v]), int(s_cur[j]), float(w[p])))
+        if abs(loop) > 1e-12:
+            recs.append((int(s_pre[v]), int(s_pre[v]), -loop))
+            recs.append((int(s_cur[v]), int(s_cur[v]), loop))
+    nsp = np.array(s_pre, np.uint32)
+    nsp[refined.astype(bool)] = np.asarray(s_cur, np.uint32)[refined.astype(bool)]
+    comp = {}
+    for a, b, x in recs:
+        key = (min(a, b), max(a, b))
+        comp[key] = comp.get(key, 0.0) + x
+    out = sorted((k, x) for k, x in comp.items() if abs(x) > 1e-9)
+    nn = max(int(np.max(s_cur)), int(np.max(s_pre))) + 1
+    return out, nsp, nn
+
+
+@pytest.mark.parametrize("seed", range(5))
+@pytest.mark.parametrize("integral", [True, False])
+def test_inc_aggregation_matches_restatement(seed, integral):
+    rng = np.random.default_rng(300 + seed)
+    n, m = 150, 700
+    s = rng.integers(0, n, m)
+    t = rng.integers(0, n, m)
+    s[:8] = t[:8]  # self-loops of the level's nodes
+    w = rng.integers(1, 4, m).astype(float) if integral else rng.uniform(0.5, 2.0, m)
+    g = O.Graph.from_edges(n, s.astype(np.uint32), t.astype(np.uint32), w)
+    g = g.apply_delta([], [], [], keep_self_loops=True)
+    off, col, ww = g.csr()
+    s_pre = rng.integers(0, 40, n).astype(np.uint32)
+    refined = (rng.random(n) < 0.3).astype(np.uint8)
+    s_cur = s_pre.copy()
+    moved = refined.astype(bool) & (rng.random(n) < 0.7)
+    s_cur[moved] = rng.integers(0, 60, int(moved.sum())).astype(np.uint32)
+    k = 40
+    ds = rng.integers(0, n, k).astype(np.uint32)
+    dd = rng.integers(0, n, k).astype(np.uint32)
+    dw = rng.integers(-2, 3, k).astype(float) if integral else rng.uniform(-2.0, 2.0, k)
+    (u, v, x), nsp, nn = O.inc_aggregation(g, ds, dd, dw, s_pre, s_cur, refined)
+    want, wsp, wnn = inc_aggregation(off, col, ww, ds, dd, dw, s_pre, s_cur, refined)
+    got = sorted(((int(a), int(b)), float(c)) for a, b, c in zip(u, v, x))
+    assert [k_ for k_, _ in got] == [k_ for k_, _ in want]
+    assert all(np.float64(a).view(np.uint64) == np.float64(b).view(np.uint64)
+               for (_, a), (_, b) in zip(got, want))
+    assert np.array_equal(nsp, wsp) and nn == wnn
