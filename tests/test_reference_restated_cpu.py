@@ -1,9 +1,10 @@
 """The throughput best-move evaluation (parallel_frontier.rs:150-230), the
-decoupled move selection (throughput.rs:204-236), apply_delta
-(in_memory.rs:103-137) and inc_aggregation (hit_leiden.rs:1639-1731)
-restated a second time, in plain Python straight from the reference, and
-compared bit for bit with the oracle's `move_eval`, `select_decoupled`,
-`Graph.apply_delta` and `inc_aggregation` on random inputs.  The GPU's evaluation
+decoupled move selection (throughput.rs:204-236), the throughput movement
+loop around them (hit_leiden.rs:1024-1101, throughput.rs:80-202),
+apply_delta (in_memory.rs:103-137) and inc_aggregation
+(hit_leiden.rs:1639-1731) restated a second time, in plain Python straight
+from the reference, and compared bit for bit with the oracle on random
+inputs.  The GPU's evaluation
 kernels are compared with the oracle in test_gpu_parity.py, so this pins the
 two restatements to each other.
 
@@ -233,3 +234,99 @@ def test_inc_aggregation_matches_restatement(seed, integral):
     assert all(np.float64(a).view(np.uint64) == np.float64(b).view(np.uint64)
                for (_, a), (_, b) in zip(got, want))
     assert np.array_equal(nsp, wsp) and nn == wnn
+
+
+def inc_movement(off, col, w, n, ds, dd, dw, f, s, gamma, tw, max_rounds=20):
+    """hit_leiden.rs:1024-1101 with throughput.rs:80-202: A and K marks from
+    the batch (all active for an empty batch); degrees in CSR order and
+    community degrees in node order; then up to 20 Jacobi rounds on a snapshot:
+    evaluate every active vertex, select decoupled moves, stop on a total gain
+    <= 0, apply the moves in selected order, and activate the neighbours of
+    moved vertices outside their new community (K marks for same-s pairs).
+    2m is the oracle's canonical value, passed in."""
+    f = [int(x) for x in f]
+    active = [False] * n
+    changed = [False] * n
+    affected = [False] * n
+    for a, b, x in zip(ds, dd, dw):
+        a, b = int(a), int(b)
+        if x > 0.0 and f[a] != f[b]:
+            active[a] = active[b] = True
+        if x < 0.0 and f[a] == f[b]:
+            active[a] = active[b] = True
+        if s[a] == s[b]:
+            affected[a] = affected[b] = True
+    if len(ds) == 0:
+        active = [True] * n
+    k = [0.0] * n
+    for i in range(n):
+        for p in range(int(off[i]), int(off[i + 1])):
+            k[i] += float(w[p])
+    d = [0.0] * (2 * n + 2)
+    for i in range(n):
+        d[f[i]] += k[i]
+    act = [i for i in range(n) if active[i]]
+    it = 0
+    while act and it < max_rounds:
+        cand = []
+        for v in act:
+            bt, bg = best_move(off, col, w, v, f, d, k, tw, gamma, n)
+            if bg > 0.0:
+                cand.append((v, f[v], bt, k[v], bg))
+        sel_nodes = select_moves([c[0] for c in cand], [c[1] for c in cand],
+                                 [c[2] for c in cand], [c[4] for c in cand])
+        by_node = {c[0]: c for c in cand}
+        sel = [by_node[v] for v in sel_nodes]
+        total = 0.0
+        for c in sel:
+            total += c[4]
+        it += 1
+        if total <= 0.0:
+            break
+        for v, fr, to, kv, _ in sel:
+            f[v] = to
+            d[fr] -= kv
+            d[to] += kv
+            changed[v] = True
+        nxt = [False] * n
+        for v, _, to, _, _ in sel:
+            for p in range(int(off[v]), int(off[v + 1])):
+                j = int(col[p])
+                if f[j] != to:
+                    nxt[j] = True
+                if s[v] == s[j]:
+                    affected[v] = affected[j] = True
+        act = [i for i in range(n) if nxt[i]]
+    return f, changed, affected, it
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("integral", [True, False])
+@pytest.mark.parametrize("empty_batch", [False, True])
+def test_inc_movement_matches_restatement(seed, integral, empty_batch):
+    rng = np.random.default_rng(400 + seed)
+    n, m = 200, 900
+    s = rng.integers(0, n, m)
+    t = rng.integers(0, n, m)
+    s[:5] = t[:5]
+    w = rng.integers(1, 4, m).astype(float) if integral else rng.uniform(0.5, 2.0, m)
+    g = O.Graph.from_edges(n, s.astype(np.uint32), t.astype(np.uint32), w)
+    g = g.apply_delta([], [], [], keep_self_loops=True)
+    off, col, ww = g.csr()
+    tw = g.total_weight() * 2.0
+    f = rng.integers(0, 30, n).astype(np.uint32)
+    sub = f.copy()
+    sub[rng.random(n) < 0.3] += 100  # some sub-communities differ from f
+    if empty_batch:
+        ds = dd = np.zeros(0, np.uint32)
+        dw = np.zeros(0)
+    else:
+        k = 60
+        ds = rng.integers(0, n, k).astype(np.uint32)
+        dd = rng.integers(0, n, k).astype(np.uint32)
+        dw = np.where(rng.random(k) < 0.8, 1.0, -1.0)
+    gf, gch, gaf, git = O.inc_movement(g, ds, dd, dw, f, sub, 1.0, O.MODE_THROUGHPUT,
+                                       compact=False)
+    wf, wch, waf, wit = inc_movement(off, col, ww, n, ds, dd, dw, f, sub, 1.0, tw)
+    assert gf.tolist() == wf and gch.tolist() == wch and gaf.tolist() == waf and git == wit
+    assert any(wch)
