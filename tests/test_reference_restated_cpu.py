@@ -1,10 +1,11 @@
 """The throughput best-move evaluation (parallel_frontier.rs:150-230), the
 decoupled move selection (throughput.rs:204-236), the throughput movement
-loop around them (hit_leiden.rs:1024-1101, throughput.rs:80-202),
-apply_delta (in_memory.rs:103-137) and inc_aggregation
-(hit_leiden.rs:1639-1731) restated a second time, in plain Python straight
-from the reference, and compared bit for bit with the oracle on random
-inputs.  The GPU's evaluation
+loop around them (hit_leiden.rs:1024-1101, throughput.rs:80-202), the
+throughput refinement (hit_leiden.rs:1265-1390, 1554-1637,
+throughput.rs:239-359), apply_delta (in_memory.rs:103-137) and
+inc_aggregation (hit_leiden.rs:1639-1731) restated a second time, in plain
+Python straight from the reference, and compared bit for bit with the oracle
+on random inputs.  The GPU's evaluation
 kernels are compared with the oracle in test_gpu_parity.py, so this pins the
 two restatements to each other.
 
@@ -330,3 +331,166 @@ def test_inc_movement_matches_restatement(seed, integral, empty_batch):
     wf, wch, waf, wit = inc_movement(off, col, ww, n, ds, dd, dw, f, sub, 1.0, tw)
     assert gf.tolist() == wf and gch.tolist() == wch and gaf.tolist() == waf and git == wit
     assert any(wch)
+
+
+def _cc_split(off, col, s, verts, visited):
+    from collections import deque
+    comps = []
+    for st in verts:
+        if visited[st]:
+            continue
+        comp, q = [], deque([st])
+        visited[st] = True
+        while q:
+            v = q.popleft()
+            comp.append(v)
+            sc = s[v]
+            for p in range(int(off[v]), int(off[v + 1])):
+                j = int(col[p])
+                if s[j] == sc and not visited[j]:
+                    visited[j] = True
+                    q.append(j)
+        comps.append(comp)
+    return comps
+
+
+def inc_refinement(off, col, w, n, f, s, affected, gamma, tw, counts=None):
+    """hit_leiden.rs:1265-1390 with the throughput merge
+    (:1554-1637, throughput.rs:239-359): affected sub-communities split into
+    connected components over same-s edges, the largest (the last of equal
+    ones) keeping its id and the others taking fresh ids from max(s) + 1; all
+    refined when s is the identity; refined nodes by degree (stable); the
+    T-filter blocks candidate sub-communities with ΔQ(S→∅) > 1e-9; then every
+    refined singleton picks its best same-community neighbour sub-community on
+    the snapshot and the moves are applied in list order.  The orders the
+    reference leaves to its hash maps are the oracle's canonical ones:
+    sub-communities ascending, candidates in first-encounter order."""
+    f = [int(x) for x in f]
+    s = [int(x) for x in s]
+    refined = [False] * n
+    aff = {s[v] for v in range(n) if affected[v]}
+    groups = {}
+    for i in range(n):
+        if s[i] in aff:
+            groups.setdefault(s[i], []).append(i)
+    nxt = max(s) + 1
+    visited = [False] * n
+    for sc in sorted(groups):
+        verts = groups[sc]
+        comps = _cc_split(off, col, s, verts, visited)
+        for v in verts:
+            visited[v] = False
+        if len(comps) <= 1:
+            continue
+        largest = max(i for i in range(len(comps))
+                      if len(comps[i]) == max(len(c) for c in comps))
+        for i, comp in enumerate(comps):
+            if i == largest:
+                continue
+            for v in comp:
+                s[v] = nxt
+                refined[v] = True
+            nxt += 1
+    if all(s[i] == i for i in range(n)):
+        refined = [True] * n
+    sizes = {}
+    for x in s:
+        sizes[x] = sizes.get(x, 0) + 1
+    k = [0.0] * n
+    for i in range(n):
+        for p in range(int(off[i]), int(off[i + 1])):
+            k[i] += float(w[p])
+    dS = {}
+    for i in range(n):
+        dS[s[i]] = dS.get(s[i], 0.0) + k[i]
+    rs = sorted((i for i in range(n) if refined[i]), key=lambda i: k[i])
+    # T-filter (compute_blocked_subcommunities)
+    cands = set()
+    for v in rs:
+        if sizes[s[v]] != 1:
+            continue
+        for p in range(int(off[v]), int(off[v + 1])):
+            j = int(col[p])
+            if f[j] == f[v] and s[j] != s[v]:
+                cands.add(s[j])
+    dpar = {}
+    for i in range(n):
+        dpar[f[i]] = dpar.get(f[i], 0.0) + k[i]
+    blocked = set()
+    for c in cands:
+        ds = dS.get(c, 0.0)
+        if ds <= 0.0:
+            continue
+        parent = f[next(i for i in range(n) if s[i] == c)]
+        wsp = 0.0
+        for i in range(n):
+            if s[i] != c:
+                continue
+            for p in range(int(off[i]), int(off[i + 1])):
+                if f[int(col[p])] == parent:
+                    wsp += float(w[p])
+        dq = -wsp / tw + gamma * ds * (dpar[parent] - ds) / (tw * tw)
+        if dq > 1e-9:
+            blocked.add(c)
+    # Jacobi merges of refined singletons (try_refinement_move)
+    upd = []
+    for v in rs:
+        if sizes[s[v]] != 1:
+            continue
+        cs, kv = s[v], k[v]
+        nbw, wcur = {}, 0.0
+        for p in range(int(off[v]), int(off[v + 1])):
+            j = int(col[p])
+            if f[j] != f[v]:
+                continue
+            nbw[s[j]] = nbw.get(s[j], 0.0) + float(w[p])
+            if s[j] == cs:
+                wcur += float(w[p])
+        best, bg = cs, 0.0
+        for c, wt in nbw.items():
+            if c == cs or c in blocked:
+                continue
+            g = (wt - wcur) / tw + gamma * kv * (dS.get(cs, 0.0) - kv - dS.get(c, 0.0)) / (tw * tw)
+            if g > bg:
+                best, bg = c, g
+        if bg > 0.0:
+            upd.append((v, cs, best, kv))
+    for v, old, new, kv in upd:
+        s[v] = new
+        dS[old] = dS.get(old, 0.0) - kv
+        dS[new] = dS.get(new, 0.0) + kv
+        sizes[old] -= 1
+        sizes[new] = sizes.get(new, 0) + 1
+    if counts is not None:
+        counts["merges"] = counts.get("merges", 0) + len(upd)
+        counts["blocked"] = counts.get("blocked", 0) + len(blocked)
+    return s, refined
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("integral", [True, False])
+@pytest.mark.parametrize("initial", [False, True])
+def test_inc_refinement_matches_restatement(seed, integral, initial):
+    rng = np.random.default_rng(500 + seed)
+    n, m = 200, 700
+    s_ = rng.integers(0, n, m)
+    t = rng.integers(0, n, m)
+    s_[:5] = t[:5]
+    w = rng.integers(1, 4, m).astype(float) if integral else rng.uniform(0.5, 2.0, m)
+    g = O.Graph.from_edges(n, s_.astype(np.uint32), t.astype(np.uint32), w)
+    g = g.apply_delta([], [], [], keep_self_loops=True)
+    off, col, ww = g.csr()
+    tw = g.total_weight() * 2.0
+    f = rng.integers(0, 12, n).astype(np.uint32)
+    if initial:
+        sub = np.arange(n, dtype=np.uint32)
+    else:
+        sub = (f * 4 + rng.integers(0, 4, n)).astype(np.uint32)
+    affected = (rng.random(n) < 0.4).astype(np.uint8)
+    counts = {}
+    for gamma in (1.0, 0.3):
+        gs, gref = O.inc_refinement(g, f, sub, affected, gamma, O.MODE_THROUGHPUT)
+        ws, wref = inc_refinement(off, col, ww, n, f, sub, affected, gamma, tw, counts)
+        assert gs.tolist() == ws and gref.tolist() == wref, gamma
+        assert any(wref)
+    assert counts["merges"] > 0 and counts["blocked"] > 0, counts
