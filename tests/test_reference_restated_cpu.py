@@ -494,3 +494,55 @@ def test_inc_refinement_matches_restatement(seed, integral, initial):
         assert gs.tolist() == ws and gref.tolist() == wref, gamma
         assert any(wref)
     assert counts["merges"] > 0 and counts["blocked"] > 0, counts
+
+
+def test_hit_leiden_one_level_matches_restatement():
+    # hit_leiden.rs:936-1018 at one level, the state the reference reaches
+    # (state.rs:35-49, an empty graph pushed first as its tests do): per batch
+    # apply_delta, inc_movement, inc_refinement; no aggregation, and def_update
+    # changes nothing with one level.  Community ids >= n are rank-compacted
+    # when movement starts (the oracle's canonical choice where the reference
+    # would index out of bounds).
+    rng = np.random.default_rng(600)
+    n = 150
+    st = O.State(n, levels=1, mode=O.MODE_THROUGHPUT)
+    st.push_empty_graph(n)
+    off = np.zeros(n + 1, np.uint64)
+    col = np.zeros(0, np.uint32)
+    w = np.zeros(0)
+    f = list(range(n))
+    s = list(range(n))
+    edges = set()
+    for b in range(6):
+        k = 120 if b == 0 else 40
+        ds, dd, dw = [], [], []
+        while len(ds) < k:
+            a, c = int(rng.integers(0, n)), int(rng.integers(0, n))
+            key = (min(a, c), max(a, c))
+            if a == c:
+                continue
+            if key in edges and rng.random() < 0.3:
+                ds.append(a), dd.append(c), dw.append(-1.0)  # delete
+                edges.discard(key)
+            elif key not in edges:
+                ds.append(a), dd.append(c), dw.append(float(rng.integers(1, 3)))
+                edges.add(key)
+        ds = np.array(ds, np.uint32)
+        dd = np.array(dd, np.uint32)
+        dw = np.array(dw)
+        st.hit_leiden(ds, dd, dw)
+        off, col, w = apply_delta(off, col, w, n, ds, dd, dw, n)
+        if max(f) >= n:
+            ids = sorted(set(f))
+            f = [ids.index(x) for x in f]
+        kdeg = np.array([w[off[i]:off[i + 1]].sum() if off[i + 1] > off[i] else 0.0
+                         for i in range(n)])
+        tw = O.tree_sum(kdeg)
+        f, _, aff, _ = inc_movement(off, col, w, n, ds, dd, dw, f, s, 1.0, tw)
+        s, _ = inc_refinement(off, col, w, n, f, s, aff, 1.0, tw)
+        go, gc, gw = st.graph(0).csr()
+        assert np.array_equal(go, off) and np.array_equal(gc, col)
+        assert np.array_equal(gw.view(np.uint64), w.view(np.uint64))
+        assert st.get_map(0, O.MAP_F).tolist() == f, b
+        assert st.get_map(0, O.MAP_S_CUR).tolist() == s, b
+    assert len(set(f)) < n
