@@ -5,7 +5,8 @@ throughput refinement (hit_leiden.rs:1265-1390, 1554-1637,
 throughput.rs:239-359), apply_delta (in_memory.rs:103-137) and
 inc_aggregation (hit_leiden.rs:1639-1731) restated a second time, in plain
 Python straight from the reference, and compared bit for bit with the oracle
-on random inputs.  The GPU's evaluation
+on random inputs; and modularity (hit_leiden.rs:121-161) evaluated exactly in
+rationals, which the oracle must meet within 1e-12 relative.  The GPU's evaluation
 kernels are compared with the oracle in test_gpu_parity.py, so this pins the
 two restatements to each other.
 
@@ -546,3 +547,53 @@ def test_hit_leiden_one_level_matches_restatement():
         assert st.get_map(0, O.MAP_F).tolist() == f, b
         assert st.get_map(0, O.MAP_S_CUR).tolist() == s, b
     assert len(set(f)) < n
+
+
+def test_modularity_matches_exact_restatement():
+    # hit_leiden.rs:121-161, Q = (Σ_intra 2w − Σ_C d(C)²/2m) / 2m, evaluated
+    # exactly in rationals from the same f64 inputs.  The reference sums
+    # Σ_C in hash order, so its value is only defined up to rounding; the
+    # oracle (double-double, one final rounding) must lie within 1e-12
+    # relative of the exact value, and so must the reference's own float
+    # formula with its sums in edge and node order.
+    from fractions import Fraction
+    rng = np.random.default_rng(700)
+    for trial in range(6):
+        n, m = 400, 2500
+        s = rng.integers(0, n, m)
+        t = rng.integers(0, n, m)
+        s[:5] = t[:5]
+        w = rng.uniform(0.5, 2.0, m) if trial % 2 else rng.integers(1, 4, m).astype(float)
+        part = rng.integers(0, 15 + 5 * trial, n).astype(np.uint32)
+        deg = [Fraction(0)] * n
+        tot = Fraction(0)
+        intra = Fraction(0)
+        for a, b, x in zip(s.tolist(), t.tolist(), w.tolist()):
+            x = Fraction(x)
+            deg[a] += x
+            deg[b] += x
+            tot += x
+            if part[a] == part[b]:
+                intra += 2 * x
+        tm = 2 * tot
+        dc = {}
+        for i in range(n):
+            dc[int(part[i])] = dc.get(int(part[i]), Fraction(0)) + deg[i]
+        exact = (intra - sum(v * v / tm for v in dc.values())) / tm
+        q = O.modularity_edges(n, s.astype(np.uint32), t.astype(np.uint32), w, part)
+        assert abs(Fraction(q) - exact) <= abs(exact) * Fraction(1, 10**12)
+        # the reference's float expression, sums in edge / node / id order
+        fd = [0.0] * n
+        ft = fi = 0.0
+        for a, b, x in zip(s.tolist(), t.tolist(), w.tolist()):
+            fd[a] += x
+            fd[b] += x
+            ft += x
+            if part[a] == part[b]:
+                fi += x * 2.0
+        ftm = ft * 2.0
+        fc = {}
+        for i in range(n):
+            fc[int(part[i])] = fc.get(int(part[i]), 0.0) + fd[i]
+        fq = (fi - sum(v * v / ftm for v in (fc[c] for c in sorted(fc)))) / ftm
+        assert abs(Fraction(fq) - exact) <= abs(exact) * Fraction(1, 10**12)
