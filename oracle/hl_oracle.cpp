@@ -545,11 +545,17 @@ static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std:
   // Deterministic (sequential Gauss–Seidel): pop the lowest active index
   // (:1109), accumulate Σw per neighbour community *including* self-loops
   // (:1119-1125), strict '>' in first-encounter order, then the empty
-  // community with id `next_empty` (:1104, :1150-1162).
+  // community with id `next_empty` (:1104, :1150-1162).  The reference starts
+  // it at the length of its community-degree array, n (:1060); `d` here is
+  // longer, to hold the throughput path's ids n + v.  An existing id >= n
+  // (a state the reference cannot reach, where it would index out of bounds)
+  // moves the start past it.
   std::set<u32> aset;
   for (u32 i = 0; i < n; ++i)
     if (active[i]) aset.insert(i);
-  size_t next_empty = d.size();
+  size_t next_empty = n;
+  for (u32 x : f)
+    if ((size_t)x >= next_empty) next_empty = (size_t)x + 1;
   std::vector<double> buf(d.size() + 1, 0.0);
   std::vector<u32> order;
   std::vector<uint8_t> seen(d.size() + 1, 0);

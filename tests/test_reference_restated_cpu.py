@@ -597,3 +597,94 @@ def test_modularity_matches_exact_restatement():
             fc[int(part[i])] = fc.get(int(part[i]), 0.0) + fd[i]
         fq = (fi - sum(v * v / ftm for v in (fc[c] for c in sorted(fc)))) / ftm
         assert abs(Fraction(fq) - exact) <= abs(exact) * Fraction(1, 10**12)
+
+
+def inc_movement_deterministic(off, col, w, n, ds, dd, dw, f, s, gamma, tw):
+    """hit_leiden.rs:1024-1066 seeding, then the deterministic loop
+    (:1103-1191): pop the lowest active vertex; neighbour weights per
+    community in CSR order with self-loops counted; strict `>` over the
+    candidates in first-encounter order, then the empty community, whose id
+    starts at the length of the community-degree array, n, and grows past each
+    one used; move, mark B, re-activate neighbours outside the new community,
+    K for same-s pairs."""
+    f = [int(x) for x in f]
+    active = set()
+    changed = [False] * n
+    affected = [False] * n
+    for a, b, x in zip(ds, dd, dw):
+        a, b = int(a), int(b)
+        if (x > 0.0 and f[a] != f[b]) or (x < 0.0 and f[a] == f[b]):
+            active.update((a, b))
+        if s[a] == s[b]:
+            affected[a] = affected[b] = True
+    if len(ds) == 0:
+        active = set(range(n))
+    k = [0.0] * n
+    for i in range(n):
+        for p in range(int(off[i]), int(off[i + 1])):
+            k[i] += float(w[p])
+    d = [0.0] * n
+    for i in range(n):
+        d[f[i]] += k[i]
+    next_empty = len(d)
+    while active:
+        v = min(active)
+        active.discard(v)
+        cur, kv = f[v], k[v]
+        nbw, wcur = {}, 0.0
+        for p in range(int(off[v]), int(off[v + 1])):
+            c = f[int(col[p])]
+            nbw[c] = nbw.get(c, 0.0) + float(w[p])
+            if c == cur:
+                wcur += float(w[p])
+        best, bg = cur, 0.0
+        for c, wt in nbw.items():
+            if c == cur:
+                continue
+            g = (wt - wcur) / tw + gamma * kv * (d[cur] - kv - d[c]) / (tw * tw)
+            if g > bg:
+                best, bg = c, g
+        eg = -wcur / tw + gamma * kv * (d[cur] - kv) / (tw * tw)
+        if eg > bg:
+            best, bg = next_empty, eg
+        if bg <= 0.0:
+            continue
+        if best >= len(d):
+            d += [0.0] * (best + 1 - len(d))
+            next_empty = best + 1
+        f[v] = best
+        changed[v] = True
+        d[cur] -= kv
+        d[best] += kv
+        for p in range(int(off[v]), int(off[v + 1])):
+            j = int(col[p])
+            if f[j] != best:
+                active.add(j)
+            if s[v] == s[j]:
+                affected[v] = affected[j] = True
+    return f, changed, affected
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("gamma", [1.0, 3.0])
+def test_deterministic_movement_matches_restatement(seed, gamma):
+    rng = np.random.default_rng(800 + seed)
+    n, m = 150, 600
+    s_ = rng.integers(0, n, m)
+    t = rng.integers(0, n, m)
+    s_[:5] = t[:5]
+    w = rng.uniform(0.5, 2.0, m)
+    g = O.Graph.from_edges(n, s_.astype(np.uint32), t.astype(np.uint32), w)
+    g = g.apply_delta([], [], [], keep_self_loops=True)
+    off, col, ww = g.csr()
+    tw = g.total_weight() * 2.0
+    f = rng.integers(0, 20, n).astype(np.uint32)
+    sub = f.copy()
+    ds = rng.integers(0, n, 50).astype(np.uint32)
+    dd = rng.integers(0, n, 50).astype(np.uint32)
+    dw = np.where(rng.random(50) < 0.8, 1.0, -1.0)
+    gf, gch, gaf, _ = O.inc_movement(g, ds, dd, dw, f, sub, gamma, O.MODE_DETERMINISTIC,
+                                     compact=False)
+    wf, wch, waf = inc_movement_deterministic(off, col, ww, n, ds, dd, dw, f, sub, gamma, tw)
+    assert gf.tolist() == wf and gch.tolist() == wch and gaf.tolist() == waf
+    assert any(wch)
