@@ -355,18 +355,11 @@ def _cc_split(off, col, s, verts, visited):
     return comps
 
 
-def inc_refinement(off, col, w, n, f, s, affected, gamma, tw, counts=None):
-    """hit_leiden.rs:1265-1390 with the throughput merge
-    (:1554-1637, throughput.rs:239-359): affected sub-communities split into
-    connected components over same-s edges, the largest (the last of equal
-    ones) keeping its id and the others taking fresh ids from max(s) + 1; all
-    refined when s is the identity; refined nodes by degree (stable); the
-    T-filter blocks candidate sub-communities with ΔQ(S→∅) > 1e-9; then every
-    refined singleton picks its best same-community neighbour sub-community on
-    the snapshot and the moves are applied in list order.  The orders the
-    reference leaves to its hash maps are the oracle's canonical ones:
-    sub-communities ascending, candidates in first-encounter order."""
-    f = [int(x) for x in f]
+def _refine_split(off, col, w, n, s, affected):
+    """The splitting half of inc_refinement (hit_leiden.rs:1265-1357), shared
+    by both modes: returns s, the refined flags, sub-community sizes, node
+    degrees, sub-community degrees (node order) and the refined nodes sorted
+    by degree (stable)."""
     s = [int(x) for x in s]
     refined = [False] * n
     aff = {s[v] for v in range(n) if affected[v]}
@@ -405,6 +398,22 @@ def inc_refinement(off, col, w, n, f, s, affected, gamma, tw, counts=None):
     for i in range(n):
         dS[s[i]] = dS.get(s[i], 0.0) + k[i]
     rs = sorted((i for i in range(n) if refined[i]), key=lambda i: k[i])
+    return s, refined, sizes, k, dS, rs
+
+
+def inc_refinement(off, col, w, n, f, s, affected, gamma, tw, counts=None):
+    """hit_leiden.rs:1265-1390 with the throughput merge
+    (:1554-1637, throughput.rs:239-359): affected sub-communities split into
+    connected components over same-s edges, the largest (the last of equal
+    ones) keeping its id and the others taking fresh ids from max(s) + 1; all
+    refined when s is the identity; refined nodes by degree (stable); the
+    T-filter blocks candidate sub-communities with ΔQ(S→∅) > 1e-9; then every
+    refined singleton picks its best same-community neighbour sub-community on
+    the snapshot and the moves are applied in list order.  The orders the
+    reference leaves to its hash maps are the oracle's canonical ones:
+    sub-communities ascending, candidates in first-encounter order."""
+    f = [int(x) for x in f]
+    s, refined, sizes, k, dS, rs = _refine_split(off, col, w, n, s, affected)
     # T-filter (compute_blocked_subcommunities)
     cands = set()
     for v in rs:
@@ -688,3 +697,77 @@ def test_deterministic_movement_matches_restatement(seed, gamma):
     wf, wch, waf = inc_movement_deterministic(off, col, ww, n, ds, dd, dw, f, sub, gamma, tw)
     assert gf.tolist() == wf and gch.tolist() == wch and gaf.tolist() == waf
     assert any(wch)
+
+
+def inc_refinement_deterministic(off, col, w, n, f, s, affected, gamma, tw):
+    """The same splits, then the deterministic merges (hit_leiden.rs:1392-1413,
+    :1419-1511): refined singletons in degree order, one at a time on the live
+    state; candidates are same-community neighbour sub-communities in
+    first-encounter order, skipped by the live T-filter (:1514-1548) with
+    d_parent summed over the node's community in node order and w(S, C) over
+    S's members in node and CSR order."""
+    f = [int(x) for x in f]
+    s, refined, sizes, k, dS, rs = _refine_split(off, col, w, n, s, affected)
+    for v in rs:
+        if sizes[s[v]] != 1:
+            continue
+        cs, kv, pc = s[v], k[v], f[v]
+        nbw, wcur = {}, 0.0
+        for p in range(int(off[v]), int(off[v + 1])):
+            j = int(col[p])
+            if f[j] != pc:
+                continue
+            nbw[s[j]] = nbw.get(s[j], 0.0) + float(w[p])
+            if s[j] == cs:
+                wcur += float(w[p])
+        dpar = 0.0
+        for i in range(n):
+            if f[i] == pc:
+                dpar += k[i]
+        best, bg = cs, 0.0
+        for c, wt in nbw.items():
+            if c == cs:
+                continue
+            ds = dS.get(c, 0.0)
+            if ds > 0.0:
+                wsp = 0.0
+                for i in range(n):
+                    if s[i] != c:
+                        continue
+                    for p in range(int(off[i]), int(off[i + 1])):
+                        if f[int(col[p])] == pc:
+                            wsp += float(w[p])
+                if -wsp / tw + gamma * ds * (dpar - ds) / (tw * tw) > 1e-9:
+                    continue
+            g = (wt - wcur) / tw + gamma * kv * (dS.get(cs, 0.0) - kv - dS.get(c, 0.0)) / (tw * tw)
+            if g > bg:
+                best, bg = c, g
+        if bg > 0.0:
+            s[v] = best
+            sizes[cs] -= 1
+            sizes[best] = sizes.get(best, 0) + 1
+            dS[cs] = dS.get(cs, 0.0) - kv
+            dS[best] = dS.get(best, 0.0) + kv
+    return s, refined
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("initial", [False, True])
+def test_deterministic_refinement_matches_restatement(seed, initial):
+    rng = np.random.default_rng(900 + seed)
+    n, m = 150, 500
+    s_ = rng.integers(0, n, m)
+    t = rng.integers(0, n, m)
+    s_[:5] = t[:5]
+    w = rng.uniform(0.5, 2.0, m)
+    g = O.Graph.from_edges(n, s_.astype(np.uint32), t.astype(np.uint32), w)
+    g = g.apply_delta([], [], [], keep_self_loops=True)
+    off, col, ww = g.csr()
+    tw = g.total_weight() * 2.0
+    f = rng.integers(0, 10, n).astype(np.uint32)
+    sub = np.arange(n, dtype=np.uint32) if initial else (f * 4 + rng.integers(0, 4, n)).astype(np.uint32)
+    affected = (rng.random(n) < 0.4).astype(np.uint8)
+    for gamma in (1.0, 0.3):
+        gs, gref = O.inc_refinement(g, f, sub, affected, gamma, O.MODE_DETERMINISTIC)
+        ws, wref = inc_refinement_deterministic(off, col, ww, n, f, sub, affected, gamma, tw)
+        assert gs.tolist() == ws and gref.tolist() == wref, gamma
