@@ -65,3 +65,36 @@ def test_graph_input_arrays():
     assert s.tolist() == [0, 2] and d.tolist() == [1, 3] and w.tolist() == [1.0, 2.5]
     s, d, w = hl.GraphInput("t", 4, [(0, 1, None)]).arrays()
     assert w is None
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    # the ctypes mirrors must have the C header's sizes and field offsets:
+    # a small C program compiled against include/hl.h prints them
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    L = importlib.import_module("hit-leiden_b200._lib")
+    structs = {"hl_config": L.Config, "hl_batch_stats": L.BatchStats,
+               "hl_request_done": L.RequestDone, "hl_kernel_stat": L.KernelStat}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hl.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            parts = line.split()
+            got[(parts[0], parts[1])] = int(parts[2])
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
