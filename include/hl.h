@@ -127,7 +127,12 @@ HL_API hl_status hl_create_device(const hl_config* cfg, uint32_t n, const uint32
 /* Apply one edge-update batch (GraphInput delta encoding, types.rs:133-147:
  * positive weight adds or strengthens, negative weakens or deletes; an edge
  * whose weight falls to <= 1e-12 is removed) and update the partition.
- * w == NULL means all weights are +1.0.  stats may be NULL. */
+ * w == NULL means all weights are +1.0.  stats may be NULL.
+ * A batch with an endpoint >= the node count is rejected with
+ * HL_ERR_INVALID_INPUT before anything changes; the handle stays usable.
+ * HL_ERR_OUT_OF_MEMORY or HL_ERR_CUDA from inside the update can leave some
+ * levels updated and others not: the handle's state is then unspecified, and
+ * the caller destroys it and loads the graph again. */
 HL_API hl_status hl_apply_batch(hl_graph* g, const uint32_t* src, const uint32_t* dst, const double* w,
                          uint64_t k, hl_batch_stats* stats);
 
@@ -203,6 +208,10 @@ HL_API hl_status hl_apply_batches(hl_graph* const* graphs, const uint32_t* const
  *     admitted for a graph while it is busy are coalesced into its next batch,
  *     in arrival order; a graph's batches are applied one after another.
  *   - Each request completes with an hl_request_done record (hl_server_poll).
+ *   - A failed batch leaves its graph as hl_apply_batch would, and the
+ *     server keeps applying later requests to it.  After HL_ERR_OUT_OF_MEMORY
+ *     or HL_ERR_CUDA in a record the caller drains the server, destroys it
+ *     and reloads that graph.
  * The server does not own the graph handles: destroy it before them. */
 typedef struct hl_server hl_server;
 typedef struct {
