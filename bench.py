@@ -91,6 +91,14 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample-batches", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-variants", action="store_true",
+                    help="reference arm: also time the faithful CPU variants (the "
+                         "reference's quadratic refinement scans; throughput on all host "
+                         "threads and deterministic on one), one batch each under --cpu-cap")
+    ap.add_argument("--cpu-cap", type=float, default=120.0,
+                    help="wall-clock cap in seconds for each faithful variant's batch")
+    ap.add_argument("--cpu-variant-run", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-variant-mode", default="throughput", help=argparse.SUPPRESS)
     ap.add_argument("--ncu-small", action="store_true",
                     help="small case for ncu captures (200k vertices)")
     ap.add_argument("--workers", type=int, default=16,
@@ -244,6 +252,70 @@ def cpu_baseline(st, batches, levels_cfg, max_batches):
             "threads": O.num_threads()}
 
 
+def _oracle_levels(st):
+    """Per-level CSR and maps of an oracle state (the form import_levels takes)."""
+    from oracle import oracle as O
+    levels = []
+    for p in range(st.levels):
+        off, col, w = st.graph(p).csr()
+        levels.append({"off": off, "col": col, "w": w, "f": st.get_map(p, O.MAP_F),
+                       "g": st.get_map(p, O.MAP_G), "s_pre": st.get_map(p, O.MAP_S_PRE),
+                       "s_cur": st.get_map(p, O.MAP_S_CUR)})
+    return levels
+
+
+def run_cpu_variant(args):
+    """One faithful variant on one batch, from a state saved by the reference
+    arm: import it with the reference's quadratic refinement scans, time the
+    batch, print a JSON line."""
+    from oracle import oracle as O
+    O.load()
+    z = np.load(args.cpu_variant_run)
+    P = int(z["levels"])
+    levels = [{k: z[f"{k}{p}"] for k in ("off", "col", "w", "f", "g", "s_pre", "s_cur")}
+              for p in range(P)]
+    det = args.cpu_variant_mode == "deterministic"
+    if det:
+        O.set_num_threads(1)
+    flags = O.FLAG_FAITHFUL_SCANS | (O.FLAG_MULTILEVEL if P > 1 else 0)
+    st = O.State(len(levels[0]["f"]), levels=1,
+                 mode=O.MODE_DETERMINISTIC if det else O.MODE_THROUGHPUT)
+    st.import_levels(levels, flags=flags)
+    t0 = time.perf_counter()
+    st.hit_leiden(z["u"], z["v"], z["w_batch"])
+    t = time.perf_counter() - t0
+    print(json.dumps({"seconds": t, "threads": O.num_threads(),
+                      "modularity": st.modularity(0)}), flush=True)
+
+
+def _time_variants(st, batch, k, cap):
+    """Save the bootstrapped state and the batch, then run each faithful variant
+    in a child process killed at `cap` seconds (plus a little for loading)."""
+    out = {}
+    u, v, ww = batch
+    with tempfile.TemporaryDirectory() as td:
+        levels = _oracle_levels(st)
+        arrays = {"levels": len(levels), "u": u, "v": v, "w_batch": ww}
+        for p, lv in enumerate(levels):
+            arrays.update({f"{kk}{p}": a for kk, a in lv.items()})
+        path = os.path.join(td, "state.npz")
+        np.savez(path, **arrays)
+        del levels, arrays
+        for name, det in (("faithful_throughput", False), ("faithful_deterministic", True)):
+            cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                   "--cpu-variant-run", path,
+                   "--cpu-variant-mode", "deterministic" if det else "throughput"]
+            try:
+                r = subprocess.run(cmd, capture_output=True, text=True, timeout=cap + 30.0)
+                res = json.loads(r.stdout.strip().splitlines()[-1])
+                out[name] = {"value": k / res["seconds"], "unit": "edge-updates/s",
+                             "seconds": res["seconds"], "cores": res["threads"],
+                             "modularity": res["modularity"]}
+            except subprocess.TimeoutExpired:
+                out[name] = {"dnf_after_s": cap, "cores": 1 if det else None}
+    return out
+
+
 def run_reference(args, cfg):
     """CPU port of the reference path alone (bootstrap untimed, then K batches)."""
     from oracle import oracle as O
@@ -260,12 +332,20 @@ def run_reference(args, cfg):
         st = O.State(n, levels=1, mode=O.MODE_THROUGHPUT)
         st.push_empty_graph()
         st.hit_leiden(s, d, w)
+    variants = _time_variants(st, batches[warm], k, args.cpu_cap) if args.cpu_variants else None
     t = 0.0
+    q_first = None
     for (u, v, ww) in batches[warm:]:
         t0 = time.perf_counter()
         st.hit_leiden(u, v, ww)
         t += time.perf_counter() - t0
+        if q_first is None:
+            q_first = st.modularity(0)
     val = steps * k / t
+    if variants and "modularity" in variants["faithful_throughput"]:
+        # the faithful scans change the cost, not the result
+        variants["faithful_throughput"]["same_result"] = (
+            variants["faithful_throughput"]["modularity"] == q_first)
     line = {
         "impl": "reference", "metric": "edge_updates_per_s", "value": val,
         "unit": "edge-updates/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
@@ -280,6 +360,8 @@ def run_reference(args, cfg):
                 "d2h_bytes_per_step": 0},
         "modularity": st.modularity(0),
     }
+    if variants is not None:
+        line["cpu_variants"] = variants
     print(json.dumps(line), flush=True)
 
 
@@ -606,6 +688,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.cpu_variant_run:
+        return run_cpu_variant(args)
     if args.impl == "reference":
         if rank == 0:
             if args.config in ("batch256", "serve32", "rmat25"):
