@@ -94,7 +94,8 @@ def parse():
     ap.add_argument("--cpu-variants", action="store_true",
                     help="reference arm: also time the faithful CPU variants (the "
                          "reference's quadratic refinement scans; throughput on all host "
-                         "threads and deterministic on one), one batch each under --cpu-cap")
+                         "threads and deterministic on one) and a from-scratch run() on "
+                         "the updated graph, one batch each under --cpu-cap")
     ap.add_argument("--cpu-cap", type=float, default=120.0,
                     help="wall-clock cap in seconds for each faithful variant's batch")
     ap.add_argument("--cpu-variant-run", default=None, help=argparse.SUPPRESS)
@@ -274,6 +275,22 @@ def run_cpu_variant(args):
     P = int(z["levels"])
     levels = [{k: z[f"{k}{p}"] for k in ("off", "col", "w", "f", "g", "s_pre", "s_cur")}
               for p in range(P)]
+    if args.cpu_variant_mode == "run":
+        # the reference benchmark's own operation: a from-scratch run() on the
+        # graph after the batch (hit_leiden.rs:30-118)
+        off, col, w = z["off0"], z["col0"], z["w0"]
+        n = len(off) - 1
+        rows = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off).astype(np.int64))
+        keep = rows < col
+        g = O.Graph.from_edges(n, rows[keep], col[keep], w[keep])
+        off2, col2, w2 = g.apply_delta(z["u"], z["v"], z["w_batch"]).csr()
+        rows2 = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off2).astype(np.int64))
+        keep2 = rows2 < col2
+        t0 = time.perf_counter()
+        _, q, _ = O.run(n, rows2[keep2], col2[keep2], w2[keep2])
+        t = time.perf_counter() - t0
+        print(json.dumps({"seconds": t, "threads": 1, "modularity": q}), flush=True)
+        return
     det = args.cpu_variant_mode == "deterministic"
     if det:
         O.set_num_threads(1)
@@ -301,10 +318,12 @@ def _time_variants(st, batch, k, cap):
         path = os.path.join(td, "state.npz")
         np.savez(path, **arrays)
         del levels, arrays
-        for name, det in (("faithful_throughput", False), ("faithful_deterministic", True)):
+        for name, mode in (("faithful_throughput", "throughput"),
+                           ("faithful_deterministic", "deterministic"),
+                           ("static_run_per_batch", "run")):
+            det = mode != "throughput"
             cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                   "--cpu-variant-run", path,
-                   "--cpu-variant-mode", "deterministic" if det else "throughput"]
+                   "--cpu-variant-run", path, "--cpu-variant-mode", mode]
             try:
                 r = subprocess.run(cmd, capture_output=True, text=True, timeout=cap + 30.0)
                 res = json.loads(r.stdout.strip().splitlines()[-1])

@@ -1,7 +1,8 @@
 """bench.py's reference arm runs on the CPU alone: its JSON line (the
 contract's keys, `impl: reference`, the CPU baseline it describes) and the
 faithful variants (the reference's quadratic refinement scans on all host
-threads, and the deterministic mode on one), on the small configuration."""
+threads, and the deterministic mode on one) with the reference benchmark's
+from-scratch run() per batch, on the small configuration."""
 import json
 import os
 import subprocess
@@ -35,6 +36,7 @@ def test_reference_arm_line():
 def test_reference_arm_faithful_variants():
     d = _run("--cpu-variants", "--cpu-cap", "120")
     v = d["cpu_variants"]
-    ft, fd = v["faithful_throughput"], v["faithful_deterministic"]
+    ft, fd, sr = v["faithful_throughput"], v["faithful_deterministic"], v["static_run_per_batch"]
     assert ft["value"] > 0 and ft["same_result"] is True
     assert fd["value"] > 0 and fd["cores"] == 1
+    assert sr["value"] > 0 and 0.0 < sr["modularity"] < 1.0
