@@ -404,19 +404,9 @@ __global__ void k_row_ranges(const u64* rkeys, u64 R, u32* rstart, u32* rend) {
   }
 }
 
-// Touched rows, merged with their sorted row-operations, so the output row is
-// again sorted by neighbour id: deleted entries are skipped, every surviving
-// entry moves by (inserts before it) - (deletes before it), and an insert
-// lands at its lower bound in the old row, after the earlier inserts and
-// before the entries it precedes.  A warp per row walks the old row in
-// chunks of 32 and consumes, per chunk, the operations whose neighbour is not
-// above the chunk's last one (all of them in the last chunk), 32 operations at
-// a time with bisections over lanes, so the row and its operations are each
-// read once and no step is serial in the number of operations.  A self-loop is stored twice in its row
-// and its operations come in pairs; operations on one neighbour come deletes
-// first (a dropped self-loop replaced by an inserted one).
 // Merge of the row slice [s0, s1) (chunks of 32 from the row start o0) of a
-// touched row, by one warp.  The state on entry is that of the operations
+// touched row, by one warp (the row merge itself is described at
+// k_merge_rows).  The state on entry is that of the operations
 // consumed before the slice: p = first operation not consumed, drun / irun =
 // deletes / inserts consumed, del_key / del_same = neighbour of the last
 // consumed delete and the consumed deletes on it.  `row_end` marks the row's
