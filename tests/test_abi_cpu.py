@@ -98,3 +98,13 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_graph_input_widens_f32_weights_exactly():
+    import numpy as np
+    hl = importlib.import_module("hit-leiden_b200")
+    w32 = np.array([0.1, 1.5, 3.25, 1e-7], np.float32)
+    g = hl.GraphInput.from_arrays("t", 5, [0, 1, 2, 3], [1, 2, 3, 4], w32)
+    src, dst, w = g.arrays()
+    assert w.dtype == np.float64 and np.array_equal(w, w32.astype(np.float64))
+    assert src.dtype == np.uint32 and dst.dtype == np.uint32
