@@ -1,7 +1,10 @@
 // api.cu — host orchestration (Algorithm 6 level loop, bootstrap) and the
 // C ABI declared in include/hl.h and include/hl_debug.h.
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 
@@ -192,6 +195,15 @@ static u32 count_flags(Engine& E, const u8* f, u32 n) {
 }
 
 // Algorithm 6 (hit_leiden.rs:936-1018) for one batch already on the device.
+// NVTX range for the scope (a level, a stage), so that profilers can select
+// one level's kernels; a no-op unless a tool is attached.
+struct NvtxScope {
+  explicit NvtxScope(const char* name) { nvtxRangePushA(name); }
+  ~NvtxScope() { nvtxRangePop(); }
+  NvtxScope(const NvtxScope&) = delete;
+  NvtxScope& operator=(const NvtxScope&) = delete;
+};
+
 static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
   Engine& E = *B.E;
   hl_batch_stats& st = E.st;
@@ -216,16 +228,30 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
   DevEdges cur = delta;
   u32 cur_n = E.levels[0].g.n;
   for (u32 p = 0; p < P; ++p) {
+    char level_name[24];
+    std::snprintf(level_name, sizeof(level_name), "level%u", p);
+    NvtxScope level_range(level_name);
     Level& L = E.levels[p];
     cudaEvent_t e0 = E.kt_begin();
-    apply_delta(E, L, cur, cur_n > L.g.n ? cur_n : L.g.n, true);
+    {
+      NvtxScope r("apply");
+      apply_delta(E, L, cur, cur_n > L.g.n ? cur_n : L.g.n, true);
+    }
     E.kt_end(KT_STAGE_APPLY, e0);
     e0 = E.kt_begin();
-    MoveOut mo = inc_movement(E, L, cur, cur.k == 0, true);
+    MoveOut mo;
+    {
+      NvtxScope r("move");
+      mo = inc_movement(E, L, cur, cur.k == 0, true);
+    }
     E.kt_end(KT_STAGE_MOVE, e0);
     if (p == 0) st.changed = count_flags(E, E.sc.changed.p, L.g.n);
     e0 = E.kt_begin();
-    RefineOut ro = inc_refinement(E, L, true);
+    RefineOut ro;
+    {
+      NvtxScope r("refine");
+      ro = inc_refinement(E, L, true);
+    }
     E.kt_end(KT_STAGE_REFINE, e0);
     st.iterations += mo.iterations;
     st.moves += mo.moves;
@@ -257,7 +283,11 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
     }
     u32 nn = 0;
     e0 = E.kt_begin();
-    u64 cnt = inc_aggregation(E, L, cur, &nn, true, true);
+    u64 cnt;
+    {
+      NvtxScope r("aggregate");
+      cnt = inc_aggregation(E, L, cur, &nn, true, true);
+    }
     E.kt_end(KT_STAGE_AGGREGATE, e0);
     int slot = (p + 1) & 1;
     B.bb.xu[slot].ensure(E.mem, cnt ? cnt : 1);
