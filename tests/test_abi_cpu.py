@@ -108,3 +108,18 @@ def test_graph_input_widens_f32_weights_exactly():
     src, dst, w = g.arrays()
     assert w.dtype == np.float64 and np.array_equal(w, w32.astype(np.float64))
     assert src.dtype == np.uint32 and dst.dtype == np.uint32
+
+
+def test_library_exports_no_undeclared_entry_points():
+    # every hl_* symbol the library exports is declared in include/*.h (the
+    # build hides everything else of its own)
+    import shutil
+    import subprocess
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("no nm")
+    lib = os.path.join(ROOT, "hit-leiden_b200", "libhl.so")
+    out = subprocess.run([nm, "-D", "--defined-only", lib], check=True, capture_output=True,
+                         text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if ln.split()[-1].startswith("hl_")}
+    assert exported == set(declared_symbols())
