@@ -358,7 +358,7 @@ def run_reference(args, cfg):
         t0 = time.perf_counter()
         st.hit_leiden(u, v, ww)
         t += time.perf_counter() - t0
-        if q_first is None:
+        if variants is not None and q_first is None:
             q_first = st.modularity(0)
     val = steps * k / t
     if variants and "modularity" in variants["faithful_throughput"]:
