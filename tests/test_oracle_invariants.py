@@ -84,3 +84,17 @@ def test_invariants_after_bootstrap_and_batches(seed, weights):
         store.apply(u, v, ww)
         st.hit_leiden(u, v, ww)
         _check(st, rel)
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_invariants_under_delete_heavy_batches(seed):
+    # 70 % deletes: communities shrink and split rather than grow
+    n, s, d, w, _ = W.planted(1500, 10.0, 0.2, seed, comm_min=5, comm_max=80)
+    st = O.State(n, mode=O.MODE_THROUGHPUT)
+    st.bootstrap(s, d, w, max_levels=10)
+    store = W.EdgeStore(n, s, d, w)
+    for b in range(5):
+        u, v, ww = W.mixed_batch(store, 300, 0.3, 50 * seed + b, preferential=False)
+        store.apply(u, v, ww)
+        st.hit_leiden(u, v, ww)
+        _check(st, 0)
