@@ -81,7 +81,6 @@ def test_invariants_after_bootstrap_and_batches(seed, weights):
     for b in range(3):
         u, v, ww = W.mixed_batch(store, 150, 0.8, 100 * seed + b, weights=weights,
                                  preferential=False)
-        store.apply(u, v, ww)
         st.hit_leiden(u, v, ww)
         _check(st, rel)
 
@@ -95,6 +94,5 @@ def test_invariants_under_delete_heavy_batches(seed):
     store = W.EdgeStore(n, s, d, w)
     for b in range(5):
         u, v, ww = W.mixed_batch(store, 300, 0.3, 50 * seed + b, preferential=False)
-        store.apply(u, v, ww)
         st.hit_leiden(u, v, ww)
         _check(st, 0)

@@ -438,7 +438,6 @@ def test_results_do_not_depend_on_host_threads():
         store = W.EdgeStore(n, s, d, w)
         for b in range(3):
             u, v, ww = W.mixed_batch(store, 300, 0.9, 50 + b, weights=(0.5, 2.0))
-            store.apply(u, v, ww)
             st.hit_leiden(u, v, ww)
         states.append(st)
     O.set_num_threads(0)
