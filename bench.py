@@ -1,30 +1,34 @@
 #!/usr/bin/env python3
 """Benchmark of the HIT-Leiden incremental update path on B200.
 
-One step = one edge-update batch applied through hl_apply_batch (G ⊕ ΔG, then
-inc-movement, inc-refinement and inc-aggregation on every level, then the
-top-down level maps), on a graph already resident in HBM.
+One step = one edge-update batch applied through the public C ABI
+(hl_apply_batch: G ⊕ ΔG, then inc-movement, inc-refinement and
+inc-aggregation on every level, then the top-down level maps) on a graph
+resident in HBM, followed by a read-back of the level-0 community map.
 
-Default workload (the mid-size plain-method configuration): LFR-style planted
-graph, 1M vertices / ~20M undirected edges, degree exponent 2.5 (mean 40, max
-2000), community sizes exponent 1.5 in [50, 5000], mixing 0.3, f64 weights
-U[0.5, 2.0]; batches of 10k updates (90% degree-preferential inserts, 10%
-uniform deletes of existing edges).  Synthetic, seeded: the reference's
-datasets are not available.
+Default workload (the large plain-method configuration, the one the target
+is stated on): R-MAT scale 25 (33.5M vertices), edge factor 16,
+(a,b,c,d) = (.57,.19,.19,.05), symmetrised, duplicates and self-loops
+removed (~524M undirected edges), unit weights summed in FP64; batches of 1M
+updates (90% R-MAT-sampled inserts, 10% uniform deletes).  Synthetic and
+seeded: the reference's datasets are not available.  `--config lfr1m` runs
+the mid-size configuration (LFR-style, 1M vertices / ~20M f64 edges, 10k
+batches), whose CPU sample also checks full-size bit-exact parity.
 
-Reported:
-  value   edge-updates/s with batches already on the device (hl_apply_batch_device),
-          timed by CUDA events on the library's stream, summed over the K steps;
-  e2e     edge-updates/s through the public host API (hl_apply_batch with
-          batches in pinned host memory, host→device copies inside) plus a
-          device→host read of the level-0 community map into pinned memory
-          every step, timed on the host clock;
-  roofline for the inc-movement evaluation kernel (algorithmic bytes / event time);
+Reported (the same K timed batches give both numbers):
+  value   edge-updates/s from the device time of each batch (CUDA events on
+          the library's stream, from the batch resident in HBM to the end of
+          the update), summed over the K steps, max over ranks;
+  e2e     edge-updates/s on the host clock around the same calls: the
+          host→device copy of the pinned host batch, the update and a
+          device→host read of the level-0 community map into pinned memory;
+  roofline for the inc-movement evaluation kernels (algorithmic bytes / event
+          time), roofline_aggregation for inc-aggregation;
   cpu_baseline: the CPU oracle (a C++ port of the reference's Rust, its
           snapshot evaluations on all host threads as the reference's rayon
-          pool) applying one batch of the same stream from the same state.
+          pool) on a bounded sample (see each configuration).
 
---impl reference runs that CPU port alone on the same configuration.
+--impl reference runs that CPU port alone, never loading libhl.so.
 Multi-GPU (--gpus N under torchrun): independent replicas, one graph per GPU,
 no collective on the data path; the time is the max over ranks.
 """
@@ -45,6 +49,27 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+
+# R-MAT stand-in for the CPU port: the port cannot bootstrap scale 25 (about
+# 1B adjacency entries) within the bench's few-minute bound, so its sample is
+# the same generator at scale 20 with batches scaled by the same factor.
+RMAT_SAMPLE_SCALE = 20
+
+
+def _module(name):
+    """One host-side module of the package, loaded by path without running the
+    package's __init__ (which maps libhl.so): the CPU arms must not load the
+    GPU library."""
+    import importlib.util
+    key = "hl_bench_" + name
+    if key in sys.modules:
+        return sys.modules[key]
+    path = os.path.join(ROOT, "hit-leiden_b200", name + ".py")
+    spec = importlib.util.spec_from_file_location(key, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[key] = mod
+    spec.loader.exec_module(mod)
+    return mod
 
 CONFIGS = {
     "lfr1m": {
@@ -86,10 +111,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=sorted(CONFIGS), default="lfr1m")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="rmat25")
     ap.add_argument("--levels", type=int, default=10)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--cpu-sample-batches", type=int, default=1)
+    ap.add_argument("--cpu-sample-batches", type=int, default=3)
+    ap.add_argument("--cpu-sample-cap", type=float, default=45.0,
+                    help="wall-clock seconds the CPU sample's timed batches may take "
+                         "(at least one batch runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-variants", action="store_true",
                     help="reference arm: also time the faithful CPU variants (the "
@@ -98,6 +126,8 @@ def parse():
                          "the updated graph, one batch each under --cpu-cap")
     ap.add_argument("--cpu-cap", type=float, default=120.0,
                     help="wall-clock cap in seconds for each faithful variant's batch")
+    ap.add_argument("--rmat-sample-scale", type=int, default=RMAT_SAMPLE_SCALE,
+                    help="R-MAT scale of the CPU port's stand-in sample for rmat25")
     ap.add_argument("--cpu-variant-run", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-variant-mode", default="throughput", help=argparse.SUPPRESS)
     ap.add_argument("--ncu-small", action="store_true",
@@ -112,7 +142,7 @@ def parse():
 
 
 def make_graph(cfg_name, seed, small=False):
-    W = importlib.import_module("hit-leiden_b200.workloads")
+    W = _module("workloads")
     if cfg_name == "lfr1m":
         if small:
             n, s, d, w = W.config2(seed, n=200_000)
@@ -124,7 +154,7 @@ def make_graph(cfg_name, seed, small=False):
 
 
 def make_batches(n, s, d, w, weights, insert_frac, preferential, count, k, seed):
-    W = importlib.import_module("hit-leiden_b200.workloads")
+    W = _module("workloads")
     store = W.EdgeStore(n, s, d, w)
     out = []
     for i in range(count):
@@ -224,23 +254,24 @@ def export_state(st):
     return levels
 
 
-def cpu_baseline(st, batches, levels_cfg, max_batches):
-    """Time the oracle port on the next batches from the GPU's state; check that
-    the GPU state after the same batches is identical (full-size parity)."""
+def cpu_baseline(st, batches, max_batches, cap_s):
+    """Time the oracle port on the next batches from the GPU's state (at least
+    one, then more while the timed total stays under cap_s); check that the
+    GPU state after the same batches is identical (full-size parity)."""
     from oracle import oracle as O
     O.load()
     ora = O.State(st.node_count, levels=1, mode=O.MODE_THROUGHPUT)
     ora.import_levels(export_state(st))
-    t_cpu = 0.0
+    per = []
     edges = 0
-    used = 0
     for (u, v, w) in batches[:max_batches]:
         t0 = time.perf_counter()
         ora.hit_leiden(u, v, w)
-        t_cpu += time.perf_counter() - t0
+        per.append(time.perf_counter() - t0)
         edges += len(u)
-        used += 1
         st.apply_batch(u, v, w)
+        if sum(per) >= cap_s:
+            break
     same = st.levels == ora.levels and all(
         np.array_equal(st.community_mapping_per_level[p], ora.get_map(p, O.MAP_F))
         and np.array_equal(st.current_subcommunity_mapping_per_level[p],
@@ -248,9 +279,65 @@ def cpu_baseline(st, batches, levels_cfg, max_batches):
         for p in range(ora.levels))
     q_gpu = st.modularity()
     q_cpu = ora.modularity(0)
-    return {"value": edges / t_cpu, "seconds": t_cpu, "batches": used, "edges": edges,
-            "parity_bit_exact": bool(same), "dq": abs(q_gpu - q_cpu),
+    return {"value": edges / sum(per), "seconds": sum(per), "batches": len(per), "edges": edges,
+            "batch_s": per, "parity_bit_exact": bool(same), "dq": abs(q_gpu - q_cpu),
             "threads": O.num_threads()}
+
+
+def rmat_sample(seed, scale=RMAT_SAMPLE_SCALE):
+    """The CPU port's R-MAT stand-in (scale RMAT_SAMPLE_SCALE, same generator
+    and parameters as the full workload, generated with torch on the host)."""
+    W = _module("workloads")
+    n, s, d = W.rmat_torch(scale, 16, seed, device="cpu")
+    k = 1_000_000 >> (25 - scale)
+
+    def batch(i):
+        u, v, w = W.rmat_batch_torch(scale, s, d, k, 0.9, 10_000 + i)
+        return (u.numpy().view(np.uint32).copy(), v.numpy().view(np.uint32).copy(),
+                w.numpy().copy())
+    return (n, s.numpy().view(np.uint32).copy(), d.numpy().view(np.uint32).copy(), k, batch)
+
+
+def cpu_rmat_sample(seed, levels, warm, max_batches, cap_s, scale=RMAT_SAMPLE_SCALE):
+    """Bootstrap the oracle on the R-MAT stand-in (untimed), apply `warm`
+    batches untimed, then time batches until max_batches or cap_s."""
+    from oracle import oracle as O
+    O.load()
+    n, s, d, k, batch = rmat_sample(seed, scale)
+    st = O.State(n, mode=O.MODE_THROUGHPUT)
+    t0 = time.perf_counter()
+    st.bootstrap(s, d, None, max_levels=levels)
+    boot = time.perf_counter() - t0
+    i = 0
+    for _ in range(warm):
+        st.hit_leiden(*batch(i))
+        i += 1
+    per = []
+    while len(per) < max_batches:
+        b = batch(i)
+        i += 1
+        t0 = time.perf_counter()
+        st.hit_leiden(*b)
+        per.append(time.perf_counter() - t0)
+        if sum(per) >= cap_s:
+            break
+    return {"value": len(per) * k / sum(per), "batches": len(per), "batch_edges": k,
+            "batch_s": per, "bootstrap_s": boot, "warmup": warm, "vertices": n,
+            "edges": int(len(s)), "levels": st.levels, "modularity": st.modularity(0),
+            "threads": O.num_threads(), "scale": scale}
+
+
+def _rmat_sample_text(r):
+    return (f"R-MAT scale {r['scale']} stand-in for scale 25 ({r['vertices']} vertices, "
+            f"{r['edges']} edges, same generator and (a,b,c,d); batches of {r['batch_edges']} "
+            f"= 1M/{1 << (25 - r['scale'])} updates, 90% R-MAT inserts / 10% deletes): "
+            f"untimed bootstrap ({r['bootstrap_s']:.1f} s, {r['levels']} levels) and "
+            f"{r['warmup']} untimed batch(es), then {r['batches']} timed batch(es) "
+            f"(median {statistics.median(r['batch_s']):.2f} s, min {min(r['batch_s']):.2f}, "
+            f"max {max(r['batch_s']):.2f}) on {r['threads']} host threads.  The port cannot "
+            f"bootstrap scale 25 within the bench's bound; its per-update work grows with the "
+            f"graph (apply_delta rewrites every row), so the stand-in overstates the CPU rate "
+            f"at scale 25")
 
 
 def _oracle_levels(st):
@@ -336,50 +423,73 @@ def _time_variants(st, batch, k, cap):
 
 
 def run_reference(args, cfg):
-    """CPU port of the reference path alone (bootstrap untimed, then K batches)."""
+    """CPU port of the reference path alone (libhl.so is never loaded).  It
+    bootstraps untimed, applies --warmup batches untimed and then times up to
+    --steps batches of the same stream, stopping early once --cpu-cap seconds
+    of timed batches have run (at least one runs)."""
     from oracle import oracle as O
     O.load()
-    n, s, d, w, wts, ins, pref = make_graph(args.config, args.seed, args.ncu_small)
-    k = cfg["batch"]
-    steps = max(1, min(args.steps, 2))
-    warm = 0
-    batches = make_batches(n, s, d, w, wts, ins, pref, warm + steps, k, args.seed)
-    st = O.State(n, mode=O.MODE_THROUGHPUT)
-    if args.levels > 1:
-        st.bootstrap(s, d, w, max_levels=args.levels)
+    if args.config == "rmat25":
+        r = cpu_rmat_sample(args.seed, args.levels, min(args.warmup, 1), args.steps,
+                            args.cpu_cap, args.rmat_sample_scale)
+        val = r["value"]
+        steps, warm, k = r["batches"], r["warmup"], r["batch_edges"]
+        ms = 1000.0 * sum(r["batch_s"]) / steps
+        sample = _rmat_sample_text(r)
+        q, levels = r["modularity"], r["levels"]
+        config = {"workload": cfg["workload"], "scale": 25, "batch_edges": cfg["batch"]}
     else:
-        st = O.State(n, levels=1, mode=O.MODE_THROUGHPUT)
-        st.push_empty_graph()
-        st.hit_leiden(s, d, w)
-    variants = _time_variants(st, batches[warm], k, args.cpu_cap) if args.cpu_variants else None
-    t = 0.0
-    q_first = None
-    for (u, v, ww) in batches[warm:]:
-        t0 = time.perf_counter()
-        st.hit_leiden(u, v, ww)
-        t += time.perf_counter() - t0
-        if variants is not None and q_first is None:
-            q_first = st.modularity(0)
-    val = steps * k / t
-    if variants and "modularity" in variants["faithful_throughput"]:
-        # the faithful scans change the cost, not the result
-        variants["faithful_throughput"]["same_result"] = (
-            variants["faithful_throughput"]["modularity"] == q_first)
+        n, s, d, w, wts, ins, pref = make_graph(args.config, args.seed, args.ncu_small)
+        k = cfg["batch"]
+        batches = make_batches(n, s, d, w, wts, ins, pref, args.warmup + args.steps, k,
+                               args.seed)
+        st = O.State(n, mode=O.MODE_THROUGHPUT)
+        if args.levels > 1:
+            st.bootstrap(s, d, w, max_levels=args.levels)
+        else:
+            st = O.State(n, levels=1, mode=O.MODE_THROUGHPUT)
+            st.push_empty_graph()
+            st.hit_leiden(s, d, w)
+        for (u, v, ww) in batches[:args.warmup]:
+            st.hit_leiden(u, v, ww)
+        variants = (_time_variants(st, batches[args.warmup], k, args.cpu_cap)
+                    if args.cpu_variants else None)
+        per = []
+        q_first = None
+        for (u, v, ww) in batches[args.warmup:]:
+            t0 = time.perf_counter()
+            st.hit_leiden(u, v, ww)
+            per.append(time.perf_counter() - t0)
+            if variants is not None and q_first is None:
+                q_first = st.modularity(0)
+            if sum(per) >= args.cpu_cap:
+                break
+        steps, warm = len(per), args.warmup
+        val = steps * k / sum(per)
+        ms = 1000.0 * sum(per) / steps
+        sample = (f"batches {warm}..{warm + steps - 1} of the stream ({k} updates each) after "
+                  f"an untimed bootstrap and {warm} untimed batches, the same batch indices the "
+                  f"GPU arm times first (median {statistics.median(per):.2f} s a batch; "
+                  "snapshot evaluations on all host threads, up to 64)")
+        q, levels = st.modularity(0), st.levels
+        config = {"workload": cfg["workload"], "vertices": n, "edges": int(len(s)),
+                  "batch_edges": k}
+        if variants is not None and "modularity" in variants["faithful_throughput"]:
+            # the faithful scans change the cost, not the result
+            variants["faithful_throughput"]["same_result"] = (
+                variants["faithful_throughput"]["modularity"] == q_first)
     line = {
         "impl": "reference", "metric": "edge_updates_per_s", "value": val,
-        "unit": "edge-updates/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * t / steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "levels": st.levels, "batch_edges": k},
+        "unit": "edge-updates/s", "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
         "cpu_baseline": {"value": val, "unit": "edge-updates/s", "cores": O.num_threads(),
-                         "kind": "port",
-                         "sample": f"{steps} batches of {k} updates after an untimed bootstrap "
-                                   "(snapshot evaluations on all host threads, up to 64)"},
+                         "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": "edge-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "modularity": st.modularity(0),
+        "modularity": q, "levels": levels,
     }
-    if variants is not None:
+    if args.config != "rmat25" and variants is not None:
         line["cpu_variants"] = variants
     print(json.dumps(line), flush=True)
 
@@ -403,7 +513,7 @@ def run_batching(args, cfg):
     host arrays, host clock with the device synchronised on both sides."""
     import torch
     R = importlib.import_module("hit-leiden_b200.replicas")
-    W = importlib.import_module("hit-leiden_b200.workloads")
+    W = _module("workloads")
     rep = R.Replicas("nccl")
     torch.cuda.set_device(rep.local)
     hl = importlib.import_module("hit-leiden_b200")
@@ -503,7 +613,7 @@ def run_serving(args, cfg):
     workers, admission against 120 GB) against the plain per-request GPU path
     (one request per batch, one at a time), on identical graph copies."""
     import torch
-    W = importlib.import_module("hit-leiden_b200.workloads")
+    W = _module("workloads")
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -576,13 +686,106 @@ def _device_bytes(L, h):
     return {"used": used.value, "peak": peak.value}
 
 
+def _pinned(batches):
+    """Batches as pinned host tensors (u32 viewed as int32, f64)."""
+    import torch
+    out = []
+    for (u, v, w) in batches:
+        if isinstance(u, np.ndarray):
+            tu = torch.from_numpy(np.ascontiguousarray(u).view(np.int32))
+            tv = torch.from_numpy(np.ascontiguousarray(v).view(np.int32))
+            tw = torch.from_numpy(np.ascontiguousarray(w))
+        else:
+            tu, tv, tw = u, v, w
+        out.append(tuple(torch.empty(t.shape, dtype=t.dtype, pin_memory=True).copy_(t)
+                         for t in (tu, tv, tw)))
+    return out
+
+
+def _timed_steps(L, h, pinned, n, rep, clocks):
+    """The K timed steps, each through the public host API: hl_apply_batch on
+    a pinned host batch (its host→device copy inside), then hl_get_map of the
+    level-0 communities into pinned host memory.  A barrier and a device
+    synchronise bracket the K steps.  Returns per-step device ms (CUDA events
+    on the library's stream, from the batch resident in HBM), per-step host
+    seconds, launches and traversed entries."""
+    import torch
+    comm = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    stats = L.BatchStats()
+    dev_ms, host_s, launches, traversed = [], [], 0, 0
+    clocks.start()
+    rep.barrier()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("hl_timed")
+    for (pu, pv, pw) in pinned:
+        t1 = time.perf_counter()
+        L.check(L.lib.hl_apply_batch(h, C.c_void_p(pu.data_ptr()), C.c_void_p(pv.data_ptr()),
+                                     C.c_void_p(pw.data_ptr()), pu.numel(), C.byref(stats)))
+        L.check(L.lib.hl_get_map(h, 0, L.HL_MAP_COMMUNITY, C.c_void_p(comm.data_ptr())))
+        host_s.append(time.perf_counter() - t1)
+        dev_ms.append(stats.device_ms)
+        launches += stats.launches
+        traversed += stats.traversed
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    rep.barrier()
+    return dev_ms, host_s, launches, traversed, clocks.stop()
+
+
+def _kernel_table(L, h):
+    kst = (L.KernelStat * 32)()
+    cnt = C.c_uint32()
+    L.check(L.lib.hl_kernel_stats(h, kst, 32, C.byref(cnt)))
+    return {kst[i].name.decode(): {"launches": kst[i].launches, "ms": kst[i].total_ms,
+                                   "bytes": kst[i].bytes, "items": kst[i].items}
+            for i in range(cnt.value)}
+
+
+def _bench_line(rep, cfg_workload, config, K, Wm, k, n, dev_ms, host_s, launches, traversed,
+                kernels, clk, roof_traffic):
+    tot_ms = rep.max_over_ranks(float(sum(dev_ms)))
+    tot_host = rep.max_over_ranks(float(sum(host_s)))
+    value = rep.whole_job_rate(K, k, tot_ms / 1000.0)
+    e2e_val = rep.whole_job_rate(K, k, tot_host)
+    lat = sorted(1000.0 * x for x in host_s)
+    dlat = sorted(dev_ms)
+    peak, peak_kind = measured_peak()
+    roof = _roof(kernels, "move_eval", "k_eval_* <EVAL_MOVE> (inc-movement best-move evaluation, "
+                 "all degree bins)", peak, peak_kind)
+    if roof is not None and roof_traffic:
+        roof["traffic"] = roof["bytes_per_launch"] * roof_traffic
+    mv = kernels.get("stage_move", {})
+    return {
+        "metric": "edge_updates_per_s", "value": value, "unit": "edge-updates/s",
+        "n_gpus": rep.world, "steps": K, "warmup": Wm, "ms_per_step": tot_ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config,
+        "e2e": {"value": e2e_val, "unit": "edge-updates/s",
+                "h2d_bytes_per_step": int(k * (4 + 4 + 8)), "d2h_bytes_per_step": int(n * 4),
+                "p50_ms": lat[len(lat) // 2],
+                "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                "note": "the same K batches as value, timed on the host clock around "
+                        "hl_apply_batch (pinned host batch in) and hl_get_map (level-0 map "
+                        "out into pinned memory)"},
+        "device_p50_ms": dlat[len(dlat) // 2],
+        "device_p99_ms": dlat[min(len(dlat) - 1, int(0.99 * len(dlat)))],
+        "gpu_launches": int(launches),
+        "traversed_edges_per_s": traversed / (mv["ms"] / 1000.0) if mv.get("ms") else None,
+        "roofline": roof,
+        "roofline_aggregation": _roof(kernels, "aggregate_compress",
+                                      "inc-aggregation (emission + compression)", peak,
+                                      peak_kind),
+        "clocks": clk,
+    }
+
+
 def run_rmat(args, cfg):
     """R-MAT scale 25: graph and batches generated on the GPU (torch, input
-    plumbing only), loaded with hl_create_device; value from device-resident
-    batches (CUDA events), e2e through hl_apply_batch with host arrays."""
+    plumbing only), the graph loaded with hl_create_device; every step applies
+    a pinned host batch through hl_apply_batch and reads the level-0 map."""
     import torch
     R = importlib.import_module("hit-leiden_b200.replicas")
-    W = importlib.import_module("hit-leiden_b200.workloads")
+    W = _module("workloads")
     rep = R.Replicas("nccl")
     local = rep.local
     torch.cuda.set_device(local)
@@ -595,7 +798,7 @@ def run_rmat(args, cfg):
     free_b, total_b = torch.cuda.mem_get_info()
     print(f"# R-MAT scale {scale}: {n} vertices, {m} edges; device free {free_b} of {total_b}",
           file=sys.stderr, flush=True)
-    k = cfg["batch"] if not args.ncu_small else 50_000
+    k = cfg["batch"] if not args.ncu_small else 1_000_000 >> 5
     rc = hl.RunConfig(max_iterations=args.levels, device=local)
     c = rc.to_c()
     c.flags |= L.HL_FLAG_KERNEL_TIMING
@@ -606,131 +809,83 @@ def run_rmat(args, cfg):
                                    C.c_void_p(bd.data_ptr()), None, m, C.byref(h)))
     boot_s = time.perf_counter() - t0
     st = hl.PartitionState(h, n, rc)
+    q_boot = st.modularity()
     K, Wm = args.steps, args.warmup
     seeds = iter(range(10_000, 20_000))
-    for _ in range(Wm):
-        u, v, w = W.rmat_batch_torch(scale, bs, bd, k, 0.9, next(seeds))
-        L.check(L.lib.hl_apply_batch_device(h, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
-                                            C.c_void_p(w.data_ptr()), k, None))
-    dev = [W.rmat_batch_torch(scale, bs, bd, k, 0.9, next(seeds)) for _ in range(K)]
+    pinned = _pinned([W.rmat_batch_torch(scale, bs, bd, k, 0.9, next(seeds))
+                      for _ in range(Wm + K)])
+    del bs, bd
+    torch.cuda.empty_cache()
+    for (pu, pv, pw) in pinned[:Wm]:
+        L.check(L.lib.hl_apply_batch(h, C.c_void_p(pu.data_ptr()), C.c_void_p(pv.data_ptr()),
+                                     C.c_void_p(pw.data_ptr()), k, None))
     torch.cuda.synchronize()
     L.check(L.lib.hl_reset_kernel_stats(h))
-    clocks = Clocks(local)
-    clocks.start()
-    rep.barrier()
-    torch.cuda.synchronize()
-    dev_ms, launches, traversed = [], 0, 0
-    stats = L.BatchStats()
-    torch.cuda.nvtx.range_push("hl_timed")
-    for (u, v, w) in dev:
-        L.check(L.lib.hl_apply_batch_device(h, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
-                                            C.c_void_p(w.data_ptr()), k, C.byref(stats)))
-        dev_ms.append(stats.device_ms)
-        launches += stats.launches
-        traversed += stats.traversed
-    torch.cuda.nvtx.range_pop()
-    torch.cuda.synchronize()
-    rep.barrier()
-    clk = clocks.stop()
-    tot_ms = rep.max_over_ranks(float(sum(dev_ms)))
-    value = rep.whole_job_rate(K, k, tot_ms / 1000.0)
-    kst = (L.KernelStat * 32)()
-    cnt = C.c_uint32()
-    L.check(L.lib.hl_kernel_stats(h, kst, 32, C.byref(cnt)))
-    kernels = {kst[i].name.decode(): {"launches": kst[i].launches, "ms": kst[i].total_ms,
-                                      "bytes": kst[i].bytes, "items": kst[i].items}
-               for i in range(cnt.value)}
-    del dev
-    # end to end: host arrays in, level-0 map out
-    host = []
-    for _ in range(K):
-        u, v, w = W.rmat_batch_torch(scale, bs, bd, k, 0.9, next(seeds))
-        host.append((u.cpu().numpy().view(np.uint32), v.cpu().numpy().view(np.uint32),
-                     w.cpu().numpy()))
-    comm = np.zeros(n, np.uint32)
-    rep.barrier()
-    torch.cuda.synchronize()
-    e2e_s = []
-    for (u, v, w) in host:
-        t1 = time.perf_counter()
-        st.apply_batch(u, v, w)
-        L.check(L.lib.hl_get_map(h, 0, L.HL_MAP_COMMUNITY, L.ptr(comm)))
-        e2e_s.append(time.perf_counter() - t1)
-    tot_e2e = rep.max_over_ranks(float(sum(e2e_s)))
-    e2e_val = rep.whole_job_rate(K, k, tot_e2e)
-    lat = sorted(1000.0 * x for x in e2e_s)
-    peak, peak_kind = measured_peak()
-    mv = kernels.get("stage_move", {})
-    if rep.rank == 0:
-        line = {
-            "metric": "edge_updates_per_s", "value": value, "unit": "edge-updates/s",
-            "n_gpus": rep.world, "steps": K, "warmup": Wm, "ms_per_step": tot_ms / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": cfg["workload"], "scale": scale, "vertices": n,
-                       "edges": int(m), "batch_edges": k, "levels": st.levels,
-                       "parallelism": f"replicas{rep.world}",
-                       "l2": "inputs larger than L2 (resident CSR > 126 MB)",
-                       "bootstrap_s": boot_s},
-            "e2e": {"value": e2e_val, "unit": "edge-updates/s",
-                    "h2d_bytes_per_step": int(k * 16), "d2h_bytes_per_step": int(n * 4),
-                    "p50_ms": lat[len(lat) // 2],
-                    "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-            "gpu_launches": int(launches),
-            "traversed_edges_per_s": traversed / (mv["ms"] / 1000.0) if mv.get("ms") else None,
-            "roofline": _roof(kernels, "move_eval",
-                              "k_eval<EVAL_MOVE> (inc-movement best-move evaluation)", peak,
-                              peak_kind),
-            "roofline_aggregation": _roof(kernels, "aggregate_compress",
-                                          "inc-aggregation (emission + compression)", peak,
-                                          peak_kind),
-            "cpu_baseline": None,
-            "cpu_baseline_note": "the CPU port is not run at 500M edges (a single batch "
-                                 "would take hours on one core)",
-            "clocks": clk, "modularity": st.modularity(), "kernels": kernels,
-            "device_bytes": _device_bytes(L, h),
-        }
-        print(json.dumps(line), flush=True)
+    dev_ms, host_s, launches, traversed, clk = _timed_steps(L, h, pinned[Wm:], n, rep,
+                                                           Clocks(local))
+    kernels = _kernel_table(L, h)
+    tr = committed_traffic()
+    ratio = (tr or {}).get("traffic_per_algorithmic_byte") if (tr or {}).get(
+        "config") == args.config else None
+    config = {"workload": cfg["workload"], "scale": scale, "vertices": n, "edges": int(m),
+              "batch_edges": k, "levels": st.levels, "parallelism": f"replicas{rep.world}",
+              "l2": "inputs larger than L2 (resident CSR > 126 MB); no flush",
+              "bootstrap_s": boot_s, "bootstrap_modularity": q_boot}
+    line = _bench_line(rep, cfg["workload"], config, K, Wm, k, n, dev_ms, host_s, launches,
+                       traversed, kernels, clk, ratio)
+    q = st.modularity()
+    dbytes = _device_bytes(L, h)
     st.close()
+    cpu = None
+    if rep.rank == 0 and rep.world == 1 and not args.no_cpu_baseline:
+        r = cpu_rmat_sample(args.seed, args.levels, 0, args.cpu_sample_batches,
+                            args.cpu_sample_cap, args.rmat_sample_scale)
+        cpu = {"value": r["value"], "unit": "edge-updates/s", "cores": r["threads"],
+               "kind": "port", "sample": _rmat_sample_text(r)}
+    if rep.rank == 0:
+        line.update({"cpu_baseline": cpu, "modularity": q, "kernels": kernels,
+                     "device_bytes": dbytes})
+        print(json.dumps(line), flush=True)
     rep.close()
 
 
 def main():
     args = parse()
     cfg = CONFIGS[args.config]
-    if args.impl == "ours" and args.config == "rmat25":
-        return run_rmat(args, cfg)
-    if args.impl == "ours" and args.config == "batch256":
-        return run_batching(args, cfg)
-    if args.impl == "ours" and args.config == "serve32":
-        return run_serving(args, cfg)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.cpu_variant_run:
         return run_cpu_variant(args)
     if args.impl == "reference":
+        # the CPU port on the host cores: rank 0 alone works under torchrun
         if rank == 0:
-            if args.config in ("batch256", "serve32", "rmat25"):
+            if args.config in ("batch256", "serve32"):
                 print(json.dumps({"impl": "reference", "unavailable":
-                                  "not run for this configuration: the CPU port's per-graph "
-                                  "path is the lfr1m / ca_hepth reference arm"}), flush=True)
+                                  "the reference updates one PartitionState per call and has no "
+                                  "batching or serving form; its per-graph path is the rmat25 / "
+                                  "lfr1m / ca_hepth reference arm"}), flush=True)
             else:
                 run_reference(args, cfg)
         return
+    if args.config == "rmat25":
+        return run_rmat(args, cfg)
+    if args.config == "batch256":
+        return run_batching(args, cfg)
+    if args.config == "serve32":
+        return run_serving(args, cfg)
     import torch
     R = importlib.import_module("hit-leiden_b200.replicas")
     rep = R.Replicas("nccl")
     torch.cuda.set_device(local)
     hl = importlib.import_module("hit-leiden_b200")
     L = importlib.import_module("hit-leiden_b200._lib")
-    barrier = rep.barrier
 
     n, s, d, w, wts, ins, pref = make_graph(args.config, args.seed, args.ncu_small)
     k = cfg["batch"]
     K, Wm = args.steps, args.warmup
     n_cpu = 0 if (args.no_cpu_baseline or rank != 0 or world != 1) else args.cpu_sample_batches
-    batches = make_batches(n, s, d, w, wts, ins, pref, Wm + 2 * K + n_cpu, k, args.seed)
+    batches = make_batches(n, s, d, w, wts, ins, pref, Wm + K + n_cpu, k, args.seed)
 
     rc = hl.RunConfig(max_iterations=args.levels, device=local)
     c = rc.to_c()
@@ -740,125 +895,36 @@ def main():
     L.check(L.lib.hl_create(C.byref(c), n, L.ptr(s), L.ptr(d), L.ptr(w), len(s), C.byref(h)))
     boot_s = time.perf_counter() - t0
     st = hl.PartitionState(h, n, rc)
-
     for (u, v, ww) in batches[:Wm]:
         st.apply_batch(u, v, ww)
-
-    # device-resident batches for the HBM-resident measurement
-    dev = []
-    for (u, v, ww) in batches[Wm:Wm + K]:
-        dev.append((torch.from_numpy(u.view(np.int32)).to(f"cuda:{local}"),
-                    torch.from_numpy(v.view(np.int32)).to(f"cuda:{local}"),
-                    torch.from_numpy(ww).to(f"cuda:{local}")))
+    pinned = _pinned(batches[Wm:Wm + K])
     torch.cuda.synchronize()
     L.check(L.lib.hl_reset_kernel_stats(h))
-    clocks = Clocks(local)
-    clocks.start()
-    barrier()
-    torch.cuda.synchronize()
-    dev_ms = []
-    launches = 0
-    traversed = 0
-    stats = L.BatchStats()
-    torch.cuda.nvtx.range_push("hl_timed")
-    for (du, dv, dw) in dev:
-        L.check(L.lib.hl_apply_batch_device(h, C.c_void_p(du.data_ptr()), C.c_void_p(dv.data_ptr()),
-                                            C.c_void_p(dw.data_ptr()), k, C.byref(stats)))
-        dev_ms.append(stats.device_ms)
-        launches += stats.launches
-        traversed += stats.traversed
-    torch.cuda.nvtx.range_pop()
-    torch.cuda.synchronize()
-    barrier()
-    clk = clocks.stop()
-    tot_ms = rep.max_over_ranks(float(sum(dev_ms)))
-    value = rep.whole_job_rate(K, k, tot_ms / 1000.0)
-
-    kst = (L.KernelStat * 32)()
-    cnt = C.c_uint32()
-    L.check(L.lib.hl_kernel_stats(h, kst, 32, C.byref(cnt)))
-    kernels = {kst[i].name.decode(): {"launches": kst[i].launches, "ms": kst[i].total_ms,
-                                      "bytes": kst[i].bytes, "items": kst[i].items}
-               for i in range(cnt.value)}
-
-    # end to end through the host API: each batch is copied in from pinned host
-    # memory and the level-0 community map read back into pinned host memory
-    e2e_s = []
-    pinned = [(torch.from_numpy(u.view(np.int32)).pin_memory(),
-               torch.from_numpy(v.view(np.int32)).pin_memory(),
-               torch.from_numpy(ww).pin_memory()) for (u, v, ww) in batches[Wm + K:Wm + 2 * K]]
-    comm = torch.empty(n, dtype=torch.int32).pin_memory()
-    e2e_stats = L.BatchStats()
-    barrier()
-    torch.cuda.synchronize()
-    for (pu, pv, pw) in pinned:
-        t1 = time.perf_counter()
-        L.check(L.lib.hl_apply_batch(h, C.c_void_p(pu.data_ptr()), C.c_void_p(pv.data_ptr()),
-                                     C.c_void_p(pw.data_ptr()), pu.numel(),
-                                     C.byref(e2e_stats)))
-        L.check(L.lib.hl_get_map(h, 0, L.HL_MAP_COMMUNITY, C.c_void_p(comm.data_ptr())))
-        e2e_s.append(time.perf_counter() - t1)
-    torch.cuda.synchronize()
-    barrier()
-    tot_e2e = rep.max_over_ranks(float(sum(e2e_s)))
-    e2e_val = rep.whole_job_rate(K, k, tot_e2e)
-    lat = sorted(1000.0 * x for x in e2e_s)
-
-    ev = kernels.get("move_eval", {})
-    peak, peak_kind = measured_peak()
-    roof = None
-    if ev.get("launches"):
-        achieved = ev["bytes"] / (ev["ms"] / 1000.0) / 1e9
-        per_launch = ev["bytes"] / ev["launches"]
-        tr = committed_traffic()
-        traffic = None
-        if tr and tr.get("config") == args.config and tr.get("traffic_per_algorithmic_byte"):
-            traffic = per_launch * tr["traffic_per_algorithmic_byte"]
-        roof = {"kernel": "k_eval<EVAL_MOVE> (inc-movement best-move evaluation)",
-                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind,
-                "bytes_per_launch": per_launch, "avg_launch_ms": ev["ms"] / ev["launches"],
-                "traffic": traffic}
-
+    dev_ms, host_s, launches, traversed, clk = _timed_steps(L, h, pinned, n, rep, Clocks(local))
+    kernels = _kernel_table(L, h)
+    tr = committed_traffic()
+    ratio = (tr or {}).get("traffic_per_algorithmic_byte") if (tr or {}).get(
+        "config") == args.config else None
+    config = {"workload": cfg["workload"], "vertices": n, "edges": int(len(s)),
+              "batch_edges": k, "levels": st.levels, "parallelism": f"replicas{world}",
+              "l2": "inputs larger than L2 (resident CSR > 126 MB); no flush",
+              "bootstrap_s": boot_s}
+    line = _bench_line(rep, cfg["workload"], config, K, Wm, k, n, dev_ms, host_s, launches,
+                       traversed, kernels, clk, ratio)
     q = st.modularity()
     cpu = None
     if n_cpu:
-        cpu_res = cpu_baseline(st, batches[Wm + 2 * K:], args.levels, n_cpu)
-        cpu = {"value": cpu_res["value"], "unit": "edge-updates/s", "cores": cpu_res["threads"],
+        r = cpu_baseline(st, batches[Wm + K:], n_cpu, args.cpu_sample_cap)
+        cpu = {"value": r["value"], "unit": "edge-updates/s", "cores": r["threads"],
                "kind": "port",
-               "sample": f"{cpu_res['batches']} batch(es) of {k} updates of the same stream, "
-                         f"from the GPU's state ({cpu_res['seconds']:.1f} s on "
-                         f"{cpu_res['threads']} host threads)",
-               "parity_bit_exact_after_sample": cpu_res["parity_bit_exact"],
-               "dq_after_sample": cpu_res["dq"]}
-
+               "sample": f"{r['batches']} batch(es) of {k} updates of the same stream, right "
+                         f"after the timed ones, from the GPU's state (median "
+                         f"{statistics.median(r['batch_s']):.2f} s a batch on {r['threads']} "
+                         "host threads)",
+               "parity_bit_exact_after_sample": r["parity_bit_exact"],
+               "dq_after_sample": r["dq"]}
     if rank == 0:
-        line = {
-            "metric": "edge_updates_per_s", "value": value, "unit": "edge-updates/s",
-            "n_gpus": world, "steps": K, "warmup": Wm, "ms_per_step": tot_ms / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": cfg["workload"], "vertices": n, "edges": int(len(s)),
-                       "batch_edges": k, "levels": st.levels, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (resident CSR > 126 MB)",
-                       "bootstrap_s": boot_s},
-            "e2e": {"value": e2e_val, "unit": "edge-updates/s",
-                    "h2d_bytes_per_step": int(k * (4 + 4 + 8)),
-                    "d2h_bytes_per_step": int(n * 4),
-                    "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1,
-                                                                    int(0.99 * len(lat)))]},
-            "gpu_launches": int(launches),
-            "traversed_edges_per_s": (traversed / (kernels["stage_move"]["ms"] / 1000.0)
-                                      if kernels.get("stage_move", {}).get("ms") else None),
-            "roofline": roof,
-            "roofline_aggregation": _roof(kernels, "aggregate_compress",
-                                          "inc-aggregation (emission + compression)", peak,
-                                          peak_kind),
-            "cpu_baseline": cpu,
-            "clocks": clk,
-            "modularity": q,
-            "kernels": kernels,
-        }
+        line.update({"cpu_baseline": cpu, "modularity": q, "kernels": kernels})
         print(json.dumps(line), flush=True)
     st.close()
     rep.close()

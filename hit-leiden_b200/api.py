@@ -51,6 +51,7 @@ class RunConfig:
     hbm_budget: int = 0
     keep_self_loops: bool = False
     batch_modularity: bool = False
+    kernel_timing: bool = False
 
     def validate(self) -> None:
         if self.max_iterations == 0:
@@ -66,7 +67,8 @@ class RunConfig:
         c.max_levels = int(self.max_iterations)
         c.max_rounds = int(self.max_rounds)
         c.flags = ((L.HL_FLAG_KEEP_SELF_LOOPS if self.keep_self_loops else 0)
-                   | (L.HL_FLAG_BATCH_MODULARITY if self.batch_modularity else 0))
+                   | (L.HL_FLAG_BATCH_MODULARITY if self.batch_modularity else 0)
+                   | (L.HL_FLAG_KERNEL_TIMING if self.kernel_timing else 0))
         c.hbm_budget = int(self.hbm_budget)
         c.device = int(self.device)
         return c
@@ -240,6 +242,16 @@ class PartitionState:
             p = L.u32(partition)
             L.check(L.lib.hl_modularity_of(self._h, L.ptr(p), C.byref(q)))
         return q.value
+
+    def kernel_stats(self) -> dict:
+        """Per-kernel launches, device ms, algorithmic bytes and items since
+        creation or the last reset (config.kernel_timing must be set)."""
+        kst = (L.KernelStat * 64)()
+        cnt = C.c_uint32()
+        L.check(L.lib.hl_kernel_stats(self._h, kst, 64, C.byref(cnt)))
+        return {kst[i].name.decode(): {"launches": kst[i].launches, "ms": kst[i].total_ms,
+                                       "bytes": kst[i].bytes, "items": kst[i].items}
+                for i in range(min(cnt.value, 64))}
 
     def apply_batch(self, src, dst, w=None) -> L.BatchStats:
         src, dst, w = L.u32(src), L.u32(dst), L.f64(w)

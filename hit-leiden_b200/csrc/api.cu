@@ -446,12 +446,14 @@ static void apply_impl(hl_graph* g, const uint32_t* src, const uint32_t* dst, co
   HL_CUDA(cudaSetDevice(E.device));
   E.st = hl_batch_stats{};
   E.launch_mark = E.nlaunch;
-  HL_CUDA(cudaEventRecord(E.ev0, E.stream));
   DevEdges D;
   if (device_ptrs)
     D = DevEdges{src, dst, w, k};
   else
     upload_edges(B, src, dst, w, k, D);
+  // device_ms starts with the batch resident on the device: the host→device
+  // copy of a host batch is not part of it.
+  HL_CUDA(cudaEventRecord(E.ev0, E.stream));
   check_endpoints(E, D, E.levels[0].g.n);
   if (E.integral && !edges_integral(E, D)) E.integral = false;
   hit_leiden_batch(B, D);

@@ -17,8 +17,12 @@
 // on one GPU share the scratch array and it keeps the last call's contents;
 // two calls whose work overlaps on the GPU (different streams, or different
 // host threads without ordering) race on it and must be serialised by the
-// caller.  The first call on a device resolves the array's device address with
-// cudaGetSymbolAddress; make that first call before any stream capture.
+// caller.  Every call made outside stream capture resolves the array's device
+// address with cudaGetSymbolAddress, with the device current, and keeps it per
+// device; a call made while its stream is being captured uses the kept address
+// instead.  So the first call on a device must come before any capture, and a
+// capture after cudaDeviceReset must again follow an uncaptured call (the
+// address is only valid for the life of the primary context).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -80,12 +84,21 @@ extern "C" HL_API hl_status hl_tree_sum_noalloc(const double* d_x, uint64_t n, d
                          cudaGetErrorString(e));
     return HL_ERR_CUDA;
   }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) {
+    hl_set_error_message(std::string("hl_tree_sum_noalloc: cudaStreamIsCapturing failed: ") +
+                         cudaGetErrorString(e));
+    return HL_ERR_CUDA;
+  }
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
       // Host code only knows a stand-in for the array; its device address is
-      // resolved once per device, with that device current.
+      // resolved with the device current.  Resolving it on every uncaptured
+      // call keeps the kept address right after a context reset.
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_tree_scratch);
       if (e != cudaSuccess || !p) {
@@ -94,10 +107,14 @@ extern "C" HL_API hl_status hl_tree_sum_noalloc(const double* d_x, uint64_t n, d
         return HL_ERR_CUDA;
       }
       g_scratch_ptr[dev] = static_cast<double*>(p);
+    } else if (!g_scratch_ptr[dev]) {
+      hl_set_error_message(
+          "hl_tree_sum_noalloc: first call on this device made during stream capture; make an "
+          "uncaptured call first");
+      return HL_ERR_INVALID_INPUT;
     }
     scratch = g_scratch_ptr[dev];
   }
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (n == 0) {
     k_store_zero<<<1, 1, 0, st>>>(d_out);
   } else {

@@ -95,7 +95,9 @@ typedef struct {
   uint64_t refined;      /* |R^1| level-0 vertices refined                         */
   uint64_t edges;        /* undirected edges in G^1 after the batch                */
   double modularity;     /* Q of the level-0 community partition after the batch   */
-  double device_ms;      /* device time of the call (CUDA events)                  */
+  double device_ms;      /* device time of the update, from the batch resident on  */
+                         /* the device to the end (CUDA events; the host copy of   */
+                         /* a host batch is excluded)                              */
   uint64_t launches;     /* kernels of this library launched by the call           */
 } hl_batch_stats;
 
@@ -267,8 +269,12 @@ HL_API const char* hl_version(void);
  * every GPU that loads the library keeps until exit.  n must not exceed
  * HL_NOALLOC_MAX_ELEMS (HL_ERR_INVALID_INPUT otherwise).  All calls on one GPU
  * share that array: calls whose work overlaps on the GPU race and must be
- * ordered by the caller.  The first call on a device resolves the array's
- * device address (cudaGetSymbolAddress); make it before any stream capture. */
+ * ordered by the caller.  Each call made outside stream capture resolves the
+ * array's device address (cudaGetSymbolAddress) and keeps it for the device; a
+ * call on a capturing stream uses the kept address, so make the first call on
+ * a device before any stream capture.  The address lives as long as the
+ * primary context: after cudaDeviceReset, make an uncaptured call again before
+ * capturing one. */
 #define HL_NOALLOC_MAX_ELEMS (1ull << 28)
 HL_API hl_status hl_tree_sum_noalloc(const double* d_x, uint64_t n, double* d_out, void* stream);
 

@@ -40,3 +40,36 @@ def test_reference_arm_faithful_variants():
     assert ft["value"] > 0 and ft["same_result"] is True
     assert fd["value"] > 0 and fd["cores"] == 1
     assert sr["value"] > 0 and 0.0 < sr["modularity"] < 1.0
+
+
+def _maps_after_reference_arm(*argv):
+    """Run the reference arm in this interpreter's child and report whether
+    libhl.so was mapped into it at the end."""
+    code = ("import runpy, sys, json\n"
+            f"sys.argv = {['bench.py', '--impl', 'reference', *argv]!r}\n"
+            "runpy.run_path('bench.py', run_name='__main__')\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('LIBHL_MAPPED', 'libhl.so' in maps)\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600,
+                       cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][0])
+    mapped = [ln for ln in r.stdout.splitlines() if ln.startswith("LIBHL_MAPPED")][0]
+    return line, mapped.endswith("True")
+
+
+def test_reference_arm_never_loads_the_gpu_library():
+    line, mapped = _maps_after_reference_arm("--config", "ca_hepth", "--steps", "1",
+                                             "--warmup", "0")
+    assert line["impl"] == "reference"
+    assert not mapped
+
+
+def test_reference_arm_rmat_stand_in():
+    # the R-MAT configuration's CPU sample: the same generator at a small scale
+    line, mapped = _maps_after_reference_arm("--config", "rmat25", "--steps", "2", "--warmup",
+                                             "1", "--rmat-sample-scale", "12")
+    assert not mapped
+    assert line["steps"] == 2 and line["warmup"] == 1 and line["value"] > 0
+    assert "scale 12 stand-in" in line["cpu_baseline"]["sample"]
+    assert line["config"]["batch_edges"] == 1_000_000

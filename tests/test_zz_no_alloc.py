@@ -33,13 +33,15 @@ def test_tree_sum_noalloc_matches_allocating_entry_point_twice():
     L = importlib.import_module("hit-leiden_b200._lib")
     torch.cuda.set_device(0)
     rng = np.random.default_rng(2024)
-    sizes = [3_000_001, 1025]  # several reduction levels, then a two-tile case
+    # several reduction levels, a two-tile case, then the single-tile path
+    # (one value, a full tile) and the empty input, which must give +0.0
+    sizes = [3_000_001, 1025, 1, 1024, 0]
     for call, n in enumerate(sizes):
         x = rng.uniform(0.1, 3.0, n)
-        d_x = torch.from_numpy(x).to("cuda:0")
+        d_x = torch.from_numpy(x).to("cuda:0") if n else None
         d_out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda:0")
         torch.cuda.synchronize()
-        st = L.lib.hl_tree_sum_noalloc(C.c_void_p(d_x.data_ptr()), n,
+        st = L.lib.hl_tree_sum_noalloc(C.c_void_p(d_x.data_ptr()) if n else None, n,
                                        C.c_void_p(d_out.data_ptr()), None)
         assert st == L.HL_OK, L.lib.hl_last_error()
         torch.cuda.synchronize()
@@ -47,6 +49,8 @@ def test_tree_sum_noalloc_matches_allocating_entry_point_twice():
         want = _allocating_sum(L, x)
         assert np.array_equal(np.array([got]).view(np.uint64), np.array([want]).view(np.uint64)), (
             call, got, want)
+        if n == 0:
+            assert np.array([got]).view(np.uint64)[0] == 0, got  # +0.0, not -0.0
 
 
 def test_tree_sum_noalloc_rejects_oversized_input():
