@@ -501,7 +501,7 @@ def _load_many(hl, graphs, levels, device, threads=16):
     def one(g):
         n, s, d, w = g
         return hl.PartitionState.load(hl.GraphInput.from_arrays("g", n, s, d, w),
-                                      hl.RunConfig(max_iterations=levels, device=device))
+                                      hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=levels, device=device))
     with ThreadPoolExecutor(threads) as ex:
         return list(ex.map(one, graphs))
 
@@ -799,7 +799,7 @@ def run_rmat(args, cfg):
     print(f"# R-MAT scale {scale}: {n} vertices, {m} edges; device free {free_b} of {total_b}",
           file=sys.stderr, flush=True)
     k = cfg["batch"] if not args.ncu_small else 1_000_000 >> 5
-    rc = hl.RunConfig(max_iterations=args.levels, device=local)
+    rc = hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=args.levels, device=local)
     c = rc.to_c()
     c.flags |= L.HL_FLAG_KERNEL_TIMING
     h = C.c_void_p()
@@ -887,7 +887,7 @@ def main():
     n_cpu = 0 if (args.no_cpu_baseline or rank != 0 or world != 1) else args.cpu_sample_batches
     batches = make_batches(n, s, d, w, wts, ins, pref, Wm + K + n_cpu, k, args.seed)
 
-    rc = hl.RunConfig(max_iterations=args.levels, device=local)
+    rc = hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=args.levels, device=local)
     c = rc.to_c()
     c.flags |= L.HL_FLAG_KERNEL_TIMING
     h = C.c_void_p()

@@ -91,6 +91,7 @@ def _load():
         "hl_apply_batch": (st, [vp, vp, vp, vp, C.c_uint64, C.POINTER(BatchStats)]),
         "hl_apply_batch_device": (st, [vp, vp, vp, vp, C.c_uint64, C.POINTER(BatchStats)]),
         "hl_set_resolution": (st, [vp, C.c_double]),
+        "hl_set_mode": (st, [vp, C.c_uint32]),
         "hl_kernel_stats": (st, [vp, vp, C.c_uint32, p32]),
         "hl_reset_kernel_stats": (st, [vp]),
         "hl_num_nodes": (st, [vp, p32]),
@@ -135,6 +136,7 @@ def _load():
         "hl_dbg_tree_sum": (st, [C.c_int32, vp, C.c_uint64, C.POINTER(C.c_double)]),
         "hl_dbg_seq_sums": (st, [C.c_int32, C.c_uint32, vp, vp, C.c_double, C.c_int32, vp]),
         "hl_dbg_set_exact_tfilter": (st, [C.c_int32]),
+        "hl_dbg_set_mode": (st, [C.c_uint32]),
         "hl_tree_sum_noalloc": (st, [vp, C.c_uint64, vp, vp]),
         "hl_dbg_modularity": (st, [C.c_int32, C.c_uint32, vp, vp, vp, vp,
                                    C.POINTER(C.c_double)]),

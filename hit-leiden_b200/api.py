@@ -30,7 +30,9 @@ from ._lib import HitLeidenError
 
 
 class RunMode(enum.IntEnum):
-    """RunMode (config.rs:19-23).  The GPU path implements Throughput."""
+    """RunMode (config.rs:19-23).  Both modes run on the GPU: Deterministic is
+    the sequential Gauss–Seidel form (the reference's default), Throughput the
+    round-based parallel form and the fast path."""
     Deterministic = 0
     Throughput = 1
     DETERMINISTIC = 0
@@ -41,8 +43,10 @@ class RunMode(enum.IntEnum):
 class RunConfig:
     """RunConfig (config.rs:25-63).  ``max_iterations`` caps the hierarchy
     levels exactly as it caps multilevel_leiden's levels (hit_leiden.rs:217);
-    1 reproduces the reference's single-level PartitionState (state.rs:42)."""
-    mode: RunMode = RunMode.Throughput
+    1 reproduces the reference's single-level PartitionState (state.rs:42).
+    The defaults are RunConfig::default() (config.rs:37-48): deterministic
+    mode, 10 iterations, resolution 1.0, tolerance 0.001."""
+    mode: RunMode = RunMode.Deterministic
     resolution: float = 1.0
     max_iterations: int = 10
     quality_tolerance: float = 0.001
@@ -263,12 +267,13 @@ class PartitionState:
 
 
 def hit_leiden(state: PartitionState, delta_g: GraphInput, gamma: float = 1.0,
-               mode: RunMode = RunMode.Throughput) -> int:
+               mode: RunMode = RunMode.Deterministic) -> int:
     """Algorithm 6 (hit_leiden.rs:936-1018): apply ``delta_g`` and update every
-    level.  Returns the total number of movement iterations."""
-    if int(mode) != int(RunMode.Throughput):
-        raise HitLeidenError(L.HL_ERR_UNSUPPORTED,
-                             "only RunMode::Throughput runs on the GPU path")
+    level in ``mode``.  Returns the total number of movement iterations (one
+    per level in deterministic mode, as the reference returns)."""
+    if int(mode) != int(state.config.mode):
+        L.check(L.lib.hl_set_mode(state._h, int(mode)))
+        state.config.mode = RunMode(int(mode))
     if gamma != state.config.resolution:
         L.check(L.lib.hl_set_resolution(state._h, float(gamma)))
         state.config.resolution = gamma

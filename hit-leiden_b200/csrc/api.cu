@@ -130,9 +130,8 @@ struct EngineBox {
 static void validate_config(const hl_config* c) {
   require(c != nullptr, "config is NULL");
   require(std::isfinite(c->resolution), "resolution must be finite");
-  if (c->mode != HL_MODE_THROUGHPUT)
-    throw Error(HL_ERR_UNSUPPORTED,
-                "only RunMode::Throughput runs on the GPU (Deterministic is sequential)");
+  require(c->mode == HL_MODE_DETERMINISTIC || c->mode == HL_MODE_THROUGHPUT,
+          "mode must be HL_MODE_DETERMINISTIC or HL_MODE_THROUGHPUT");
   require(c->max_levels >= 1 && c->max_levels <= 64, "max_levels must be in [1, 64]");
 }
 
@@ -495,7 +494,7 @@ hl_status hl_config_default(hl_config* cfg) {
   }
   std::memset(cfg, 0, sizeof(*cfg));
   cfg->resolution = 1.0;
-  cfg->mode = HL_MODE_THROUGHPUT;
+  cfg->mode = HL_MODE_DETERMINISTIC;  // RunConfig::default() (config.rs:40-43)
   cfg->max_levels = 10;
   cfg->max_rounds = 20;
   cfg->flags = 0;
@@ -553,6 +552,13 @@ hl_status hl_set_resolution(hl_graph* g, double gamma) {
   HL_TRY(require(g != nullptr, "graph handle is NULL");
          require(std::isfinite(gamma), "resolution must be finite");
          box(g)->E->cfg.resolution = gamma);
+}
+
+hl_status hl_set_mode(hl_graph* g, uint32_t mode) {
+  HL_TRY(require(g != nullptr, "graph handle is NULL");
+         require(mode == HL_MODE_DETERMINISTIC || mode == HL_MODE_THROUGHPUT,
+                 "mode must be HL_MODE_DETERMINISTIC or HL_MODE_THROUGHPUT");
+         box(g)->E->cfg.mode = mode);
 }
 
 hl_status hl_num_nodes(const hl_graph* g, uint32_t* n) {
@@ -680,10 +686,14 @@ const char* hl_version(void) { return "hit-leiden-b200 0.1.0 (sm_100a)"; }
 // ---------------------------------------------------------------------------
 namespace {
 
+// RunMode of the stage entry points (hl_dbg_set_mode); Throughput unless set.
+std::atomic<uint32_t> g_dbg_mode{HL_MODE_THROUGHPUT};
+
 std::unique_ptr<EngineBox> scratch_engine(int32_t device) {
   hl_config cfg;
   hl_config_default(&cfg);
   cfg.device = device;
+  cfg.mode = g_dbg_mode.load();
   std::unique_ptr<EngineBox> B(new EngineBox());
   engine_init(*B, &cfg);
   return B;
@@ -918,6 +928,15 @@ hl_status hl_dbg_inc_refinement(int32_t device, uint32_t n, const uint64_t* off,
 
 hl_status hl_dbg_set_exact_tfilter(int32_t on) {
   g_exact_tfilter.store(on ? 1 : 0);
+  return HL_OK;
+}
+
+hl_status hl_dbg_set_mode(uint32_t mode) {
+  if (mode != HL_MODE_DETERMINISTIC && mode != HL_MODE_THROUGHPUT) {
+    g_err = "mode must be HL_MODE_DETERMINISTIC or HL_MODE_THROUGHPUT";
+    return HL_ERR_INVALID_INPUT;
+  }
+  g_dbg_mode.store(mode);
   return HL_OK;
 }
 

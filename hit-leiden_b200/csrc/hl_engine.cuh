@@ -92,6 +92,12 @@ struct Scratch {
   DBuf<u32> foldseg, foldcnt;   // ordered sums: long segments, folded in runs, and their count
   DBuf<double> fvals;           // ordered sums: the terms gathered into sum order
   DBuf<double> huge_val;
+  // deterministic mode (det.cu)
+  DBuf<u32> det_bits, det_bp, det_keys, det_rsort, det_mkey, det_mkey2, det_mval, det_members,
+      det_mstart, det_mcount, det_xhead, det_xnext;
+  DBuf<double> det_bw, det_wsp;
+  DBuf<u64> det_out, det_k64, det_k64b;
+  DBuf<u8> det_wvalid;
 };
 
 // Per-kernel device timing (CUDA events on the engine's stream), enabled by
@@ -213,6 +219,12 @@ struct RefineOut {
   u32 smax_before = 0;
 };
 RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community);
+
+// det.cu: the sequential (RunMode::Deterministic) steps
+void inc_movement_det(Engine& E, Level& L, double* d, size_t dcap, bool mark_moved, u64* moves,
+                      u64* traversed);
+u64 merge_singletons_det(Engine& E, Level& L, const u32* rv, u32 nr, u32* sizes, double* dS,
+                         const double* dcomm, size_t scap);
 
 // Test switch: decide every T-filter candidate from the ordered sum.
 extern std::atomic<int> g_exact_tfilter;

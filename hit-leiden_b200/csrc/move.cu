@@ -517,6 +517,13 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   const size_t ncap = 2 * (size_t)n + 2;
   ensure_comm_arrays(E, ncap);
   recompute_comm_degrees(E, L, L.f.p, (u32)ncap, S.d.p);
+  if (E.cfg.mode == HL_MODE_DETERMINISTIC) {
+    // sequential Gauss–Seidel (hit_leiden.rs:1103-1191): one iteration
+    inc_movement_det(E, L, S.d.p, ncap, mark_moved, &out.moves, &out.traversed);
+    out.iterations = 1;
+    E.kagg[KT_MOVE_EVAL].bytes += 16ull * out.traversed;
+    return out;
+  }
 
   S.act.ensure(E.mem, n);
   S.cand_to.ensure(E.mem, n);

@@ -508,6 +508,17 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   u32 nr = select_flagged(E, S.refined.p, n, S.act.p, cnt + 6);
   out.refined = nr;
   if (!nr) return out;
+  if (E.cfg.mode == HL_MODE_DETERMINISTIC) {
+    // sequential merges in (k, node) order with the live T-filter
+    // (hit_leiden.rs:1392-1548)
+    S.dS.ensure(E.mem, s2cap);
+    recompute_comm_degrees(E, L, s, (u32)s2cap, S.dS.p);
+    const size_t fcap = 2 * (size_t)n + 2;
+    S.dcomm.ensure(E.mem, fcap);
+    recompute_comm_degrees(E, L, L.f.p, (u32)fcap, S.dcomm.p);
+    out.merges = merge_singletons_det(E, L, S.act.p, nr, S.sizes.p, S.dS.p, S.dcomm.p, s2cap);
+    return out;
+  }
   S.nmask.ensure(E.mem, nr);
   ++E.nlaunch, k_singletons<<<grid_for(nr), 256, 0, st>>>(S.act.p, nr, s, S.sizes.p, S.nmask.p);
   HL_LAUNCH_CHECK();

@@ -48,8 +48,11 @@ typedef enum {
   HL_ERR_UNSUPPORTED = 5    /* mode / feature not available on this path     */
 } hl_status;
 
-/* RunMode (src/core/config.rs:19-23).  The GPU path implements Throughput;
- * Deterministic (sequential Gauss–Seidel) is rejected with HL_ERR_UNSUPPORTED. */
+/* RunMode (src/core/config.rs:19-23).  Both run on the GPU.  Deterministic
+ * (the reference's default) is the sequential Gauss–Seidel movement and the
+ * sequential singleton merges (hit_leiden.rs:1103-1191, :1392-1548), run as
+ * one persistent block per stage; Throughput is the round-based parallel form
+ * (hit_leiden.rs:1068-1101, throughput.rs:80-359) and the fast path. */
 typedef enum { HL_MODE_DETERMINISTIC = 0, HL_MODE_THROUGHPUT = 1 } hl_mode;
 
 /* Which per-level map hl_get_map returns (state.rs:19-32). */
@@ -62,7 +65,7 @@ typedef enum {
 
 typedef struct {
   double resolution;    /* gamma (RunConfig.resolution, config.rs:35); default 1.0 */
-  uint32_t mode;        /* hl_mode; default HL_MODE_THROUGHPUT                     */
+  uint32_t mode;        /* hl_mode; default HL_MODE_DETERMINISTIC (config.rs:40-43) */
   uint32_t max_levels;  /* 1 = the reference's single-level state (state.rs:42);   */
                         /* >1 = multi-level bootstrap, levels created on demand    */
                         /* up to this cap (default 10, RunConfig.max_iterations)   */
@@ -112,7 +115,8 @@ typedef struct {
 
 typedef struct hl_graph hl_graph;
 
-/* Default configuration (gamma 1, throughput, 10 levels, 20 rounds). */
+/* Default configuration, RunConfig::default() (config.rs:37-48): gamma 1,
+ * deterministic mode, 10 levels; 20 throughput rounds. */
 HL_API hl_status hl_config_default(hl_config* cfg);
 
 /* Load an undirected weighted graph of n vertices (m edges; w == NULL means
@@ -152,6 +156,10 @@ HL_API hl_status hl_reset_kernel_stats(hl_graph* g);
 /* Change gamma for subsequent batches (hit_leiden takes it per call,
  * hit_leiden.rs:939). */
 HL_API hl_status hl_set_resolution(hl_graph* g, double gamma);
+
+/* Change the RunMode for subsequent batches (hit_leiden takes it per call,
+ * hit_leiden.rs:940): HL_MODE_DETERMINISTIC or HL_MODE_THROUGHPUT. */
+HL_API hl_status hl_set_mode(hl_graph* g, uint32_t mode);
 
 HL_API hl_status hl_num_nodes(const hl_graph* g, uint32_t* n);
 HL_API hl_status hl_num_levels(const hl_graph* g, uint32_t* levels);

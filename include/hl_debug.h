@@ -37,7 +37,8 @@ HL_API hl_status hl_dbg_apply_delta(int32_t device, uint32_t n, const uint64_t* 
                              int32_t keep_self_loops, uint64_t* out_off, uint32_t* out_col,
                              double* out_w, uint64_t cap, uint64_t* out_nnz);
 
-/* inc_movement, throughput mode: hit_leiden.rs:1024-1101.  f is updated in
+/* inc_movement in the mode hl_dbg_set_mode selects (throughput by default):
+ * hit_leiden.rs:1024-1101, deterministic :1103-1191.  f is updated in
  * place; changed / affected (may be NULL) receive B and K as 0/1 bytes. */
 HL_API hl_status hl_dbg_inc_movement(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
                               const double* w, const uint32_t* dsrc, const uint32_t* ddst,
@@ -45,7 +46,8 @@ HL_API hl_status hl_dbg_inc_movement(int32_t device, uint32_t n, const uint64_t*
                               double gamma, uint32_t max_rounds, int32_t mark_moved,
                               uint8_t* changed, uint8_t* affected, uint32_t* iterations);
 
-/* inc_refinement, throughput mode: hit_leiden.rs:1265-1390 with
+/* inc_refinement in the mode hl_dbg_set_mode selects (throughput by default,
+ * deterministic merges hit_leiden.rs:1392-1548): hit_leiden.rs:1265-1390 with
  * throughput.rs:239-359.  s is updated in place; refined receives R. */
 HL_API hl_status hl_dbg_inc_refinement(int32_t device, uint32_t n, const uint64_t* off,
                                 const uint32_t* col, const double* w, const uint32_t* f,
@@ -82,6 +84,12 @@ HL_API hl_status hl_dbg_seq_sums(int32_t device, uint32_t nseg, const uint64_t* 
  * either way; the switch lets tests cover the ordered path.  No reference
  * counterpart. */
 HL_API hl_status hl_dbg_set_exact_tfilter(int32_t on);
+
+/* RunMode of the stage entry points above (hl_dbg_inc_movement,
+ * hl_dbg_inc_refinement, ...): HL_MODE_THROUGHPUT (the default) or
+ * HL_MODE_DETERMINISTIC, so that the reference's dual-mode tests
+ * (dual_mode_test!, hit_leiden.rs:1823-1841) run on both GPU paths. */
+HL_API hl_status hl_dbg_set_mode(uint32_t mode);
 
 /* Modularity of `part` on the CSR (hit_leiden.rs:121-161). */
 HL_API hl_status hl_dbg_modularity(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,

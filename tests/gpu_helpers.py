@@ -80,6 +80,16 @@ def exact_tfilter(on=True):
         L.check(L.lib.hl_dbg_set_exact_tfilter(0))
 
 
+@contextlib.contextmanager
+def stage_mode(mode):
+    """Run the stage entry points in `mode` (hl.RunMode), throughput after."""
+    L.check(L.lib.hl_dbg_set_mode(int(mode)))
+    try:
+        yield
+    finally:
+        L.check(L.lib.hl_dbg_set_mode(L.HL_MODE_THROUGHPUT))
+
+
 def inc_refinement(g: O.Graph, f, s, affected, gamma, cc_same_community=False):
     n, off, col, w = csr_of(g)
     f = L.u32(f)

@@ -37,7 +37,9 @@ def test_version_and_default_config():
     assert b"sm_100a" in L.lib.hl_version()
     c = L.Config()
     assert L.lib.hl_config_default(C.byref(c)) == 0
-    assert c.resolution == 1.0 and c.mode == 1 and c.max_levels == 10 and c.max_rounds == 20
+    # RunConfig::default() (config.rs:37-48): deterministic mode, 10 iterations
+    assert c.resolution == 1.0 and c.mode == L.HL_MODE_DETERMINISTIC
+    assert c.max_levels == 10 and c.max_rounds == 20
     assert L.lib.hl_config_default(None) == L.HL_ERR_INVALID_INPUT
 
 
@@ -56,6 +58,7 @@ def test_config_validation_mirrors_reference():
     with pytest.raises(hl.HitLeidenError):
         hl.RunConfig(quality_tolerance=-1.0).validate()
     hl.RunConfig().validate()
+    assert hl.RunConfig().mode == hl.RunMode.Deterministic
 
 
 def test_graph_input_arrays():

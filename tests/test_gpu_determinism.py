@@ -32,7 +32,7 @@ def test_identical_handles_stay_identical(weights):
     n, s, d, w, _ = W.planted(60_000, 24.0, 0.3, 5, comm_min=20, comm_max=2000,
                               weights=weights)
     handles = [hl.PartitionState.load(hl.GraphInput.from_arrays("g", n, s, d, w),
-                                      hl.RunConfig(max_iterations=10)) for _ in range(3)]
+                                      hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=10)) for _ in range(3)]
     ref = _state(handles[0])
     for h in handles[1:]:
         assert all(np.array_equal(a, b) for a, b in zip(ref, _state(h)))

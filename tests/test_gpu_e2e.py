@@ -61,7 +61,7 @@ def small_planted(seed, n=2000, weights=None):
 @pytest.mark.parametrize("seed", [0, 1, 2])
 def test_e2e_unit_weights_inserts(levels, seed):
     n, s, d, w = small_planted(seed)
-    cfg = hl.RunConfig(max_iterations=levels)
+    cfg = hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=levels)
     gs = hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w), cfg)
     os_ = oracle_state(n, s, d, w, levels)
     compare(gs, os_)
@@ -83,7 +83,7 @@ def test_e2e_f64_weights_mixed(levels, seed, exact):
 
 def _f64_weights_mixed(levels, seed):
     n, s, d, w = small_planted(seed, weights=(0.5, 2.0))
-    cfg = hl.RunConfig(max_iterations=levels)
+    cfg = hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=levels)
     gs = hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w), cfg)
     os_ = oracle_state(n, s, d, w, levels)
     compare(gs, os_)
@@ -97,7 +97,7 @@ def _f64_weights_mixed(levels, seed):
 
 def test_e2e_config1_shape():
     n, s, d, w = W.config1(0)
-    gs = hl.PartitionState.load(hl.GraphInput.from_arrays("c1", n, s, d, w), hl.RunConfig())
+    gs = hl.PartitionState.load(hl.GraphInput.from_arrays("c1", n, s, d, w), hl.RunConfig(mode=hl.RunMode.Throughput))
     os_ = oracle_state(n, s, d, w, 10)
     compare(gs, os_)
     ex = set(zip(s.tolist(), d.tolist()))
@@ -110,7 +110,7 @@ def test_e2e_config1_shape():
 
 def test_e2e_deletes_and_empty_batch():
     n, s, d, w = small_planted(5)
-    gs = hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w), hl.RunConfig())
+    gs = hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w), hl.RunConfig(mode=hl.RunMode.Throughput))
     os_ = oracle_state(n, s, d, w, 10)
     # delete 100 existing edges exactly, then an empty batch (all vertices active)
     idx = np.random.default_rng(0).choice(len(s), 100, replace=False)
@@ -126,7 +126,7 @@ def test_reference_hit_leiden_api_mirror():
     # hit_leiden.rs:3136-3177: strong cross edges must not increase the count.
     e = [(0, 1, 10.0), (1, 2, 10.0), (0, 2, 10.0), (3, 4, 10.0), (4, 5, 10.0), (3, 5, 10.0),
          (2, 3, 0.1)]
-    st = hl.PartitionState.load(hl.GraphInput("t", 6, e), hl.RunConfig(max_iterations=1))
+    st = hl.PartitionState.load(hl.GraphInput("t", 6, e), hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=1))
     c0 = len(set(st.community_mapping_per_level[0].tolist()))
     it = hl.hit_leiden(st, hl.GraphInput("d", 6, [(0, 3, 100.0), (1, 4, 100.0)]), 1.0,
                        hl.RunMode.Throughput)
@@ -142,10 +142,10 @@ def test_errors_are_reported_not_raised_across_abi():
     with pytest.raises(hl.HitLeidenError) as e:
         hl.PartitionState.load(hl.GraphInput("t", 3, [(0, 5, None)]))
     assert e.value.kind == "InvalidInput"
-    with pytest.raises(hl.HitLeidenError) as e:
-        hl.PartitionState.load(hl.GraphInput("t", 3, [(0, 1, None)]),
-                               hl.RunConfig(mode=hl.RunMode.Deterministic))
-    assert e.value.kind == "Unsupported"
+    # the reference's default mode runs on the GPU too
+    det = hl.PartitionState.load(hl.GraphInput("t", 3, [(0, 1, None)]))
+    assert det.config.mode == hl.RunMode.Deterministic and det.levels >= 1
+    det.close()
     with pytest.raises(hl.HitLeidenError) as e:
         hl.RunConfig(max_iterations=0).validate()
     assert e.value.kind == "InvalidInput"
@@ -162,7 +162,7 @@ def test_hbm_budget_is_enforced():
     n, s, d, w = small_planted(0)
     with pytest.raises(hl.HitLeidenError) as e:
         hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w),
-                               hl.RunConfig(hbm_budget=64 * 1024))
+                               hl.RunConfig(mode=hl.RunMode.Throughput, hbm_budget=64 * 1024))
     assert e.value.kind == "OutOfMemory"
 
 
@@ -170,7 +170,7 @@ def test_empty_and_tiny_graphs():
     for n, edges in [(1, []), (4, []), (2, [(0, 1, None)]), (3, [(0, 0, 2.0), (1, 2, None)])]:
         for lv in [1, 10]:
             g = hl.GraphInput("t", n, edges)
-            st = hl.PartitionState.load(g, hl.RunConfig(max_iterations=lv))
+            st = hl.PartitionState.load(g, hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=lv))
             src, dst, w = g.arrays()
             os_ = oracle_state(n, src, dst, w, lv)
             compare(st, os_)
@@ -187,7 +187,7 @@ def test_e2e_rmat_integral_hubs(seed):
     d = bd.cpu().numpy().view(np.uint32)
     w = np.ones(len(s))
     gs = hl.PartitionState.load(hl.GraphInput.from_arrays("rmat", n, s, d, None),
-                                hl.RunConfig(max_iterations=10))
+                                hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=10))
     os_ = oracle_state(n, s, d, w, 10)
     compare(gs, os_)
     for b in range(3):

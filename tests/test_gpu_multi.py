@@ -34,7 +34,7 @@ def _graphs(count, seed, n_lo=400, n_hi=3000, weights=None):
 def _load(gr, levels=10):
     n, s, d, w = gr
     return hl.PartitionState.load(hl.GraphInput.from_arrays("g", n, s, d, w),
-                                  hl.RunConfig(max_iterations=levels))
+                                  hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=levels))
 
 
 def _same(a, b):

@@ -23,7 +23,7 @@ IO = importlib.import_module("hit-leiden_b200.io")
 @pytest.mark.parametrize("seed", [0, 1, 2])
 def test_incremental_quality_close_to_fresh_run(seed):
     n, s, d, w = W.config1(seed)
-    st = hl.PartitionState.load(hl.GraphInput.from_arrays("c1", n, s, d, w), hl.RunConfig())
+    st = hl.PartitionState.load(hl.GraphInput.from_arrays("c1", n, s, d, w), hl.RunConfig(mode=hl.RunMode.Throughput))
     ex = set(zip(s.tolist(), d.tolist()))
     us, vs = [s], [d]
     for b in range(5):

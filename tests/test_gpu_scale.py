@@ -42,7 +42,7 @@ def test_e2e_rmat_scale18_bit_exact():
     # singletons at the first bootstrap round: distinct keys = degree
     assert deg.max() > 2048
     gs = hl.PartitionState.load(hl.GraphInput.from_arrays("rmat18", n, s, d, None),
-                                hl.RunConfig(max_iterations=10, kernel_timing=True))
+                                hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=10, kernel_timing=True))
     os_ = E2E.oracle_state(n, s, d, np.ones(len(s)), 10)
     E2E.compare(gs, os_)
     ks = gs.kernel_stats()
@@ -63,7 +63,7 @@ def test_e2e_rmat_scale18_bit_exact():
 def test_seed_sweep_ca_hepth_shape(seed):
     n, s, d, w = W.config1(seed)
     gs = hl.PartitionState.load(hl.GraphInput.from_arrays("c1", n, s, d, w),
-                                hl.RunConfig(max_iterations=10))
+                                hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=10))
     os_ = E2E.oracle_state(n, s, d, w, 10)
     E2E.compare(gs, os_, check_csr=False)
     ex = set(zip(s.tolist(), d.tolist()))
@@ -82,7 +82,7 @@ def test_seed_sweep_ca_hepth_shape(seed):
 def test_seed_sweep_reduced_lfr(seed):
     n, s, d, w = W.config2(seed, n=20_000, mean_degree=20.0)
     gs = hl.PartitionState.load(hl.GraphInput.from_arrays("c2", n, s, d, w),
-                                hl.RunConfig(max_iterations=10))
+                                hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=10))
     os_ = E2E.oracle_state(n, s, d, w, 10)
     store = W.EdgeStore(n, s, d, w)
     for b in range(3):
@@ -161,7 +161,7 @@ def _upper(off, col, w):
 def test_invariants_rmat_after_batches(seed):
     n, ts, td, s, d = _rmat_host(14, seed)
     gs = hl.PartitionState.load(hl.GraphInput.from_arrays("rmat14", n, s, d, None),
-                                hl.RunConfig(max_iterations=10))
+                                hl.RunConfig(mode=hl.RunMode.Throughput, max_iterations=10))
     for b in range(3):
         u, v, w = W.rmat_batch_torch(14, ts, td, 1_000_000 >> 11, 0.9, 40 + 10 * seed + b)
         gs.apply_batch(u.numpy().view(np.uint32), v.numpy().view(np.uint32), w.numpy())
