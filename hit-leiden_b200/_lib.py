@@ -59,10 +59,17 @@ class RequestDone(C.Structure):
                 ("edges", C.c_uint64), ("batch_edges", C.c_uint64), ("changed", C.c_uint64),
                 ("modularity", C.c_double), ("queue_ms", C.c_double), ("service_ms", C.c_double),
                 ("latency_ms", C.c_double), ("graph", C.c_uint32), ("batch_requests", C.c_uint32),
-                ("status", C.c_int32), ("pad_", C.c_uint32)]
+                ("status", C.c_int32), ("pad_", C.c_uint32), ("level0_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+
+# hl_level_fn / hl_server_level_fn (per-level output callbacks)
+LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32),
+                       C.POINTER(C.c_uint32))
+SERVER_LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint64,
+                              C.POINTER(C.c_uint32), C.POINTER(C.c_uint32))
 
 
 class HitLeidenError(RuntimeError):
@@ -116,6 +123,8 @@ def _load():
                                   C.POINTER(C.c_uint64)]),
         "hl_server_poll": (st, [vp, C.POINTER(RequestDone), C.c_uint32, p32, C.c_int32]),
         "hl_server_drain": (st, [vp]),
+        "hl_server_set_level_callback": (st, [vp, SERVER_LEVEL_FN, vp]),
+        "hl_set_level_callback": (st, [vp, LEVEL_FN, vp]),
         "hl_server_destroy": (None, [vp]),
         "hl_last_error": (C.c_char_p, []),
         "hl_version": (C.c_char_p, []),

@@ -247,6 +247,23 @@ class PartitionState:
             L.check(L.lib.hl_modularity_of(self._h, L.ptr(p), C.byref(q)))
         return q.value
 
+    def set_level_callback(self, fn) -> None:
+        """Per-level output (hl_set_level_callback): during apply_batch,
+        ``fn(level, nodes, sub_ids)`` is called after each level's refinement
+        with the level's nodes whose sub-community changed in the batch and
+        their new ids (numpy copies).  None turns it off."""
+        if fn is None:
+            self._level_cb = None
+            L.check(L.lib.hl_set_level_callback(self._h, L.LEVEL_FN(), None))
+            return
+
+        def tramp(user, level, count, nodes, ids):
+            nn = np.ctypeslib.as_array(nodes, (count,)).copy() if count else np.zeros(0, np.uint32)
+            ii = np.ctypeslib.as_array(ids, (count,)).copy() if count else np.zeros(0, np.uint32)
+            fn(int(level), nn, ii)
+        self._level_cb = L.LEVEL_FN(tramp)  # kept alive with the state
+        L.check(L.lib.hl_set_level_callback(self._h, self._level_cb, None))
+
     def kernel_stats(self) -> dict:
         """Per-kernel launches, device ms, algorithmic bytes and items since
         creation or the last reset (config.kernel_timing must be set)."""
@@ -335,6 +352,23 @@ class Server:
         L.check(L.lib.hl_server_add_graph(self._s, state._h, C.byref(gid)))
         self._states.append(state)
         return gid.value
+
+    def set_level_callback(self, fn) -> None:
+        """Per-level output of the served batches: ``fn(graph, batch_id, level,
+        nodes, sub_ids)`` from the worker thread, after each level's
+        refinement and before the batch's requests complete.  None turns it
+        off.  Set it before submitting."""
+        if fn is None:
+            self._level_cb = None
+            L.check(L.lib.hl_server_set_level_callback(self._s, L.SERVER_LEVEL_FN(), None))
+            return
+
+        def tramp(user, graph, batch_id, level, count, nodes, ids):
+            nn = np.ctypeslib.as_array(nodes, (count,)).copy() if count else np.zeros(0, np.uint32)
+            ii = np.ctypeslib.as_array(ids, (count,)).copy() if count else np.zeros(0, np.uint32)
+            fn(int(graph), int(batch_id), int(level), nn, ii)
+        self._level_cb = L.SERVER_LEVEL_FN(tramp)
+        L.check(L.lib.hl_server_set_level_callback(self._s, self._level_cb, None))
 
     def set_edge_estimate(self, bytes_per_edge: int) -> None:
         L.check(L.lib.hl_server_set_edge_estimate(self._s, int(bytes_per_edge)))

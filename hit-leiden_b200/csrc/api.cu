@@ -203,6 +203,63 @@ struct NvtxScope {
   NvtxScope& operator=(const NvtxScope&) = delete;
 };
 
+// Per-level output (hl_set_level_callback): the level's sub-community map is
+// copied before its refinement, and the nodes whose entry changed are handed
+// to the callback right after it (hit_leiden.rs gives the same point: nothing
+// after inc_refinement at level p writes s_cur^p).
+__global__ void k_changed_flags(const u32* a, const u32* b, u32 n, u8* flag) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    flag[i] = a[i] != b[i] ? 1 : 0;
+}
+__global__ void k_gather_u32(const u32* idx, u32 m, const u32* src, u32* out) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < m; i += (u64)gridDim.x * blockDim.x)
+    out[i] = src[idx[i]];
+}
+
+static void level_snapshot(Engine& E, Level& L) {
+  if (!E.level_fn || !L.g.n) return;
+  E.sc.lvl_prev.ensure(E.mem, L.g.n);
+  HL_CUDA(cudaMemcpyAsync(E.sc.lvl_prev.p, L.s_cur.p, sizeof(u32) * L.g.n,
+                          cudaMemcpyDeviceToDevice, E.stream));
+}
+
+static void level_emit(Engine& E, Level& L, u32 p) {
+  if (!E.level_fn) return;
+  const u32 n = L.g.n;
+  std::vector<u32> nodes, ids;
+  if (n) {
+    Scratch& S = E.sc;
+    S.lvl_flag.ensure(E.mem, n);
+    S.lvl_nodes.ensure(E.mem, n);
+    S.lvl_ids.ensure(E.mem, n);
+    S.cnt.ensure(E.mem, 16);
+    const u32 g = (u32)std::min<u64>((n + 255) / 256, 148ull * 32);
+    ++E.nlaunch, k_changed_flags<<<g, 256, 0, E.stream>>>(S.lvl_prev.p, L.s_cur.p, n, S.lvl_flag.p);
+    HL_LAUNCH_CHECK();
+    u8* fl = S.lvl_flag.p;
+    u32* out = S.lvl_nodes.p;
+    u32* cnt = S.cnt.p + 14;
+    cub_run(E, [&](void* t, size_t& b) {
+      return cub::DeviceSelect::Flagged(t, b, cub::CountingInputIterator<u32>(0), fl, out, cnt,
+                                        (int64_t)n, E.stream);
+    });
+    const u32 m = E.read_u32(cnt);
+    if (m) {
+      ++E.nlaunch, k_gather_u32<<<(u32)std::min<u64>((m + 255) / 256, 148ull * 32), 256, 0,
+                                   E.stream>>>(out, m, L.s_cur.p, S.lvl_ids.p);
+      HL_LAUNCH_CHECK();
+      nodes.resize(m);
+      ids.resize(m);
+      HL_CUDA(cudaMemcpyAsync(nodes.data(), out, sizeof(u32) * m, cudaMemcpyDeviceToHost,
+                              E.stream));
+      HL_CUDA(cudaMemcpyAsync(ids.data(), S.lvl_ids.p, sizeof(u32) * m, cudaMemcpyDeviceToHost,
+                              E.stream));
+      E.sync();
+    }
+  }
+  E.level_fn(E.level_user, p, (uint64_t)nodes.size(), nodes.data(), ids.data());
+}
+
 static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
   Engine& E = *B.E;
   hl_batch_stats& st = E.st;
@@ -214,7 +271,9 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
     apply_delta(E, L, delta, L.g.n, (E.cfg.flags & HL_FLAG_KEEP_SELF_LOOPS) != 0);
     MoveOut mo = inc_movement(E, L, delta, delta.k == 0, false);
     st.changed = count_flags(E, E.sc.changed.p, L.g.n);
+    level_snapshot(E, L);
     RefineOut ro = inc_refinement(E, L, false);
+    level_emit(E, L, 0);
     st.iterations += mo.iterations;
     st.moves += mo.moves;
     st.candidates += mo.candidates;
@@ -247,11 +306,13 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
     if (p == 0) st.changed = count_flags(E, E.sc.changed.p, L.g.n);
     e0 = E.kt_begin();
     RefineOut ro;
+    level_snapshot(E, L);
     {
       NvtxScope r("refine");
       ro = inc_refinement(E, L, true);
     }
     E.kt_end(KT_STAGE_REFINE, e0);
+    level_emit(E, L, p);
     st.iterations += mo.iterations;
     st.moves += mo.moves;
     st.candidates += mo.candidates;
@@ -552,6 +613,11 @@ hl_status hl_set_resolution(hl_graph* g, double gamma) {
   HL_TRY(require(g != nullptr, "graph handle is NULL");
          require(std::isfinite(gamma), "resolution must be finite");
          box(g)->E->cfg.resolution = gamma);
+}
+
+hl_status hl_set_level_callback(hl_graph* g, hl_level_fn fn, void* user) {
+  HL_TRY(require(g != nullptr, "graph handle is NULL"); box(g)->E->level_fn = fn;
+         box(g)->E->level_user = fn ? user : nullptr);
 }
 
 hl_status hl_set_mode(hl_graph* g, uint32_t mode) {

@@ -98,6 +98,9 @@ struct Scratch {
   DBuf<double> det_bw, det_wsp;
   DBuf<u64> det_out, det_k64, det_k64b;
   DBuf<u8> det_wvalid;
+  // per-level output: the level's s_cur before the batch, the changed nodes
+  DBuf<u32> lvl_prev, lvl_nodes, lvl_ids;
+  DBuf<u8> lvl_flag;
 };
 
 // Per-kernel device timing (CUDA events on the engine's stream), enabled by
@@ -151,6 +154,9 @@ struct Engine {
   // per-call statistics
   hl_batch_stats st{};
   std::vector<std::pair<u32, u32>> new_ids;  // (new sub-community id, origin) of the last refinement
+  // per-level output (hl_set_level_callback): called after each level's refinement
+  hl_level_fn level_fn = nullptr;
+  void* level_user = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // kernel timing
   bool ktiming = false;

@@ -21,6 +21,8 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <limits>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <stdexcept>
@@ -58,8 +60,11 @@ struct Request {
   Clock::time_point t_submit, t_admit;
 };
 
+struct LevelCtx;  // per-graph context of the per-level output trampoline
+
 struct GraphSlot {
   hl_graph* g = nullptr;
+  std::unique_ptr<LevelCtx> lvl;  // stable address handed to the handle's callback
   std::deque<Request> pending;  // admitted, waiting for the graph
   bool busy = false;
   bool queued = false;          // in the ready list
@@ -67,6 +72,19 @@ struct GraphSlot {
   uint64_t bytes = 0;           // device bytes the handle holds (refreshed by
                                 // the worker that last updated it)
 };
+
+// The graph and batch a handle's level callback belongs to, and when its
+// level 0 was ready.
+struct LevelCtx {
+  hl_server* server = nullptr;
+  uint32_t graph = 0;
+  uint64_t batch_id = 0;
+  bool have_l0 = false;
+  Clock::time_point t_l0;
+};
+
+void level_trampoline(void* user, uint32_t level, uint64_t count, const uint32_t* nodes,
+                      const uint32_t* ids);
 
 }  // namespace
 
@@ -87,6 +105,8 @@ struct hl_server {
   uint64_t bytes_per_edge = 512;
   uint32_t max_coalesce = 0;        // requests per batch at most (0 = all pending)
   bool stop = false;
+  std::atomic<hl_server_level_fn> level_fn{nullptr};  // per-level output, if set
+  std::atomic<void*> level_user{nullptr};
 
   uint64_t resident_bytes() const {
     uint64_t s = 0;
@@ -173,6 +193,15 @@ struct hl_server {
           else w.insert(w.end(), r.w.begin(), r.w.end());
         }
       }
+      LevelCtx* lc = nullptr;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        lc = graphs[gid].lvl.get();
+      }
+      lc->batch_id = batch_id;
+      lc->have_l0 = false;
+      if (level_fn.load()) hl_set_level_callback(g, level_trampoline, lc);
+      else hl_set_level_callback(g, nullptr, nullptr);
       const Clock::time_point t0 = Clock::now();
       hl_batch_stats st{};
       std::string err;
@@ -198,6 +227,8 @@ struct hl_server {
           d.queue_ms = ms_between(r.t_submit, t0);
           d.service_ms = ms_between(t0, t1);
           d.latency_ms = ms_between(r.t_submit, t1);
+          d.level0_ms = lc->have_l0 ? ms_between(r.t_submit, lc->t_l0)
+                                    : std::numeric_limits<double>::quiet_NaN();
           done.push_back(d);
           reserved -= r.estimate;
           --outstanding;
@@ -218,6 +249,17 @@ struct hl_server {
 };
 
 namespace {
+
+void level_trampoline(void* user, uint32_t level, uint64_t count, const uint32_t* nodes,
+                      const uint32_t* ids) {
+  LevelCtx* c = static_cast<LevelCtx*>(user);
+  if (level == 0) {
+    c->t_l0 = Clock::now();
+    c->have_l0 = true;
+  }
+  hl_server_level_fn fn = c->server->level_fn.load();
+  if (fn) fn(c->server->level_user.load(), c->graph, c->batch_id, level, count, nodes, ids);
+}
 
 #define HLM_TRY(...)                   \
   try {                                \
@@ -304,6 +346,9 @@ HL_API hl_status hl_server_add_graph(hl_server* S, hl_graph* g, uint32_t* graph_
   HLM_TRY(need(S && g && graph_id, "NULL argument"); std::lock_guard<std::mutex> lk(S->mu);
           for (const GraphSlot& x : S->graphs) need(x.g != g, "graph already registered");
           S->graphs.emplace_back(); S->graphs.back().g = g;
+          S->graphs.back().lvl.reset(new LevelCtx());
+          S->graphs.back().lvl->server = S;
+          S->graphs.back().lvl->graph = (uint32_t)(S->graphs.size() - 1);
           S->graphs.back().bytes = hl::handle_device_bytes(g);
           *graph_id = (uint32_t)(S->graphs.size() - 1));
 }
@@ -348,6 +393,11 @@ HL_API hl_status hl_server_poll(hl_server* S, hl_request_done* out, uint32_t cap
           *count = n);
 }
 
+HL_API hl_status hl_server_set_level_callback(hl_server* S, hl_server_level_fn fn, void* user) {
+  HLM_TRY(need(S != nullptr, "NULL argument"); S->level_user.store(fn ? user : nullptr);
+          S->level_fn.store(fn));
+}
+
 HL_API hl_status hl_server_drain(hl_server* S) {
   HLM_TRY(need(S != nullptr, "NULL argument"); std::unique_lock<std::mutex> lk(S->mu);
           S->cv_done.wait(lk, [&] { return S->outstanding == 0; }));
@@ -362,6 +412,7 @@ HL_API void hl_server_destroy(hl_server* S) {
   }
   S->cv_work.notify_all();
   for (std::thread& t : S->workers) t.join();
+  for (GraphSlot& x : S->graphs) hl_set_level_callback(x.g, nullptr, nullptr);
   delete S;
 }
 

@@ -157,6 +157,23 @@ HL_API hl_status hl_reset_kernel_stats(hl_graph* g);
  * hit_leiden.rs:939). */
 HL_API hl_status hl_set_resolution(hl_graph* g, double gamma);
 
+/* Per-level output: the reference's goal of emitting stabilised communities
+ * as soon as they are ready instead of after the whole pass (README.md,
+ * "Incremental community output"; no entry point in the crate).  While a
+ * callback is set, hl_apply_batch calls it once per level, in level order,
+ * right after that level's refinement: from there on the batch no longer
+ * changes the level's sub-community map (s_cur^p, the refined communities
+ * whose summaries a pipeline builds bottom-up).  It receives the level-p
+ * nodes whose sub-community changed in this batch and their new
+ * sub-community ids, in ascending node order (host arrays, valid during the
+ * call only).  The communities f^p of every level are final when
+ * hl_apply_batch returns.  Each call costs one device→host copy of the
+ * level's changes.  fn == NULL turns it off.  The callback runs on the thread
+ * that applies the batch and must not call back into this handle. */
+typedef void (*hl_level_fn)(void* user, uint32_t level, uint64_t count, const uint32_t* nodes,
+                            const uint32_t* sub_ids);
+HL_API hl_status hl_set_level_callback(hl_graph* g, hl_level_fn fn, void* user);
+
 /* Change the RunMode for subsequent batches (hit_leiden takes it per call,
  * hit_leiden.rs:940): HL_MODE_DETERMINISTIC or HL_MODE_THROUGHPUT. */
 HL_API hl_status hl_set_mode(hl_graph* g, uint32_t mode);
@@ -239,6 +256,8 @@ typedef struct {
   uint32_t batch_requests; /* requests coalesced into that batch                */
   int32_t status;          /* hl_status of the batch                            */
   uint32_t pad_;
+  double level0_ms;        /* submit -> its batch's level-0 sub-communities     */
+                           /* settled (NaN without a server level callback)     */
 } hl_request_done;
 
 HL_API hl_status hl_server_create(uint32_t workers, uint64_t hbm_budget, hl_server** out);
@@ -255,6 +274,16 @@ HL_API hl_status hl_server_submit(hl_server* s, uint32_t graph_id, const uint32_
  * is outstanding, > 0 = wait at most that long. */
 HL_API hl_status hl_server_poll(hl_server* s, hl_request_done* out, uint32_t cap, uint32_t* count,
                                 int32_t wait_ms);
+/* Per-level output of the served batches: fn gets the graph id and the
+ * batch id with each level's changed sub-communities (hl_set_level_callback),
+ * from the worker thread applying the batch, before the batch's requests
+ * complete; level0_ms in the completion records then says when level 0 was
+ * ready.  Set it before submitting; fn == NULL turns it off.  The server sets
+ * the level callback of its graphs' handles while it holds them, and clears
+ * it when it is destroyed. */
+typedef void (*hl_server_level_fn)(void* user, uint32_t graph, uint64_t batch_id, uint32_t level,
+                                   uint64_t count, const uint32_t* nodes, const uint32_t* sub_ids);
+HL_API hl_status hl_server_set_level_callback(hl_server* s, hl_server_level_fn fn, void* user);
 /* Wait until every submitted request has completed. */
 HL_API hl_status hl_server_drain(hl_server* s);
 /* Waits for outstanding requests, then stops the workers. */

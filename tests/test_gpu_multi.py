@@ -163,3 +163,96 @@ def test_server_admission_within_budget_and_rejection():
     assert done[big]["status"] == L.HL_ERR_OUT_OF_MEMORY
     for s in A:
         s.close()
+
+
+def test_server_each_request_same_alone_and_in_mix_within_tolerance():
+    """Coalescing changes the batches, so the mix is not bit-identical to each
+    request applied alone; the bar is |ΔQ| <= 2e-3.  At the end of every
+    coalesced batch the graph has seen a prefix of its requests in arrival
+    order; a copy that applies those requests one per batch must be within
+    2e-3 of the modularity the server reported for that batch."""
+    grs = _graphs(3, 13, n_lo=1500, n_hi=3000)
+    A = [hl.PartitionState.load(hl.GraphInput.from_arrays("g", *g),
+                                hl.RunConfig(mode=hl.RunMode.Throughput, batch_modularity=True))
+         for g in grs]
+    C = [_load(g) for g in grs]
+    rng = np.random.default_rng(17)
+    reqs = {}
+    with hl.Server(workers=1) as srv:  # one worker: requests pile up and coalesce
+        ids = [srv.add(s) for s in A]
+        for r in range(60):
+            gi = int(rng.integers(0, len(grs)))
+            u, v, w = _batch(grs[gi], int(rng.integers(5, 60)), 2000 + r)
+            reqs[srv.submit(ids[gi], u, v, w)] = (gi, u, v, w)
+        srv.drain()
+        done = []
+        while True:
+            part = srv.poll(cap=64)
+            if not part:
+                break
+            done += part
+    assert all(d["status"] == 0 for d in done)
+    batches = {}
+    for d in done:
+        batches.setdefault((d["graph"], d["batch_seq"]), []).append(d)
+    assert any(len(x) > 1 for x in batches.values()), "no request was coalesced"
+    worst = 0.0
+    for (gi, seq) in sorted(batches):
+        recs = sorted(batches[(gi, seq)], key=lambda d: d["request_id"])
+        for d in recs:  # alone: one request per batch, in arrival order
+            _, u, v, w = reqs[d["request_id"]]
+            C[gi].apply_batch(u, v, w)
+        q_alone = C[gi].modularity()
+        q_mix = recs[0]["modularity"]
+        worst = max(worst, abs(q_alone - q_mix))
+        assert abs(q_alone - q_mix) <= 2e-3, (gi, seq, q_alone, q_mix)
+    for s in A + C:
+        s.close()
+
+
+def test_level_callback_reports_each_settled_level():
+    g = _graphs(1, 21, n_lo=2500, n_hi=3000)[0]
+    st = _load(g)
+    before = [m.copy() for m in st.current_subcommunity_mapping_per_level]
+    seen = []
+    st.set_level_callback(lambda level, nodes, ids: seen.append((level, nodes, ids)))
+    st.apply_batch(*_batch(g, 200, 5))
+    st.set_level_callback(None)
+    after = st.current_subcommunity_mapping_per_level
+    assert [x[0] for x in seen] == list(range(st.levels))
+    for level, nodes, ids in seen:
+        assert np.all(np.diff(nodes.astype(np.int64)) > 0)
+        assert np.array_equal(ids, after[level][nodes])
+        old = len(before[level])
+        moved = np.nonzero(before[level] != after[level][:old])[0]
+        assert np.array_equal(nodes[nodes < old], moved), level
+    # off again: no more calls
+    n0 = len(seen)
+    st.apply_batch(*_batch(g, 50, 6))
+    assert len(seen) == n0
+    st.close()
+
+
+def test_server_emits_levels_before_completion():
+    grs = _graphs(3, 23)
+    A = [_load(g) for g in grs]
+    events = []
+    with hl.Server(workers=2) as srv:
+        srv.set_level_callback(lambda graph, batch, level, nodes, ids:
+                               events.append((graph, batch, level, len(nodes))))
+        ids = [srv.add(s) for s in A]
+        for r in range(12):
+            gi = r % len(grs)
+            srv.submit(ids[gi], *_batch(grs[gi], 30, 3000 + r))
+        srv.drain()
+        done = srv.poll(cap=64)
+    assert len(done) == 12 and all(d["status"] == 0 for d in done)
+    per_batch = {}
+    for graph, batch, level, _ in events:
+        per_batch.setdefault(batch, []).append(level)
+    for d in done:
+        levels = per_batch[d["batch_id"]]
+        assert levels == list(range(len(levels))) and len(levels) == A[d["graph"]].levels
+        assert 0.0 <= d["level0_ms"] <= d["latency_ms"]
+    for s in A:
+        s.close()
