@@ -146,6 +146,7 @@ def _load():
         "hl_dbg_seq_sums": (st, [C.c_int32, C.c_uint32, vp, vp, C.c_double, C.c_int32, vp]),
         "hl_dbg_set_exact_tfilter": (st, [C.c_int32]),
         "hl_dbg_set_mode": (st, [C.c_uint32]),
+        "hl_dbg_set_bucket_slots": (st, [C.c_uint32]),
         "hl_tree_sum_noalloc": (st, [vp, C.c_uint64, vp, vp]),
         "hl_dbg_modularity": (st, [C.c_int32, C.c_uint32, vp, vp, vp, vp,
                                    C.POINTER(C.c_double)]),

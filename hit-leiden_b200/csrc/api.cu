@@ -997,6 +997,11 @@ hl_status hl_dbg_set_exact_tfilter(int32_t on) {
   return HL_OK;
 }
 
+hl_status hl_dbg_set_bucket_slots(uint32_t slots) {
+  g_pb_slots.store(slots ? slots : 4096u);
+  return HL_OK;
+}
+
 hl_status hl_dbg_set_mode(uint32_t mode) {
   if (mode != HL_MODE_DETERMINISTIC && mode != HL_MODE_THROUGHPUT) {
     g_err = "mode must be HL_MODE_DETERMINISTIC or HL_MODE_THROUGHPUT";

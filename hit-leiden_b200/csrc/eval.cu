@@ -793,6 +793,314 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
 }
 
 // ---------------------------------------------------------------------------
+// Second pass for integral weights: the rows deferred by pass 1 (more than
+// BIG_TAB / 2 distinct keys) are hash-partitioned into buckets that fit a
+// shared-memory table, so that every block of the GPU folds one bucket
+// instead of a few blocks walking global tables.  Integral sums are exact in
+// any order, and a key's first CSR position is the minimum of its entries'
+// positions, so neither the partition order nor the fold order matters.
+//   plan     per row: buckets B = 2^k >= deg / PB_TARGET, 4096-entry chunks;
+//   hist     per chunk: each entry's key (saved), its bucket's count, and the
+//            row's w(v, cur);
+//   scatter  per chunk: (key, position, weight) into its bucket's range;
+//   fold     per bucket: shared table, then the bucket's best candidate;
+//   final    per row: the best over its buckets, then the empty community.
+// A bucket whose keys overflow its table (more than PB_TAB / 2 distinct: far
+// out in the tail of the hash spread) fails its row, which then takes the
+// global-table pass.
+// ---------------------------------------------------------------------------
+constexpr u32 PB_TARGET = 1024;  // expected entries per bucket
+constexpr u32 PB_TAB = 4096;     // table slots of the fold kernel
+constexpr u32 PB_CHUNK = 4096;   // entries per block of the hist / scatter kernels
+constexpr u32 PB_HIST = 8192;    // buckets a block counts in shared memory
+
+__global__ void k_pb_plan(const u32* ovf, const u32* novf, const u32* verts, const u64* off,
+                          u32* nb, u64* ne, u32* nc) {
+  const u32 m = *novf;
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < m; t += (u64)gridDim.x * blockDim.x) {
+    const u32 v = verts[ovf[t]];
+    const u64 d = off[v + 1] - off[v];
+    u32 b = 1;
+    while ((u64)b * PB_TARGET < d) b <<= 1;
+    nb[t] = b;
+    ne[t] = d;
+    nc[t] = (u32)((d + PB_CHUNK - 1) / PB_CHUNK);
+  }
+}
+
+// Largest r in [lo, hi) with base[r] <= x (base ascending, base[lo] <= x).
+template <typename T>
+__device__ __forceinline__ u32 pb_row_of(const T* base, u32 lo, u32 hi, T x) {
+  while (hi - lo > 1) {
+    const u32 mid = (lo + hi) >> 1;
+    if (base[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+struct PbArgs {
+  const u32* ovf;      // deferred idx values
+  const u32* nb;       // buckets per row
+  const u64* ebase;    // exclusive scan of row degrees
+  const u32* bbase;    // exclusive scan of bucket counts
+  const u32* cbase;    // exclusive scan of chunk counts
+  u32 r0, r1;          // rows of this round
+  u64 e0;              // ebase[r0]
+  u32 b0, c0, c1;      // bbase[r0], cbase[r0], the round's end chunk
+  u32* ktmp;           // entry keys (NONE32: skipped)
+  u32* bcnt;           // per bucket: count, then scatter cursor
+  u32* boff;           // per bucket: first entry (exclusive scan of bcnt)
+  u32* ekey;
+  u32* epos;
+  double* ew;
+  double* wcur;        // per row w(v, cur)
+  double* bg;          // per bucket best gain, position, key
+  u32* bp;
+  u32* bk;
+  u32* rowfail;        // per row: a bucket overflowed
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(256) k_pb_hist(EvalArgs A, PbArgs P) {
+  __shared__ u32 s_hist[PB_HIST];
+  __shared__ double s_red[8];
+  __shared__ u32 s_row;
+  for (u32 c = P.c0 + blockIdx.x; c < P.c1; c += gridDim.x) {
+    if (threadIdx.x == 0) s_row = pb_row_of(P.cbase, P.r0, P.r1, c);
+    __syncthreads();
+    const u32 r = s_row;
+    const u32 i = P.ovf[r];
+    const u32 v = A.verts[i];
+    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u64 lo = o0 + (u64)(c - P.cbase[r]) * PB_CHUNK;
+    const u64 hi = lo + PB_CHUNK < o1 ? lo + PB_CHUNK : o1;
+    const u32 fv = A.f[v];
+    const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+    const u32 B = P.nb[r];
+    const bool local = B <= PB_HIST;
+    u32* gcnt = P.bcnt + (P.bbase[r] - P.b0);
+    if (local)
+      for (u32 x = threadIdx.x; x < B; x += blockDim.x) s_hist[x] = 0;
+    __syncthreads();
+    double wc = 0.0;
+    const u64 ebase = P.ebase[r] - P.e0 + (lo - o0);
+    for (u64 q = lo + threadIdx.x; q < hi; q += blockDim.x) {
+      u32 key = NONE32;
+      if (!entry_key<KIND>(A, v, A.col[q], fv, key)) key = NONE32;
+      P.ktmp[ebase + (q - lo)] = key;
+      if (key == NONE32) continue;
+      if (key == cur) wc += A.w[q];
+      const u32 b = hash32(key) & (B - 1);
+      if (local) atomicAdd(&s_hist[b], 1u);
+      else atomicAdd(&gcnt[b], 1u);
+    }
+    for (int o = 16; o; o >>= 1) wc += __shfl_xor_sync(0xffffffffu, wc, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = wc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (u32 x = 0; x < blockDim.x / 32; ++x) t += s_red[x];
+      if (t != 0.0) atomicAdd(&P.wcur[r], t);  // integral: exact in any order
+    }
+    if (local)
+      for (u32 x = threadIdx.x; x < B; x += blockDim.x)
+        if (s_hist[x]) atomicAdd(&gcnt[x], s_hist[x]);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
+  __shared__ u32 s_row;
+  for (u32 c = P.c0 + blockIdx.x; c < P.c1; c += gridDim.x) {
+    if (threadIdx.x == 0) s_row = pb_row_of(P.cbase, P.r0, P.r1, c);
+    __syncthreads();
+    const u32 r = s_row;
+    const u32 v = A.verts[P.ovf[r]];
+    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u64 lo = o0 + (u64)(c - P.cbase[r]) * PB_CHUNK;
+    const u64 hi = lo + PB_CHUNK < o1 ? lo + PB_CHUNK : o1;
+    const u32 B = P.nb[r];
+    u32* cursor = P.bcnt + (P.bbase[r] - P.b0);
+    const u32* start = P.boff + (P.bbase[r] - P.b0);
+    const u64 ebase = P.ebase[r] - P.e0 + (lo - o0);
+    for (u64 q = lo + threadIdx.x; q < hi; q += blockDim.x) {
+      const u32 key = P.ktmp[ebase + (q - lo)];
+      if (key == NONE32) continue;
+      const u32 b = hash32(key) & (B - 1);
+      const u32 slot = start[b] + atomicAdd(&cursor[b], 1u);
+      P.ekey[slot] = key;
+      P.epos[slot] = (u32)(q - o0);
+      P.ew[slot] = A.w[q];
+    }
+    __syncthreads();
+  }
+}
+
+constexpr size_t PB_FOLD_SMEM = (size_t)PB_TAB * (8 + 4 + 4);
+
+// Table slots the fold kernel may use (hl_dbg_set_bucket_slots lowers it so
+// that tests reach the overflow path).
+std::atomic<u32> g_pb_slots{PB_TAB};
+
+template <int KIND>
+__global__ void __launch_bounds__(256) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuckets,
+                                                 u32 tab_limit) {
+  extern __shared__ __align__(16) unsigned char pb_smem[];
+  unsigned long long* s_tv = reinterpret_cast<unsigned long long*>(pb_smem);
+  u32* s_tk = reinterpret_cast<u32*>(s_tv + PB_TAB);
+  u32* s_tp = s_tk + PB_TAB;
+  __shared__ double r_g[8];
+  __shared__ u32 r_p[8], r_k[8];
+  __shared__ u32 s_row, s_ovf;
+  const u32 tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  unsigned long long ncand = 0;
+  for (u32 bl = blockIdx.x; bl < nbuckets; bl += gridDim.x) {
+    const u32 b = P.b0 + bl;
+    if (tid == 0) {
+      s_row = pb_row_of(P.bbase, P.r0, P.r1, b);
+      s_ovf = 0;
+    }
+    const u32 e_lo = P.boff[bl], e_hi = P.boff[bl + 1];
+    const u32 cnt = e_hi - e_lo;
+    u32 cap = 64;
+    while (cap < 2 * cnt && cap < tab_limit) cap <<= 1;
+    for (u32 x = tid; x < cap; x += 256) {
+      s_tk[x] = NONE32;
+      s_tp[x] = NONE32;
+      s_tv[x] = 0ull;
+    }
+    __syncthreads();
+    const u32 r = s_row;
+    const u32 mask = cap - 1;
+    for (u32 e = e_lo + tid; e < e_hi; e += 256) {
+      const u32 key = P.ekey[e];
+      u32 slot = hash32(key) & mask;
+      u32 probes = 0;
+      bool ok = false;
+      while (probes++ < cap) {
+        const u32 prev = atomicCAS(&s_tk[slot], NONE32, key);
+        if (prev == NONE32 || prev == key) {
+          ok = true;
+          break;
+        }
+        slot = (slot + 1) & mask;
+      }
+      if (!ok) {
+        s_ovf = 1;
+        continue;
+      }
+      // integral weights: the running sum is an exact integer
+      atomicAdd(&s_tv[slot], (unsigned long long)(long long)P.ew[e]);
+      atomicMin(&s_tp[slot], P.epos[e]);
+    }
+    __syncthreads();
+    double g = -1.0;
+    u32 p = NONE32, kk = NONE32;
+    if (!s_ovf && A.tw != 0.0) {
+      const u32 i = P.ovf[r];
+      const u32 v = A.verts[i];
+      const u32 cur = (KIND == EVAL_MOVE) ? A.f[v] : A.s[v];
+      const double kv = A.kdeg[v];
+      const double wcur = P.wcur[r];
+      const double dcur = A.d[cur];
+      for (u32 x = tid; x < cap; x += 256) {
+        const u32 key = s_tk[x];
+        if (key == NONE32 || key == cur) continue;
+        if (KIND == EVAL_REFINE && A.blocked[key]) continue;
+        const double val = (double)(long long)s_tv[x];
+        const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, A.d[key]);
+        ++ncand;
+        const u32 pp = s_tp[x];
+        if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+          g = gn;
+          p = pp;
+          kk = key;
+        }
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      const double og = __shfl_xor_sync(0xffffffffu, g, o);
+      const u32 op = __shfl_xor_sync(0xffffffffu, p, o);
+      const u32 ok = __shfl_xor_sync(0xffffffffu, kk, o);
+      if (op != NONE32 && (p == NONE32 || og > g || (og == g && op < p))) {
+        g = og;
+        p = op;
+        kk = ok;
+      }
+    }
+    if (lane == 0) {
+      r_g[wib] = g;
+      r_p[wib] = p;
+      r_k[wib] = kk;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (u32 x = 1; x < 8; ++x)
+        if (r_p[x] != NONE32 && (p == NONE32 || r_g[x] > g || (r_g[x] == g && r_p[x] < p))) {
+          g = r_g[x];
+          p = r_p[x];
+          kk = r_k[x];
+        }
+      P.bg[bl] = g;
+      P.bp[bl] = p;
+      P.bk[bl] = kk;
+      if (s_ovf) P.rowfail[r] = 1;
+    }
+    __syncthreads();
+  }
+  block_count(A, 0, ncand);
+}
+
+// One warp per row: the best over the row's buckets, then the decision.
+template <int KIND>
+__global__ void k_pb_final(EvalArgs A, PbArgs P, u32* fail_list, u32* fail_count) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  unsigned long long trav = 0;
+  for (u64 r = P.r0 + warp; r < P.r1; r += nwarps) {
+    const u32 i = P.ovf[r];
+    if (P.rowfail[r]) {
+      if (lane == 0) fail_list[atomicAdd(fail_count, 1u)] = i;
+      continue;
+    }
+    const u32 v = A.verts[i];
+    const u32 B = P.nb[r];
+    const u32 bb = P.bbase[r] - P.b0;
+    double g = -1.0;
+    u32 p = NONE32, kk = NONE32;
+    for (u32 x = lane; x < B; x += 32) {
+      const u32 pp = P.bp[bb + x];
+      if (pp == NONE32) continue;
+      const double gn = P.bg[bb + x];
+      if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+        g = gn;
+        p = pp;
+        kk = P.bk[bb + x];
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      const double og = __shfl_xor_sync(0xffffffffu, g, o);
+      const u32 op = __shfl_xor_sync(0xffffffffu, p, o);
+      const u32 ok = __shfl_xor_sync(0xffffffffu, kk, o);
+      if (op != NONE32 && (p == NONE32 || og > g || (og == g && op < p))) {
+        g = og;
+        p = op;
+        kk = ok;
+      }
+    }
+    if (lane == 0) {
+      const u32 fv = A.f[v];
+      const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+      trav += A.off[v + 1] - A.off[v];
+      finish<KIND>(A, i, v, cur, A.kdeg[v], P.wcur[r], g, kk, p != NONE32);
+    }
+  }
+  block_count(A, trav, 0);
+}
+
+// ---------------------------------------------------------------------------
 // Host side: bin the list by degree and launch the three kernels.
 // ---------------------------------------------------------------------------
 __global__ void k_bin(const u32* verts, u32 nv, const u64* off, u32* bin, u32* idx,
@@ -838,6 +1146,119 @@ constexpr u32 WIDE_MAX_BLOCKS = 148u * 3u;
 constexpr u32 BIG_MAX_BLOCKS = 148u * 3u;
 constexpr u32 OVF_BLOCKS = 32;  // least blocks (global regions) for rows deferred by pass 1
 constexpr u64 OVF_TABLE_BYTES = 4ull << 30;  // table bytes pass 2 may spread over its blocks
+
+// The partitioned second pass over the rows pass 1 deferred (integral
+// weights).  Rows are taken in rounds whose entries fit PB_ROUND_ENTRIES;
+// rows with an overflowing bucket are returned in S.pb_fail (count in
+// S.pb_failcnt[0]) for the global-table pass.  Returns that count.
+constexpr u64 PB_ROUND_ENTRIES = 96ull << 20;
+
+template <int KIND>
+static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
+  Scratch& S = E.sc;
+  cudaStream_t st = E.stream;
+  const u32 m = E.read_u32(S.ovf_cnt.p);
+  if (!m) return 0;
+  S.pb_nb.ensure(E.mem, m);
+  S.pb_nc.ensure(E.mem, m);
+  S.pb_bbase.ensure(E.mem, m);
+  S.pb_cbase.ensure(E.mem, m);
+  S.pb_ne.ensure(E.mem, m);
+  S.pb_ebase.ensure(E.mem, m);
+  S.pb_wcur.ensure(E.mem, m);
+  S.pb_rowfail.ensure(E.mem, m);
+  S.pb_fail.ensure(E.mem, m);
+  S.pb_failcnt.ensure(E.mem, 2);
+  ++E.nlaunch, k_pb_plan<<<grid_for(m), 256, 0, st>>>(S.ovf.p, S.ovf_cnt.p, a.verts, a.off,
+                                                       S.pb_nb.p, S.pb_ne.p, S.pb_nc.p);
+  HL_LAUNCH_CHECK();
+  {
+    u32* x = S.pb_nb.p;
+    u32* y = S.pb_bbase.p;
+    cub_run(E, [&](void* t, size_t& b) { return cub::DeviceScan::ExclusiveSum(t, b, x, y, (int64_t)m, st); });
+    u32* x2 = S.pb_nc.p;
+    u32* y2 = S.pb_cbase.p;
+    cub_run(E, [&](void* t, size_t& b) { return cub::DeviceScan::ExclusiveSum(t, b, x2, y2, (int64_t)m, st); });
+    u64* x3 = S.pb_ne.p;
+    u64* y3 = S.pb_ebase.p;
+    cub_run(E, [&](void* t, size_t& b) { return cub::DeviceScan::ExclusiveSum(t, b, x3, y3, (int64_t)m, st); });
+  }
+  HL_CUDA(cudaMemsetAsync(S.pb_wcur.p, 0, sizeof(double) * m, st));
+  HL_CUDA(cudaMemsetAsync(S.pb_rowfail.p, 0, sizeof(u32) * m, st));
+  HL_CUDA(cudaMemsetAsync(S.pb_failcnt.p, 0, sizeof(u32) * 2, st));
+  // the per-row plan on the host, to cut the rows into rounds
+  std::vector<u64> ne(m), eb(m);
+  std::vector<u32> nb(m), bb(m), nc(m), cb(m);
+  HL_CUDA(cudaMemcpyAsync(ne.data(), S.pb_ne.p, sizeof(u64) * m, cudaMemcpyDeviceToHost, st));
+  HL_CUDA(cudaMemcpyAsync(eb.data(), S.pb_ebase.p, sizeof(u64) * m, cudaMemcpyDeviceToHost, st));
+  HL_CUDA(cudaMemcpyAsync(nb.data(), S.pb_nb.p, sizeof(u32) * m, cudaMemcpyDeviceToHost, st));
+  HL_CUDA(cudaMemcpyAsync(bb.data(), S.pb_bbase.p, sizeof(u32) * m, cudaMemcpyDeviceToHost, st));
+  HL_CUDA(cudaMemcpyAsync(nc.data(), S.pb_nc.p, sizeof(u32) * m, cudaMemcpyDeviceToHost, st));
+  HL_CUDA(cudaMemcpyAsync(cb.data(), S.pb_cbase.p, sizeof(u32) * m, cudaMemcpyDeviceToHost, st));
+  E.sync();
+  PbArgs P;
+  P.ovf = S.ovf.p;
+  P.nb = S.pb_nb.p;
+  P.ebase = S.pb_ebase.p;
+  P.bbase = S.pb_bbase.p;
+  P.cbase = S.pb_cbase.p;
+  P.wcur = S.pb_wcur.p;
+  P.rowfail = S.pb_rowfail.p;
+  u32 r0 = 0;
+  while (r0 < m) {
+    u32 r1 = r0 + 1;
+    while (r1 < m && eb[r1] + ne[r1] - eb[r0] <= PB_ROUND_ENTRIES) ++r1;
+    const u64 te = eb[r1 - 1] + ne[r1 - 1] - eb[r0];
+    const u32 tb = bb[r1 - 1] + nb[r1 - 1] - bb[r0];
+    S.pb_ktmp.ensure(E.mem, te);
+    S.pb_ekey.ensure(E.mem, te);
+    S.pb_epos.ensure(E.mem, te);
+    S.pb_ew.ensure(E.mem, te);
+    S.pb_bcnt.ensure(E.mem, (size_t)tb + 1);
+    S.pb_boff.ensure(E.mem, (size_t)tb + 1);
+    S.pb_bg.ensure(E.mem, tb);
+    S.pb_bp.ensure(E.mem, tb);
+    S.pb_bk.ensure(E.mem, tb);
+    P.ktmp = S.pb_ktmp.p;
+    P.bcnt = S.pb_bcnt.p;
+    P.boff = S.pb_boff.p;
+    P.ekey = S.pb_ekey.p;
+    P.epos = S.pb_epos.p;
+    P.ew = S.pb_ew.p;
+    P.bg = S.pb_bg.p;
+    P.bp = S.pb_bp.p;
+    P.bk = S.pb_bk.p;
+    P.r0 = r0;
+    P.r1 = r1;
+    P.e0 = eb[r0];
+    P.b0 = bb[r0];
+    P.c0 = cb[r0];
+    P.c1 = cb[r1 - 1] + nc[r1 - 1];
+    const u32 nchunks = P.c1 - P.c0;
+    const u32 cgrid = nchunks < 148u * 8u ? nchunks : 148u * 8u;
+    HL_CUDA(cudaMemsetAsync(S.pb_bcnt.p, 0, sizeof(u32) * ((size_t)tb + 1), st));
+    ++E.nlaunch, k_pb_hist<KIND><<<cgrid, 256, 0, st>>>(a, P);
+    HL_LAUNCH_CHECK();
+    {
+      u32* x = S.pb_bcnt.p;
+      u32* y = S.pb_boff.p;
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, x, y, (int64_t)tb + 1, st);
+      });
+    }
+    HL_CUDA(cudaMemsetAsync(S.pb_bcnt.p, 0, sizeof(u32) * ((size_t)tb + 1), st));
+    ++E.nlaunch, k_pb_scatter<<<cgrid, 256, 0, st>>>(a, P);
+    const u32 fgrid = tb < 148u * 8u ? tb : 148u * 8u;
+    u32 lim = g_pb_slots.load();
+    if (lim < 64 || lim > PB_TAB) lim = PB_TAB;
+    ++E.nlaunch, k_pb_fold<KIND><<<fgrid, 256, PB_FOLD_SMEM, st>>>(a, P, tb, lim);
+    ++E.nlaunch, k_pb_final<KIND><<<grid_for((u64)(r1 - r0) * 32), 256, 0, st>>>(
+        a, P, S.pb_fail.p, S.pb_failcnt.p);
+    HL_LAUNCH_CHECK();
+    r0 = r1;
+  }
+  return E.read_u32(S.pb_failcnt.p);
+}
 
 void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
               const double* d, const u8* blocked, bool allow_empty, u32* out_to, double* out_gain,
@@ -887,6 +1308,10 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
     HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_REFINE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(WideSmem)));
+    HL_CUDA(cudaFuncSetAttribute(k_pb_fold<EVAL_MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)PB_FOLD_SMEM));
+    HL_CUDA(cudaFuncSetAttribute(k_pb_fold<EVAL_REFINE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_FOLD_SMEM));
     g_big_attr_set[dev] = true;
   }
 
@@ -1006,7 +1431,19 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
     else
       ++E.nlaunch, k_eval_big<EVAL_REFINE><<<blocks, BIG_THREADS, big_smem(), st>>>(a);
     HL_LAUNCH_CHECK();
-    if (big_maxdeg > BIG_TAB / 2) {
+    const u32* pass2_list = S.ovf.p;
+    const u32* pass2_count = S.ovf_cnt.p;
+    bool pass2 = big_maxdeg > BIG_TAB / 2;
+    if (pass2 && E.integral) {
+      // Integral weights: the deferred rows go through the partitioned pass;
+      // only rows with an overflowing bucket are left for the global tables.
+      const u32 nfail = kind == EVAL_MOVE ? huge_partitioned<EVAL_MOVE>(E, a)
+                                          : huge_partitioned<EVAL_REFINE>(E, a);
+      pass2 = nfail != 0;
+      pass2_list = S.pb_fail.p;
+      pass2_count = S.pb_failcnt.p;
+    }
+    if (pass2) {
       // Pass 2: the deferred rows (their number is read on the device), on as
       // many blocks as OVF_TABLE_BYTES of global regions allow, each region
       // sized for the largest row of the bin.
@@ -1030,9 +1467,9 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
         HL_LAUNCH_CHECK();
       }
       EvalArgs a2 = a;
-      a2.idx = S.ovf.p;
+      a2.idx = pass2_list;
       a2.nidx = 0;
-      a2.nidx_dev = S.ovf_cnt.p;
+      a2.nidx_dev = pass2_count;
       a2.tkey = S.huge_key.p;
       a2.tpos = S.huge_pos.p;
       a2.tval = S.huge_val.p;

@@ -98,6 +98,11 @@ struct Scratch {
   DBuf<double> det_bw, det_wsp;
   DBuf<u64> det_out, det_k64, det_k64b;
   DBuf<u8> det_wvalid;
+  // partitioned second pass of the block kernel (integral weights)
+  DBuf<u32> pb_nb, pb_nc, pb_bbase, pb_cbase, pb_rowfail, pb_fail, pb_failcnt, pb_ktmp, pb_ekey,
+      pb_epos, pb_bcnt, pb_boff, pb_bp, pb_bk;
+  DBuf<u64> pb_ne, pb_ebase;
+  DBuf<double> pb_wcur, pb_ew, pb_bg;
   // per-level output: the level's s_cur before the batch, the changed nodes
   DBuf<u32> lvl_prev, lvl_nodes, lvl_ids;
   DBuf<u8> lvl_flag;
@@ -234,6 +239,8 @@ u64 merge_singletons_det(Engine& E, Level& L, const u32* rv, u32 nr, u32* sizes,
 
 // Test switch: decide every T-filter candidate from the ordered sum.
 extern std::atomic<int> g_exact_tfilter;
+// Test switch: table slots of the partitioned hub pass (eval.cu).
+extern std::atomic<u32> g_pb_slots;
 
 // aggregate.cu
 u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n,

@@ -91,6 +91,12 @@ HL_API hl_status hl_dbg_set_exact_tfilter(int32_t on);
  * (dual_mode_test!, hit_leiden.rs:1823-1841) run on both GPU paths. */
 HL_API hl_status hl_dbg_set_mode(uint32_t mode);
 
+/* Table slots (64..4096, 0 = 4096) of the partitioned pass that evaluates
+ * hub rows with more than 2048 distinct neighbour keys under integral
+ * weights.  A small table makes buckets overflow, so tests reach the
+ * global-table pass those rows fall back to.  Results do not depend on it. */
+HL_API hl_status hl_dbg_set_bucket_slots(uint32_t slots);
+
 /* Modularity of `part` on the CSR (hit_leiden.rs:121-161). */
 HL_API hl_status hl_dbg_modularity(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
                             const double* w, const uint32_t* part, double* q);

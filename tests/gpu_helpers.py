@@ -81,6 +81,16 @@ def exact_tfilter(on=True):
 
 
 @contextlib.contextmanager
+def bucket_slots(slots):
+    """Shrink the partitioned hub pass's tables (0 = default) for a block."""
+    L.check(L.lib.hl_dbg_set_bucket_slots(int(slots)))
+    try:
+        yield
+    finally:
+        L.check(L.lib.hl_dbg_set_bucket_slots(0))
+
+
+@contextlib.contextmanager
 def stage_mode(mode):
     """Run the stage entry points in `mode` (hl.RunMode), throughput after."""
     L.check(L.lib.hl_dbg_set_mode(int(mode)))
