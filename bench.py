@@ -126,6 +126,10 @@ def parse():
                          "the updated graph, one batch each under --cpu-cap")
     ap.add_argument("--cpu-cap", type=float, default=120.0,
                     help="wall-clock cap in seconds for each faithful variant's batch")
+    ap.add_argument("--no-served", action="store_true",
+                    help="rmat25: skip the serving-form phase after the timed steps")
+    ap.add_argument("--served-requests", type=int, default=48,
+                    help="rmat25: requests of the serving-form phase")
     ap.add_argument("--rmat-sample-scale", type=int, default=RMAT_SAMPLE_SCALE,
                     help="R-MAT scale of the CPU port's stand-in sample for rmat25")
     ap.add_argument("--cpu-variant-run", default=None, help=argparse.SUPPRESS)
@@ -814,7 +818,12 @@ def run_rmat(args, cfg):
     seeds = iter(range(10_000, 20_000))
     pinned = _pinned([W.rmat_batch_torch(scale, bs, bd, k, 0.9, next(seeds))
                       for _ in range(Wm + K)])
-    del bs, bd
+    # base edges the serving phase's requests delete from
+    gsel = torch.Generator(device=bs.device)
+    gsel.manual_seed(args.seed + 77)
+    pick = torch.randint(0, bs.numel(), (1 << 21,), generator=gsel, device=bs.device)
+    del_pool = (bs[pick].cpu().numpy().view(np.uint32), bd[pick].cpu().numpy().view(np.uint32))
+    del bs, bd, pick
     torch.cuda.empty_cache()
     for (pu, pv, pw) in pinned[:Wm]:
         L.check(L.lib.hl_apply_batch(h, C.c_void_p(pu.data_ptr()), C.c_void_p(pv.data_ptr()),
@@ -835,6 +844,9 @@ def run_rmat(args, cfg):
                        traversed, kernels, clk, ratio)
     q = st.modularity()
     dbytes = _device_bytes(L, h)
+    served = None
+    if not args.no_served:
+        served = _served_rmat(hl, st, scale, del_pool, args.seed, torch, args.served_requests)
     st.close()
     cpu = None
     if rep.rank == 0 and rep.world == 1 and not args.no_cpu_baseline:
@@ -844,9 +856,86 @@ def run_rmat(args, cfg):
                "kind": "port", "sample": _rmat_sample_text(r)}
     if rep.rank == 0:
         line.update({"cpu_baseline": cpu, "modularity": q, "kernels": kernels,
-                     "device_bytes": dbytes})
+                     "device_bytes": dbytes, "served": served})
         print(json.dumps(line), flush=True)
     rep.close()
+
+
+def _served_rmat(hl, st, scale, del_pool, seed, torch, requests):
+    """The serving form on the resident R-MAT graph: `requests` edge-update
+    requests (sizes log-uniform in [10, 100k], 85% R-MAT inserts / 15% deletes)
+    arrive as a Poisson stream at 10,000 requests/s; the server coalesces the
+    ones that arrive while the graph is busy.  Against it, the plain
+    per-request path applies a few requests of the same stream one per batch.
+    Host clock; requests from host memory."""
+    rng = np.random.default_rng(seed + 123)
+    sizes = np.exp(rng.uniform(np.log(10), np.log(100_000), requests)).astype(np.int64)
+    eu, ev = del_pool  # base edges (deleting one that is already gone is a no-op)
+
+    def request(j, sz):
+        g = np.random.default_rng(seed * 7919 + j)
+        ki = int(round(sz * 0.85))
+        kd = int(sz) - ki
+        u = np.zeros(ki, np.int64)
+        v = np.zeros(ki, np.int64)
+        for lvl in range(scale):
+            r = g.random(ki)
+            u |= (r >= 0.76).astype(np.int64) << lvl
+            v |= (((r >= 0.57) & (r < 0.76)) | (r >= 0.95)).astype(np.int64) << lvl
+        keep = u != v
+        u, v = u[keep], v[keep]
+        di = g.integers(0, len(eu), kd)
+        uu = np.concatenate([np.minimum(u, v), eu[di]]).astype(np.uint32)
+        vv = np.concatenate([np.maximum(u, v), ev[di]]).astype(np.uint32)
+        ww = np.concatenate([np.ones(len(u)), -np.ones(kd)])
+        return uu, vv, ww
+    reqs = [request(j, sz) for j, sz in enumerate(sizes)]
+    plain_reqs = [request(10_000 + j, sz) for j, sz in enumerate(sizes[:3])]
+    arrivals = np.cumsum(rng.exponential(1.0 / 10_000.0, requests))
+    torch.cuda.synchronize()
+    level_events = []
+    srv = hl.Server(workers=1)
+    srv.set_level_callback(lambda graph, batch, level, nodes, ids:
+                           level_events.append((batch, level, len(nodes))))
+    gid = srv.add(st)
+    t0 = time.perf_counter()
+    for (u, v, w), ta in zip(reqs, arrivals):
+        while time.perf_counter() - t0 < ta:
+            pass
+        srv.submit(gid, u, v, w)
+    srv.drain()
+    wall = time.perf_counter() - t0
+    done = []
+    while True:
+        part = srv.poll(cap=4096)
+        if not part:
+            break
+        done += part
+    srv.close()
+    ok = [d for d in done if d["status"] == 0]
+    edges = sum(d["edges"] for d in ok)
+    lat = sorted(d["latency_ms"] for d in ok)
+    l0 = sorted(d["level0_ms"] for d in ok)
+    # plain per-request path: one request per batch, same stream
+    tp = 0.0
+    ep = 0
+    for (u, v, w) in plain_reqs:
+        t1 = time.perf_counter()
+        st.apply_batch(u, v, w)
+        tp += time.perf_counter() - t1
+        ep += len(u)
+    served_rate = edges / wall
+    plain_rate = ep / tp
+    return {"requests": len(ok), "rejected": len(done) - len(ok), "edges": int(edges),
+            "batches": len({d["batch_id"] for d in ok}), "arrival_rate_req_s": 10_000,
+            "edge_updates_per_s": served_rate, "p50_ms": lat[len(lat) // 2],
+            "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+            "level0_p50_ms": l0[len(l0) // 2],
+            "plain_per_request_edge_updates_per_s": plain_rate,
+            "plain_requests_timed": len(plain_reqs),
+            "served_over_plain": served_rate / plain_rate,
+            "timing": "host clock: first submit to last completion (served); the plain "
+                      "requests one per hl_apply_batch"}
 
 
 def main():

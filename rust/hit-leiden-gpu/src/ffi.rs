@@ -84,7 +84,17 @@ pub struct hl_request_done {
     pub batch_requests: u32,
     pub status: i32,
     pub pad_: u32,
+    pub level0_ms: f64,
 }
+
+/// Per-level output callback (`hl_level_fn`).
+pub type hl_level_fn = Option<unsafe extern "C" fn(user: *mut c_void, level: u32, count: u64,
+                                                    nodes: *const u32, sub_ids: *const u32)>;
+/// Per-level output callback of the server (`hl_server_level_fn`).
+pub type hl_server_level_fn = Option<unsafe extern "C" fn(user: *mut c_void, graph: u32,
+                                                           batch_id: u64, level: u32, count: u64,
+                                                           nodes: *const u32,
+                                                           sub_ids: *const u32)>;
 
 /// Opaque graph handle.
 #[repr(C)]
@@ -115,6 +125,8 @@ extern "C" {
     pub fn hl_reset_kernel_stats(g: *mut hl_graph) -> hl_status;
     pub fn hl_set_resolution(g: *mut hl_graph, gamma: f64) -> hl_status;
     pub fn hl_set_mode(g: *mut hl_graph, mode: u32) -> hl_status;
+    pub fn hl_set_level_callback(g: *mut hl_graph, fn_: hl_level_fn, user: *mut c_void)
+                                 -> hl_status;
     pub fn hl_num_nodes(g: *const hl_graph, n: *mut u32) -> hl_status;
     pub fn hl_num_levels(g: *const hl_graph, levels: *mut u32) -> hl_status;
     pub fn hl_level_size(g: *const hl_graph, level: u32, n_level: *mut u32) -> hl_status;
@@ -144,6 +156,8 @@ extern "C" {
                             w: *const f64, k: u64, request_id: *mut u64) -> hl_status;
     pub fn hl_server_poll(s: *mut hl_server, out: *mut hl_request_done, cap: u32,
                           count: *mut u32, wait_ms: i32) -> hl_status;
+    pub fn hl_server_set_level_callback(s: *mut hl_server, fn_: hl_server_level_fn,
+                                        user: *mut c_void) -> hl_status;
     pub fn hl_server_drain(s: *mut hl_server) -> hl_status;
     pub fn hl_server_destroy(s: *mut hl_server);
 

@@ -126,3 +126,20 @@ def test_library_exports_no_undeclared_entry_points():
                          text=True).stdout
     exported = {ln.split()[-1] for ln in out.splitlines() if ln.split()[-1].startswith("hl_")}
     assert exported == set(declared_symbols())
+
+
+def test_rust_binding_mirrors_the_header():
+    """rust/hit-leiden-gpu/src/ffi.rs declares every entry point of
+    include/hl.h, and its #[repr(C)] structs have the header's fields in the
+    header's order (the crate is not compiled in this image: no cargo)."""
+    ffi = open(os.path.join(ROOT, "rust", "hit-leiden-gpu", "src", "ffi.rs")).read()
+    text = open(os.path.join(ROOT, "include", "hl.h")).read()
+    public = sorted(set(re.findall(r"HL_API\s+[\w\s\*]+?\b(hl_\w+)\s*\(", text)))
+    for name in public:
+        assert re.search(rf"pub fn {name}\s*\(", ffi), f"ffi.rs lacks {name}"
+    for cname in ("hl_config", "hl_batch_stats", "hl_kernel_stat", "hl_request_done"):
+        body_c = re.search(r"typedef struct \{([^{}]*)\}\s*" + cname + ";", text).group(1)
+        fields_c = re.findall(r"\b(\w+)(?:\[\d+\])?;", re.sub(r"/\*.*?\*/", "", body_c, flags=re.S))
+        body_r = re.search(r"pub struct " + cname + r" \{(.*?)\}", ffi, re.S).group(1)
+        fields_r = re.findall(r"pub (\w+):", body_r)
+        assert fields_c == fields_r, (cname, fields_c, fields_r)
