@@ -503,6 +503,13 @@ __device__ __forceinline__ u64 claim_slot(u32* tk, u64 mask, u32 key, bool& fres
   }
 }
 
+// A table value of the block kernel: a double, or with integral weights the
+// bits of an exact integer sum (added with 64-bit integer atomics).
+__device__ __forceinline__ double tab_value(double raw, bool integer) {
+  if (!integer) return raw;
+  return (double)(long long)__double_as_longlong(raw);
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -652,7 +659,9 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
             if (global) g_list[atomicAdd(&s_gused, 1u)] = (u32)slot;
             else atomicAdd(&s_used, 1u);
           }
-          atomicAdd(&tv[slot], gsum);
+          // the slot holds the integer sum (0.0 and integer 0 share their bits)
+          atomicAdd(reinterpret_cast<unsigned long long*>(&tv[slot]),
+                    (unsigned long long)(long long)gsum);
           atomicMin(&tp[slot], pos);
         }
         __syncwarp();
@@ -726,7 +735,7 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
       u64 sl = hash32(cur) & mask;
       while (tk[sl] != NONE32) {
         if (tk[sl] == cur) {
-          wc = tv[sl];
+          wc = tab_value(tv[sl], A.concurrent);
           break;
         }
         sl = (sl + 1) & mask;
@@ -743,7 +752,7 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
       const u64 sl = global ? g_list[x] : x;
       const u32 key = tk[sl];
       if (key == NONE32) continue;
-      const double val = tv[sl];
+      const double val = tab_value(tv[sl], A.concurrent);
       const u32 pp = tp[sl];
       if (global) {
         tk[sl] = NONE32;
