@@ -28,6 +28,7 @@ HL_MAP_COMMUNITY, HL_MAP_REFINED, HL_MAP_SUB_PREVIOUS, HL_MAP_SUB_CURRENT = 0, 1
 HL_FLAG_KEEP_SELF_LOOPS = 1 << 0
 HL_FLAG_BATCH_MODULARITY = 1 << 1
 HL_FLAG_KERNEL_TIMING = 1 << 2
+HL_FLAG_NO_AUTOTUNE = 1 << 3
 HL_NOALLOC_MAX_ELEMS = 1 << 28
 
 
@@ -147,6 +148,8 @@ def _load():
         "hl_dbg_set_exact_tfilter": (st, [C.c_int32]),
         "hl_dbg_set_mode": (st, [C.c_uint32]),
         "hl_dbg_set_bucket_slots": (st, [C.c_uint32]),
+        "hl_dbg_set_bins": (st, [C.c_uint32, C.c_uint32]),
+        "hl_autotune_info": (st, [vp, p32, p32, p32]),
         "hl_tree_sum_noalloc": (st, [vp, C.c_uint64, vp, vp]),
         "hl_dbg_modularity": (st, [C.c_int32, C.c_uint32, vp, vp, vp, vp,
                                    C.POINTER(C.c_double)]),

@@ -487,7 +487,9 @@ static void create_impl(const hl_config* cfg, uint32_t n, const uint32_t* src, c
   E.integral = edges_integral(E, G);
   E.st = hl_batch_stats{};
   HL_CUDA(cudaEventRecord(E.ev0, E.stream));
+  E.in_bootstrap = true;
   bootstrap(*B, n, G);
+  E.in_bootstrap = false;
   if (E.levels[0].tw >= 4503599627370496.0) E.integral = false;  // 2^52
   finish_stats(*B, nullptr);
   // The bootstrap's scratch (sorts over the whole edge list) is far larger
@@ -618,6 +620,14 @@ hl_status hl_set_resolution(hl_graph* g, double gamma) {
 hl_status hl_set_level_callback(hl_graph* g, hl_level_fn fn, void* user) {
   HL_TRY(require(g != nullptr, "graph handle is NULL"); box(g)->E->level_fn = fn;
          box(g)->E->level_user = fn ? user : nullptr);
+}
+
+hl_status hl_autotune_info(const hl_graph* g, uint32_t* mid_max, uint32_t* wide_max,
+                           uint32_t* frontier) {
+  HL_TRY(require(g && mid_max && wide_max && frontier, "NULL argument");
+         const Engine& E = *box(g)->E; *mid_max = E.tune.mid_max ? E.tune.mid_max : 128;
+         *wide_max = E.tune.wide_max ? E.tune.wide_max : 512;
+         *frontier = E.tune.done ? E.tune.frontier : 0);
 }
 
 hl_status hl_set_mode(hl_graph* g, uint32_t mode) {
@@ -754,6 +764,8 @@ namespace {
 
 // RunMode of the stage entry points (hl_dbg_set_mode); Throughput unless set.
 std::atomic<uint32_t> g_dbg_mode{HL_MODE_THROUGHPUT};
+// Degree-bin thresholds of the stage entry points (hl_dbg_set_bins).
+std::atomic<uint32_t> g_dbg_mid{0}, g_dbg_wide{0};
 
 std::unique_ptr<EngineBox> scratch_engine(int32_t device) {
   hl_config cfg;
@@ -762,6 +774,9 @@ std::unique_ptr<EngineBox> scratch_engine(int32_t device) {
   cfg.mode = g_dbg_mode.load();
   std::unique_ptr<EngineBox> B(new EngineBox());
   engine_init(*B, &cfg);
+  B->E->tune.mid_max = g_dbg_mid.load();
+  B->E->tune.wide_max = g_dbg_wide.load();
+  B->E->tune.done = true;
   return B;
 }
 
@@ -994,6 +1009,17 @@ hl_status hl_dbg_inc_refinement(int32_t device, uint32_t n, const uint64_t* off,
 
 hl_status hl_dbg_set_exact_tfilter(int32_t on) {
   g_exact_tfilter.store(on ? 1 : 0);
+  return HL_OK;
+}
+
+hl_status hl_dbg_set_bins(uint32_t mid_max, uint32_t wide_max) {
+  if ((mid_max && (mid_max < 33 || mid_max > 128)) ||
+      (wide_max && (wide_max > 512 || wide_max < (mid_max ? mid_max : 128)))) {
+    g_err = "bins: mid_max in [33, 128], wide_max in [mid_max, 512] (0 = default)";
+    return HL_ERR_INVALID_INPUT;
+  }
+  g_dbg_mid.store(mid_max);
+  g_dbg_wide.store(wide_max);
   return HL_OK;
 }
 

@@ -1113,15 +1113,15 @@ __global__ void k_pb_final(EvalArgs A, PbArgs P, u32* fail_list, u32* fail_count
 // Host side: bin the list by degree and launch the three kernels.
 // ---------------------------------------------------------------------------
 __global__ void k_bin(const u32* verts, u32 nv, const u64* off, u32* bin, u32* idx,
-                      u32* counts, unsigned long long* maxdeg) {
+                      u32* counts, unsigned long long* maxdeg, u32 mid_max, u32 wide_max) {
   __shared__ u32 sc[6];
   if (threadIdx.x < 6) sc[threadIdx.x] = 0;
   __syncthreads();
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < nv; i += (u64)gridDim.x * blockDim.x) {
     u32 v = verts[i];
     u64 deg = off[v + 1] - off[v];
-    u32 b = deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= MID_MAX ? 3
-          : deg <= WIDE_MAX ? 4 : 5;
+    u32 b = deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= mid_max ? 3
+          : deg <= wide_max ? 4 : 5;
     bin[i] = b;
     idx[i] = (u32)i;
     atomicAdd(&sc[b], 1u);
@@ -1287,8 +1287,12 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   S.ovf_cnt.ensure(E.mem, 6);
   unsigned long long* maxdeg = reinterpret_cast<unsigned long long*>(S.ovf_cnt.p + 2);
   HL_CUDA(cudaMemsetAsync(S.ovf_cnt.p, 0, 6 * sizeof(u32), st));
+  // degree thresholds of the warp bins (autotuned per handle, within the
+  // compile-time table sizes: mid <= MID_MAX, wide <= WIDE_MAX)
+  const u32 mid_max = E.tune.mid_max ? E.tune.mid_max : MID_MAX;
+  const u32 wide_max = E.tune.wide_max ? E.tune.wide_max : WIDE_MAX;
   ++E.nlaunch, k_bin<<<grid_for(nv), 256, 0, st>>>(verts, nv, L.g.off.p, S.used.p, S.order.p, cnt,
-                                                    maxdeg);
+                                                    maxdeg, mid_max, wide_max);
   HL_LAUNCH_CHECK();
   u32* ki = S.used.p;
   u32* ko = S.rank.p;
@@ -1494,6 +1498,51 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   }
   E.kt_end(KT_EVAL_HUGE, e_h);
   E.kt_end(kind == EVAL_MOVE ? KT_MOVE_EVAL : KT_REFINE_EVAL, ev);
+}
+
+// Autotuner of the degree bins: the evaluation of one frontier is run with
+// each candidate pair of warp-bin thresholds (every pair gives the same
+// results; only the split between the sub-warp, warp and block kernels
+// changes) and the fastest pair is kept for the handle.  Runs once, on the
+// first movement round whose frontier has at least AUTOTUNE_MIN vertices.
+constexpr u32 AUTOTUNE_MIN = 20000;
+
+void autotune_bins(Engine& E, const u32* verts, u32 nv, const Level& L, const u32* s,
+                   const double* d, u32* out_to, double* out_gain) {
+  if (E.tune.done || nv < AUTOTUNE_MIN || (E.cfg.flags & HL_FLAG_NO_AUTOTUNE)) return;
+  static const u32 cand[][2] = {{128, 512}, {64, 512}, {128, 256}, {64, 256}, {96, 384}};
+  cudaEvent_t a, b;
+  HL_CUDA(cudaEventCreate(&a));
+  HL_CUDA(cudaEventCreate(&b));
+  const bool kt = E.ktiming;
+  E.ktiming = false;  // the trial runs stay out of the kernel statistics
+  float best = 0.f;
+  u32 bm = MID_MAX, bw = WIDE_MAX;
+  for (int rep = 0; rep < 2; ++rep) {  // the first pass warms the caches and allocations
+    for (const auto& c : cand) {
+      E.tune.mid_max = c[0];
+      E.tune.wide_max = c[1];
+      HL_CUDA(cudaEventRecord(a, E.stream));
+      run_eval(E, EVAL_MOVE, verts, nv, L, s, d, nullptr, true, out_to, out_gain, nullptr);
+      HL_CUDA(cudaEventRecord(b, E.stream));
+      HL_CUDA(cudaEventSynchronize(b));
+      float ms = 0.f;
+      HL_CUDA(cudaEventElapsedTime(&ms, a, b));
+      if (rep == 1 && (best == 0.f || ms < best)) {
+        best = ms;
+        bm = c[0];
+        bw = c[1];
+      }
+    }
+  }
+  E.ktiming = kt;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  E.tune.mid_max = bm;
+  E.tune.wide_max = bw;
+  E.tune.done = true;
+  E.tune.frontier = nv;
+  E.tune.best_ms = best;
 }
 
 }  // namespace hl

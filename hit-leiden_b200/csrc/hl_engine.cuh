@@ -150,6 +150,7 @@ struct Engine {
   std::vector<Level> levels;
   bool multilevel = false;
   bool integral = true;  // every weight integral: all FP64 sums exact in any order
+  bool in_bootstrap = false;  // hl_create's bootstrap is running
   HostScalars hs;
   u64 epoch = 1;         // selection epochs (reservation keys)
   u32 sel_round = 0;     // role tag of the current selection
@@ -159,6 +160,13 @@ struct Engine {
   // per-call statistics
   hl_batch_stats st{};
   std::vector<std::pair<u32, u32>> new_ids;  // (new sub-community id, origin) of the last refinement
+  // degree-bin thresholds picked by the autotuner (0 = compile-time default)
+  struct Tune {
+    u32 mid_max = 0, wide_max = 0;
+    bool done = false;
+    u32 frontier = 0;
+    float best_ms = 0.f;
+  } tune;
   // per-level output (hl_set_level_callback): called after each level's refinement
   hl_level_fn level_fn = nullptr;
   void* level_user = nullptr;
@@ -230,6 +238,10 @@ struct RefineOut {
   u32 smax_before = 0;
 };
 RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community);
+
+// eval.cu: degree-bin autotuner (once per handle)
+void autotune_bins(Engine& E, const u32* verts, u32 nv, const Level& L, const u32* s,
+                   const double* d, u32* out_to, double* out_gain);
 
 // det.cu: the sequential (RunMode::Deterministic) steps
 void inc_movement_det(Engine& E, Level& L, double* d, size_t dcap, bool mark_moved, u64* moves,

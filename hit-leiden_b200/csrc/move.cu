@@ -557,6 +557,8 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     u32 na = E.read_u32(cnt + 4);
     if (!na) break;
     sum_nv += na;
+    if (!E.in_bootstrap)
+      autotune_bins(E, S.act.p, na, L, L.s_cur.p, S.d.p, S.cand_to.p, S.cand_gain.p);
     run_eval(E, EVAL_MOVE, S.act.p, na, L, L.s_cur.p, S.d.p, nullptr, true, S.cand_to.p,
              S.cand_gain.p, (unsigned long long*)S.red64.p);
     // Candidates with positive gain, still in ascending node order.

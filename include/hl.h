@@ -85,6 +85,12 @@ typedef struct {
 /* Time the main kernels with CUDA events on the handle's stream and count
  * their algorithmic bytes (read with hl_kernel_stats). */
 #define HL_FLAG_KERNEL_TIMING (1u << 2)
+/* Keep the compile-time degree bins instead of autotuning them.  By default
+ * the first movement round after the bootstrap with at least 20,000 active
+ * vertices runs the evaluation once per candidate pair of warp-bin
+ * thresholds (results are identical for every pair) and keeps the fastest
+ * pair for the handle (hl_autotune_info). */
+#define HL_FLAG_NO_AUTOTUNE (1u << 3)
 
 typedef struct {
   uint32_t iterations;   /* movement rounds summed over levels (hit_leiden return) */
@@ -173,6 +179,13 @@ HL_API hl_status hl_set_resolution(hl_graph* g, double gamma);
 typedef void (*hl_level_fn)(void* user, uint32_t level, uint64_t count, const uint32_t* nodes,
                             const uint32_t* sub_ids);
 HL_API hl_status hl_set_level_callback(hl_graph* g, hl_level_fn fn, void* user);
+
+/* Degree-bin thresholds the handle uses: vertices of degree 33..mid_max take
+ * the warp kernel with a shared table, mid_max+1..wide_max the wide warp
+ * kernel, larger ones the block kernel.  frontier is the frontier size the
+ * autotuner measured on (0: not tuned yet, or HL_FLAG_NO_AUTOTUNE). */
+HL_API hl_status hl_autotune_info(const hl_graph* g, uint32_t* mid_max, uint32_t* wide_max,
+                                  uint32_t* frontier);
 
 /* Change the RunMode for subsequent batches (hit_leiden takes it per call,
  * hit_leiden.rs:940): HL_MODE_DETERMINISTIC or HL_MODE_THROUGHPUT. */

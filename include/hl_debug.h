@@ -97,6 +97,11 @@ HL_API hl_status hl_dbg_set_mode(uint32_t mode);
  * global-table pass those rows fall back to.  Results do not depend on it. */
 HL_API hl_status hl_dbg_set_bucket_slots(uint32_t slots);
 
+/* Warp-bin thresholds of the stage entry points (mid_max in [33, 128],
+ * wide_max in [mid_max, 512]; 0 = default), the pairs the autotuner picks
+ * from.  Results do not depend on them. */
+HL_API hl_status hl_dbg_set_bins(uint32_t mid_max, uint32_t wide_max);
+
 /* Modularity of `part` on the CSR (hit_leiden.rs:121-161). */
 HL_API hl_status hl_dbg_modularity(int32_t device, uint32_t n, const uint64_t* off, const uint32_t* col,
                             const double* w, const uint32_t* part, double* q);

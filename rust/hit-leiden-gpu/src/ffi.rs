@@ -24,6 +24,7 @@ pub const HL_MAP_SUB_CURRENT: u32 = 3;
 pub const HL_FLAG_KEEP_SELF_LOOPS: u32 = 1 << 0;
 pub const HL_FLAG_BATCH_MODULARITY: u32 = 1 << 1;
 pub const HL_FLAG_KERNEL_TIMING: u32 = 1 << 2;
+pub const HL_FLAG_NO_AUTOTUNE: u32 = 1 << 3;
 
 pub const HL_NOALLOC_MAX_ELEMS: u64 = 1 << 28;
 
@@ -125,6 +126,8 @@ extern "C" {
     pub fn hl_reset_kernel_stats(g: *mut hl_graph) -> hl_status;
     pub fn hl_set_resolution(g: *mut hl_graph, gamma: f64) -> hl_status;
     pub fn hl_set_mode(g: *mut hl_graph, mode: u32) -> hl_status;
+    pub fn hl_autotune_info(g: *const hl_graph, mid_max: *mut u32, wide_max: *mut u32,
+                            frontier: *mut u32) -> hl_status;
     pub fn hl_set_level_callback(g: *mut hl_graph, fn_: hl_level_fn, user: *mut c_void)
                                  -> hl_status;
     pub fn hl_num_nodes(g: *const hl_graph, n: *mut u32) -> hl_status;

@@ -91,6 +91,16 @@ def bucket_slots(slots):
 
 
 @contextlib.contextmanager
+def bins(mid_max, wide_max):
+    """Warp-bin thresholds of the stage entry points for a block."""
+    L.check(L.lib.hl_dbg_set_bins(int(mid_max), int(wide_max)))
+    try:
+        yield
+    finally:
+        L.check(L.lib.hl_dbg_set_bins(0, 0))
+
+
+@contextlib.contextmanager
 def stage_mode(mode):
     """Run the stage entry points in `mode` (hl.RunMode), throughput after."""
     L.check(L.lib.hl_dbg_set_mode(int(mode)))

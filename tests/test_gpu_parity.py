@@ -4,6 +4,8 @@ KATs replayed through the CUDA kernels.  Every call goes through libhl's C ABI.
 Tolerance: bit-exact for every integer output and every FP64 value that feeds a
 decision (weights, gains, community totals); modularity within 1e-12 relative.
 """
+import importlib
+
 import numpy as np
 import pytest
 
@@ -394,3 +396,64 @@ def test_inc_refinement_hub_bit_exact(integral, ncomm, exact):
     with gh.exact_tfilter(exact):
         gs, gr = gh.inc_refinement(g, f, s0, aff, 1.0)
     assert np.array_equal(ref_s, gs) and np.array_equal(ref_r, gr)
+
+
+# ---- degree-bin thresholds (the autotuner's candidates) -------------------
+@pytest.mark.parametrize("integral", [True, False])
+@pytest.mark.parametrize("pair", [(128, 512), (64, 512), (128, 256), (64, 256), (96, 384),
+                                  (33, 33)])
+def test_move_eval_same_for_every_bin_split(integral, pair):
+    rng = np.random.default_rng(31)
+    n = 12000
+    src, dst, w = gh.random_graph(rng, n, 60000, integral)
+    # a spread of degrees across every bin: a few vertices of 40..1500 entries
+    hubs = rng.choice(n, 40, replace=False).astype(np.uint32)
+    hs, hd = [], []
+    for i, h in enumerate(hubs):
+        deg = int(40 + 40 * i)
+        hs.append(np.full(deg, h, np.uint32))
+        hd.append(rng.choice(n, deg, replace=False).astype(np.uint32))
+    hs, hd = np.concatenate(hs), np.concatenate(hd)
+    keep = hs != hd
+    hw = (rng.integers(1, 3, keep.sum()).astype(float) if integral
+          else rng.uniform(0.5, 2, keep.sum()))
+    g = O.Graph.from_edges(n, np.concatenate([src, hs[keep]]), np.concatenate([dst, hd[keep]]),
+                           np.concatenate([w, hw])).apply_delta([], [], [], keep_self_loops=True)
+    k = g.degrees()
+    tw = O.tree_sum(k)
+    f = gh.random_partition(rng, n, 300)
+    d = np.zeros(2 * n + 2)
+    np.add.at(d, f, k)
+    verts = np.arange(n, dtype=np.uint32)
+    to_o, g_o = O.move_eval(g, f, d, k, tw, 1.0, verts)
+    with gh.bins(*pair):
+        to_g, g_g = gh.move_eval(g, f, d, k, tw, 1.0, verts)
+    assert gh.same_bits(g_o, g_g)
+    pos = g_o > 0
+    assert np.array_equal(to_o[pos], to_g[pos])
+
+
+def test_autotuned_handle_stays_bit_exact():
+    """A frontier of at least 20,000 vertices triggers the degree-bin
+    autotuner; the state stays bit-exact with the oracle through it."""
+    import ctypes as C
+    hl = importlib.import_module("hit-leiden_b200")
+    L = importlib.import_module("hit-leiden_b200._lib")
+    E2E = importlib.import_module("tests.test_gpu_e2e")
+    W = importlib.import_module("hit-leiden_b200.workloads")
+    n, s, d, w = W.config2(4, n=40_000, mean_degree=12.0)
+    gs = hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w),
+                                hl.RunConfig(mode=hl.RunMode.Throughput))
+    os_ = E2E.oracle_state(n, s, d, w, 10)
+    gs.apply_batch([], [], [])  # empty batch: every vertex active at level 0
+    os_.hit_leiden([], [], [])
+    mid, wide, fr = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    L.check(L.lib.hl_autotune_info(gs._h, C.byref(mid), C.byref(wide), C.byref(fr)))
+    assert fr.value >= 20000 and 33 <= mid.value <= 128 and mid.value <= wide.value <= 512
+    E2E.compare(gs, os_)
+    store = W.EdgeStore(n, s, d, w)
+    u, v, ww = W.mixed_batch(store, 500, 0.9, 8, weights=(0.5, 2.0), preferential=True)
+    gs.apply_batch(u, v, ww)
+    os_.hit_leiden(u, v, ww)
+    E2E.compare(gs, os_)
+    gs.close()
