@@ -29,6 +29,7 @@ HL_FLAG_KEEP_SELF_LOOPS = 1 << 0
 HL_FLAG_BATCH_MODULARITY = 1 << 1
 HL_FLAG_KERNEL_TIMING = 1 << 2
 HL_FLAG_NO_AUTOTUNE = 1 << 3
+HL_FLAG_NO_SMALL_ROUNDS = 1 << 4
 HL_NOALLOC_MAX_ELEMS = 1 << 28
 
 

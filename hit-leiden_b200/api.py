@@ -56,6 +56,8 @@ class RunConfig:
     keep_self_loops: bool = False
     batch_modularity: bool = False
     kernel_timing: bool = False
+    autotune: bool = True        # degree-bin autotuner (HL_FLAG_NO_AUTOTUNE when off)
+    small_rounds: bool = True    # one-block rounds for small frontiers (HL_FLAG_NO_SMALL_ROUNDS)
 
     def validate(self) -> None:
         if self.max_iterations == 0:
@@ -72,7 +74,9 @@ class RunConfig:
         c.max_rounds = int(self.max_rounds)
         c.flags = ((L.HL_FLAG_KEEP_SELF_LOOPS if self.keep_self_loops else 0)
                    | (L.HL_FLAG_BATCH_MODULARITY if self.batch_modularity else 0)
-                   | (L.HL_FLAG_KERNEL_TIMING if self.kernel_timing else 0))
+                   | (L.HL_FLAG_KERNEL_TIMING if self.kernel_timing else 0)
+                   | (0 if self.autotune else L.HL_FLAG_NO_AUTOTUNE)
+                   | (0 if self.small_rounds else L.HL_FLAG_NO_SMALL_ROUNDS))
         c.hbm_budget = int(self.hbm_budget)
         c.device = int(self.device)
         return c

@@ -103,6 +103,9 @@ struct Scratch {
       pb_epos, pb_bcnt, pb_boff, pb_bp, pb_bk;
   DBuf<u64> pb_ne, pb_ebase;
   DBuf<double> pb_wcur, pb_ew, pb_bg;
+  // movement rounds of a small frontier (small.cu)
+  DBuf<u32> sm_list_a, sm_list_b;
+  DBuf<u64> sm_out;
   // per-level output: the level's s_cur before the batch, the changed nodes
   DBuf<u32> lvl_prev, lvl_nodes, lvl_ids;
   DBuf<u8> lvl_flag;
@@ -138,6 +141,7 @@ enum KernelId : int {
   KT_STAGE_AGGREGATE,
   KT_HOST_SYNC,    // host waits on the stream (launches = count; no time)
   KT_COPY_ROWS,    // untouched CSR rows copied into the new buffer
+  KT_MOVE_SMALL,   // movement rounds of a small frontier in one block (small.cu)
   KT_COUNT
 };
 
@@ -238,6 +242,12 @@ struct RefineOut {
   u32 smax_before = 0;
 };
 RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community);
+
+// small.cu: movement rounds of a small frontier in one block.  Returns true
+// when the movement stage is finished, false when the host rounds continue
+// from S.active (*big_degree: an active vertex exceeds the block's tables).
+bool move_rounds_small(Engine& E, Level& L, bool mark_moved, u32& it, u64& moves, u64& cands,
+                       u64& trav, u64& sum_nv, bool* big_degree);
 
 // eval.cu: degree-bin autotuner (once per handle)
 void autotune_bins(Engine& E, const u32* verts, u32 nv, const Level& L, const u32* s,

@@ -500,8 +500,10 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   Scratch& S = E.sc;
   cudaStream_t st = E.stream;
   const u32 n = L.g.n;
-  S.active.ensure(E.mem, n ? n : 1);
-  S.next.ensure(E.mem, n ? n : 1);
+  // flag arrays padded to whole 32-bit words (small.cu marks them by word)
+  const size_t nflag = (((size_t)n + 3) & ~(size_t)3) ? (((size_t)n + 3) & ~(size_t)3) : 4;
+  S.active.ensure(E.mem, nflag);
+  S.next.ensure(E.mem, nflag);
   S.changed.ensure(E.mem, n ? n : 1);
   S.affected.ensure(E.mem, n ? n : 1);
   HL_CUDA(cudaMemsetAsync(S.active.p, all_active ? 1 : 0, n ? n : 1, st));
@@ -548,13 +550,26 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   u32 it = 0;
   S.acc_cnt.ensure(E.mem, 1);
   HL_CUDA(cudaMemsetAsync(S.acc_cnt.p, 0, sizeof(u32), st));  // accepted moves, all rounds
+  // Small frontiers run whole rounds in one block (small.cu); the host
+  // rounds below take over while the frontier is large or a hub is active.
+  u64 sm_moves = 0, sm_cands = 0, sm_trav = 0, sm_nv = 0;
+  bool small_on = !(E.cfg.flags & HL_FLAG_NO_SMALL_ROUNDS);
+  u32 last_na = 0;
   while (it < max_rounds) {
+    if (small_on && last_na <= 16384) {
+      bool big = false;
+      if (move_rounds_small(E, L, mark_moved, it, sm_moves, sm_cands, sm_trav, sm_nv, &big))
+        break;
+      if (big) small_on = false;
+      if (it >= max_rounds) break;
+    }
     // Active list, ascending (iter_ones order).
     cub_run(E, [&](void* t, size_t& b) {
       return cub::DeviceSelect::Flagged(t, b, cub::CountingInputIterator<u32>(0), S.active.p,
                                         S.act.p, cnt + 4, (int64_t)n, st);
     });
     u32 na = E.read_u32(cnt + 4);
+    last_na = na;
     if (!na) break;
     sum_nv += na;
     if (!E.in_bootstrap)
@@ -652,6 +667,9 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
   E.kagg[KT_MOVE_EVAL].bytes += 52ull * sum_nv + 16ull * out.traversed + 8ull * ncand;
   const int bins[4] = {KT_EVAL_SMALL, KT_EVAL_MID, KT_EVAL_BIG, KT_EVAL_HUGE};
   for (int b = 0; b < 4; ++b) E.kagg[bins[b]].bytes += 16ull * cnt8[2 * b] + 8ull * cnt8[2 * b + 1];
+  out.moves += sm_moves;
+  out.candidates += sm_cands;
+  out.traversed += sm_trav;
   return out;
 }
 

@@ -91,6 +91,11 @@ typedef struct {
  * thresholds (results are identical for every pair) and keeps the fastest
  * pair for the handle (hl_autotune_info). */
 #define HL_FLAG_NO_AUTOTUNE (1u << 3)
+/* Keep every throughput movement round on the multi-kernel path.  By default
+ * rounds whose frontier has at most 4096 vertices of at most 256 entries each
+ * (levels of up to 2^18 nodes) run whole inside one block, without host round
+ * trips between them; the results are identical either way. */
+#define HL_FLAG_NO_SMALL_ROUNDS (1u << 4)
 
 typedef struct {
   uint32_t iterations;   /* movement rounds summed over levels (hit_leiden return) */

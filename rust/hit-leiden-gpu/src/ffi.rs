@@ -25,6 +25,7 @@ pub const HL_FLAG_KEEP_SELF_LOOPS: u32 = 1 << 0;
 pub const HL_FLAG_BATCH_MODULARITY: u32 = 1 << 1;
 pub const HL_FLAG_KERNEL_TIMING: u32 = 1 << 2;
 pub const HL_FLAG_NO_AUTOTUNE: u32 = 1 << 3;
+pub const HL_FLAG_NO_SMALL_ROUNDS: u32 = 1 << 4;
 
 pub const HL_NOALLOC_MAX_ELEMS: u64 = 1 << 28;
 

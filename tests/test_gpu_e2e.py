@@ -199,3 +199,28 @@ def test_e2e_rmat_integral_hubs(seed):
         os_.hit_leiden(u, v, ww)
         compare(gs, os_)
     del torch
+
+
+@pytest.mark.parametrize("weights", [None, (0.5, 2.0)])
+def test_small_frontier_rounds_change_nothing(weights):
+    """Rounds of a small frontier run whole in one block (small.cu); with that
+    path off every round takes the multi-kernel path.  Both give the same
+    state, bit for bit, and both equal the oracle."""
+    n, s, d, w, _ = W.planted(6000, 8.0, 0.25, 13, comm_min=5, comm_max=80, triangle_frac=0.2,
+                              weights=weights)
+    on = hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w),
+                                hl.RunConfig(mode=hl.RunMode.Throughput))
+    off = hl.PartitionState.load(hl.GraphInput.from_arrays("t", n, s, d, w),
+                                 hl.RunConfig(mode=hl.RunMode.Throughput, small_rounds=False))
+    os_ = oracle_state(n, s, d, w, 10)
+    store = W.EdgeStore(n, s, d, w)
+    for b in range(4):
+        u, v, ww = W.mixed_batch(store, 300, 0.8, 40 + b, weights=weights, preferential=True)
+        st_on = on.apply_batch(u, v, ww)
+        st_off = off.apply_batch(u, v, ww)
+        os_.hit_leiden(u, v, ww)
+        assert st_on.iterations == st_off.iterations and st_on.moves == st_off.moves
+        compare(on, os_)
+        compare(off, os_)
+    on.close()
+    off.close()
