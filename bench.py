@@ -590,6 +590,9 @@ def _serve(hl, states, reqs, arrivals, workers, coalesce, budget):
     srv = hl.Server(workers=workers, hbm_budget=budget)
     if coalesce is not None:
         srv.set_coalescing(coalesce)
+    # per-level output on: the records then say when each batch's level 0
+    # was settled (level0_ms), the point a pipeline can start summarising
+    srv.set_level_callback(lambda graph, batch, level, nodes, ids: None)
     ids = [srv.add(s) for s in states]
     t0 = time.perf_counter()
     for (g, u, v, w), ta in zip(reqs, arrivals):
@@ -645,8 +648,10 @@ def run_serving(args, cfg):
             ok = [d for d in done if d["status"] == 0]
             lat = sorted(d["latency_ms"] for d in ok)
             e = sum(d["edges"] for d in ok)
+            l0 = sorted(d["level0_ms"] for d in ok)
             res[name] = {"edge_updates_per_s": e / wall, "p50_ms": lat[len(lat) // 2],
                          "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                         "level0_p50_ms": l0[len(l0) // 2],
                          "batches": len({d["batch_id"] for d in ok}), "requests": len(ok),
                          "rejected": len(done) - len(ok)}
         per_rate.append({"rate_req_s": rate, **{f"{k}_{m}": v for k, r in res.items()
