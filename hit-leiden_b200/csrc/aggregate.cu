@@ -391,20 +391,26 @@ __global__ void k_last_member(u32 n, const u32* s, u32* last) {
   for (u64 v = blockIdx.x * (u64)blockDim.x + threadIdx.x; v < n; v += (u64)gridDim.x * blockDim.x)
     atomicMax(&last[s[v]], (u32)v + 1);
 }
-__global__ void k_project(u32 nh, const u32* last, const u32* flo, u32* fhi) {
+__global__ void k_project(u32 nh, const u32* last, const u32* flo, u32* fhi, u8* changed) {
   for (u64 x = blockIdx.x * (u64)blockDim.x + threadIdx.x; x < nh; x += (u64)gridDim.x * blockDim.x) {
     u32 l = last[x];
-    if (l) fhi[x] = flo[l - 1];
+    if (!l) continue;
+    const u32 nf = flo[l - 1];
+    if (fhi[x] != nf) {
+      fhi[x] = nf;
+      if (changed) changed[x] = 1;  // M8: its sub-community is split again above
+    }
   }
 }
 
-void project_up(Engine& E, Level& lo, Level& hi) {
+void project_up(Engine& E, Level& lo, Level& hi, u8* changed_flags) {
   Scratch& S = E.sc;
   u32 nh = hi.g.n;
   S.minmem.ensure(E.mem, (size_t)nh + 1);
   HL_CUDA(cudaMemsetAsync(S.minmem.p, 0, sizeof(u32) * ((size_t)nh + 1), E.stream));
   ++E.nlaunch, k_last_member<<<grid_for(lo.g.n), 256, 0, E.stream>>>(lo.g.n, lo.s_cur.p, S.minmem.p);
-  ++E.nlaunch, k_project<<<grid_for(nh), 256, 0, E.stream>>>(nh, S.minmem.p, lo.f.p, hi.f.p);
+  ++E.nlaunch, k_project<<<grid_for(nh), 256, 0, E.stream>>>(nh, S.minmem.p, lo.f.p, hi.f.p,
+                                                              changed_flags);
   HL_LAUNCH_CHECK();
 }
 

@@ -216,6 +216,11 @@ __global__ void k_gather_u32(const u32* idx, u32 m, const u32* src, u32* out) {
     out[i] = src[idx[i]];
 }
 
+__global__ void k_flag_ids(const u32* ids, u32 m, u32 n, u8* flags) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < m; i += (u64)gridDim.x * blockDim.x)
+    if (ids[i] < n) flags[ids[i]] = 1;
+}
+
 static void level_snapshot(Engine& E, Level& L) {
   if (!E.level_fn || !L.g.n) return;
   E.sc.lvl_prev.ensure(E.mem, L.g.n);
@@ -285,6 +290,7 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
   }
   DevEdges cur = delta;
   u32 cur_n = E.levels[0].g.n;
+  E.k_flags_set = false;
   for (u32 p = 0; p < P; ++p) {
     char level_name[24];
     std::snprintf(level_name, sizeof(level_name), "level%u", p);
@@ -335,7 +341,23 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
     }
     graph_grow_nodes(E, H, need);
     inherit_new_nodes(E, H, E.new_ids);
-    project_up(E, L, H);
+    // M8: the nodes level p+1 gains from this level's splits, and those whose
+    // community the projection changes, join K at level p+1
+    E.sc.kflag.ensure(E.mem, H.g.n ? H.g.n : 1);
+    HL_CUDA(cudaMemsetAsync(E.sc.kflag.p, 0, H.g.n ? H.g.n : 1, E.stream));
+    if (!E.new_ids.empty()) {
+      std::vector<u32> ids;
+      for (auto& xo : E.new_ids) ids.push_back(xo.first);
+      E.sc.kflag_ids.ensure(E.mem, ids.size());
+      HL_CUDA(cudaMemcpyAsync(E.sc.kflag_ids.p, ids.data(), sizeof(u32) * ids.size(),
+                              cudaMemcpyHostToDevice, E.stream));
+      ++E.nlaunch, k_flag_ids<<<(u32)std::min<size_t>((ids.size() + 255) / 256, 148 * 32), 256, 0,
+                                E.stream>>>(E.sc.kflag_ids.p, (u32)ids.size(), H.g.n,
+                                            E.sc.kflag.p);
+      HL_LAUNCH_CHECK();
+    }
+    project_up(E, L, H, E.sc.kflag.p);
+    E.k_flags_set = true;
     if (cur.k == 0 && ro.refined == 0) {  // should_skip_aggregation (:1020-1022)
       cur = DevEdges{};
       cur_n = H.g.n;

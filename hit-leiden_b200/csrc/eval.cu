@@ -837,6 +837,13 @@ __global__ void k_pb_plan(const u32* ovf, const u32* novf, const u32* verts, con
   }
 }
 
+// Bucket of a key among B = 2^k buckets: the top k bits of its hash.  The
+// fold kernel's table slot takes the low bits of the same hash, so a bucket's
+// keys still spread over the whole table.
+__device__ __forceinline__ u32 pb_bucket(u32 key, u32 B) {
+  return B <= 1 ? 0u : hash32(key) >> (32 - (__ffs(B) - 1));
+}
+
 // Largest r in [lo, hi) with base[r] <= x (base ascending, base[lo] <= x).
 template <typename T>
 __device__ __forceinline__ u32 pb_row_of(const T* base, u32 lo, u32 hi, T x) {
@@ -900,7 +907,7 @@ __global__ void __launch_bounds__(256) k_pb_hist(EvalArgs A, PbArgs P) {
       P.ktmp[ebase + (q - lo)] = key;
       if (key == NONE32) continue;
       if (key == cur) wc += A.w[q];
-      const u32 b = hash32(key) & (B - 1);
+      const u32 b = pb_bucket(key, B);
       if (local) atomicAdd(&s_hist[b], 1u);
       else atomicAdd(&gcnt[b], 1u);
     }
@@ -936,7 +943,7 @@ __global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
     for (u64 q = lo + threadIdx.x; q < hi; q += blockDim.x) {
       const u32 key = P.ktmp[ebase + (q - lo)];
       if (key == NONE32) continue;
-      const u32 b = hash32(key) & (B - 1);
+      const u32 b = pb_bucket(key, B);
       const u32 slot = start[b] + atomicAdd(&cursor[b], 1u);
       P.ekey[slot] = key;
       P.epos[slot] = (u32)(q - o0);

@@ -103,6 +103,9 @@ struct Scratch {
       pb_epos, pb_bcnt, pb_boff, pb_bp, pb_bk;
   DBuf<u64> pb_ne, pb_ebase;
   DBuf<double> pb_wcur, pb_ew, pb_bg;
+  DBuf<u32> mark_long, mark_long_cnt;
+  DBuf<u8> kflag;     // K marks for the next level (M8), level-size bytes
+  DBuf<u32> kflag_ids;  // moved hubs whose rows k_mark_next_long marks
   // movement rounds of a small frontier (small.cu)
   DBuf<u32> sm_list_a, sm_list_b;
   DBuf<u64> sm_out;
@@ -164,6 +167,9 @@ struct Engine {
   // per-call statistics
   hl_batch_stats st{};
   std::vector<std::pair<u32, u32>> new_ids;  // (new sub-community id, origin) of the last refinement
+  // K marks handed to the next level's inc_movement (M8): the nodes it gained
+  // from splits below and the nodes whose community the projection changed
+  bool k_flags_set = false;
   // degree-bin thresholds picked by the autotuner (0 = compile-time default)
   struct Tune {
     u32 mid_max = 0, wide_max = 0;
@@ -268,7 +274,7 @@ extern std::atomic<u32> g_pb_slots;
 u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n,
                     bool changed_only, bool edge_weight_loops);  // output in sc.eu2/ev2/ew2
 u64 aggregate_full(Engine& E, Level& L, const u32* s, u32* out_u, u32* out_v, double* out_w);
-void project_up(Engine& E, Level& lo, Level& hi);
+void project_up(Engine& E, Level& lo, Level& hi, u8* changed_flags = nullptr);
 void top_down(Engine& E);
 void inherit_new_nodes(Engine& E, Level& hi, const std::vector<std::pair<u32, u32>>& ids);
 

@@ -27,6 +27,12 @@ static inline u32 grid_for(u64 n, u32 block = 256) {
 // ----------------------------------------------------------------------------
 // Seeding: inc_movement lines 2-8 (hit_leiden.rs:1037-1057).
 // ----------------------------------------------------------------------------
+// M8 of the multi-level extension: the K marks the level below handed up.
+__global__ void k_or_flags(const u8* src, u32 n, u8* dst) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    if (src[i]) dst[i] = 1;
+}
+
 __global__ void k_seed(const u32* u, const u32* v, const double* w, u64 k, const u32* f,
                        const u32* s, u8* active, u8* affected) {
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < k; i += (u64)gridDim.x * blockDim.x) {
@@ -411,15 +417,24 @@ __global__ void k_apply_ordered(const u32* seg_last, const u32* head_last, const
 }
 
 // Next frontier and K marks (throughput.rs:189-199), on f after all moves.
+// Rows longer than MARK_LONG entries (moved hubs) are left to
+// k_mark_next_long, a block per row, so that no warp walks a row of millions
+// of entries alone while the others idle.
+constexpr u64 MARK_LONG = 4096;
+
 __global__ void k_mark_next(u32 M, const u8* status, const u32* sel_node, const u32* sel_to,
                             const u64* off, const u32* col, const u32* f, const u32* s, u8* next,
-                            u8* affected) {
+                            u8* affected, u32* long_list, u32* long_count) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 r = warp; r < M; r += nwarps) {
     if (status[r] != ST_ACCEPTED) continue;
     u32 v = sel_node[r], to = sel_to[r];
+    if (off[v + 1] - off[v] > MARK_LONG) {
+      if (lane == 0) long_list[atomicAdd(long_count, 1u)] = (u32)r;
+      continue;
+    }
     u32 sv = s[v];
     bool any_same = false;
     const u64 o1 = off[v + 1];
@@ -445,6 +460,31 @@ __global__ void k_mark_next(u32 M, const u8* status, const u32* sel_node, const 
         }
     }
     if (__any_sync(0xffffffffu, any_same) && lane == 0) affected[v] = 1;
+  }
+}
+
+// The long rows k_mark_next listed: a block per moved hub, the same marks.
+__global__ void __launch_bounds__(256) k_mark_next_long(const u32* long_list, const u32* long_count,
+                                                        const u32* sel_node, const u32* sel_to,
+                                                        const u64* off, const u32* col,
+                                                        const u32* f, const u32* s, u8* next,
+                                                        u8* affected) {
+  const u32 cnt = *long_count;
+  for (u32 t = blockIdx.x; t < cnt; t += gridDim.x) {
+    const u32 r = long_list[t];
+    const u32 v = sel_node[r], to = sel_to[r];
+    const u32 sv = s[v];
+    bool any_same = false;
+    const u64 o1 = off[v + 1];
+    for (u64 p = off[v] + threadIdx.x; p < o1; p += blockDim.x) {
+      const u32 nb = col[p];
+      if (f[nb] != to) next[nb] = 1;
+      if (s[nb] == sv) {
+        affected[nb] = 1;
+        any_same = true;
+      }
+    }
+    if (__syncthreads_or(any_same) && threadIdx.x == 0) affected[v] = 1;
   }
 }
 
@@ -514,6 +554,11 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     ++E.nlaunch, k_seed<<<grid_for(delta.k), 256, 0, st>>>(delta.u, delta.v, delta.w, delta.k, L.f.p,
                                                L.s_cur.p, S.active.p, S.affected.p);
   HL_LAUNCH_CHECK();
+  if (E.k_flags_set) {  // M8: K marks handed up from the level below
+    ++E.nlaunch, k_or_flags<<<grid_for(n), 256, 0, st>>>(S.kflag.p, n, S.affected.p);
+    HL_LAUNCH_CHECK();
+    E.k_flags_set = false;
+  }
   // Community ids must stay below n so that n + v is a fresh empty community.
   compact_labels_if_needed(E, L.f.p, n, n);
   const size_t ncap = 2 * (size_t)n + 2;
@@ -645,9 +690,18 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     // round): such a round marks nothing, so the next frontier is empty and
     // the loop ends on it with the same iteration count.
     HL_CUDA(cudaMemsetAsync(S.next.p, 0, n, st));
+    S.mark_long.ensure(E.mem, M);
+    S.mark_long_cnt.ensure(E.mem, 1);
+    HL_CUDA(cudaMemsetAsync(S.mark_long_cnt.p, 0, sizeof(u32), st));
     ++E.nlaunch, k_mark_next<<<grid_for((u64)M * 32), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_to.p,
                                                         L.g.off.p, L.g.col.p, L.f.p, L.s_cur.p,
-                                                        S.next.p, S.affected.p);
+                                                        S.next.p, S.affected.p, S.mark_long.p,
+                                                        S.mark_long_cnt.p);
+    ++E.nlaunch, k_mark_next_long<<<148 * 2, 256, 0, st>>>(S.mark_long.p, S.mark_long_cnt.p,
+                                                           S.sel_node.p,
+                                                           S.sel_to.p, L.g.off.p, L.g.col.p,
+                                                           L.f.p, L.s_cur.p, S.next.p,
+                                                           S.affected.p);
     HL_LAUNCH_CHECK();
     E.kt_end(KT_MARK_NEXT, ev_mark);
     S.active.swap(S.next);

@@ -454,7 +454,8 @@ struct MoveOut {
 // (:1103-1191).
 static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std::vector<u32>& f,
                             const std::vector<u32>& s, double gamma, int mode, u32 max_rounds,
-                            bool compact, bool mark_moved = false) {
+                            bool compact, bool mark_moved = false,
+                            const std::vector<u32>* extra_k = nullptr) {
   u32 n = g.n;
   MoveOut out;
   out.changed.assign(n, 0);
@@ -467,6 +468,12 @@ static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std:
     if (s[e.u] == s[e.v]) out.affected[e.u] = out.affected[e.v] = 1;
   }
   if (delta.empty()) std::fill(active.begin(), active.end(), 1);
+  // M8 (multi-level): the nodes this level gained from splits at the level
+  // below join K, so the sub-community they inherited (M6) is split again
+  // when they are not connected to it.
+  if (extra_k)
+    for (u32 x : *extra_k)
+      if (x < n) out.affected[x] = 1;
   if (compact) compact_ids_if_needed(f, n);
 
   std::vector<double> k = node_degrees(g);
@@ -603,9 +610,12 @@ static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std:
     }
     if (bestg <= 0.0) continue;
     u32 old = f[v];
+    // An empty-community move allocates next_empty and moves the counter on
+    // (:1170-1173: the reference's array grows by one, and its length is the
+    // next id).
+    if ((size_t)best == next_empty) next_empty = (size_t)best + 1;
     if (best >= d.size()) {
       d.resize((size_t)best + 1, 0.0);
-      next_empty = (size_t)best + 1;
       if (buf.size() < d.size()) {
         buf.resize(d.size(), 0.0);
         seen.resize(d.size(), 0);
@@ -1147,7 +1157,11 @@ static u32 hit_leiden(State& st, u32 delta_n, const std::vector<Edge>& delta, do
 //   M6 a sub-community id X handed out at level p for a component split from
 //      S starts at level p+1 with S's s_pre / s_cur / g values;
 //   M7 def-update recomputes f^p = f^{p+1}∘s^p and g^p = g^{p+1}∘s^p top-down
-//      for every vertex (g at the top level is the identity).
+//      for every vertex (g at the top level is the identity);
+//   M8 the level-(p+1) nodes created by M6, and those whose community M5
+//      changed, join K at level p+1, so that their sub-community is split
+//      again when it is no longer connected or no longer inside one community
+//      (refined communities stay connected and nested at every level).
 // ---------------------------------------------------------------------------
 static void ensure_level_size(State& st, u32 p, u32 n) {
   grow_map(st.f[p], n);
@@ -1170,11 +1184,12 @@ static u32 hit_leiden_ml(State& st, const std::vector<Edge>& delta, double gamma
   std::vector<Edge> cur = delta;
   u32 cur_n = st.sg[0].n;
   u32 total_it = 0;
+  std::vector<u32> gained;  // nodes this level gained from splits below (M8)
   for (u32 p = 0; p < P; ++p) {
     st.sg[p] = apply_delta(st.sg[p], std::max(cur_n, st.sg[p].n), cur, true);
     ensure_level_size(st, p, st.sg[p].n);
     MoveOut mo = inc_movement(st.sg[p], cur, st.f[p], st.s_cur[p], gamma, mode, max_rounds,
-                              compact, true);
+                              compact, true, &gained);
     total_it += mo.iterations;
     RefineOut ro =
         inc_refinement(st.sg[p], st.f[p], st.s_cur[p], mo.affected, gamma, mode, faithful, true);
@@ -1205,13 +1220,19 @@ static u32 hit_leiden_ml(State& st, const std::vector<Edge>& delta, double gamma
     for (u32 x : st.s_cur[p]) need = std::max(need, x + 1);
     for (const auto& xo : ro.new_ids) need = std::max(need, xo.first + 1);
     ensure_level_size(st, p + 1, need);
+    gained.clear();
     for (const auto& xo : ro.new_ids) {
       st.s_pre[p + 1][xo.first] = st.s_pre[p + 1][xo.second];
       st.s_cur[p + 1][xo.first] = st.s_cur[p + 1][xo.second];
       st.g[p + 1][xo.first] = st.g[p + 1][xo.second];
+      gained.push_back(xo.first);
     }
-    // M5: project communities up.
+    // M5: project communities up; M8: a node whose community the projection
+    // changes joins K at level p+1 as well.
+    std::vector<u32> f_before = st.f[p + 1];
     for (u32 v = 0; v < st.sg[p].n; ++v) st.f[p + 1][st.s_cur[p][v]] = st.f[p][v];
+    for (u32 x = 0; x < (u32)f_before.size(); ++x)
+      if (st.f[p + 1][x] != f_before[x]) gained.push_back(x);
     bool any_r = false;
     for (uint8_t c : ro.refined) any_r |= (c != 0);
     if (cur.empty() && !any_r) {

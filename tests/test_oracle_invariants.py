@@ -96,3 +96,36 @@ def test_invariants_under_delete_heavy_batches(seed):
         u, v, ww = W.mixed_batch(store, 300, 0.3, 50 * seed + b, preferential=False)
         st.hit_leiden(u, v, ww)
         _check(st, 0)
+
+
+def _levels_of(st):
+    out = []
+    for p in range(st.levels):
+        off, col, w = st.graph(p).csr()
+        out.append((off, col, w, st.get_map(p, O.MAP_F), st.get_map(p, O.MAP_S_CUR)))
+    return out
+
+
+@pytest.mark.parametrize("mode", [O.MODE_DETERMINISTIC, O.MODE_THROUGHPUT])
+@pytest.mark.parametrize("seed", [0, 1])
+def test_hierarchy_quality_invariants(mode, seed):
+    """Nesting and local optimality (no single move gains more than 2e-3) in
+    both modes; connected sub-communities at every level in deterministic
+    mode (the nodes a level gains from splits below join K there, M8)."""
+    import importlib
+    INV = importlib.import_module("tests.invariants")
+    n, s, d, w = W.config1(seed)
+    st = O.State(n, mode=mode)
+    st.bootstrap(s, d, w, max_levels=10)
+    ex = set(zip(s.tolist(), d.tolist()))
+    for b in range(4):
+        u, v, ww = W.uniform_inserts(n, 1000, 7000 + 10 * seed + b, ex)
+        st.hit_leiden(u, v, ww)
+    lv = _levels_of(st)
+    INV.check_nested(lv)
+    INV.check_local_moves(lv)
+    if mode == O.MODE_DETERMINISTIC:
+        INV.check_connected(lv)
+    else:
+        bad, total = INV.disconnected(*lv[0][:2], lv[0][4])
+        assert 0 < bad < 0.25 * total  # the Jacobi merges' known effect

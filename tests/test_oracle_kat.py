@@ -480,3 +480,16 @@ def test_run_partition_length_matches_node_count(n):
         st = O.State(n, mode=O.MODE_THROUGHPUT)
         st.bootstrap([], [], [], max_levels=10)
         assert len(st.get_map(0, O.MAP_F)) == n
+
+
+def test_deterministic_empty_moves_take_successive_ids():
+    """Deterministic movement (hit_leiden.rs:1150-1173): each move to the
+    empty community takes community_degrees.len(), and the array grows by
+    one, so a second empty move gets the next id.  At gamma = 3 on
+    0-1 (10), 0-2 (0.5), node 0 leaves for id 3, then node 1 (whose only
+    neighbour is now in 3, at a negative gain) leaves for id 4."""
+    g = O.Graph.from_edges(3, np.array([0, 0], np.uint32), np.array([1, 2], np.uint32),
+                           np.array([10.0, 0.5]))
+    f, changed, _, it = O.inc_movement(g, [], [], None, [0, 0, 0], [0, 0, 0], 3.0,
+                                       O.MODE_DETERMINISTIC)
+    assert f.tolist() == [3, 4, 0] and changed.tolist() == [True, True, False] and it == 1
