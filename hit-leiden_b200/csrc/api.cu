@@ -174,24 +174,61 @@ static void engine_free(EngineBox* B) {
   delete B;  // members: bb, E (frees on the stream), then so (destroys the stream)
 }
 
-__global__ void k_count_u8(const u8* f, u32 n, u32* out) {
+namespace hl {
+
+__global__ void k_stats_acc64(const unsigned long long* src, u32 count, unsigned long long* acc) {
+  if (threadIdx.x < count) acc[threadIdx.x] += src[threadIdx.x];
+}
+__global__ void k_stats_acc32(const u32* src, unsigned long long* acc) {
+  if (threadIdx.x == 0) *acc += *src;
+}
+__global__ void k_stats_count_u8(const u8* f, u32 n, unsigned long long* out) {
   u32 local = 0;
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
     local += f[i] ? 1u : 0u;
   for (int o = 16; o; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
-  if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, (unsigned long long)local);
 }
 
-static u32 count_flags(Engine& E, const u8* f, u32 n) {
-  if (!n) return 0;
-  E.sc.cnt.ensure(E.mem, 16);
-  HL_CUDA(cudaMemsetAsync(E.sc.cnt.p + 15, 0, sizeof(u32), E.stream));
+static void stats_ready(Engine& E) {
+  if (E.sc.bacc.cap >= 16) return;
+  E.sc.bacc.ensure(E.mem, 16);
+  HL_CUDA(cudaMemsetAsync(E.sc.bacc.p, 0, 16 * sizeof(u64), E.stream));
+}
+
+void stats_acc_u64(Engine& E, const unsigned long long* src, u32 count, u32 slot) {
+  stats_ready(E);
+  ++E.nlaunch, k_stats_acc64<<<1, 32, 0, E.stream>>>(
+      src, count, reinterpret_cast<unsigned long long*>(E.sc.bacc.p) + slot);
+  HL_LAUNCH_CHECK();
+}
+
+void stats_acc_u32(Engine& E, const u32* src, u32 slot) {
+  stats_ready(E);
+  ++E.nlaunch, k_stats_acc32<<<1, 32, 0, E.stream>>>(
+      src, reinterpret_cast<unsigned long long*>(E.sc.bacc.p) + slot);
+  HL_LAUNCH_CHECK();
+}
+
+void stats_count_flags(Engine& E, const u8* flags, u32 n, u32 slot) {
+  stats_ready(E);
+  if (!n) return;
   u32 g = (n + 255) / 256;
   if (g > 148 * 32) g = 148 * 32;
-  ++E.nlaunch, k_count_u8<<<g, 256, 0, E.stream>>>(f, n, E.sc.cnt.p + 15);
+  ++E.nlaunch, k_stats_count_u8<<<g, 256, 0, E.stream>>>(
+      flags, n, reinterpret_cast<unsigned long long*>(E.sc.bacc.p) + slot);
   HL_LAUNCH_CHECK();
-  return E.read_u32(E.sc.cnt.p + 15);
 }
+
+// A call's statistics start from zero on the device.
+static void stats_begin(Engine& E) {
+  stats_ready(E);
+  HL_CUDA(cudaMemsetAsync(E.sc.bacc.p, 0, 16 * sizeof(u64), E.stream));
+  E.sum_nv_batch = 0;
+}
+
+}  // namespace hl
+
 
 // Algorithm 6 (hit_leiden.rs:936-1018) for one batch already on the device.
 // NVTX range for the scope (a level, a stage), so that profilers can select
@@ -275,7 +312,7 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
     Level& L = E.levels[0];
     apply_delta(E, L, delta, L.g.n, (E.cfg.flags & HL_FLAG_KEEP_SELF_LOOPS) != 0);
     MoveOut mo = inc_movement(E, L, delta, delta.k == 0, false);
-    st.changed = count_flags(E, E.sc.changed.p, L.g.n);
+    stats_count_flags(E, E.sc.changed.p, L.g.n, 10);
     level_snapshot(E, L);
     RefineOut ro = inc_refinement(E, L, false);
     level_emit(E, L, 0);
@@ -309,7 +346,7 @@ static void hit_leiden_batch(EngineBox& B, const DevEdges& delta) {
       mo = inc_movement(E, L, cur, cur.k == 0, true);
     }
     E.kt_end(KT_STAGE_MOVE, e0);
-    if (p == 0) st.changed = count_flags(E, E.sc.changed.p, L.g.n);
+    if (p == 0) stats_count_flags(E, E.sc.changed.p, L.g.n, 10);
     e0 = E.kt_begin();
     RefineOut ro;
     level_snapshot(E, L);
@@ -478,12 +515,33 @@ static void upload_edges(EngineBox& B, const uint32_t* src, const uint32_t* dst,
 
 static void finish_stats(EngineBox& B, hl_batch_stats* stats) {
   Engine& E = *B.E;
+  // the statistics kept on the device come back with the call's last wait
+  stats_ready(E);
+  HL_CUDA(cudaMemcpyAsync(E.hs.p + 40, E.sc.bacc.p, 16 * sizeof(u64), cudaMemcpyDeviceToHost,
+                          E.stream));
   HL_CUDA(cudaEventRecord(E.ev1, E.stream));
   HL_CUDA(cudaEventSynchronize(E.ev1));
   float ms = 0.f;
   HL_CUDA(cudaEventElapsedTime(&ms, E.ev0, E.ev1));
   E.st.device_ms = ms;
   E.st.launches = E.nlaunch - E.launch_mark;
+  u64 acc[16];
+  std::memcpy(acc, E.hs.p + 40, sizeof(acc));
+  u64 trav = 0, ncand = 0;
+  const int bins[4] = {KT_EVAL_SMALL, KT_EVAL_MID, KT_EVAL_BIG, KT_EVAL_HUGE};
+  for (int b = 0; b < 4; ++b) {
+    trav += acc[2 * b];
+    ncand += acc[2 * b + 1];
+    E.kagg[bins[b]].bytes += 16ull * acc[2 * b] + 8ull * acc[2 * b + 1];
+  }
+  // Algorithmic bytes of the evaluation: per active vertex its list entry,
+  // offsets, f, k, d(f) and outputs; per adjacency entry the neighbour,
+  // weight and neighbour community; per evaluated candidate its d(C).
+  E.kagg[KT_MOVE_EVAL].bytes += 52ull * E.sum_nv_batch + 16ull * trav + 8ull * ncand;
+  E.st.traversed += trav;
+  E.st.moves += acc[8];
+  E.st.merges += acc[9];
+  E.st.changed = acc[10];
   E.kt_collect();
   E.st.levels = (u32)E.levels.size();
   E.st.edges = E.levels.empty() ? 0 : E.levels[0].g.nnz / 2;
@@ -508,6 +566,7 @@ static void create_impl(const hl_config* cfg, uint32_t n, const uint32_t* src, c
   check_endpoints(E, G, n);
   E.integral = edges_integral(E, G);
   E.st = hl_batch_stats{};
+  stats_begin(E);
   HL_CUDA(cudaEventRecord(E.ev0, E.stream));
   E.in_bootstrap = true;
   bootstrap(*B, n, G);
@@ -529,6 +588,7 @@ static void apply_impl(hl_graph* g, const uint32_t* src, const uint32_t* dst, co
   Engine& E = *B.E;
   HL_CUDA(cudaSetDevice(E.device));
   E.st = hl_batch_stats{};
+  stats_begin(E);
   E.launch_mark = E.nlaunch;
   DevEdges D;
   if (device_ptrs)

@@ -104,6 +104,10 @@ struct Scratch {
   DBuf<u64> pb_ne, pb_ebase;
   DBuf<double> pb_wcur, pb_ew, pb_bg;
   DBuf<u32> mark_long, mark_long_cnt;
+  // batch statistics accumulated on the device and read once at the end of
+  // the call: [0..7] traversed / candidates of the four evaluation bins,
+  // [8] accepted moves, [9] refinement merges, [10] |B^1|
+  DBuf<u64> bacc;
   DBuf<u8> kflag;     // K marks for the next level (M8), level-size bytes
   DBuf<u32> kflag_ids;  // moved hubs whose rows k_mark_next_long marks
   // movement rounds of a small frontier (small.cu)
@@ -170,6 +174,7 @@ struct Engine {
   // K marks handed to the next level's inc_movement (M8): the nodes it gained
   // from splits below and the nodes whose community the projection changed
   bool k_flags_set = false;
+  u64 sum_nv_batch = 0;  // frontier sizes of the multi-kernel evaluations, this call
   // degree-bin thresholds picked by the autotuner (0 = compile-time default)
   struct Tune {
     u32 mid_max = 0, wide_max = 0;
@@ -248,6 +253,11 @@ struct RefineOut {
   u32 smax_before = 0;
 };
 RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community);
+
+// api.cu: device-side batch statistics (Scratch::bacc)
+void stats_acc_u64(Engine& E, const unsigned long long* src, u32 count, u32 slot);
+void stats_acc_u32(Engine& E, const u32* src, u32 slot);
+void stats_count_flags(Engine& E, const u8* flags, u32 n, u32 slot);
 
 // small.cu: movement rounds of a small frontier in one block.  Returns true
 // when the movement stage is finished, false when the host rounds continue

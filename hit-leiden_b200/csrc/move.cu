@@ -707,20 +707,11 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     S.active.swap(S.next);
   }
   out.iterations = it;
-  u64 cnt8[8];
-  HL_CUDA(cudaMemcpyAsync(E.hs.p, S.red64.p, 8 * sizeof(u64), cudaMemcpyDeviceToHost, st));
-  HL_CUDA(cudaMemcpyAsync(E.hs.p + 8, S.acc_cnt.p, sizeof(u32), cudaMemcpyDeviceToHost, st));
-  E.sync();
-  std::memcpy(cnt8, E.hs.p, sizeof(cnt8));
-  out.moves = (u32)(E.hs.p[8] & 0xFFFFFFFFull);
-  out.traversed = cnt8[0] + cnt8[2] + cnt8[4] + cnt8[6];
-  u64 ncand = cnt8[1] + cnt8[3] + cnt8[5] + cnt8[7];
-  // Algorithmic bytes of the evaluation kernel: per active vertex its list
-  // entry, offsets, f, k, d(f) and outputs; per adjacency entry the neighbour,
-  // weight and neighbour community; per evaluated candidate its d(C).
-  E.kagg[KT_MOVE_EVAL].bytes += 52ull * sum_nv + 16ull * out.traversed + 8ull * ncand;
-  const int bins[4] = {KT_EVAL_SMALL, KT_EVAL_MID, KT_EVAL_BIG, KT_EVAL_HUGE};
-  for (int b = 0; b < 4; ++b) E.kagg[bins[b]].bytes += 16ull * cnt8[2 * b] + 8ull * cnt8[2 * b + 1];
+  // The evaluation counters and the accepted moves stay on the device until
+  // the call ends (Scratch::bacc; the algorithmic bytes are counted there).
+  stats_acc_u64(E, reinterpret_cast<const unsigned long long*>(S.red64.p), 8, 0);
+  stats_acc_u32(E, S.acc_cnt.p, 8);
+  E.sum_nv_batch += sum_nv;
   out.moves += sm_moves;
   out.candidates += sm_cands;
   out.traversed += sm_trav;

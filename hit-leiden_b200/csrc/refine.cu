@@ -627,7 +627,7 @@ RefineOut inc_refinement(Engine& E, Level& L, bool cc_same_community) {
   ++E.nlaunch, k_apply_merges<<<grid_for(ns), 256, 0, st>>>(single, ns, S.cand_to.p, S.cand_gain.p, s,
                                                cnt + 9);
   HL_LAUNCH_CHECK();
-  out.merges = E.read_u32(cnt + 9);
+  stats_acc_u32(E, cnt + 9, 9);  // merges, read when the call ends
   return out;
 }
 
