@@ -849,10 +849,11 @@ def run_rmat(args, cfg):
                        traversed, kernels, clk, ratio)
     q = st.modularity()
     dbytes = _device_bytes(L, h)
-    tmid, twide, tfr = C.c_uint32(), C.c_uint32(), C.c_uint32()
-    L.check(L.lib.hl_autotune_info(h, C.byref(tmid), C.byref(twide), C.byref(tfr)))
+    tmid, twide, tdef, tfr = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+    L.check(L.lib.hl_autotune_info(h, C.byref(tmid), C.byref(twide), C.byref(tdef),
+                                   C.byref(tfr)))
     config["degree_bins"] = {"warp_table_max": tmid.value, "wide_max": twide.value,
-                             "tuned_on_frontier": tfr.value}
+                             "hub_defer_entries": tdef.value, "tuned_on_frontier": tfr.value}
     served = None
     if not args.no_served:
         served = _served_rmat(hl, st, scale, del_pool, args.seed, torch, args.served_requests)

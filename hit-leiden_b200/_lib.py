@@ -149,8 +149,9 @@ def _load():
         "hl_dbg_set_exact_tfilter": (st, [C.c_int32]),
         "hl_dbg_set_mode": (st, [C.c_uint32]),
         "hl_dbg_set_bucket_slots": (st, [C.c_uint32]),
+        "hl_dbg_set_hub_defer": (st, [C.c_uint32]),
         "hl_dbg_set_bins": (st, [C.c_uint32, C.c_uint32]),
-        "hl_autotune_info": (st, [vp, p32, p32, p32]),
+        "hl_autotune_info": (st, [vp, p32, p32, p32, p32]),
         "hl_tree_sum_noalloc": (st, [vp, C.c_uint64, vp, vp]),
         "hl_dbg_modularity": (st, [C.c_int32, C.c_uint32, vp, vp, vp, vp,
                                    C.POINTER(C.c_double)]),

@@ -705,10 +705,11 @@ hl_status hl_set_level_callback(hl_graph* g, hl_level_fn fn, void* user) {
 }
 
 hl_status hl_autotune_info(const hl_graph* g, uint32_t* mid_max, uint32_t* wide_max,
-                           uint32_t* frontier) {
+                           uint32_t* hub_defer, uint32_t* frontier) {
   HL_TRY(require(g && mid_max && wide_max && frontier, "NULL argument");
          const Engine& E = *box(g)->E; *mid_max = E.tune.mid_max ? E.tune.mid_max : 128;
          *wide_max = E.tune.wide_max ? E.tune.wide_max : 512;
+         if (hub_defer) *hub_defer = E.tune.hub_defer ? E.tune.hub_defer : 8192;
          *frontier = E.tune.done ? E.tune.frontier : 0);
 }
 
@@ -1106,7 +1107,12 @@ hl_status hl_dbg_set_bins(uint32_t mid_max, uint32_t wide_max) {
 }
 
 hl_status hl_dbg_set_bucket_slots(uint32_t slots) {
-  g_pb_slots.store(slots ? slots : 4096u);
+  g_pb_slots.store(slots);  // 0 (or out of range): the fold kernel's full table
+  return HL_OK;
+}
+
+hl_status hl_dbg_set_hub_defer(uint32_t entries) {
+  g_dbg_hub_defer.store(entries);  // 0: each handle's own (autotuned) bound
   return HL_OK;
 }
 

@@ -13,7 +13,8 @@
 // vertex waits on a table far larger than it needs:
 //   deg <= 8, 16, 32    sub-warp groups of 8 / 16 / 32 lanes, one chunk, no table;
 //   33 .. MID_MAX       a warp per vertex, shared-memory table sized 2·deg;
-//   MID_MAX .. WIDE_MAX a warp per vertex, a per-warp global table;
+//   MID_MAX .. WIDE_MAX a warp per vertex, a per-warp shared-memory table
+//                       (half-size tables up to WIDE_SPLIT);
 //   larger              a block per vertex: 256-entry adjacency tiles bucketed
 //                       by a hash partition of their keys, one partition per
 //                       warp, each warp folding its own keys in CSR order into
@@ -63,6 +64,8 @@ struct EvalArgs {
   u32* ovf_count;  // they passed BIG_TAB / 2 distinct keys (idx values)
   const u32* nidx_dev;  // if set, the number of idx entries is read here
   u32* work;            // block kernel: next idx position to take (zeroed per launch)
+  u64 defer_deg;        // block kernel pass 1: rows longer than this go to the
+                        // partitioned pass unread (0: none)
 };
 
 constexpr u32 MID_MAX = 128;
@@ -208,13 +211,19 @@ __global__ void __launch_bounds__(256) k_eval_small(EvalArgs A) {
 
 // ---------------------------------------------------------------------------
 // Mid degrees: a warp per vertex with a shared table sized to the vertex.
+// The row's chunks (at most MID_MAX / 32) are loaded together and their keys
+// gathered together, then folded in CSR order; the candidates' community
+// degrees are gathered MID_SCAN_UNROLL at a time.
 // ---------------------------------------------------------------------------
+constexpr u32 MID_CHUNKS = MID_MAX / 32;
+constexpr u32 MID_SCAN_UNROLL = 4;
+
 template <int KIND>
-__global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
+__global__ void __launch_bounds__(MID_WARPS * 32, 4) k_eval_mid(EvalArgs A) {
   __shared__ u32 s_key[MID_WARPS][MID_TAB];
   __shared__ u32 s_pos[MID_WARPS][MID_TAB];
   __shared__ double s_val[MID_WARPS][MID_TAB];
-  __shared__ double s_w[MID_WARPS][32];
+  __shared__ double s_w[MID_WARPS][MID_CHUNKS * 32];
   const u32 lane = threadIdx.x & 31;
   const u32 wib = threadIdx.x >> 5;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
@@ -223,6 +232,7 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
   u32* tk = s_key[wib];
   u32* tp = s_pos[wib];
   double* tv = s_val[wib];
+  double* sw = s_w[wib];
   for (u64 t = warp; t < A.nidx; t += nwarps) {
     const u32 i = A.idx[t];
     const u32 v = A.verts[i];
@@ -231,33 +241,42 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
     const u32 fv = A.f[v];
     const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
     const double kv = A.kdeg[v];
+    const double dcur = A.d[cur];
     if (lane == 0) trav += deg;
     u32 cap = 64;
     while (cap < 2 * deg) cap <<= 1;
     const u32 mask = cap - 1;
     for (u32 x = lane; x < cap; x += 32) tk[x] = NONE32;
-    __syncwarp();
-    for (u64 b0 = o0; b0 < o1; b0 += 32) {
-      u64 q = b0 + lane;
-      u32 key = NONE32;
+    u32 nb[MID_CHUNKS], key[MID_CHUNKS];
+#pragma unroll
+    for (u32 j = 0; j < MID_CHUNKS; ++j) {
+      const u64 q = o0 + j * 32 + lane;
+      nb[j] = NONE32;
       double wv = 0.0;
-      bool has = false;
       if (q < o1) {
-        u32 nb = A.col[q];
+        nb[j] = A.col[q];
         wv = A.w[q];
-        has = entry_key<KIND>(A, v, nb, fv, key);
-        if (!has) key = NONE32;
       }
-      s_w[wib][lane] = wv;
-      __syncwarp();
-      u32 grp = __match_any_sync(0xffffffffu, key);
-      if (has && lane == (u32)(__ffs(grp) - 1)) {
-        u32 slot = hash32(key) & mask;
+      sw[j * 32 + lane] = wv;
+    }
+#pragma unroll
+    for (u32 j = 0; j < MID_CHUNKS; ++j) {
+      key[j] = NONE32;
+      if (nb[j] != NONE32 && !entry_key<KIND>(A, v, nb[j], fv, key[j])) key[j] = NONE32;
+    }
+    __syncwarp();
+#pragma unroll
+    for (u32 j = 0; j < MID_CHUNKS; ++j) {
+      if (o0 + j * 32 >= o1) break;  // warp-uniform
+      const u64 q = o0 + j * 32 + lane;
+      const u32 grp = __match_any_sync(0xffffffffu, key[j]);
+      if (key[j] != NONE32 && lane == (u32)(__ffs(grp) - 1)) {
+        u32 slot = hash32(key[j]) & mask;
         while (true) {
-          u32 prev = atomicCAS(&tk[slot], NONE32, key);
-          if (prev == NONE32 || prev == key) {
+          u32 prev = atomicCAS(&tk[slot], NONE32, key[j]);
+          if (prev == NONE32 || prev == key[j]) {
             double sum = prev == NONE32 ? 0.0 : tv[slot];
-            for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, s_w[wib][__ffs(m) - 1]);
+            for (u32 m = grp; m; m &= m - 1) sum = __dadd_rn(sum, sw[j * 32 + __ffs(m) - 1]);
             tv[slot] = sum;
             if (prev == NONE32) tp[slot] = (u32)(q - o0);
             break;
@@ -280,17 +299,30 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
     double g = -1.0;
     u32 p = NONE32, kk = cur;
     if (A.tw != 0.0) {
-      for (u32 x = lane; x < cap; x += 32) {
-        u32 key = tk[x];
-        if (key == NONE32 || key == cur) continue;
-        if (KIND == EVAL_REFINE && A.blocked[key]) continue;
-        double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, A.d[cur], A.d[key]);
-        ++ncand;
-        u32 pp = tp[x];
-        if (p == NONE32 || gn > g || (gn == g && pp < p)) {
-          g = gn;
-          p = pp;
-          kk = key;
+      for (u32 x0 = lane; x0 < cap; x0 += 32 * MID_SCAN_UNROLL) {
+        u32 kq[MID_SCAN_UNROLL];
+        double dk[MID_SCAN_UNROLL];
+#pragma unroll
+        for (u32 j = 0; j < MID_SCAN_UNROLL; ++j) {
+          const u32 x = x0 + 32 * j;
+          kq[j] = x < cap ? tk[x] : NONE32;
+          if (kq[j] == cur) kq[j] = NONE32;
+          if (KIND == EVAL_REFINE && kq[j] != NONE32 && A.blocked[kq[j]]) kq[j] = NONE32;
+        }
+#pragma unroll
+        for (u32 j = 0; j < MID_SCAN_UNROLL; ++j) dk[j] = kq[j] != NONE32 ? A.d[kq[j]] : 0.0;
+#pragma unroll
+        for (u32 j = 0; j < MID_SCAN_UNROLL; ++j) {
+          if (kq[j] == NONE32) continue;
+          const u32 x = x0 + 32 * j;
+          const double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
+          ++ncand;
+          const u32 pp = tp[x];
+          if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+            g = gn;
+            p = pp;
+            kk = kq[j];
+          }
         }
       }
     }
@@ -313,29 +345,33 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_eval_mid(EvalArgs A) {
 // ---------------------------------------------------------------------------
 // Wide degrees (MID_MAX < deg <= WIDE_MAX): a warp per vertex.  The warp
 // issues the loads of up to 8 chunks (256 entries) at once, then folds the
-// chunks in CSR order into its own shared-memory table (1024 slots: keys,
-// 16-bit first positions, sums).  Every new key's slot is appended to a
-// per-warp list, so the argmax scan visits only used slots and resets them:
-// the table is clean again for the warp's next vertex without a clearing pass.
+// chunks in CSR order into its own shared-memory table (TAB = 2 x the bin's
+// largest degree slots: keys, 16-bit first positions, sums).  Every new key's
+// slot is appended to a per-warp list, so the argmax scan visits only used
+// slots and resets them: the table is clean again for the warp's next vertex
+// without a clearing pass.  The bin is split at WIDE_SPLIT: rows up to it
+// take half-size tables, so more warps fit on an SM.
 // ---------------------------------------------------------------------------
 constexpr u32 WIDE_MAX = 512;
-constexpr u32 WIDE_TAB = 2 * WIDE_MAX;  // slots of one warp's table
+constexpr u32 WIDE_SPLIT = 256;
 constexpr u32 WIDE_WARPS = 4;
 constexpr u32 WIDE_BATCH = 8;  // chunks loaded before folding
+constexpr u32 WIDE_SCAN_UNROLL = 4;  // table slots whose community degrees are gathered together
 
+template <u32 TAB>
 struct WideSmem {
-  double tv[WIDE_WARPS][WIDE_TAB];
+  double tv[WIDE_WARPS][TAB];
   double sw[WIDE_WARPS][WIDE_BATCH * 32];
-  u32 tk[WIDE_WARPS][WIDE_TAB];
-  unsigned short tp[WIDE_WARPS][WIDE_TAB];
-  unsigned short list[WIDE_WARPS][WIDE_MAX];
+  u32 tk[WIDE_WARPS][TAB];
+  unsigned short tp[WIDE_WARPS][TAB];
+  unsigned short list[WIDE_WARPS][TAB / 2];
   u32 cnt[WIDE_WARPS];
 };
 
-template <int KIND>
+template <int KIND, u32 TAB>
 __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
   extern __shared__ __align__(16) unsigned char wide_raw[];
-  WideSmem& W = *reinterpret_cast<WideSmem*>(wide_raw);
+  WideSmem<TAB>& W = *reinterpret_cast<WideSmem<TAB>*>(wide_raw);
   const u32 lane = threadIdx.x & 31;
   const u32 wib = threadIdx.x >> 5;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
@@ -346,7 +382,7 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
   double* tv = W.tv[wib];
   unsigned short* list = W.list[wib];
   double* sw = W.sw[wib];
-  for (u32 x = lane; x < WIDE_TAB; x += 32) tk[x] = NONE32;
+  for (u32 x = lane; x < TAB; x += 32) tk[x] = NONE32;
   __syncwarp();
   for (u64 t = warp; t < A.nidx; t += nwarps) {
     const u32 i = A.idx[t];
@@ -420,20 +456,31 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
     __syncwarp();
     double g = -1.0;
     u32 p = NONE32, kk = cur;
-    for (u32 x = lane; x < used; x += 32) {
-      u32 sl = list[x];
-      u32 key = tk[sl];
-      double val = tv[sl];
-      u32 pp = tp[sl];
-      tk[sl] = NONE32;
-      if (key == cur || A.tw == 0.0) continue;
-      if (KIND == EVAL_REFINE && A.blocked[key]) continue;
-      double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, A.d[key]);
-      ++ncand;
-      if (p == NONE32 || gn > g || (gn == g && pp < p)) {
-        g = gn;
-        p = pp;
-        kk = key;
+    for (u32 x0 = lane; x0 < used; x0 += 32 * WIDE_SCAN_UNROLL) {
+      u32 key[WIDE_SCAN_UNROLL], sl[WIDE_SCAN_UNROLL];
+      double dk[WIDE_SCAN_UNROLL];
+#pragma unroll
+      for (u32 j = 0; j < WIDE_SCAN_UNROLL; ++j) {
+        const u32 x = x0 + 32 * j;
+        sl[j] = x < used ? list[x] : 0u;
+        key[j] = x < used ? tk[sl[j]] : NONE32;
+        if (x < used) tk[sl[j]] = NONE32;
+        if (key[j] == cur || A.tw == 0.0) key[j] = NONE32;
+        if (KIND == EVAL_REFINE && key[j] != NONE32 && A.blocked[key[j]]) key[j] = NONE32;
+      }
+#pragma unroll
+      for (u32 j = 0; j < WIDE_SCAN_UNROLL; ++j) dk[j] = key[j] != NONE32 ? A.d[key[j]] : 0.0;
+#pragma unroll
+      for (u32 j = 0; j < WIDE_SCAN_UNROLL; ++j) {
+        if (key[j] == NONE32) continue;
+        const double gn = move_gain(tv[sl[j]], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
+        ++ncand;
+        const u32 pp = tp[sl[j]];
+        if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+          g = gn;
+          p = pp;
+          kk = key[j];
+        }
       }
     }
     for (int o = 16; o; o >>= 1) {
@@ -475,6 +522,8 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
 // regions, moving a row's table there when it passes the same bound.
 // ---------------------------------------------------------------------------
 constexpr u32 BIG_TAB = 4096;
+constexpr u64 BIG_DIRECT_DEFER = 2 * BIG_TAB;  // integral weights: longer rows are deferred unread
+// (the autotuner may pick another bound; see HUB_DEFER_CAND)
 constexpr u32 BIG_WARPS = BIG_THREADS / 32;
 constexpr u32 BIG_PART_BITS = 3;  // log2(BIG_WARPS)
 static_assert((1u << BIG_PART_BITS) == BIG_WARPS, "one key partition per warp");
@@ -550,6 +599,14 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
     const u32 fv = A.f[v];
     const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
     const double kv = A.kdeg[v];
+    // Integral weights: a row this long goes straight to the partitioned
+    // pass (it almost always passes BIG_TAB / 2 distinct keys, found only
+    // after part of the row has been folded).
+    if (A.defer_deg && !g_tk && deg > A.defer_deg) {
+      if (tid == 0) A.ovf_list[atomicAdd(A.ovf_count, 1u)] = i;
+      __syncthreads();
+      continue;
+    }
     u64 gcap = 64;
     while (gcap < 2 * deg) gcap <<= 1;
     const u32 cap = gcap < BIG_TAB ? (u32)gcap : BIG_TAB;
@@ -814,14 +871,17 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
 //   scatter  per chunk: (key, position, weight) into its bucket's range;
 //   fold     per bucket: shared table, then the bucket's best candidate;
 //   final    per row: the best over its buckets, then the empty community.
-// A bucket whose keys overflow its table (more than PB_TAB / 2 distinct: far
-// out in the tail of the hash spread) fails its row, which then takes the
+// A bucket holds at most about PB_TARGET entries plus the repeats of its
+// keys (a heavy key adds entries, not keys), so its distinct keys fit a
+// table of 2 x PB_TARGET slots.  A bucket whose keys fill its table (far out
+// in the tail of the hash spread) fails its row, which then takes the
 // global-table pass.
 // ---------------------------------------------------------------------------
 constexpr u32 PB_TARGET = 1024;  // expected entries per bucket
-constexpr u32 PB_TAB = 4096;     // table slots of the fold kernel
+constexpr u32 PB_TAB = 2048;     // table slots of the fold kernel
 constexpr u32 PB_CHUNK = 4096;   // entries per block of the hist / scatter kernels
 constexpr u32 PB_HIST = 8192;    // buckets a block counts in shared memory
+constexpr u32 PB_FOLD_UNROLL = 4;  // chunks (or table slots) a fold thread has in flight
 
 __global__ void k_pb_plan(const u32* ovf, const u32* novf, const u32* verts, const u64* off,
                           u32* nb, u64* ne, u32* nc) {
@@ -901,15 +961,35 @@ __global__ void __launch_bounds__(256) k_pb_hist(EvalArgs A, PbArgs P) {
     __syncthreads();
     double wc = 0.0;
     const u64 ebase = P.ebase[r] - P.e0 + (lo - o0);
-    for (u64 q = lo + threadIdx.x; q < hi; q += blockDim.x) {
-      u32 key = NONE32;
-      if (!entry_key<KIND>(A, v, A.col[q], fv, key)) key = NONE32;
-      P.ktmp[ebase + (q - lo)] = key;
-      if (key == NONE32) continue;
-      if (key == cur) wc += A.w[q];
-      const u32 b = pb_bucket(key, B);
-      if (local) atomicAdd(&s_hist[b], 1u);
-      else atomicAdd(&gcnt[b], 1u);
+    const u32 lane = threadIdx.x & 31;
+    // PB_FOLD_UNROLL entries per thread in flight (neighbours, then their
+    // keys); lanes counting into the same bucket add once
+    for (u64 w0 = lo + (threadIdx.x & ~31u); w0 < hi; w0 += 256 * PB_FOLD_UNROLL) {
+      u32 nb[PB_FOLD_UNROLL], key[PB_FOLD_UNROLL];
+#pragma unroll
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        const u64 q = w0 + j * 256 + lane;
+        nb[j] = q < hi ? A.col[q] : NONE32;
+      }
+#pragma unroll
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        key[j] = NONE32;
+        if (nb[j] != NONE32 && !entry_key<KIND>(A, v, nb[j], fv, key[j])) key[j] = NONE32;
+      }
+#pragma unroll
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        const u64 q = w0 + j * 256 + lane;
+        if (q < hi) P.ktmp[ebase + (q - lo)] = key[j];
+        const bool ok = key[j] != NONE32;
+        if (ok && key[j] == cur) wc += A.w[q];
+        const u32 b = ok ? pb_bucket(key[j], B) : 0u;
+        const u32 grp = __match_any_sync(0xffffffffu, ok ? (unsigned long long)b
+                                                         : ((1ull << 32) | lane));
+        if (ok && lane == (u32)(__ffs(grp) - 1)) {
+          if (local) atomicAdd(&s_hist[b], (u32)__popc(grp));
+          else atomicAdd(&gcnt[b], (u32)__popc(grp));
+        }
+      }
     }
     for (int o = 16; o; o >>= 1) wc += __shfl_xor_sync(0xffffffffu, wc, o);
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = wc;
@@ -928,6 +1008,7 @@ __global__ void __launch_bounds__(256) k_pb_hist(EvalArgs A, PbArgs P) {
 
 __global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
   __shared__ u32 s_row;
+  const u32 lane = threadIdx.x & 31;
   for (u32 c = P.c0 + blockIdx.x; c < P.c1; c += gridDim.x) {
     if (threadIdx.x == 0) s_row = pb_row_of(P.cbase, P.r0, P.r1, c);
     __syncthreads();
@@ -940,14 +1021,36 @@ __global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
     u32* cursor = P.bcnt + (P.bbase[r] - P.b0);
     const u32* start = P.boff + (P.bbase[r] - P.b0);
     const u64 ebase = P.ebase[r] - P.e0 + (lo - o0);
-    for (u64 q = lo + threadIdx.x; q < hi; q += blockDim.x) {
-      const u32 key = P.ktmp[ebase + (q - lo)];
-      if (key == NONE32) continue;
-      const u32 b = pb_bucket(key, B);
-      const u32 slot = start[b] + atomicAdd(&cursor[b], 1u);
-      P.ekey[slot] = key;
-      P.epos[slot] = (u32)(q - o0);
-      P.ew[slot] = A.w[q];
+    // PB_FOLD_UNROLL entries per thread in flight; lanes bound for the same
+    // bucket take their slots with one atomic (a heavy key fills one bucket)
+    for (u64 w0 = lo + (threadIdx.x & ~31u); w0 < hi; w0 += 256 * PB_FOLD_UNROLL) {
+      const u64 q0 = w0 + lane;
+      u32 key[PB_FOLD_UNROLL];
+      double wq[PB_FOLD_UNROLL];
+#pragma unroll
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        const u64 q = q0 + j * 256;
+        key[j] = q < hi ? P.ktmp[ebase + (q - lo)] : NONE32;
+        wq[j] = key[j] != NONE32 ? A.w[q] : 0.0;
+      }
+#pragma unroll
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        const u64 q = q0 + j * 256;
+        const bool ok = key[j] != NONE32;
+        const u32 b = ok ? pb_bucket(key[j], B) : 0u;
+        const u32 grp = __match_any_sync(0xffffffffu, ok ? (unsigned long long)b
+                                                         : ((1ull << 32) | lane));
+        const u32 leader = __ffs(grp) - 1;
+        u32 at = 0;
+        if (ok && lane == leader) at = start[b] + atomicAdd(&cursor[b], (u32)__popc(grp));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (ok) {
+          const u32 slot = at + __popc(grp & ((1u << lane) - 1u));
+          P.ekey[slot] = key[j];
+          P.epos[slot] = (u32)(q - o0);
+          P.ew[slot] = wq[j];
+        }
+      }
     }
     __syncthreads();
   }
@@ -959,8 +1062,11 @@ constexpr size_t PB_FOLD_SMEM = (size_t)PB_TAB * (8 + 4 + 4);
 // that tests reach the overflow path).
 std::atomic<u32> g_pb_slots{PB_TAB};
 
+// Hub-row deferral bound forced by hl_dbg_set_hub_defer (0: the handle's).
+std::atomic<u32> g_dbg_hub_defer{0};
+
 template <int KIND>
-__global__ void __launch_bounds__(256) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuckets,
+__global__ void __launch_bounds__(256, 5) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuckets,
                                                  u32 tab_limit) {
   extern __shared__ __align__(16) unsigned char pb_smem[];
   unsigned long long* s_tv = reinterpret_cast<unsigned long long*>(pb_smem);
@@ -969,6 +1075,8 @@ __global__ void __launch_bounds__(256) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuck
   __shared__ double r_g[8];
   __shared__ u32 r_p[8], r_k[8];
   __shared__ u32 s_row, s_ovf;
+  __shared__ unsigned long long s_wb[8][32];  // a chunk's weights, per warp
+  __shared__ u32 s_pb[8][32];                 // and positions
   const u32 tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   unsigned long long ncand = 0;
   for (u32 bl = blockIdx.x; bl < nbuckets; bl += gridDim.x) {
@@ -989,26 +1097,59 @@ __global__ void __launch_bounds__(256) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuck
     __syncthreads();
     const u32 r = s_row;
     const u32 mask = cap - 1;
-    for (u32 e = e_lo + tid; e < e_hi; e += 256) {
-      const u32 key = P.ekey[e];
-      u32 slot = hash32(key) & mask;
-      u32 probes = 0;
-      bool ok = false;
-      while (probes++ < cap) {
-        const u32 prev = atomicCAS(&s_tk[slot], NONE32, key);
-        if (prev == NONE32 || prev == key) {
-          ok = true;
-          break;
+    // Each warp takes PB_FOLD_UNROLL chunks of 32 entries at a time, their
+    // loads issued together.  Lanes of a chunk that share a key are combined
+    // first (match_any), so a heavy key (a large community holding much of
+    // the row) costs one shared-memory atomic per chunk, not one per entry.
+    for (u32 base = e_lo + wib * 32; base < e_hi; base += 256 * PB_FOLD_UNROLL) {
+      u32 ek[PB_FOLD_UNROLL], ep[PB_FOLD_UNROLL];
+      unsigned long long ew[PB_FOLD_UNROLL];
+#pragma unroll
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        const u32 e = base + j * 256 + lane;
+        const bool ok = e < e_hi;
+        ek[j] = ok ? P.ekey[e] : NONE32;
+        ep[j] = ok ? P.epos[e] : NONE32;
+        // integral weights: every partial sum is an exact integer
+        ew[j] = ok ? (unsigned long long)(long long)P.ew[e] : 0ull;
+      }
+#pragma unroll
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        if (base + j * 256 >= e_hi) break;  // warp-uniform
+        const bool ok = ek[j] != NONE32;
+        const u32 grp = __match_any_sync(0xffffffffu, ok ? (unsigned long long)ek[j]
+                                                         : ((1ull << 32) | lane));
+        s_wb[wib][lane] = ew[j];
+        s_pb[wib][lane] = ep[j];
+        __syncwarp();
+        if (ok && lane == (u32)(__ffs(grp) - 1)) {
+          unsigned long long sum = 0;
+          u32 pmin = NONE32;
+          for (u32 m = grp; m; m &= m - 1) {
+            const u32 l = __ffs(m) - 1;
+            sum += s_wb[wib][l];
+            pmin = min(pmin, s_pb[wib][l]);
+          }
+          u32 slot = hash32(ek[j]) & mask;
+          u32 probes = 0;
+          bool ins = false;
+          while (probes++ < cap) {
+            const u32 prev = atomicCAS(&s_tk[slot], NONE32, ek[j]);
+            if (prev == NONE32 || prev == ek[j]) {
+              ins = true;
+              break;
+            }
+            slot = (slot + 1) & mask;
+          }
+          if (ins) {
+            atomicAdd(&s_tv[slot], sum);
+            atomicMin(&s_tp[slot], pmin);
+          } else {
+            s_ovf = 1;
+          }
         }
-        slot = (slot + 1) & mask;
+        __syncwarp();
       }
-      if (!ok) {
-        s_ovf = 1;
-        continue;
-      }
-      // integral weights: the running sum is an exact integer
-      atomicAdd(&s_tv[slot], (unsigned long long)(long long)P.ew[e]);
-      atomicMin(&s_tp[slot], P.epos[e]);
     }
     __syncthreads();
     double g = -1.0;
@@ -1020,18 +1161,32 @@ __global__ void __launch_bounds__(256) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuck
       const double kv = A.kdeg[v];
       const double wcur = P.wcur[r];
       const double dcur = A.d[cur];
-      for (u32 x = tid; x < cap; x += 256) {
-        const u32 key = s_tk[x];
-        if (key == NONE32 || key == cur) continue;
-        if (KIND == EVAL_REFINE && A.blocked[key]) continue;
-        const double val = (double)(long long)s_tv[x];
-        const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, A.d[key]);
-        ++ncand;
-        const u32 pp = s_tp[x];
-        if (p == NONE32 || gn > g || (gn == g && pp < p)) {
-          g = gn;
-          p = pp;
-          kk = key;
+      // the community degrees of PB_FOLD_UNROLL slots are gathered together
+      for (u32 x0 = tid; x0 < cap; x0 += 256 * PB_FOLD_UNROLL) {
+        u32 key[PB_FOLD_UNROLL];
+        double dk[PB_FOLD_UNROLL];
+#pragma unroll
+        for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+          const u32 x = x0 + j * 256;
+          key[j] = x < cap ? s_tk[x] : NONE32;
+          if (key[j] == cur) key[j] = NONE32;
+          if (KIND == EVAL_REFINE && key[j] != NONE32 && A.blocked[key[j]]) key[j] = NONE32;
+        }
+#pragma unroll
+        for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) dk[j] = key[j] != NONE32 ? A.d[key[j]] : 0.0;
+#pragma unroll
+        for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+          if (key[j] == NONE32) continue;
+          const u32 x = x0 + j * 256;
+          const double val = (double)(long long)s_tv[x];
+          const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, dk[j]);
+          ++ncand;
+          const u32 pp = s_tp[x];
+          if (p == NONE32 || gn > g || (gn == g && pp < p)) {
+            g = gn;
+            p = pp;
+            kk = key[j];
+          }
         }
       }
     }
@@ -1119,23 +1274,27 @@ __global__ void k_pb_final(EvalArgs A, PbArgs P, u32* fail_list, u32* fail_count
 // ---------------------------------------------------------------------------
 // Host side: bin the list by degree and launch the three kernels.
 // ---------------------------------------------------------------------------
+// Bins: 0-2 sub-warp (deg <= 8, 16, 32), 3 warp table (<= mid_max), 4 wide
+// (<= WIDE_SPLIT), 6 wide (<= wide_max) with full-size tables, 5 block.
+constexpr int NBINS = 7;
+
 __global__ void k_bin(const u32* verts, u32 nv, const u64* off, u32* bin, u32* idx,
                       u32* counts, unsigned long long* maxdeg, u32 mid_max, u32 wide_max) {
-  __shared__ u32 sc[6];
-  if (threadIdx.x < 6) sc[threadIdx.x] = 0;
+  __shared__ u32 sc[NBINS];
+  if (threadIdx.x < NBINS) sc[threadIdx.x] = 0;
   __syncthreads();
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < nv; i += (u64)gridDim.x * blockDim.x) {
     u32 v = verts[i];
     u64 deg = off[v + 1] - off[v];
     u32 b = deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= mid_max ? 3
-          : deg <= wide_max ? 4 : 5;
+          : deg <= wide_max ? (deg <= WIDE_SPLIT ? 4 : 6) : 5;
     bin[i] = b;
     idx[i] = (u32)i;
     atomicAdd(&sc[b], 1u);
     if (b == 5) atomicMax(maxdeg, (unsigned long long)deg);
   }
   __syncthreads();
-  if (threadIdx.x < 6 && sc[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sc[threadIdx.x]);
+  if (threadIdx.x < NBINS && sc[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sc[threadIdx.x]);
 }
 
 // Sort keys that order vertices by degree, largest first.
@@ -1158,7 +1317,8 @@ static size_t big_smem() {
 
 static std::atomic<bool> g_big_attr_set[64];
 
-constexpr u32 WIDE_MAX_BLOCKS = 148u * 3u;
+constexpr u32 WIDE_MAX_BLOCKS = 148u * 3u;        // resident blocks of the full-size wide kernel
+constexpr u32 WIDE_SPLIT_MAX_BLOCKS = 148u * 5u;  // and of the half-size one
 constexpr u32 BIG_MAX_BLOCKS = 148u * 3u;
 constexpr u32 OVF_BLOCKS = 32;  // least blocks (global regions) for rows deferred by pass 1
 constexpr u64 OVF_TABLE_BYTES = 4ull << 30;  // table bytes pass 2 may spread over its blocks
@@ -1287,8 +1447,8 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   S.used.ensure(E.mem, nv);
   S.rank.ensure(E.mem, nv);
   S.cnt.ensure(E.mem, 16);
-  u32* cnt = S.cnt.p + 2;  // six bin counters (cnt[2..7])
-  HL_CUDA(cudaMemsetAsync(cnt, 0, 6 * sizeof(u32), st));
+  u32* cnt = S.cnt.p + 2;  // NBINS bin counters (cnt[2..8])
+  HL_CUDA(cudaMemsetAsync(cnt, 0, NBINS * sizeof(u32), st));
   // [0] deferred rows, [2..3] largest degree of the block bin, [4..5] work
   // counters of the block kernel's two passes
   S.ovf_cnt.ensure(E.mem, 6);
@@ -1308,14 +1468,15 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   cub_run(E, [&](void* t, size_t& b) {
     return cub::DeviceRadixSort::SortPairs(t, b, ki, ko, vi, vo, (int64_t)nv, 0, 3, st);
   });
-  u32 c[6];
-  HL_CUDA(cudaMemcpyAsync(E.hs.p, cnt, 6 * sizeof(u32), cudaMemcpyDeviceToHost, st));
+  u32 c[NBINS];
+  static_assert(NBINS * sizeof(u32) <= 4 * sizeof(u64), "bin counts fit before the degree");
+  HL_CUDA(cudaMemcpyAsync(E.hs.p, cnt, NBINS * sizeof(u32), cudaMemcpyDeviceToHost, st));
   HL_CUDA(cudaMemcpyAsync(E.hs.p + 4, maxdeg, sizeof(u64), cudaMemcpyDeviceToHost, st));
   E.sync();
   std::memcpy(c, E.hs.p, sizeof(c));
   const u64 big_maxdeg = E.hs.p[4];
-  u32 start[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < 6; ++b) start[b + 1] = start[b] + c[b];
+  u32 start[NBINS + 1] = {0};
+  for (int b = 0; b < NBINS; ++b) start[b + 1] = start[b] + c[b];
 
   int dev = E.device;
   if (dev >= 0 && dev < 64 && !g_big_attr_set[dev]) {
@@ -1323,11 +1484,18 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
                                  (int)big_smem()));
     HL_CUDA(cudaFuncSetAttribute(k_eval_big<EVAL_REFINE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem()));
-    HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(WideSmem)));
-    HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_REFINE>,
+    HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_MOVE, 2 * WIDE_SPLIT>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(WideSmem)));
+                                 (int)sizeof(WideSmem<2 * WIDE_SPLIT>)));
+    HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_REFINE, 2 * WIDE_SPLIT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(WideSmem<2 * WIDE_SPLIT>)));
+    HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_MOVE, 2 * WIDE_MAX>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(WideSmem<2 * WIDE_MAX>)));
+    HL_CUDA(cudaFuncSetAttribute(k_eval_wide<EVAL_REFINE, 2 * WIDE_MAX>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(WideSmem<2 * WIDE_MAX>)));
     HL_CUDA(cudaFuncSetAttribute(k_pb_fold<EVAL_MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)PB_FOLD_SMEM));
     HL_CUDA(cudaFuncSetAttribute(k_pb_fold<EVAL_REFINE>,
@@ -1361,6 +1529,11 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   A.ovf_count = nullptr;
   A.nidx_dev = nullptr;
   A.work = nullptr;
+  {
+    const u32 dbg = g_dbg_hub_defer.load();
+    const u64 tuned = E.tune.hub_defer ? E.tune.hub_defer : BIG_DIRECT_DEFER;
+    A.defer_deg = E.integral ? (dbg ? dbg : tuned) : 0;
+  }
 
   cudaEvent_t ev = E.kt_begin();
   cudaEvent_t e_s = E.kt_begin();
@@ -1386,7 +1559,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
   E.kt_end(KT_EVAL_SMALL, e_s);
   E.kagg[KT_EVAL_SMALL].items += (u64)c[0] + c[1] + c[2];
   E.kagg[KT_EVAL_MID].items += c[3];
-  E.kagg[KT_EVAL_BIG].items += c[4];
+  E.kagg[KT_EVAL_BIG].items += (u64)c[4] + c[6];
   E.kagg[KT_EVAL_HUGE].items += c[5];
   cudaEvent_t e_m = E.kt_begin();
   if (c[3]) {
@@ -1409,11 +1582,26 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
     a.idx = vo + start[4];
     a.nidx = c[4];
     u32 blocks = grid_for((u64)c[4] * 32, WIDE_WARPS * 32);
-    if (blocks > WIDE_MAX_BLOCKS) blocks = WIDE_MAX_BLOCKS;
+    if (blocks > WIDE_SPLIT_MAX_BLOCKS) blocks = WIDE_SPLIT_MAX_BLOCKS;
+    constexpr u32 T = 2 * WIDE_SPLIT;
     if (kind == EVAL_MOVE)
-      ++E.nlaunch, k_eval_wide<EVAL_MOVE><<<blocks, WIDE_WARPS * 32, sizeof(WideSmem), st>>>(a);
+      ++E.nlaunch, k_eval_wide<EVAL_MOVE, T><<<blocks, WIDE_WARPS * 32, sizeof(WideSmem<T>), st>>>(a);
     else
-      ++E.nlaunch, k_eval_wide<EVAL_REFINE><<<blocks, WIDE_WARPS * 32, sizeof(WideSmem), st>>>(a);
+      ++E.nlaunch, k_eval_wide<EVAL_REFINE, T><<<blocks, WIDE_WARPS * 32, sizeof(WideSmem<T>), st>>>(a);
+    HL_LAUNCH_CHECK();
+  }
+  if (c[6]) {
+    EvalArgs a = A;
+    a.counters = counters ? counters + 4 : nullptr;
+    a.idx = vo + start[6];
+    a.nidx = c[6];
+    u32 blocks = grid_for((u64)c[6] * 32, WIDE_WARPS * 32);
+    if (blocks > WIDE_MAX_BLOCKS) blocks = WIDE_MAX_BLOCKS;
+    constexpr u32 T = 2 * WIDE_MAX;
+    if (kind == EVAL_MOVE)
+      ++E.nlaunch, k_eval_wide<EVAL_MOVE, T><<<blocks, WIDE_WARPS * 32, sizeof(WideSmem<T>), st>>>(a);
+    else
+      ++E.nlaunch, k_eval_wide<EVAL_REFINE, T><<<blocks, WIDE_WARPS * 32, sizeof(WideSmem<T>), st>>>(a);
     HL_LAUNCH_CHECK();
   }
   E.kt_end(KT_EVAL_BIG, e_b);
@@ -1510,9 +1698,12 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
 // Autotuner of the degree bins: the evaluation of one frontier is run with
 // each candidate pair of warp-bin thresholds (every pair gives the same
 // results; only the split between the sub-warp, warp and block kernels
-// changes) and the fastest pair is kept for the handle.  Runs once, on the
-// first movement round whose frontier has at least AUTOTUNE_MIN vertices.
+// changes) and the fastest pair is kept for the handle.  With integral
+// weights the bound above which hub rows skip the block kernel's shared
+// tables for the partitioned pass is then tuned the same way.  Runs once, on
+// the first movement round whose frontier has at least AUTOTUNE_MIN vertices.
 constexpr u32 AUTOTUNE_MIN = 20000;
+constexpr u32 HUB_DEFER_CAND[] = {2048, 8192, 32768};
 
 void autotune_bins(Engine& E, const u32* verts, u32 nv, const Level& L, const u32* s,
                    const double* d, u32* out_to, double* out_gain) {
@@ -1542,11 +1733,32 @@ void autotune_bins(Engine& E, const u32* verts, u32 nv, const Level& L, const u3
       }
     }
   }
+  E.tune.mid_max = bm;
+  E.tune.wide_max = bw;
+  u32 bd = 0;
+  if (E.integral) {
+    float bdt = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      for (u32 c : HUB_DEFER_CAND) {
+        E.tune.hub_defer = c;
+        HL_CUDA(cudaEventRecord(a, E.stream));
+        run_eval(E, EVAL_MOVE, verts, nv, L, s, d, nullptr, true, out_to, out_gain, nullptr);
+        HL_CUDA(cudaEventRecord(b, E.stream));
+        HL_CUDA(cudaEventSynchronize(b));
+        float ms = 0.f;
+        HL_CUDA(cudaEventElapsedTime(&ms, a, b));
+        if (rep == 1 && (bdt == 0.f || ms < bdt)) {
+          bdt = ms;
+          bd = c;
+        }
+      }
+    }
+    best = bdt;
+  }
   E.ktiming = kt;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  E.tune.mid_max = bm;
-  E.tune.wide_max = bw;
+  E.tune.hub_defer = bd;
   E.tune.done = true;
   E.tune.frontier = nv;
   E.tune.best_ms = best;

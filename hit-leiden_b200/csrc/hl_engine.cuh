@@ -103,7 +103,8 @@ struct Scratch {
       pb_epos, pb_bcnt, pb_boff, pb_bp, pb_bk;
   DBuf<u64> pb_ne, pb_ebase;
   DBuf<double> pb_wcur, pb_ew, pb_bg;
-  DBuf<u32> mark_long, mark_long_cnt;
+  DBuf<unsigned long long> mark_long;  // (rank << 32 | segment) of long moved rows
+  DBuf<u32> mark_long_cnt;
   // batch statistics accumulated on the device and read once at the end of
   // the call: [0..7] traversed / candidates of the four evaluation bins,
   // [8] accepted moves, [9] refinement merges, [10] |B^1|
@@ -178,6 +179,7 @@ struct Engine {
   // degree-bin thresholds picked by the autotuner (0 = compile-time default)
   struct Tune {
     u32 mid_max = 0, wide_max = 0;
+    u32 hub_defer = 0;  // integral weights: hub rows above this many entries skip pass 1
     bool done = false;
     u32 frontier = 0;
     float best_ms = 0.f;
@@ -279,6 +281,7 @@ u64 merge_singletons_det(Engine& E, Level& L, const u32* rv, u32 nr, u32* sizes,
 extern std::atomic<int> g_exact_tfilter;
 // Test switch: table slots of the partitioned hub pass (eval.cu).
 extern std::atomic<u32> g_pb_slots;
+extern std::atomic<u32> g_dbg_hub_defer;
 
 // aggregate.cu
 u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n,

@@ -417,74 +417,85 @@ __global__ void k_apply_ordered(const u32* seg_last, const u32* head_last, const
 }
 
 // Next frontier and K marks (throughput.rs:189-199), on f after all moves.
-// Rows longer than MARK_LONG entries (moved hubs) are left to
-// k_mark_next_long, a block per row, so that no warp walks a row of millions
-// of entries alone while the others idle.
+// Rows longer than MARK_LONG entries (moved hubs) are cut into segments of
+// MARK_LONG entries, listed as (rank, segment) pairs for k_mark_next_long, so
+// that no warp walks a row of millions of entries alone while the others idle.
 constexpr u64 MARK_LONG = 4096;
+
+// One row's marks over entries [p_lo, p_hi): four entries per lane in
+// flight, their neighbours, then their labels.  Returns whether a neighbour
+// shares v's sub-community.
+__device__ __forceinline__ bool mark_entries(u64 p_lo, u64 p_hi, u32 lane, u32 to, u32 sv,
+                                             const u32* col, const u32* f, const u32* s, u8* next,
+                                             u8* affected) {
+  bool any_same = false;
+  for (u64 p0 = p_lo + lane; p0 < p_hi; p0 += 128) {
+    u32 nb[4], fn[4], sn[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) nb[j] = p0 + 32 * j < p_hi ? col[p0 + 32 * j] : NONE32;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (nb[j] != NONE32) {
+        fn[j] = f[nb[j]];
+        sn[j] = s[nb[j]];
+      }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (nb[j] != NONE32) {
+        if (fn[j] != to) next[nb[j]] = 1;
+        if (sn[j] == sv) {
+          affected[nb[j]] = 1;
+          any_same = true;
+        }
+      }
+  }
+  return any_same;
+}
 
 __global__ void k_mark_next(u32 M, const u8* status, const u32* sel_node, const u32* sel_to,
                             const u64* off, const u32* col, const u32* f, const u32* s, u8* next,
-                            u8* affected, u32* long_list, u32* long_count) {
+                            u8* affected, unsigned long long* long_list, u32* long_count) {
   const u32 lane = threadIdx.x & 31;
   const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
   const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   for (u64 r = warp; r < M; r += nwarps) {
     if (status[r] != ST_ACCEPTED) continue;
     u32 v = sel_node[r], to = sel_to[r];
-    if (off[v + 1] - off[v] > MARK_LONG) {
-      if (lane == 0) long_list[atomicAdd(long_count, 1u)] = (u32)r;
+    const u64 deg = off[v + 1] - off[v];
+    if (deg > MARK_LONG) {
+      const u32 nseg = (u32)((deg + MARK_LONG - 1) / MARK_LONG);
+      u32 at = 0;
+      if (lane == 0) at = atomicAdd(long_count, nseg);
+      at = __shfl_sync(0xffffffffu, at, 0);
+      for (u32 x = lane; x < nseg; x += 32)
+        long_list[at + x] = ((unsigned long long)r << 32) | x;
       continue;
     }
-    u32 sv = s[v];
-    bool any_same = false;
-    const u64 o1 = off[v + 1];
-    // four entries per lane in flight: their neighbours, then their labels
-    for (u64 p0 = off[v] + lane; p0 < o1; p0 += 128) {
-      u32 nb[4], fn[4], sn[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) nb[j] = p0 + 32 * j < o1 ? col[p0 + 32 * j] : NONE32;
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (nb[j] != NONE32) {
-          fn[j] = f[nb[j]];
-          sn[j] = s[nb[j]];
-        }
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (nb[j] != NONE32) {
-          if (fn[j] != to) next[nb[j]] = 1;
-          if (sn[j] == sv) {
-            affected[nb[j]] = 1;
-            any_same = true;
-          }
-        }
-    }
+    const bool any_same = mark_entries(off[v], off[v + 1], lane, to, s[v], col, f, s, next,
+                                       affected);
     if (__any_sync(0xffffffffu, any_same) && lane == 0) affected[v] = 1;
   }
 }
 
-// The long rows k_mark_next listed: a block per moved hub, the same marks.
-__global__ void __launch_bounds__(256) k_mark_next_long(const u32* long_list, const u32* long_count,
-                                                        const u32* sel_node, const u32* sel_to,
-                                                        const u64* off, const u32* col,
-                                                        const u32* f, const u32* s, u8* next,
-                                                        u8* affected) {
+// The segments of long rows k_mark_next listed: a warp per segment, the same
+// marks (every segment that meets v's sub-community marks v itself).
+__global__ void k_mark_next_long(const unsigned long long* long_list, const u32* long_count,
+                                 const u32* sel_node, const u32* sel_to, const u64* off,
+                                 const u32* col, const u32* f, const u32* s, u8* next,
+                                 u8* affected) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
   const u32 cnt = *long_count;
-  for (u32 t = blockIdx.x; t < cnt; t += gridDim.x) {
-    const u32 r = long_list[t];
+  for (u64 t = warp; t < cnt; t += nwarps) {
+    const unsigned long long item = long_list[t];
+    const u32 r = (u32)(item >> 32), seg = (u32)item;
     const u32 v = sel_node[r], to = sel_to[r];
-    const u32 sv = s[v];
-    bool any_same = false;
-    const u64 o1 = off[v + 1];
-    for (u64 p = off[v] + threadIdx.x; p < o1; p += blockDim.x) {
-      const u32 nb = col[p];
-      if (f[nb] != to) next[nb] = 1;
-      if (s[nb] == sv) {
-        affected[nb] = 1;
-        any_same = true;
-      }
-    }
-    if (__syncthreads_or(any_same) && threadIdx.x == 0) affected[v] = 1;
+    const u64 o0 = off[v], o1 = off[v + 1];
+    const u64 lo = o0 + (u64)seg * MARK_LONG;
+    const u64 hi = lo + MARK_LONG < o1 ? lo + MARK_LONG : o1;
+    const bool any_same = mark_entries(lo, hi, lane, to, s[v], col, f, s, next, affected);
+    if (__any_sync(0xffffffffu, any_same) && lane == 0) affected[v] = 1;
   }
 }
 
@@ -690,14 +701,15 @@ MoveOut inc_movement(Engine& E, Level& L, const DevEdges& delta, bool all_active
     // round): such a round marks nothing, so the next frontier is empty and
     // the loop ends on it with the same iteration count.
     HL_CUDA(cudaMemsetAsync(S.next.p, 0, n, st));
-    S.mark_long.ensure(E.mem, M);
+    // segments of the long rows: at most M + nnz / MARK_LONG
+    S.mark_long.ensure(E.mem, (size_t)M + L.g.nnz / MARK_LONG + 1);
     S.mark_long_cnt.ensure(E.mem, 1);
     HL_CUDA(cudaMemsetAsync(S.mark_long_cnt.p, 0, sizeof(u32), st));
     ++E.nlaunch, k_mark_next<<<grid_for((u64)M * 32), 256, 0, st>>>(M, S.status.p, S.sel_node.p, S.sel_to.p,
                                                         L.g.off.p, L.g.col.p, L.f.p, L.s_cur.p,
                                                         S.next.p, S.affected.p, S.mark_long.p,
                                                         S.mark_long_cnt.p);
-    ++E.nlaunch, k_mark_next_long<<<148 * 2, 256, 0, st>>>(S.mark_long.p, S.mark_long_cnt.p,
+    ++E.nlaunch, k_mark_next_long<<<148 * 8, 256, 0, st>>>(S.mark_long.p, S.mark_long_cnt.p,
                                                            S.sel_node.p,
                                                            S.sel_to.p, L.g.off.p, L.g.col.p,
                                                            L.f.p, L.s_cur.p, S.next.p,

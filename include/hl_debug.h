@@ -91,11 +91,19 @@ HL_API hl_status hl_dbg_set_exact_tfilter(int32_t on);
  * (dual_mode_test!, hit_leiden.rs:1823-1841) run on both GPU paths. */
 HL_API hl_status hl_dbg_set_mode(uint32_t mode);
 
-/* Table slots (64..4096, 0 = 4096) of the partitioned pass that evaluates
- * hub rows with more than 2048 distinct neighbour keys under integral
- * weights.  A small table makes buckets overflow, so tests reach the
- * global-table pass those rows fall back to.  Results do not depend on it. */
+/* Table slots (64..2048, 0 = 2048) of the partitioned pass that evaluates
+ * long hub rows under integral weights (rows above 8192 entries, or with
+ * more than 2048 distinct neighbour keys).  A small table makes buckets
+ * overflow, so tests reach the global-table pass those rows fall back to.
+ * Results do not depend on it. */
 HL_API hl_status hl_dbg_set_bucket_slots(uint32_t slots);
+
+/* Integral weights: hub rows (above the wide bin) longer than `entries` go
+ * straight to the partitioned pass instead of the block kernel's shared
+ * tables (0 = each handle's bound: 8192, or the autotuner's pick).  Every
+ * bound gives the same results; tests use it to send all hub rows through
+ * either path. */
+HL_API hl_status hl_dbg_set_hub_defer(uint32_t entries);
 
 /* Warp-bin thresholds of the stage entry points (mid_max in [33, 128],
  * wide_max in [mid_max, 512]; 0 = default), the pairs the autotuner picks

@@ -128,7 +128,7 @@ extern "C" {
     pub fn hl_set_resolution(g: *mut hl_graph, gamma: f64) -> hl_status;
     pub fn hl_set_mode(g: *mut hl_graph, mode: u32) -> hl_status;
     pub fn hl_autotune_info(g: *const hl_graph, mid_max: *mut u32, wide_max: *mut u32,
-                            frontier: *mut u32) -> hl_status;
+                            hub_defer: *mut u32, frontier: *mut u32) -> hl_status;
     pub fn hl_set_level_callback(g: *mut hl_graph, fn_: hl_level_fn, user: *mut c_void)
                                  -> hl_status;
     pub fn hl_num_nodes(g: *const hl_graph, n: *mut u32) -> hl_status;

@@ -91,6 +91,17 @@ def bucket_slots(slots):
 
 
 @contextlib.contextmanager
+def hub_defer(entries):
+    """Send integral hub rows longer than `entries` straight to the
+    partitioned pass (0 = default) for a block."""
+    L.check(L.lib.hl_dbg_set_hub_defer(int(entries)))
+    try:
+        yield
+    finally:
+        L.check(L.lib.hl_dbg_set_hub_defer(0))
+
+
+@contextlib.contextmanager
 def bins(mid_max, wide_max):
     """Warp-bin thresholds of the stage entry points for a block."""
     L.check(L.lib.hl_dbg_set_bins(int(mid_max), int(wide_max)))

@@ -348,6 +348,41 @@ def test_canonicalize_gpu():
     assert np.array_equal(hl.canonicalize_community_ids(x), O.canonicalize(x))
 
 
+# ---- integral hub rows through either hub path: the block kernel's shared
+# tables (no direct deferral) or the partitioned pass (every hub row) -------
+@pytest.mark.parametrize("defer", [1, 0xFFFFFFFF, 0])
+def test_move_eval_hub_paths_bit_exact(defer):
+    rng = np.random.default_rng(defer & 0xFFFF)
+    n = 60000
+    src, dst, w = gh.random_graph(rng, n, 40000, True)
+    hubs = [(0, 700), (1, 3000), (2, 9000), (3, 40000)]
+    hs, hd = [], []
+    for h, deg in hubs:
+        nb = rng.choice(np.arange(10, n), deg, replace=False).astype(np.uint32)
+        hs.append(np.full(deg, h, np.uint32))
+        hd.append(nb)
+    hw = rng.integers(1, 4, sum(d for _, d in hubs)).astype(float)
+    g = O.Graph.from_edges(n, np.concatenate([src] + hs), np.concatenate([dst] + hd),
+                           np.concatenate([w, hw])).apply_delta([], [], [], keep_self_loops=True)
+    k = g.degrees()
+    tw = O.tree_sum(k)
+    for ncomm in [7, 3000, 50000]:
+        f = gh.random_partition(rng, n, ncomm)
+        # a heavy key: 30 % of the largest hub's neighbours in one community
+        heavy = hd[-1][: len(hd[-1]) * 3 // 10]
+        f[heavy] = f[hd[-1][0]]
+        d = np.zeros(2 * n + 2)
+        np.add.at(d, f, k)
+        verts = np.concatenate([np.arange(4, dtype=np.uint32),
+                                np.arange(4, n, 11, dtype=np.uint32)])
+        to_o, g_o = O.move_eval(g, f, d, k, tw, 1.0, verts)
+        with gh.hub_defer(defer):
+            to_g, g_g = gh.move_eval(g, f, d, k, tw, 1.0, verts)
+        assert gh.same_bits(g_o, g_g)
+        pos = g_o > 0
+        assert np.array_equal(to_o[pos], to_g[pos])
+
+
 # ---- very high degree vertices (block kernel, shared and global tables) -----
 @pytest.mark.parametrize("integral", [True, False])
 @pytest.mark.parametrize("hub_deg", [300, 3000, 6000, 20000])
@@ -447,9 +482,11 @@ def test_autotuned_handle_stays_bit_exact():
     os_ = E2E.oracle_state(n, s, d, w, 10)
     gs.apply_batch([], [], [])  # empty batch: every vertex active at level 0
     os_.hit_leiden([], [], [])
-    mid, wide, fr = C.c_uint32(), C.c_uint32(), C.c_uint32()
-    L.check(L.lib.hl_autotune_info(gs._h, C.byref(mid), C.byref(wide), C.byref(fr)))
+    mid, wide, hd, fr = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+    L.check(L.lib.hl_autotune_info(gs._h, C.byref(mid), C.byref(wide), C.byref(hd),
+                                   C.byref(fr)))
     assert fr.value >= 20000 and 33 <= mid.value <= 128 and mid.value <= wide.value <= 512
+    assert hd.value in (2048, 8192, 32768)
     E2E.compare(gs, os_)
     store = W.EdgeStore(n, s, d, w)
     u, v, ww = W.mixed_batch(store, 500, 0.9, 8, weights=(0.5, 2.0), preferential=True)
