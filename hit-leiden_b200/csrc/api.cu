@@ -674,7 +674,7 @@ static const char* kernel_names[KT_COUNT] = {
     "apply_and_mark",
     "refine_cc",   "t_filter",    "row_sums",         "delta_resolve",  "stage_apply",
     "stage_move",  "stage_refine", "stage_aggregate", "host_syncs",
-    "csr_copy_untouched", "move_small_rounds"};
+    "csr_copy_untouched", "move_small_rounds", "eval_huge_partitioned"};
 
 hl_status hl_kernel_stats(const hl_graph* g, hl_kernel_stat* out, uint32_t cap, uint32_t* count) {
   HL_TRY(require(g && count, "NULL argument"); Engine& E = *const_cast<EngineBox*>(box(g))->E;

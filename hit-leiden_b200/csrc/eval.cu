@@ -233,11 +233,22 @@ __global__ void __launch_bounds__(MID_WARPS * 32, 4) k_eval_mid(EvalArgs A) {
   u32* tp = s_pos[wib];
   double* tv = s_val[wib];
   double* sw = s_w[wib];
+  // the next vertex's list entry, id and row bounds, one step at a time
+  u32 i_nx = 0, v_nx = 0;
+  u64 o0_nx = 0, o1_nx = 0;
+  if (warp < A.nidx) {
+    i_nx = A.idx[warp];
+    v_nx = A.verts[i_nx];
+    o0_nx = A.off[v_nx];
+    o1_nx = A.off[v_nx + 1];
+  }
   for (u64 t = warp; t < A.nidx; t += nwarps) {
-    const u32 i = A.idx[t];
-    const u32 v = A.verts[i];
-    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u32 i = i_nx;
+    const u32 v = v_nx;
+    const u64 o0 = o0_nx, o1 = o1_nx;
     const u64 deg = o1 - o0;
+    const bool has_nx = t + nwarps < A.nidx;
+    if (has_nx) i_nx = A.idx[t + nwarps];
     const u32 fv = A.f[v];
     const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
     const double kv = A.kdeg[v];
@@ -264,6 +275,7 @@ __global__ void __launch_bounds__(MID_WARPS * 32, 4) k_eval_mid(EvalArgs A) {
       key[j] = NONE32;
       if (nb[j] != NONE32 && !entry_key<KIND>(A, v, nb[j], fv, key[j])) key[j] = NONE32;
     }
+    if (has_nx) v_nx = A.verts[i_nx];
     __syncwarp();
 #pragma unroll
     for (u32 j = 0; j < MID_CHUNKS; ++j) {
@@ -296,6 +308,10 @@ __global__ void __launch_bounds__(MID_WARPS * 32, 4) k_eval_mid(EvalArgs A) {
     u32 fm = __ballot_sync(0xffffffffu, found);
     wcur = __shfl_sync(0xffffffffu, wcur, fm ? __ffs(fm) - 1 : 0);
     if (!fm) wcur = 0.0;
+    if (has_nx) {
+      o0_nx = A.off[v_nx];
+      o1_nx = A.off[v_nx + 1];
+    }
     double g = -1.0;
     u32 p = NONE32, kk = cur;
     if (A.tw != 0.0) {
@@ -384,11 +400,23 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
   double* sw = W.sw[wib];
   for (u32 x = lane; x < TAB; x += 32) tk[x] = NONE32;
   __syncwarp();
+  // The next vertex's list entry, id and row bounds are loaded one step at a
+  // time while this vertex is folded, so that its row loads can start at once.
+  u32 i_nx = 0, v_nx = 0;
+  u64 o0_nx = 0, o1_nx = 0;
+  if (warp < A.nidx) {
+    i_nx = A.idx[warp];
+    v_nx = A.verts[i_nx];
+    o0_nx = A.off[v_nx];
+    o1_nx = A.off[v_nx + 1];
+  }
   for (u64 t = warp; t < A.nidx; t += nwarps) {
-    const u32 i = A.idx[t];
-    const u32 v = A.verts[i];
-    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u32 i = i_nx;
+    const u32 v = v_nx;
+    const u64 o0 = o0_nx, o1 = o1_nx;
     const u64 deg = o1 - o0;
+    const bool has_nx = t + nwarps < A.nidx;
+    if (has_nx) i_nx = A.idx[t + nwarps];
     const u32 fv = A.f[v];
     const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
     const double kv = A.kdeg[v];
@@ -439,6 +467,7 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
         __syncwarp();
       }
     }
+    if (has_nx) v_nx = A.verts[i_nx];
     const u32 used = W.cnt[wib];
     // w(v, cur), then the argmax over the used slots, resetting them.
     double wcur = 0.0;
@@ -454,6 +483,10 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
     wcur = __shfl_sync(0xffffffffu, wcur, fm ? __ffs(fm) - 1 : 0);
     if (!fm) wcur = 0.0;
     __syncwarp();
+    if (has_nx) {
+      o0_nx = A.off[v_nx];
+      o1_nx = A.off[v_nx + 1];
+    }
     double g = -1.0;
     u32 p = NONE32, kk = cur;
     for (u32 x0 = lane; x0 < used; x0 += 32 * WIDE_SCAN_UNROLL) {
@@ -522,6 +555,7 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
 // regions, moving a row's table there when it passes the same bound.
 // ---------------------------------------------------------------------------
 constexpr u32 BIG_TAB = 4096;
+constexpr u32 BIG_SCAN_UNROLL = 4;  // table slots a thread scans at a time
 constexpr u64 BIG_DIRECT_DEFER = 2 * BIG_TAB;  // integral weights: longer rows are deferred unread
 // (the autotuner may pick another bound; see HUB_DEFER_CAND)
 constexpr u32 BIG_WARPS = BIG_THREADS / 32;
@@ -805,25 +839,41 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
     const u32 nscan = global ? s_gused : cap;
     double g = -1.0;
     u32 p = NONE32, kk = cur;
-    for (u32 x = tid; x < nscan; x += BIG_THREADS) {
-      const u64 sl = global ? g_list[x] : x;
-      const u32 key = tk[sl];
-      if (key == NONE32) continue;
-      const double val = tab_value(tv[sl], A.concurrent);
-      const u32 pp = tp[sl];
-      if (global) {
-        tk[sl] = NONE32;
-        tv[sl] = 0.0;
-        tp[sl] = NONE32;
+    // BIG_SCAN_UNROLL slots per thread at a time: their community degrees
+    // are gathered together
+    for (u32 x0 = tid; x0 < nscan; x0 += BIG_THREADS * BIG_SCAN_UNROLL) {
+      u32 key[BIG_SCAN_UNROLL], pq[BIG_SCAN_UNROLL];
+      double val[BIG_SCAN_UNROLL], dk[BIG_SCAN_UNROLL];
+#pragma unroll
+      for (u32 j = 0; j < BIG_SCAN_UNROLL; ++j) {
+        const u32 x = x0 + j * BIG_THREADS;
+        key[j] = NONE32;
+        if (x >= nscan) continue;
+        const u64 sl = global ? g_list[x] : x;
+        key[j] = tk[sl];
+        if (key[j] == NONE32) continue;
+        val[j] = tab_value(tv[sl], A.concurrent);
+        pq[j] = tp[sl];
+        if (global) {
+          tk[sl] = NONE32;
+          tv[sl] = 0.0;
+          tp[sl] = NONE32;
+        }
+        if (key[j] == cur || A.tw == 0.0) key[j] = NONE32;
+        else if (KIND == EVAL_REFINE && A.blocked[key[j]]) key[j] = NONE32;
       }
-      if (key == cur || A.tw == 0.0) continue;
-      if (KIND == EVAL_REFINE && A.blocked[key]) continue;
-      const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, A.d[key]);
-      ++ncand;
-      if (p == NONE32 || gn > g || (gn == g && pp < p)) {
-        g = gn;
-        p = pp;
-        kk = key;
+#pragma unroll
+      for (u32 j = 0; j < BIG_SCAN_UNROLL; ++j) dk[j] = key[j] != NONE32 ? A.d[key[j]] : 0.0;
+#pragma unroll
+      for (u32 j = 0; j < BIG_SCAN_UNROLL; ++j) {
+        if (key[j] == NONE32) continue;
+        const double gn = move_gain(val[j], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
+        ++ncand;
+        if (p == NONE32 || gn > g || (gn == g && pq[j] < p)) {
+          g = gn;
+          p = pq[j];
+          kk = key[j];
+        }
       }
     }
     for (int o = 16; o; o >>= 1) {
@@ -904,17 +954,6 @@ __device__ __forceinline__ u32 pb_bucket(u32 key, u32 B) {
   return B <= 1 ? 0u : hash32(key) >> (32 - (__ffs(B) - 1));
 }
 
-// Largest r in [lo, hi) with base[r] <= x (base ascending, base[lo] <= x).
-template <typename T>
-__device__ __forceinline__ u32 pb_row_of(const T* base, u32 lo, u32 hi, T x) {
-  while (hi - lo > 1) {
-    const u32 mid = (lo + hi) >> 1;
-    if (base[mid] <= x) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
 struct PbArgs {
   const u32* ovf;      // deferred idx values
   const u32* nb;       // buckets per row
@@ -935,24 +974,59 @@ struct PbArgs {
   u32* bp;
   u32* bk;
   u32* rowfail;        // per row: a bucket overflowed
+  // filled once per pass by k_pb_rows, so that no kernel searches for its row
+  // or walks idx -> vertex -> label -> degree before its real work
+  const u32* brow;     // global bucket -> row
+  const u32* crow;     // global chunk -> row
+  const u32* rv;       // per row: vertex, f[v], its current label, k_v, d[cur], off[v]
+  const u32* rfv;
+  const u32* rcur;
+  const double* rkv;
+  const double* rdcur;
+  const u64* ro0;
+  const u64* ne;       // per row: degree
 };
+
+// Per row of the pass: its scalars, and its entries in the bucket -> row and
+// chunk -> row maps (a warp per row).
+template <int KIND>
+__global__ void k_pb_rows(EvalArgs A, const u32* ovf, u32 m, const u32* nb, const u32* bbase,
+                          const u32* nc, const u32* cbase, u32* brow, u32* crow, u32* rv, u32* rfv,
+                          u32* rcur, double* rkv, double* rdcur, u64* ro0) {
+  const u32 lane = threadIdx.x & 31;
+  const u64 warp = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 r = warp; r < m; r += nwarps) {
+    if (lane == 0) {
+      const u32 v = A.verts[ovf[r]];
+      const u32 fv = A.f[v];
+      const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+      rv[r] = v;
+      rfv[r] = fv;
+      rcur[r] = cur;
+      rkv[r] = A.kdeg[v];
+      rdcur[r] = A.d[cur];
+      ro0[r] = A.off[v];
+    }
+    const u32 b0 = bbase[r], b1 = b0 + nb[r];
+    for (u32 x = b0 + lane; x < b1; x += 32) brow[x] = (u32)r;
+    const u32 c0 = cbase[r], c1 = c0 + nc[r];
+    for (u32 x = c0 + lane; x < c1; x += 32) crow[x] = (u32)r;
+  }
+}
 
 template <int KIND>
 __global__ void __launch_bounds__(256) k_pb_hist(EvalArgs A, PbArgs P) {
   __shared__ u32 s_hist[PB_HIST];
   __shared__ double s_red[8];
-  __shared__ u32 s_row;
   for (u32 c = P.c0 + blockIdx.x; c < P.c1; c += gridDim.x) {
-    if (threadIdx.x == 0) s_row = pb_row_of(P.cbase, P.r0, P.r1, c);
-    __syncthreads();
-    const u32 r = s_row;
-    const u32 i = P.ovf[r];
-    const u32 v = A.verts[i];
-    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u32 r = P.crow[c];
+    const u32 v = P.rv[r];
+    const u64 o0 = P.ro0[r], o1 = o0 + P.ne[r];
     const u64 lo = o0 + (u64)(c - P.cbase[r]) * PB_CHUNK;
     const u64 hi = lo + PB_CHUNK < o1 ? lo + PB_CHUNK : o1;
-    const u32 fv = A.f[v];
-    const u32 cur = (KIND == EVAL_MOVE) ? fv : A.s[v];
+    const u32 fv = P.rfv[r];
+    const u32 cur = P.rcur[r];
     const u32 B = P.nb[r];
     const bool local = B <= PB_HIST;
     u32* gcnt = P.bcnt + (P.bbase[r] - P.b0);
@@ -1007,14 +1081,10 @@ __global__ void __launch_bounds__(256) k_pb_hist(EvalArgs A, PbArgs P) {
 }
 
 __global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
-  __shared__ u32 s_row;
   const u32 lane = threadIdx.x & 31;
   for (u32 c = P.c0 + blockIdx.x; c < P.c1; c += gridDim.x) {
-    if (threadIdx.x == 0) s_row = pb_row_of(P.cbase, P.r0, P.r1, c);
-    __syncthreads();
-    const u32 r = s_row;
-    const u32 v = A.verts[P.ovf[r]];
-    const u64 o0 = A.off[v], o1 = A.off[v + 1];
+    const u32 r = P.crow[c];
+    const u64 o0 = P.ro0[r], o1 = o0 + P.ne[r];
     const u64 lo = o0 + (u64)(c - P.cbase[r]) * PB_CHUNK;
     const u64 hi = lo + PB_CHUNK < o1 ? lo + PB_CHUNK : o1;
     const u32 B = P.nb[r];
@@ -1074,17 +1144,15 @@ __global__ void __launch_bounds__(256, 5) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
   u32* s_tp = s_tk + PB_TAB;
   __shared__ double r_g[8];
   __shared__ u32 r_p[8], r_k[8];
-  __shared__ u32 s_row, s_ovf;
+  __shared__ u32 s_ovf;
   __shared__ unsigned long long s_wb[8][32];  // a chunk's weights, per warp
   __shared__ u32 s_pb[8][32];                 // and positions
   const u32 tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   unsigned long long ncand = 0;
   for (u32 bl = blockIdx.x; bl < nbuckets; bl += gridDim.x) {
     const u32 b = P.b0 + bl;
-    if (tid == 0) {
-      s_row = pb_row_of(P.bbase, P.r0, P.r1, b);
-      s_ovf = 0;
-    }
+    const u32 r = P.brow[b];
+    if (tid == 0) s_ovf = 0;
     const u32 e_lo = P.boff[bl], e_hi = P.boff[bl + 1];
     const u32 cnt = e_hi - e_lo;
     u32 cap = 64;
@@ -1095,7 +1163,6 @@ __global__ void __launch_bounds__(256, 5) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
       s_tv[x] = 0ull;
     }
     __syncthreads();
-    const u32 r = s_row;
     const u32 mask = cap - 1;
     // Each warp takes PB_FOLD_UNROLL chunks of 32 entries at a time, their
     // loads issued together.  Lanes of a chunk that share a key are combined
@@ -1155,12 +1222,10 @@ __global__ void __launch_bounds__(256, 5) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
     double g = -1.0;
     u32 p = NONE32, kk = NONE32;
     if (!s_ovf && A.tw != 0.0) {
-      const u32 i = P.ovf[r];
-      const u32 v = A.verts[i];
-      const u32 cur = (KIND == EVAL_MOVE) ? A.f[v] : A.s[v];
-      const double kv = A.kdeg[v];
+      const u32 cur = P.rcur[r];
+      const double kv = P.rkv[r];
       const double wcur = P.wcur[r];
-      const double dcur = A.d[cur];
+      const double dcur = P.rdcur[r];
       // the community degrees of PB_FOLD_UNROLL slots are gathered together
       for (u32 x0 = tid; x0 < cap; x0 += 256 * PB_FOLD_UNROLL) {
         u32 key[PB_FOLD_UNROLL];
@@ -1333,8 +1398,12 @@ template <int KIND>
 static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
   Scratch& S = E.sc;
   cudaStream_t st = E.stream;
+  cudaEvent_t ev = E.kt_begin();
   const u32 m = E.read_u32(S.ovf_cnt.p);
-  if (!m) return 0;
+  if (!m) {
+    E.kt_end(KT_EVAL_PB, ev);
+    return 0;
+  }
   S.pb_nb.ensure(E.mem, m);
   S.pb_nc.ensure(E.mem, m);
   S.pb_bbase.ensure(E.mem, m);
@@ -1372,6 +1441,19 @@ static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
   HL_CUDA(cudaMemcpyAsync(nc.data(), S.pb_nc.p, sizeof(u32) * m, cudaMemcpyDeviceToHost, st));
   HL_CUDA(cudaMemcpyAsync(cb.data(), S.pb_cbase.p, sizeof(u32) * m, cudaMemcpyDeviceToHost, st));
   E.sync();
+  const u32 nbk = bb[m - 1] + nb[m - 1], nch = cb[m - 1] + nc[m - 1];
+  S.pb_brow.ensure(E.mem, nbk);
+  S.pb_crow.ensure(E.mem, nch);
+  S.pb_rv.ensure(E.mem, m);
+  S.pb_rfv.ensure(E.mem, m);
+  S.pb_rcur.ensure(E.mem, m);
+  S.pb_rkv.ensure(E.mem, m);
+  S.pb_rdcur.ensure(E.mem, m);
+  S.pb_ro0.ensure(E.mem, m);
+  ++E.nlaunch, k_pb_rows<KIND><<<grid_for((u64)m * 32), 256, 0, st>>>(
+      a, S.ovf.p, m, S.pb_nb.p, S.pb_bbase.p, S.pb_nc.p, S.pb_cbase.p, S.pb_brow.p, S.pb_crow.p,
+      S.pb_rv.p, S.pb_rfv.p, S.pb_rcur.p, S.pb_rkv.p, S.pb_rdcur.p, S.pb_ro0.p);
+  HL_LAUNCH_CHECK();
   PbArgs P;
   P.ovf = S.ovf.p;
   P.nb = S.pb_nb.p;
@@ -1380,6 +1462,15 @@ static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
   P.cbase = S.pb_cbase.p;
   P.wcur = S.pb_wcur.p;
   P.rowfail = S.pb_rowfail.p;
+  P.brow = S.pb_brow.p;
+  P.crow = S.pb_crow.p;
+  P.rv = S.pb_rv.p;
+  P.rfv = S.pb_rfv.p;
+  P.rcur = S.pb_rcur.p;
+  P.rkv = S.pb_rkv.p;
+  P.rdcur = S.pb_rdcur.p;
+  P.ro0 = S.pb_ro0.p;
+  P.ne = S.pb_ne.p;
   u32 r0 = 0;
   while (r0 < m) {
     u32 r1 = r0 + 1;
@@ -1433,7 +1524,9 @@ static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
     HL_LAUNCH_CHECK();
     r0 = r1;
   }
-  return E.read_u32(S.pb_failcnt.p);
+  const u32 nfail = E.read_u32(S.pb_failcnt.p);
+  E.kt_end(KT_EVAL_PB, ev);
+  return nfail;
 }
 
 void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, const u32* s,
@@ -1703,7 +1796,7 @@ void run_eval(Engine& E, int kind, const u32* verts, u32 nv, const Level& L, con
 // tables for the partitioned pass is then tuned the same way.  Runs once, on
 // the first movement round whose frontier has at least AUTOTUNE_MIN vertices.
 constexpr u32 AUTOTUNE_MIN = 20000;
-constexpr u32 HUB_DEFER_CAND[] = {2048, 8192, 32768};
+constexpr u32 HUB_DEFER_CAND[] = {1, 2048, 8192, 32768};  // 1: every hub row
 
 void autotune_bins(Engine& E, const u32* verts, u32 nv, const Level& L, const u32* s,
                    const double* d, u32* out_to, double* out_gain) {

@@ -101,8 +101,9 @@ struct Scratch {
   // partitioned second pass of the block kernel (integral weights)
   DBuf<u32> pb_nb, pb_nc, pb_bbase, pb_cbase, pb_rowfail, pb_fail, pb_failcnt, pb_ktmp, pb_ekey,
       pb_epos, pb_bcnt, pb_boff, pb_bp, pb_bk;
-  DBuf<u64> pb_ne, pb_ebase;
-  DBuf<double> pb_wcur, pb_ew, pb_bg;
+  DBuf<u64> pb_ne, pb_ebase, pb_ro0;
+  DBuf<double> pb_wcur, pb_ew, pb_bg, pb_rkv, pb_rdcur;
+  DBuf<u32> pb_brow, pb_crow, pb_rv, pb_rfv, pb_rcur;  // bucket / chunk -> row; row scalars
   DBuf<unsigned long long> mark_long;  // (rank << 32 | segment) of long moved rows
   DBuf<u32> mark_long_cnt;
   // batch statistics accumulated on the device and read once at the end of
@@ -150,6 +151,7 @@ enum KernelId : int {
   KT_HOST_SYNC,    // host waits on the stream (launches = count; no time)
   KT_COPY_ROWS,    // untouched CSR rows copied into the new buffer
   KT_MOVE_SMALL,   // movement rounds of a small frontier in one block (small.cu)
+  KT_EVAL_PB,      // the partitioned pass of the block bin (inside KT_EVAL_HUGE)
   KT_COUNT
 };
 

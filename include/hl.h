@@ -189,7 +189,7 @@ HL_API hl_status hl_set_level_callback(hl_graph* g, hl_level_fn fn, void* user);
  * the warp kernel with a shared table, mid_max+1..wide_max the wide warp
  * kernel, larger ones the block kernel.  hub_defer (may be NULL): with
  * integral weights, hub rows longer than this go straight to the partitioned
- * pass.  frontier is the frontier size the autotuner measured on (0: not
+ * pass (1: every row of the block bin).  frontier is the frontier size the autotuner measured on (0: not
  * tuned yet, or HL_FLAG_NO_AUTOTUNE). */
 HL_API hl_status hl_autotune_info(const hl_graph* g, uint32_t* mid_max, uint32_t* wide_max,
                                   uint32_t* hub_defer, uint32_t* frontier);
