@@ -150,6 +150,7 @@ def _load():
         "hl_dbg_set_mode": (st, [C.c_uint32]),
         "hl_dbg_set_bucket_slots": (st, [C.c_uint32]),
         "hl_dbg_set_hub_defer": (st, [C.c_uint32]),
+        "hl_dbg_set_pb_round": (st, [C.c_uint64]),
         "hl_dbg_set_bins": (st, [C.c_uint32, C.c_uint32]),
         "hl_autotune_info": (st, [vp, p32, p32, p32, p32]),
         "hl_tree_sum_noalloc": (st, [vp, C.c_uint64, vp, vp]),

@@ -1116,6 +1116,11 @@ hl_status hl_dbg_set_hub_defer(uint32_t entries) {
   return HL_OK;
 }
 
+hl_status hl_dbg_set_pb_round(uint64_t entries) {
+  g_dbg_pb_round.store(entries);  // 0: the default round size
+  return HL_OK;
+}
+
 hl_status hl_dbg_set_mode(uint32_t mode) {
   if (mode != HL_MODE_DETERMINISTIC && mode != HL_MODE_THROUGHPUT) {
     g_err = "mode must be HL_MODE_DETERMINISTIC or HL_MODE_THROUGHPUT";

@@ -83,6 +83,19 @@ __device__ __forceinline__ u32 hash32(u32 x) {
   return x;
 }
 
+// Integral weights and sums in [0, 2^52) (the handle keeps 2m below 2^52, and
+// every partial sum of a row is at most its k_v) between double and integer
+// without a conversion instruction: 2^52 + x is exact there, and its bits are
+// those of 2^52 plus x.
+constexpr double TWO52 = 4503599627370496.0;
+constexpr unsigned long long TWO52_BITS = 0x4330000000000000ull;
+__device__ __forceinline__ unsigned long long int_of(double w) {
+  return (unsigned long long)__double_as_longlong(__dadd_rn(w, TWO52)) - TWO52_BITS;
+}
+__device__ __forceinline__ double dbl_of(unsigned long long s) {
+  return __dsub_rn(__longlong_as_double((long long)(s + TWO52_BITS)), TWO52);
+}
+
 template <int KIND>
 __device__ __forceinline__ bool entry_key(const EvalArgs& A, u32 v, u32 nb, u32 fv, u32& key) {
   if (KIND == EVAL_MOVE) {
@@ -590,7 +603,7 @@ __device__ __forceinline__ u64 claim_slot(u32* tk, u64 mask, u32 key, bool& fres
 // bits of an exact integer sum (added with 64-bit integer atomics).
 __device__ __forceinline__ double tab_value(double raw, bool integer) {
   if (!integer) return raw;
-  return (double)(long long)__double_as_longlong(raw);
+  return dbl_of((unsigned long long)__double_as_longlong(raw));
 }
 
 template <int KIND>
@@ -739,21 +752,34 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         const bool okk = key != NONE32;
         const u32 grp = __match_any_sync(0xffffffffu, okk ? (unsigned long long)key
                                                            : ((1ull << 32) | lane));
-        b_w[tid] = wv;
-        __syncwarp();
-        if (okk && lane == (u32)(__ffs(grp) - 1)) {
-          double gsum = 0.0;
-          for (u32 m = grp; m; m &= m - 1) gsum += b_w[(tid & ~31u) + __ffs(m) - 1];
-          bool fresh;
-          const u64 slot = claim_slot(tk, mask, key, fresh);
-          if (fresh) {
-            if (global) g_list[atomicAdd(&s_gused, 1u)] = (u32)slot;
-            else atomicAdd(&s_used, 1u);
+        const bool leader = okk && lane == (u32)(__ffs(grp) - 1);
+        // the group's integer sum: one reduction over the match_any partition
+        // when 32 of the weights fit 32 bits, else the leader adds them up
+        unsigned long long isum = 0;
+        if (__all_sync(0xffffffffu, !okk || wv < 67108864.0)) {
+          isum = __reduce_add_sync(grp, okk ? (u32)int_of(wv) : 0u);
+        } else {
+          b_w[tid] = wv;
+          __syncwarp();
+          if (leader) {
+            double gsum = 0.0;
+            for (u32 m = grp; m; m &= m - 1) gsum += b_w[(tid & ~31u) + __ffs(m) - 1];
+            isum = int_of(gsum);
           }
-          // the slot holds the integer sum (0.0 and integer 0 share their bits)
-          atomicAdd(reinterpret_cast<unsigned long long*>(&tv[slot]),
-                    (unsigned long long)(long long)gsum);
+          __syncwarp();
+        }
+        bool fresh = false;
+        if (leader) {
+          const u64 slot = claim_slot(tk, mask, key, fresh);
+          if (fresh && global) g_list[atomicAdd(&s_gused, 1u)] = (u32)slot;
+          // the slot holds the integer sum (0.0 and integer 0 share their bits);
+          // the leader's position is the group's first
+          atomicAdd(reinterpret_cast<unsigned long long*>(&tv[slot]), isum);
           atomicMin(&tp[slot], pos);
+        }
+        if (!global) {
+          const u32 fm = __ballot_sync(0xffffffffu, fresh);
+          if (lane == 0 && fm) atomicAdd(&s_used, (u32)__popc(fm));
         }
         __syncwarp();
         continue;
@@ -1126,7 +1152,7 @@ __global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
   }
 }
 
-constexpr size_t PB_FOLD_SMEM = (size_t)PB_TAB * (8 + 4 + 4);
+constexpr size_t PB_FOLD_SMEM = (size_t)PB_TAB * (8 + 4 + 4 + 2);
 
 // Table slots the fold kernel may use (hl_dbg_set_bucket_slots lowers it so
 // that tests reach the overflow path).
@@ -1135,33 +1161,40 @@ std::atomic<u32> g_pb_slots{PB_TAB};
 // Hub-row deferral bound forced by hl_dbg_set_hub_defer (0: the handle's).
 std::atomic<u32> g_dbg_hub_defer{0};
 
+// One bucket per block at a time.  The table starts clean and every key
+// inserted is appended to a list (a warp's new keys take their list places
+// with one atomic), so the argmax scan and the reset visit only used slots.
 template <int KIND>
-__global__ void __launch_bounds__(256, 5) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuckets,
+__global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuckets,
                                                  u32 tab_limit) {
   extern __shared__ __align__(16) unsigned char pb_smem[];
   unsigned long long* s_tv = reinterpret_cast<unsigned long long*>(pb_smem);
   u32* s_tk = reinterpret_cast<u32*>(s_tv + PB_TAB);
   u32* s_tp = s_tk + PB_TAB;
+  unsigned short* s_list = reinterpret_cast<unsigned short*>(s_tp + PB_TAB);
   __shared__ double r_g[8];
   __shared__ u32 r_p[8], r_k[8];
-  __shared__ u32 s_ovf;
+  __shared__ u32 s_ovf, s_nused;
   __shared__ unsigned long long s_wb[8][32];  // a chunk's weights, per warp
   __shared__ u32 s_pb[8][32];                 // and positions
   const u32 tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   unsigned long long ncand = 0;
+  for (u32 x = tid; x < PB_TAB; x += 256) {
+    s_tk[x] = NONE32;
+    s_tp[x] = NONE32;
+    s_tv[x] = 0ull;
+  }
   for (u32 bl = blockIdx.x; bl < nbuckets; bl += gridDim.x) {
     const u32 b = P.b0 + bl;
     const u32 r = P.brow[b];
-    if (tid == 0) s_ovf = 0;
+    if (tid == 0) {
+      s_ovf = 0;
+      s_nused = 0;
+    }
     const u32 e_lo = P.boff[bl], e_hi = P.boff[bl + 1];
     const u32 cnt = e_hi - e_lo;
     u32 cap = 64;
     while (cap < 2 * cnt && cap < tab_limit) cap <<= 1;
-    for (u32 x = tid; x < cap; x += 256) {
-      s_tk[x] = NONE32;
-      s_tp[x] = NONE32;
-      s_tv[x] = 0ull;
-    }
     __syncthreads();
     const u32 mask = cap - 1;
     // Each warp takes PB_FOLD_UNROLL chunks of 32 entries at a time, their
@@ -1178,7 +1211,7 @@ __global__ void __launch_bounds__(256, 5) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
         ek[j] = ok ? P.ekey[e] : NONE32;
         ep[j] = ok ? P.epos[e] : NONE32;
         // integral weights: every partial sum is an exact integer
-        ew[j] = ok ? (unsigned long long)(long long)P.ew[e] : 0ull;
+        ew[j] = ok ? int_of(P.ew[e]) : 0ull;
       }
 #pragma unroll
       for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
@@ -1186,24 +1219,38 @@ __global__ void __launch_bounds__(256, 5) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
         const bool ok = ek[j] != NONE32;
         const u32 grp = __match_any_sync(0xffffffffu, ok ? (unsigned long long)ek[j]
                                                          : ((1ull << 32) | lane));
-        s_wb[wib][lane] = ew[j];
-        s_pb[wib][lane] = ep[j];
-        __syncwarp();
-        if (ok && lane == (u32)(__ffs(grp) - 1)) {
-          unsigned long long sum = 0;
-          u32 pmin = NONE32;
-          for (u32 m = grp; m; m &= m - 1) {
-            const u32 l = __ffs(m) - 1;
-            sum += s_wb[wib][l];
-            pmin = min(pmin, s_pb[wib][l]);
-          }
-          u32 slot = hash32(ek[j]) & mask;
+        const bool leader = ok && lane == (u32)(__ffs(grp) - 1);
+        // the group's sum and first position: one reduction over the
+        // match_any partition when 32 of the weights fit 32 bits, else the
+        // leader adds them up from shared memory
+        unsigned long long sum = 0;
+        u32 pmin = NONE32;
+        if (__all_sync(0xffffffffu, ew[j] < (1ull << 26))) {
+          sum = __reduce_add_sync(grp, (u32)ew[j]);
+          pmin = __reduce_min_sync(grp, ep[j]);
+        } else {
+          s_wb[wib][lane] = ew[j];
+          s_pb[wib][lane] = ep[j];
+          __syncwarp();
+          if (leader)
+            for (u32 m = grp; m; m &= m - 1) {
+              const u32 l = __ffs(m) - 1;
+              sum += s_wb[wib][l];
+              pmin = min(pmin, s_pb[wib][l]);
+            }
+          __syncwarp();
+        }
+        bool fresh = false;
+        u32 slot = 0;
+        if (leader) {
+          slot = hash32(ek[j]) & mask;
           u32 probes = 0;
           bool ins = false;
           while (probes++ < cap) {
             const u32 prev = atomicCAS(&s_tk[slot], NONE32, ek[j]);
             if (prev == NONE32 || prev == ek[j]) {
               ins = true;
+              fresh = prev == NONE32;
               break;
             }
             slot = (slot + 1) & mask;
@@ -1215,43 +1262,58 @@ __global__ void __launch_bounds__(256, 5) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
             s_ovf = 1;
           }
         }
+        const u32 fm = __ballot_sync(0xffffffffu, fresh);
+        if (fm) {
+          u32 at = 0;
+          if (lane == 0) at = atomicAdd(&s_nused, (u32)__popc(fm));
+          at = __shfl_sync(0xffffffffu, at, 0);
+          if (fresh) s_list[at + __popc(fm & ((1u << lane) - 1u))] = (unsigned short)slot;
+        }
         __syncwarp();
       }
     }
     __syncthreads();
     double g = -1.0;
     u32 p = NONE32, kk = NONE32;
-    if (!s_ovf && A.tw != 0.0) {
-      const u32 cur = P.rcur[r];
-      const double kv = P.rkv[r];
-      const double wcur = P.wcur[r];
-      const double dcur = P.rdcur[r];
-      // the community degrees of PB_FOLD_UNROLL slots are gathered together
-      for (u32 x0 = tid; x0 < cap; x0 += 256 * PB_FOLD_UNROLL) {
-        u32 key[PB_FOLD_UNROLL];
-        double dk[PB_FOLD_UNROLL];
+    const u32 nused = s_nused;
+    const bool scan = !s_ovf && A.tw != 0.0;
+    const u32 cur = P.rcur[r];
+    const double kv = P.rkv[r];
+    const double wcur = P.wcur[r];
+    const double dcur = P.rdcur[r];
+    // the used slots, PB_FOLD_UNROLL at a time (their community degrees are
+    // gathered together), each reset after it is read
+    for (u32 x0 = tid; x0 < nused; x0 += 256 * PB_FOLD_UNROLL) {
+      u32 key[PB_FOLD_UNROLL], pq[PB_FOLD_UNROLL];
+      unsigned long long vq[PB_FOLD_UNROLL];
+      double dk[PB_FOLD_UNROLL];
 #pragma unroll
-        for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
-          const u32 x = x0 + j * 256;
-          key[j] = x < cap ? s_tk[x] : NONE32;
-          if (key[j] == cur) key[j] = NONE32;
-          if (KIND == EVAL_REFINE && key[j] != NONE32 && A.blocked[key[j]]) key[j] = NONE32;
-        }
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        const u32 x = x0 + j * 256;
+        key[j] = NONE32;
+        if (x >= nused) continue;
+        const u32 sl = s_list[x];
+        key[j] = s_tk[sl];
+        vq[j] = s_tv[sl];
+        pq[j] = s_tp[sl];
+        s_tk[sl] = NONE32;
+        s_tv[sl] = 0ull;
+        s_tp[sl] = NONE32;
+        if (!scan || key[j] == cur) key[j] = NONE32;
+        else if (KIND == EVAL_REFINE && A.blocked[key[j]]) key[j] = NONE32;
+      }
 #pragma unroll
-        for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) dk[j] = key[j] != NONE32 ? A.d[key[j]] : 0.0;
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) dk[j] = key[j] != NONE32 ? A.d[key[j]] : 0.0;
 #pragma unroll
-        for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
-          if (key[j] == NONE32) continue;
-          const u32 x = x0 + j * 256;
-          const double val = (double)(long long)s_tv[x];
-          const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, dk[j]);
-          ++ncand;
-          const u32 pp = s_tp[x];
-          if (p == NONE32 || gn > g || (gn == g && pp < p)) {
-            g = gn;
-            p = pp;
-            kk = key[j];
-          }
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
+        if (key[j] == NONE32) continue;
+        const double val = dbl_of(vq[j]);
+        const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, dk[j]);
+        ++ncand;
+        if (p == NONE32 || gn > g || (gn == g && pq[j] < p)) {
+          g = gn;
+          p = pq[j];
+          kk = key[j];
         }
       }
     }
@@ -1394,6 +1456,10 @@ constexpr u64 OVF_TABLE_BYTES = 4ull << 30;  // table bytes pass 2 may spread ov
 // S.pb_failcnt[0]) for the global-table pass.  Returns that count.
 constexpr u64 PB_ROUND_ENTRIES = 96ull << 20;
 
+// Entries per round of the partitioned pass forced by hl_dbg_set_pb_round
+// (0: PB_ROUND_ENTRIES).
+std::atomic<u64> g_dbg_pb_round{0};
+
 template <int KIND>
 static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
   Scratch& S = E.sc;
@@ -1471,10 +1537,11 @@ static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
   P.rdcur = S.pb_rdcur.p;
   P.ro0 = S.pb_ro0.p;
   P.ne = S.pb_ne.p;
+  const u64 round_entries = g_dbg_pb_round.load() ? g_dbg_pb_round.load() : PB_ROUND_ENTRIES;
   u32 r0 = 0;
   while (r0 < m) {
     u32 r1 = r0 + 1;
-    while (r1 < m && eb[r1] + ne[r1] - eb[r0] <= PB_ROUND_ENTRIES) ++r1;
+    while (r1 < m && eb[r1] + ne[r1] - eb[r0] <= round_entries) ++r1;
     const u64 te = eb[r1 - 1] + ne[r1 - 1] - eb[r0];
     const u32 tb = bb[r1 - 1] + nb[r1 - 1] - bb[r0];
     S.pb_ktmp.ensure(E.mem, te);

@@ -284,6 +284,7 @@ extern std::atomic<int> g_exact_tfilter;
 // Test switch: table slots of the partitioned hub pass (eval.cu).
 extern std::atomic<u32> g_pb_slots;
 extern std::atomic<u32> g_dbg_hub_defer;
+extern std::atomic<u64> g_dbg_pb_round;
 
 // aggregate.cu
 u64 inc_aggregation(Engine& E, Level& L, const DevEdges& delta, u32* next_n,

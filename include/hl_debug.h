@@ -105,6 +105,12 @@ HL_API hl_status hl_dbg_set_bucket_slots(uint32_t slots);
  * either path. */
 HL_API hl_status hl_dbg_set_hub_defer(uint32_t entries);
 
+/* Entries the partitioned pass takes per round of its kernels (0 = 96 Mi).
+ * Smaller rounds keep a round's keys and bucketed entries in L2 between the
+ * scatter and the fold, at the price of more launches.  Results do not
+ * depend on it. */
+HL_API hl_status hl_dbg_set_pb_round(uint64_t entries);
+
 /* Warp-bin thresholds of the stage entry points (mid_max in [33, 128],
  * wide_max in [mid_max, 512]; 0 = default), the pairs the autotuner picks
  * from.  Results do not depend on them. */
