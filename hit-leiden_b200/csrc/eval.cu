@@ -569,6 +569,9 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
 // ---------------------------------------------------------------------------
 constexpr u32 BIG_TAB = 4096;
 constexpr u32 BIG_SCAN_UNROLL = 4;  // table slots a thread scans at a time
+// Used-slot list of the shared table: a row is checked against BIG_TAB / 2
+// distinct keys after every tile, so it holds at most that plus one tile's
+constexpr u32 BIG_LIST = BIG_TAB / 2 + BIG_THREADS;
 constexpr u64 BIG_DIRECT_DEFER = 2 * BIG_TAB;  // integral weights: longer rows are deferred unread
 // (the autotuner may pick another bound; see HUB_DEFER_CAND)
 constexpr u32 BIG_WARPS = BIG_THREADS / 32;
@@ -615,6 +618,9 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
   double* b_w = reinterpret_cast<double*>(s_tp + BIG_TAB);   // bucketed tile: weights
   u32* b_key = reinterpret_cast<u32*>(b_w + BIG_THREADS);    // keys
   u32* b_pos = b_key + BIG_THREADS;                          // positions in the row
+  // used slots of the shared table, in insertion order (the scan visits and
+  // resets only these)
+  unsigned short* s_list = reinterpret_cast<unsigned short*>(b_pos + BIG_THREADS);
   __shared__ u32 s_cnt[BIG_WARPS * BIG_WARPS];               // [partition][warp]
   __shared__ u32 s_off[BIG_WARPS * BIG_WARPS + 1];
   __shared__ double r_g[BIG_WARPS];
@@ -631,6 +637,12 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
   double* g_tv = A.tval ? A.tval + (u64)blockIdx.x * A.region : nullptr;
   u32* g_list = A.tlist ? A.tlist + (u64)blockIdx.x * (A.region / 2) : nullptr;
   const u32 nidx = A.nidx_dev ? *A.nidx_dev : A.nidx;
+  // the shared table starts clean; each row resets the slots it used
+  for (u32 x = tid; x < BIG_TAB; x += BIG_THREADS) {
+    s_tk[x] = NONE32;
+    s_tv[x] = 0.0;
+    s_tp[x] = NONE32;
+  }
   // Vertices are taken from a shared counter (the list is ordered by degree,
   // largest first), so the longest rows start first and no block queues
   // several of them behind each other.
@@ -660,11 +672,6 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
     if (tid == 0) {
       s_used = 0;
       s_gused = 0;
-    }
-    for (u32 x = tid; x < cap; x += BIG_THREADS) {
-      s_tk[x] = NONE32;
-      s_tv[x] = 0.0;
-      s_tp[x] = NONE32;
     }
     // pipeline prologue: keys of tile 0, neighbours of tile 1
     u32 key1;
@@ -729,21 +736,27 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         break;
       }
       if (!global && s_used > BIG_TAB / 2) {
+        // the used shared slots move to the global table and are reset
         const u64 gmask = gcap - 1;
-        for (u32 x = tid; x < BIG_TAB; x += BIG_THREADS) {
-          const u32 k = s_tk[x];
-          if (k == NONE32) continue;
+        const u32 nu = s_used;
+        for (u32 x = tid; x < nu; x += BIG_THREADS) {
+          const u32 sx = s_list[x];
           bool fresh;
-          const u64 sl = claim_slot(g_tk, gmask, k, fresh);
-          g_tv[sl] = s_tv[x];
-          g_tp[sl] = s_tp[x];
+          const u64 sl = claim_slot(g_tk, gmask, s_tk[sx], fresh);
+          g_tv[sl] = s_tv[sx];
+          g_tp[sl] = s_tp[sx];
           g_list[atomicAdd(&s_gused, 1u)] = (u32)sl;
+          s_tk[sx] = NONE32;
+          s_tv[sx] = 0.0;
+          s_tp[sx] = NONE32;
         }
         global = true;
         tk = g_tk;
         tp = g_tp;
         tv = g_tv;
         mask = gmask;
+        // every moved slot is written before any entry is added to it
+        __syncthreads();
       }
       if (A.concurrent) {
         // Integral weights: every order of additions gives the same sums, so
@@ -769,8 +782,9 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
           __syncwarp();
         }
         bool fresh = false;
+        u64 slot = 0;
         if (leader) {
-          const u64 slot = claim_slot(tk, mask, key, fresh);
+          slot = claim_slot(tk, mask, key, fresh);
           if (fresh && global) g_list[atomicAdd(&s_gused, 1u)] = (u32)slot;
           // the slot holds the integer sum (0.0 and integer 0 share their bits);
           // the leader's position is the group's first
@@ -779,7 +793,12 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         }
         if (!global) {
           const u32 fm = __ballot_sync(0xffffffffu, fresh);
-          if (lane == 0 && fm) atomicAdd(&s_used, (u32)__popc(fm));
+          if (fm) {
+            u32 at = 0;
+            if (lane == 0) at = atomicAdd(&s_used, (u32)__popc(fm));
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (fresh) s_list[at + __popc(fm & lt_mask)] = (unsigned short)slot;
+          }
         }
         __syncwarp();
         continue;
@@ -824,7 +843,7 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
           if (fresh) {
             tp[slot] = b_pos[e];
             if (global) g_list[atomicAdd(&s_gused, 1u)] = (u32)slot;
-            else atomicAdd(&s_used, 1u);
+            else s_list[atomicAdd(&s_used, 1u)] = (unsigned short)slot;
           }
           acc = tv[slot];
         }
@@ -841,12 +860,19 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
       }
     }
     if (deferred) {
+      const u32 nu = s_used;  // stable: the loop left right after a barrier
+      for (u32 x = tid; x < nu; x += BIG_THREADS) {
+        const u32 sx = s_list[x];
+        s_tk[sx] = NONE32;
+        s_tv[sx] = 0.0;
+        s_tp[sx] = NONE32;
+      }
       if (tid == 0) A.ovf_list[atomicAdd(A.ovf_count, 1u)] = i;
       __syncthreads();
       continue;
     }
     __syncthreads();
-    // w(v, cur), then the argmax over the table (resetting a global table).
+    // w(v, cur), then the argmax over the used slots (each reset after it is read).
     if (tid == 0) {
       double wc = 0.0;
       u64 sl = hash32(cur) & mask;
@@ -862,7 +888,7 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
     __syncthreads();
     const double wcur = s_wcur;
     const double dcur = A.d[cur];
-    const u32 nscan = global ? s_gused : cap;
+    const u32 nscan = global ? s_gused : s_used;
     double g = -1.0;
     u32 p = NONE32, kk = cur;
     // BIG_SCAN_UNROLL slots per thread at a time: their community degrees
@@ -875,16 +901,14 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         const u32 x = x0 + j * BIG_THREADS;
         key[j] = NONE32;
         if (x >= nscan) continue;
-        const u64 sl = global ? g_list[x] : x;
+        const u64 sl = global ? g_list[x] : s_list[x];
         key[j] = tk[sl];
         if (key[j] == NONE32) continue;
         val[j] = tab_value(tv[sl], A.concurrent);
         pq[j] = tp[sl];
-        if (global) {
-          tk[sl] = NONE32;
-          tv[sl] = 0.0;
-          tp[sl] = NONE32;
-        }
+        tk[sl] = NONE32;
+        tv[sl] = 0.0;
+        tp[sl] = NONE32;
         if (key[j] == cur || A.tw == 0.0) key[j] = NONE32;
         else if (KIND == EVAL_REFINE && A.blocked[key[j]]) key[j] = NONE32;
       }
@@ -1439,7 +1463,8 @@ __global__ void k_fill_u32(u32* p, u32 v, u64 n) {
 }
 
 static size_t big_smem() {
-  return (size_t)BIG_TAB * (8 + 4 + 4) + (size_t)BIG_THREADS * (8 + 4 + 4);
+  return (size_t)BIG_TAB * (8 + 4 + 4) + (size_t)BIG_THREADS * (8 + 4 + 4) +
+         (size_t)BIG_LIST * sizeof(unsigned short);
 }
 
 static std::atomic<bool> g_big_attr_set[64];
