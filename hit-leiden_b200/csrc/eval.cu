@@ -328,6 +328,8 @@ __global__ void __launch_bounds__(MID_WARPS * 32, 4) k_eval_mid(EvalArgs A) {
     double g = -1.0;
     u32 p = NONE32, kk = cur;
     if (A.tw != 0.0) {
+      GainScreen scr;  // exact gains only for candidates that may win
+      scr.init(wcur, A.tw, A.gamma, kv, dcur);
       for (u32 x0 = lane; x0 < cap; x0 += 32 * MID_SCAN_UNROLL) {
         u32 kq[MID_SCAN_UNROLL];
         double dk[MID_SCAN_UNROLL];
@@ -344,8 +346,9 @@ __global__ void __launch_bounds__(MID_WARPS * 32, 4) k_eval_mid(EvalArgs A) {
         for (u32 j = 0; j < MID_SCAN_UNROLL; ++j) {
           if (kq[j] == NONE32) continue;
           const u32 x = x0 + 32 * j;
-          const double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
           ++ncand;
+          if (!scr.keep(tv[x], dk[j])) continue;
+          const double gn = move_gain(tv[x], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
           const u32 pp = tp[x];
           if (p == NONE32 || gn > g || (gn == g && pp < p)) {
             g = gn;
@@ -502,6 +505,8 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
     }
     double g = -1.0;
     u32 p = NONE32, kk = cur;
+    GainScreen scr;  // exact gains only for candidates that may win
+    scr.init(wcur, A.tw, A.gamma, kv, dcur);
     for (u32 x0 = lane; x0 < used; x0 += 32 * WIDE_SCAN_UNROLL) {
       u32 key[WIDE_SCAN_UNROLL], sl[WIDE_SCAN_UNROLL];
       double dk[WIDE_SCAN_UNROLL];
@@ -519,8 +524,9 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32) k_eval_wide(EvalArgs A) {
 #pragma unroll
       for (u32 j = 0; j < WIDE_SCAN_UNROLL; ++j) {
         if (key[j] == NONE32) continue;
-        const double gn = move_gain(tv[sl[j]], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
         ++ncand;
+        if (!scr.keep(tv[sl[j]], dk[j])) continue;
+        const double gn = move_gain(tv[sl[j]], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
         const u32 pp = tp[sl[j]];
         if (p == NONE32 || gn > g || (gn == g && pp < p)) {
           g = gn;
@@ -893,6 +899,8 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
     u32 p = NONE32, kk = cur;
     // BIG_SCAN_UNROLL slots per thread at a time: their community degrees
     // are gathered together
+    GainScreen scr;  // exact gains only for candidates that may win
+    scr.init(wcur, A.tw, A.gamma, kv, dcur);
     for (u32 x0 = tid; x0 < nscan; x0 += BIG_THREADS * BIG_SCAN_UNROLL) {
       u32 key[BIG_SCAN_UNROLL], pq[BIG_SCAN_UNROLL];
       double val[BIG_SCAN_UNROLL], dk[BIG_SCAN_UNROLL];
@@ -917,8 +925,9 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
 #pragma unroll
       for (u32 j = 0; j < BIG_SCAN_UNROLL; ++j) {
         if (key[j] == NONE32) continue;
-        const double gn = move_gain(val[j], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
         ++ncand;
+        if (!scr.keep(val[j], dk[j])) continue;
+        const double gn = move_gain(val[j], wcur, A.tw, A.gamma, kv, dcur, dk[j]);
         if (p == NONE32 || gn > g || (gn == g && pq[j] < p)) {
           g = gn;
           p = pq[j];
@@ -1307,6 +1316,8 @@ __global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
     const double dcur = P.rdcur[r];
     // the used slots, PB_FOLD_UNROLL at a time (their community degrees are
     // gathered together), each reset after it is read
+    GainScreen scr;  // exact gains only for candidates that may win
+    scr.init(wcur, A.tw, A.gamma, kv, dcur);
     for (u32 x0 = tid; x0 < nused; x0 += 256 * PB_FOLD_UNROLL) {
       u32 key[PB_FOLD_UNROLL], pq[PB_FOLD_UNROLL];
       unsigned long long vq[PB_FOLD_UNROLL];
@@ -1332,8 +1343,9 @@ __global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
       for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
         if (key[j] == NONE32) continue;
         const double val = dbl_of(vq[j]);
-        const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, dk[j]);
         ++ncand;
+        if (!scr.keep(val, dk[j])) continue;
+        const double gn = move_gain(val, wcur, A.tw, A.gamma, kv, dcur, dk[j]);
         if (p == NONE32 || gn > g || (gn == g && pq[j] < p)) {
           g = gn;
           p = pq[j];
@@ -1568,6 +1580,10 @@ static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
     u32 r1 = r0 + 1;
     while (r1 < m && eb[r1] + ne[r1] - eb[r0] <= round_entries) ++r1;
     const u64 te = eb[r1 - 1] + ne[r1 - 1] - eb[r0];
+    // adjacency entries through the pass (16 algorithmic bytes each: col, w,
+    // the neighbour's label)
+    E.kagg[KT_EVAL_PB].items += te;
+    E.kagg[KT_EVAL_PB].bytes += 16 * te;
     const u32 tb = bb[r1 - 1] + nb[r1 - 1] - bb[r0];
     S.pb_ktmp.ensure(E.mem, te);
     S.pb_ekey.ensure(E.mem, te);

@@ -167,6 +167,48 @@ __device__ __forceinline__ double move_gain(double w_to, double w_cur, double tw
   double b = __dmul_rn(__dmul_rn(gamma, kv), __dsub_rn(__dsub_rn(d_cur, kv), d_to));
   return __dadd_rn(a, __ddiv_rn(b, __dmul_rn(tw, tw)));
 }
+// Division-free screening of one vertex's candidates before move_gain.
+//
+// With x = fl(w_to - w_cur), b = fl(fl(γ·k_v)·fl(fl(d_cur - k_v) - d_to)) and
+// c = fl(2m·2m) computed exactly as move_gain computes them, the gain is
+// g = fl(fl(x/2m) + fl(b/c)) while R = x/2m + b/c is its real value, so
+// |g - R| <= 2.01u·(|x|/2m + |b|/c) (u = 2^-53: three roundings).  The proxy
+// Q = fl(fl(x·c) + fl(b·2m)) equals R·2m·c up to 2.01u·T with
+// T = |x·c| + |b·2m|.  If a candidate R' seen before has Q' - Q > 4.02u·(T + T')
+// then R' - R exceeds both gains' rounding errors and g' > g strictly: the
+// candidate can neither win nor tie and needs no exact gain.  keep() tests that
+// with a margin of 16u·(T + T') (and an absolute 1e-300 for subnormal terms),
+// against the largest proxy seen so far; every candidate it keeps gets its
+// exact move_gain and the usual comparison, so the winner and its gain bits
+// are those of the unscreened scan.  Rounding is monotone, so the comparison
+// fl(Q + margin) < Q' implies Q + margin < Q'.
+struct GainScreen {
+  double tw, c, g, dk, wcur, qmax, tmax;
+  __device__ __forceinline__ void init(double w_cur, double tw_, double gamma, double kv,
+                                       double d_cur) {
+    tw = tw_;
+    c = __dmul_rn(tw_, tw_);
+    g = __dmul_rn(gamma, kv);
+    dk = __dsub_rn(d_cur, kv);
+    wcur = w_cur;
+    qmax = -1.0 / 0.0;
+    tmax = 0.0;
+  }
+  __device__ __forceinline__ bool keep(double w_to, double d_to) {
+    const double p1 = __dmul_rn(__dsub_rn(w_to, wcur), c);
+    const double p2 = __dmul_rn(__dmul_rn(g, __dsub_rn(dk, d_to)), tw);
+    const double q = __dadd_rn(p1, p2);
+    const double t = __dadd_rn(fabs(p1), fabs(p2));
+    const double margin = __dadd_rn(__dmul_rn(1.7763568394002505e-15, __dadd_rn(t, tmax)), 1e-300);
+    if (__dadd_rn(q, margin) < qmax) return false;  // 1.776e-15 = 16u
+    if (q > qmax) {
+      qmax = q;
+      tmax = t;
+    }
+    return true;
+  }
+};
+
 // Gain of moving to the empty community (parallel_frontier.rs:207-211).
 __device__ __forceinline__ double empty_gain(double w_cur, double tw, double gamma, double kv,
                                              double d_cur) {
