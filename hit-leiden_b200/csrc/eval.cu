@@ -1014,6 +1014,8 @@ __device__ __forceinline__ u32 pb_bucket(u32 key, u32 B) {
 }
 
 struct PbArgs {
+  const u32* border;   // the round's buckets, most entries first (fold order)
+  u32* fold_work;      // next position of border a fold block takes
   const u32* ovf;      // deferred idx values
   const u32* nb;       // buckets per row
   const u64* ebase;    // exclusive scan of row degrees
@@ -1045,6 +1047,14 @@ struct PbArgs {
   const u64* ro0;
   const u64* ne;       // per row: degree
 };
+
+// Sort keys of the fold order: each bucket's entry count, and its index.
+__global__ void k_pb_order_keys(const u32* boff, u32 nb, u32* key, u32* val) {
+  for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < nb; t += (u64)gridDim.x * blockDim.x) {
+    key[t] = boff[t + 1] - boff[t];
+    val[t] = (u32)t;
+  }
+}
 
 // Per row of the pass: its scalars, and its entries in the bucket -> row and
 // chunk -> row maps (a warp per row).
@@ -1207,7 +1217,7 @@ __global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
   unsigned short* s_list = reinterpret_cast<unsigned short*>(s_tp + PB_TAB);
   __shared__ double r_g[8];
   __shared__ u32 r_p[8], r_k[8];
-  __shared__ u32 s_ovf, s_nused;
+  __shared__ u32 s_ovf, s_nused, s_item;
   __shared__ unsigned long long s_wb[8][32];  // a chunk's weights, per warp
   __shared__ u32 s_pb[8][32];                 // and positions
   const u32 tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
@@ -1217,7 +1227,15 @@ __global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
     s_tp[x] = NONE32;
     s_tv[x] = 0ull;
   }
-  for (u32 bl = blockIdx.x; bl < nbuckets; bl += gridDim.x) {
+  // Buckets are taken largest first from a shared counter, so that a hub's
+  // heavy-key bucket (a large community holding much of its row) starts at
+  // once instead of trailing the launch.
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(P.fold_work, 1u);
+    __syncthreads();
+    const u32 item = s_item;
+    if (item >= nbuckets) break;
+    const u32 bl = P.border[item];
     const u32 b = P.b0 + bl;
     const u32 r = P.brow[b];
     if (tid == 0) {
@@ -1557,7 +1575,7 @@ static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
       a, S.ovf.p, m, S.pb_nb.p, S.pb_bbase.p, S.pb_nc.p, S.pb_cbase.p, S.pb_brow.p, S.pb_crow.p,
       S.pb_rv.p, S.pb_rfv.p, S.pb_rcur.p, S.pb_rkv.p, S.pb_rdcur.p, S.pb_ro0.p);
   HL_LAUNCH_CHECK();
-  PbArgs P;
+  PbArgs P{};
   P.ovf = S.ovf.p;
   P.nb = S.pb_nb.p;
   P.ebase = S.pb_ebase.p;
@@ -1623,6 +1641,28 @@ static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
     }
     HL_CUDA(cudaMemsetAsync(S.pb_bcnt.p, 0, sizeof(u32) * ((size_t)tb + 1), st));
     ++E.nlaunch, k_pb_scatter<<<cgrid, 256, 0, st>>>(a, P);
+    // fold order: buckets by entry count, largest first
+    S.pb_okey.ensure(E.mem, tb);
+    S.pb_okey2.ensure(E.mem, tb);
+    S.pb_oval.ensure(E.mem, tb);
+    S.pb_ord.ensure(E.mem, tb);
+    S.pb_fwork.ensure(E.mem, 1);
+    ++E.nlaunch, k_pb_order_keys<<<grid_for(tb), 256, 0, st>>>(S.pb_boff.p, tb, S.pb_okey.p,
+                                                                S.pb_oval.p);
+    {
+      u32* ki = S.pb_okey.p;
+      u32* ko = S.pb_okey2.p;
+      u32* vi = S.pb_oval.p;
+      u32* vo = S.pb_ord.p;
+      const int kb = bits_for(te);
+      cub_run(E, [&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairsDescending(t, b, ki, ko, vi, vo, (int64_t)tb, 0,
+                                                         kb, st);
+      });
+    }
+    HL_CUDA(cudaMemsetAsync(S.pb_fwork.p, 0, sizeof(u32), st));
+    P.border = S.pb_ord.p;
+    P.fold_work = S.pb_fwork.p;
     const u32 fgrid = tb < 148u * 8u ? tb : 148u * 8u;
     u32 lim = g_pb_slots.load();
     if (lim < 64 || lim > PB_TAB) lim = PB_TAB;

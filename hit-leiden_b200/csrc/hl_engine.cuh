@@ -104,6 +104,7 @@ struct Scratch {
   DBuf<u64> pb_ne, pb_ebase, pb_ro0;
   DBuf<double> pb_wcur, pb_ew, pb_bg, pb_rkv, pb_rdcur;
   DBuf<u32> pb_brow, pb_crow, pb_rv, pb_rfv, pb_rcur;  // bucket / chunk -> row; row scalars
+  DBuf<u32> pb_okey, pb_okey2, pb_oval, pb_ord, pb_fwork;  // fold order (largest bucket first)
   DBuf<unsigned long long> mark_long;  // (rank << 32 | segment) of long moved rows
   DBuf<u32> mark_long_cnt;
   // batch statistics accumulated on the device and read once at the end of
