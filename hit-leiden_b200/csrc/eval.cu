@@ -968,17 +968,17 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-// Second pass for integral weights: the rows deferred by pass 1 (more than
-// BIG_TAB / 2 distinct keys) are hash-partitioned into buckets that fit a
-// shared-memory table, so that every block of the GPU folds one bucket
-// instead of a few blocks walking global tables.  Integral sums are exact in
+// Second pass for integral weights: the rows deferred by pass 1 (long rows,
+// or more than BIG_TAB / 2 distinct keys) are hash-partitioned into buckets
+// that fit a warp's shared-memory table, so that every warp of the GPU folds
+// one bucket instead of a few blocks walking global tables.  Integral sums are exact in
 // any order, and a key's first CSR position is the minimum of its entries'
 // positions, so neither the partition order nor the fold order matters.
 //   plan     per row: buckets B = 2^k >= deg / PB_TARGET, 4096-entry chunks;
 //   hist     per chunk: each entry's key (saved), its bucket's count, and the
 //            row's w(v, cur);
 //   scatter  per chunk: (key, position, weight) into its bucket's range;
-//   fold     per bucket: shared table, then the bucket's best candidate;
+//   fold     per bucket: a warp's shared table, then the bucket's best candidate;
 //   final    per row: the best over its buckets, then the empty community.
 // A bucket holds at most about PB_TARGET entries plus the repeats of its
 // keys (a heavy key adds entries, not keys), so its distinct keys fit a
@@ -986,8 +986,8 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
 // in the tail of the hash spread) fails its row, which then takes the
 // global-table pass.
 // ---------------------------------------------------------------------------
-constexpr u32 PB_TARGET = 1024;  // expected entries per bucket
-constexpr u32 PB_TAB = 2048;     // table slots of the fold kernel
+constexpr u32 PB_TARGET = 256;  // expected entries per bucket
+constexpr u32 PB_TAB = 512;     // table slots of a fold warp
 constexpr u32 PB_CHUNK = 4096;   // entries per block of the hist / scatter kernels
 constexpr u32 PB_HIST = 8192;    // buckets a block counts in shared memory
 constexpr u32 PB_FOLD_UNROLL = 4;  // chunks (or table slots) a fold thread has in flight
@@ -1195,7 +1195,8 @@ __global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
   }
 }
 
-constexpr size_t PB_FOLD_SMEM = (size_t)PB_TAB * (8 + 4 + 4 + 2);
+constexpr u32 PB_FOLD_WARPS = 4;  // warps of a fold block, one bucket each
+constexpr size_t PB_FOLD_SMEM = (size_t)PB_FOLD_WARPS * PB_TAB * (8 + 4 + 4 + 2);
 
 // Table slots the fold kernel may use (hl_dbg_set_bucket_slots lowers it so
 // that tests reach the overflow path).
@@ -1204,60 +1205,55 @@ std::atomic<u32> g_pb_slots{PB_TAB};
 // Hub-row deferral bound forced by hl_dbg_set_hub_defer (0: the handle's).
 std::atomic<u32> g_dbg_hub_defer{0};
 
-// One bucket per block at a time.  The table starts clean and every key
-// inserted is appended to a list (a warp's new keys take their list places
-// with one atomic), so the argmax scan and the reset visit only used slots.
+// One bucket per warp at a time, taken largest first from a shared counter
+// (a hub's heavy-key bucket, a large community holding much of its row,
+// starts at once instead of trailing the launch).  Each warp owns a table
+// in shared memory that starts clean; every key it inserts is appended to
+// the warp's used-slot list, so the argmax scan and the reset visit only used
+// slots, and no block barrier is needed anywhere.
 template <int KIND>
-__global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nbuckets,
-                                                 u32 tab_limit) {
+__global__ void __launch_bounds__(PB_FOLD_WARPS * 32) k_pb_fold(EvalArgs A, PbArgs P,
+                                                                u32 nbuckets, u32 tab_limit) {
   extern __shared__ __align__(16) unsigned char pb_smem[];
-  unsigned long long* s_tv = reinterpret_cast<unsigned long long*>(pb_smem);
-  u32* s_tk = reinterpret_cast<u32*>(s_tv + PB_TAB);
-  u32* s_tp = s_tk + PB_TAB;
-  unsigned short* s_list = reinterpret_cast<unsigned short*>(s_tp + PB_TAB);
-  __shared__ double r_g[8];
-  __shared__ u32 r_p[8], r_k[8];
-  __shared__ u32 s_ovf, s_nused, s_item;
-  __shared__ unsigned long long s_wb[8][32];  // a chunk's weights, per warp
-  __shared__ u32 s_pb[8][32];                 // and positions
-  const u32 tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  const u32 lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  unsigned long long* tv = reinterpret_cast<unsigned long long*>(pb_smem) + (size_t)wib * PB_TAB;
+  u32* tk = reinterpret_cast<u32*>(reinterpret_cast<unsigned long long*>(pb_smem) +
+                                   (size_t)PB_FOLD_WARPS * PB_TAB) + (size_t)wib * PB_TAB;
+  u32* tp = tk + (size_t)PB_FOLD_WARPS * PB_TAB;
+  unsigned short* list = reinterpret_cast<unsigned short*>(
+                             reinterpret_cast<u32*>(pb_smem + (size_t)PB_FOLD_WARPS * PB_TAB * 8) +
+                             (size_t)2 * PB_FOLD_WARPS * PB_TAB) + (size_t)wib * PB_TAB;
+  const u32 lt = (1u << lane) - 1u;
   unsigned long long ncand = 0;
-  for (u32 x = tid; x < PB_TAB; x += 256) {
-    s_tk[x] = NONE32;
-    s_tp[x] = NONE32;
-    s_tv[x] = 0ull;
+  for (u32 x = lane; x < PB_TAB; x += 32) {
+    tk[x] = NONE32;
+    tp[x] = NONE32;
+    tv[x] = 0ull;
   }
-  // Buckets are taken largest first from a shared counter, so that a hub's
-  // heavy-key bucket (a large community holding much of its row) starts at
-  // once instead of trailing the launch.
+  __syncwarp();
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(P.fold_work, 1u);
-    __syncthreads();
-    const u32 item = s_item;
+    u32 item = 0;
+    if (lane == 0) item = atomicAdd(P.fold_work, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= nbuckets) break;
     const u32 bl = P.border[item];
-    const u32 b = P.b0 + bl;
-    const u32 r = P.brow[b];
-    if (tid == 0) {
-      s_ovf = 0;
-      s_nused = 0;
-    }
+    const u32 r = P.brow[P.b0 + bl];
     const u32 e_lo = P.boff[bl], e_hi = P.boff[bl + 1];
     const u32 cnt = e_hi - e_lo;
     u32 cap = 64;
     while (cap < 2 * cnt && cap < tab_limit) cap <<= 1;
-    __syncthreads();
     const u32 mask = cap - 1;
-    // Each warp takes PB_FOLD_UNROLL chunks of 32 entries at a time, their
-    // loads issued together.  Lanes of a chunk that share a key are combined
-    // first (match_any), so a heavy key (a large community holding much of
-    // the row) costs one shared-memory atomic per chunk, not one per entry.
-    for (u32 base = e_lo + wib * 32; base < e_hi; base += 256 * PB_FOLD_UNROLL) {
+    u32 nused = 0;
+    bool ovf = false;
+    // PB_FOLD_UNROLL chunks of 32 entries at a time, their loads issued
+    // together.  Lanes of a chunk that share a key are combined first
+    // (match_any), so a heavy key costs one table update per chunk.
+    for (u32 base = e_lo; base < e_hi; base += 32 * PB_FOLD_UNROLL) {
       u32 ek[PB_FOLD_UNROLL], ep[PB_FOLD_UNROLL];
       unsigned long long ew[PB_FOLD_UNROLL];
 #pragma unroll
       for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
-        const u32 e = base + j * 256 + lane;
+        const u32 e = base + j * 32 + lane;
         const bool ok = e < e_hi;
         ek[j] = ok ? P.ekey[e] : NONE32;
         ep[j] = ok ? P.epos[e] : NONE32;
@@ -1266,39 +1262,37 @@ __global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
       }
 #pragma unroll
       for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
-        if (base + j * 256 >= e_hi) break;  // warp-uniform
+        if (base + j * 32 >= e_hi) break;  // warp-uniform
         const bool ok = ek[j] != NONE32;
         const u32 grp = __match_any_sync(0xffffffffu, ok ? (unsigned long long)ek[j]
                                                          : ((1ull << 32) | lane));
         const bool leader = ok && lane == (u32)(__ffs(grp) - 1);
         // the group's sum and first position: one reduction over the
         // match_any partition when 32 of the weights fit 32 bits, else the
-        // leader adds them up from shared memory
+        // leader adds them up with shuffles
         unsigned long long sum = 0;
         u32 pmin = NONE32;
         if (__all_sync(0xffffffffu, ew[j] < (1ull << 26))) {
           sum = __reduce_add_sync(grp, (u32)ew[j]);
           pmin = __reduce_min_sync(grp, ep[j]);
         } else {
-          s_wb[wib][lane] = ew[j];
-          s_pb[wib][lane] = ep[j];
-          __syncwarp();
-          if (leader)
-            for (u32 m = grp; m; m &= m - 1) {
-              const u32 l = __ffs(m) - 1;
-              sum += s_wb[wib][l];
-              pmin = min(pmin, s_pb[wib][l]);
+          for (u32 l = 0; l < 32; ++l) {
+            const unsigned long long wl = __shfl_sync(0xffffffffu, ew[j], l);
+            const u32 pl = __shfl_sync(0xffffffffu, ep[j], l);
+            if ((grp >> l) & 1u) {
+              sum += wl;
+              pmin = min(pmin, pl);
             }
-          __syncwarp();
+          }
         }
-        bool fresh = false;
+        bool fresh = false, failed = false;
         u32 slot = 0;
         if (leader) {
           slot = hash32(ek[j]) & mask;
           u32 probes = 0;
           bool ins = false;
           while (probes++ < cap) {
-            const u32 prev = atomicCAS(&s_tk[slot], NONE32, ek[j]);
+            const u32 prev = atomicCAS(&tk[slot], NONE32, ek[j]);
             if (prev == NONE32 || prev == ek[j]) {
               ins = true;
               fresh = prev == NONE32;
@@ -1307,51 +1301,46 @@ __global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
             slot = (slot + 1) & mask;
           }
           if (ins) {
-            atomicAdd(&s_tv[slot], sum);
-            atomicMin(&s_tp[slot], pmin);
+            tv[slot] += sum;  // one leader per key in the warp: no atomics needed
+            tp[slot] = min(tp[slot], pmin);
           } else {
-            s_ovf = 1;
+            failed = true;
           }
         }
         const u32 fm = __ballot_sync(0xffffffffu, fresh);
-        if (fm) {
-          u32 at = 0;
-          if (lane == 0) at = atomicAdd(&s_nused, (u32)__popc(fm));
-          at = __shfl_sync(0xffffffffu, at, 0);
-          if (fresh) s_list[at + __popc(fm & ((1u << lane) - 1u))] = (unsigned short)slot;
-        }
+        if (fresh) list[nused + __popc(fm & lt)] = (unsigned short)slot;
+        nused += __popc(fm);
+        ovf |= __any_sync(0xffffffffu, failed);
         __syncwarp();
       }
     }
-    __syncthreads();
     double g = -1.0;
     u32 p = NONE32, kk = NONE32;
-    const u32 nused = s_nused;
-    const bool scan = !s_ovf && A.tw != 0.0;
+    const bool scan = !ovf && A.tw != 0.0;
     const u32 cur = P.rcur[r];
     const double kv = P.rkv[r];
     const double wcur = P.wcur[r];
     const double dcur = P.rdcur[r];
-    // the used slots, PB_FOLD_UNROLL at a time (their community degrees are
-    // gathered together), each reset after it is read
     GainScreen scr;  // exact gains only for candidates that may win
     scr.init(wcur, A.tw, A.gamma, kv, dcur);
-    for (u32 x0 = tid; x0 < nused; x0 += 256 * PB_FOLD_UNROLL) {
+    // the used slots, PB_FOLD_UNROLL per lane at a time (their community
+    // degrees gathered together), each reset after it is read
+    for (u32 x0 = lane; x0 < nused; x0 += 32 * PB_FOLD_UNROLL) {
       u32 key[PB_FOLD_UNROLL], pq[PB_FOLD_UNROLL];
       unsigned long long vq[PB_FOLD_UNROLL];
       double dk[PB_FOLD_UNROLL];
 #pragma unroll
       for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
-        const u32 x = x0 + j * 256;
+        const u32 x = x0 + j * 32;
         key[j] = NONE32;
         if (x >= nused) continue;
-        const u32 sl = s_list[x];
-        key[j] = s_tk[sl];
-        vq[j] = s_tv[sl];
-        pq[j] = s_tp[sl];
-        s_tk[sl] = NONE32;
-        s_tv[sl] = 0ull;
-        s_tp[sl] = NONE32;
+        const u32 sl = list[x];
+        key[j] = tk[sl];
+        vq[j] = tv[sl];
+        pq[j] = tp[sl];
+        tk[sl] = NONE32;
+        tv[sl] = 0ull;
+        tp[sl] = NONE32;
         if (!scan || key[j] == cur) key[j] = NONE32;
         else if (KIND == EVAL_REFINE && A.blocked[key[j]]) key[j] = NONE32;
       }
@@ -1382,24 +1371,12 @@ __global__ void __launch_bounds__(256, 4) k_pb_fold(EvalArgs A, PbArgs P, u32 nb
       }
     }
     if (lane == 0) {
-      r_g[wib] = g;
-      r_p[wib] = p;
-      r_k[wib] = kk;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      for (u32 x = 1; x < 8; ++x)
-        if (r_p[x] != NONE32 && (p == NONE32 || r_g[x] > g || (r_g[x] == g && r_p[x] < p))) {
-          g = r_g[x];
-          p = r_p[x];
-          kk = r_k[x];
-        }
       P.bg[bl] = g;
       P.bp[bl] = p;
       P.bk[bl] = kk;
-      if (s_ovf) P.rowfail[r] = 1;
+      if (ovf) P.rowfail[r] = 1;
     }
-    __syncthreads();
+    __syncwarp();
   }
   block_count(A, 0, ncand);
 }
@@ -1663,10 +1640,11 @@ static u32 huge_partitioned(Engine& E, const EvalArgs& a) {
     HL_CUDA(cudaMemsetAsync(S.pb_fwork.p, 0, sizeof(u32), st));
     P.border = S.pb_ord.p;
     P.fold_work = S.pb_fwork.p;
-    const u32 fgrid = tb < 148u * 8u ? tb : 148u * 8u;
+    const u32 fblocks = (tb + PB_FOLD_WARPS - 1) / PB_FOLD_WARPS;
+    const u32 fgrid = fblocks < 148u * 6u ? fblocks : 148u * 6u;
     u32 lim = g_pb_slots.load();
     if (lim < 64 || lim > PB_TAB) lim = PB_TAB;
-    ++E.nlaunch, k_pb_fold<KIND><<<fgrid, 256, PB_FOLD_SMEM, st>>>(a, P, tb, lim);
+    ++E.nlaunch, k_pb_fold<KIND><<<fgrid, PB_FOLD_WARPS * 32, PB_FOLD_SMEM, st>>>(a, P, tb, lim);
     ++E.nlaunch, k_pb_final<KIND><<<grid_for((u64)(r1 - r0) * 32), 256, 0, st>>>(
         a, P, S.pb_fail.p, S.pb_failcnt.p);
     HL_LAUNCH_CHECK();

@@ -91,7 +91,7 @@ HL_API hl_status hl_dbg_set_exact_tfilter(int32_t on);
  * (dual_mode_test!, hit_leiden.rs:1823-1841) run on both GPU paths. */
 HL_API hl_status hl_dbg_set_mode(uint32_t mode);
 
-/* Table slots (64..2048, 0 = 2048) of the partitioned pass that evaluates
+/* Table slots (64..512, 0 = 512) of the partitioned pass that evaluates
  * long hub rows under integral weights (rows above 8192 entries, or with
  * more than 2048 distinct neighbour keys).  A small table makes buckets
  * overflow, so tests reach the global-table pass those rows fall back to.
