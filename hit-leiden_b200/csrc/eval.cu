@@ -772,12 +772,10 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         const u32 grp = __match_any_sync(0xffffffffu, okk ? (unsigned long long)key
                                                            : ((1ull << 32) | lane));
         const bool leader = okk && lane == (u32)(__ffs(grp) - 1);
-        // the group's integer sum: one reduction over the match_any partition
-        // when 32 of the weights fit 32 bits, else the leader adds them up
-        unsigned long long isum = 0;
-        if (__all_sync(0xffffffffu, !okk || wv < 67108864.0)) {
-          isum = __reduce_add_sync(grp, okk ? (u32)int_of(wv) : 0u);
-        } else {
+        // the group's integer sum: a lane alone in its group has it already;
+        // otherwise its leader adds the group up from shared memory
+        unsigned long long isum = okk ? int_of(wv) : 0ull;
+        if (!__all_sync(0xffffffffu, (grp & (grp - 1)) == 0)) {
           b_w[tid] = wv;
           __syncwarp();
           if (leader) {
@@ -1215,6 +1213,8 @@ template <int KIND>
 __global__ void __launch_bounds__(PB_FOLD_WARPS * 32) k_pb_fold(EvalArgs A, PbArgs P,
                                                                 u32 nbuckets, u32 tab_limit) {
   extern __shared__ __align__(16) unsigned char pb_smem[];
+  __shared__ unsigned long long s_wb[PB_FOLD_WARPS][32];  // a chunk's weights, per warp
+  __shared__ u32 s_pb[PB_FOLD_WARPS][32];                 // and positions
   const u32 lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   unsigned long long* tv = reinterpret_cast<unsigned long long*>(pb_smem) + (size_t)wib * PB_TAB;
   u32* tk = reinterpret_cast<u32*>(reinterpret_cast<unsigned long long*>(pb_smem) +
@@ -1267,23 +1267,25 @@ __global__ void __launch_bounds__(PB_FOLD_WARPS * 32) k_pb_fold(EvalArgs A, PbAr
         const u32 grp = __match_any_sync(0xffffffffu, ok ? (unsigned long long)ek[j]
                                                          : ((1ull << 32) | lane));
         const bool leader = ok && lane == (u32)(__ffs(grp) - 1);
-        // the group's sum and first position: one reduction over the
-        // match_any partition when 32 of the weights fit 32 bits, else the
-        // leader adds them up with shuffles
-        unsigned long long sum = 0;
-        u32 pmin = NONE32;
-        if (__all_sync(0xffffffffu, ew[j] < (1ull << 26))) {
-          sum = __reduce_add_sync(grp, (u32)ew[j]);
-          pmin = __reduce_min_sync(grp, ep[j]);
-        } else {
-          for (u32 l = 0; l < 32; ++l) {
-            const unsigned long long wl = __shfl_sync(0xffffffffu, ew[j], l);
-            const u32 pl = __shfl_sync(0xffffffffu, ep[j], l);
-            if ((grp >> l) & 1u) {
-              sum += wl;
-              pmin = min(pmin, pl);
+        // the group's sum and first position: a lane alone in its group has
+        // them already; otherwise its leader adds the group up from shared
+        // memory (as many steps as the largest group of the chunk)
+        unsigned long long sum = ew[j];
+        u32 pmin = ep[j];
+        if (!__all_sync(0xffffffffu, (grp & (grp - 1)) == 0)) {
+          s_wb[wib][lane] = ew[j];
+          s_pb[wib][lane] = ep[j];
+          __syncwarp();
+          if (leader) {
+            sum = 0;
+            pmin = NONE32;
+            for (u32 m = grp; m; m &= m - 1) {
+              const u32 l = __ffs(m) - 1;
+              sum += s_wb[wib][l];
+              pmin = min(pmin, s_pb[wib][l]);
             }
           }
+          __syncwarp();
         }
         bool fresh = false, failed = false;
         u32 slot = 0;
