@@ -96,6 +96,33 @@ __device__ __forceinline__ double dbl_of(unsigned long long s) {
   return __dsub_rn(__longlong_as_double((long long)(s + TWO52_BITS)), TWO52);
 }
 
+// Sum and smallest position of each match_any group of a warp (grp: this
+// lane's group; w < 2^26 on every lane, so a group's sum fits 32 bits).  A
+// lane alone in its group keeps its own values.  The groups of two or more
+// lanes (in a chunk of a hub row these are its few heavy keys) take one
+// full-warp reduction each: reductions whose lanes name different masks
+// would run once per distinct mask, which a chunk of mostly distinct keys
+// turns into 32.
+__device__ __forceinline__ void group_sums(u32 grp, u32 lane, bool valid, u32 w, u32 pos,
+                                           unsigned long long& sum, u32& pmin) {
+  sum = w;
+  pmin = pos;
+  u32 multi = __ballot_sync(0xffffffffu, valid && (grp & (grp - 1)) != 0 &&
+                                              lane == (u32)(__ffs(grp) - 1));
+  while (multi) {
+    const u32 l = __ffs(multi) - 1;
+    const u32 gm = __shfl_sync(0xffffffffu, grp, l);
+    const bool in = (gm >> lane) & 1u;
+    const u32 s = __reduce_add_sync(0xffffffffu, in ? w : 0u);
+    const u32 m = __reduce_min_sync(0xffffffffu, in ? pos : 0xFFFFFFFFu);
+    if (lane == l) {
+      sum = s;
+      pmin = m;
+    }
+    multi &= multi - 1;
+  }
+}
+
 template <int KIND>
 __device__ __forceinline__ bool entry_key(const EvalArgs& A, u32 v, u32 nb, u32 fv, u32& key) {
   if (KIND == EVAL_MOVE) {
@@ -775,7 +802,10 @@ __global__ void __launch_bounds__(BIG_THREADS) k_eval_big(EvalArgs A) {
         // the group's integer sum: a lane alone in its group has it already;
         // otherwise its leader adds the group up from shared memory
         unsigned long long isum = okk ? int_of(wv) : 0ull;
-        if (!__all_sync(0xffffffffu, (grp & (grp - 1)) == 0)) {
+        if (__all_sync(0xffffffffu, isum < (1ull << 26))) {
+          u32 pdummy;
+          group_sums(grp, lane, okk, (u32)isum, 0u, isum, pdummy);
+        } else if (!__all_sync(0xffffffffu, (grp & (grp - 1)) == 0)) {
           b_w[tid] = wv;
           __syncwarp();
           if (leader) {
@@ -1272,7 +1302,9 @@ __global__ void __launch_bounds__(PB_FOLD_WARPS * 32) k_pb_fold(EvalArgs A, PbAr
         // memory (as many steps as the largest group of the chunk)
         unsigned long long sum = ew[j];
         u32 pmin = ep[j];
-        if (!__all_sync(0xffffffffu, (grp & (grp - 1)) == 0)) {
+        if (__all_sync(0xffffffffu, ew[j] < (1ull << 26))) {
+          group_sums(grp, lane, ok, (u32)ew[j], ep[j], sum, pmin);
+        } else if (!__all_sync(0xffffffffu, (grp & (grp - 1)) == 0)) {
           s_wb[wib][lane] = ew[j];
           s_pb[wib][lane] = ep[j];
           __syncwarp();
