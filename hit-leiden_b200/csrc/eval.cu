@@ -1177,20 +1177,8 @@ __global__ void __launch_bounds__(256) k_pb_hist(EvalArgs A, PbArgs P) {
   }
 }
 
-// Rows of at most PB_SCAT_LOCAL buckets are scattered a chunk at a time:
-// each entry first takes its rank among the chunk's entries of its bucket
-// (shared-memory counters), then each bucket the chunk touches reserves its
-// run with one global atomic, and the entries are written to consecutive
-// slots.  Longer rows (more buckets than a chunk has entries to spread) take
-// their slots per warp group directly.
-constexpr u32 PB_SCAT_LOCAL = 2048;
-
 __global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
-  __shared__ u32 s_cnt[PB_SCAT_LOCAL];
-  __shared__ u32 s_base[PB_SCAT_LOCAL];
-  __shared__ unsigned short s_rank[PB_CHUNK];
   const u32 lane = threadIdx.x & 31;
-  const u32 lt = (1u << lane) - 1u;
   for (u32 c = P.c0 + blockIdx.x; c < P.c1; c += gridDim.x) {
     const u32 r = P.crow[c];
     const u64 o0 = P.ro0[r], o1 = o0 + P.ne[r];
@@ -1200,49 +1188,6 @@ __global__ void __launch_bounds__(256) k_pb_scatter(EvalArgs A, PbArgs P) {
     u32* cursor = P.bcnt + (P.bbase[r] - P.b0);
     const u32* start = P.boff + (P.bbase[r] - P.b0);
     const u64 ebase = P.ebase[r] - P.e0 + (lo - o0);
-    if (B <= PB_SCAT_LOCAL) {
-      for (u32 x = threadIdx.x; x < B; x += blockDim.x) s_cnt[x] = 0;
-      __syncthreads();
-      // ranks within the chunk's share of each bucket (lanes of a warp bound
-      // for the same bucket take theirs with one shared atomic)
-      for (u64 w0 = lo + (threadIdx.x & ~31u); w0 < hi; w0 += 256 * PB_FOLD_UNROLL) {
-        u32 key[PB_FOLD_UNROLL];
-#pragma unroll
-        for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
-          const u64 q = w0 + lane + j * 256;
-          key[j] = q < hi ? P.ktmp[ebase + (q - lo)] : NONE32;
-        }
-#pragma unroll
-        for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
-          const u64 q = w0 + lane + j * 256;
-          const bool ok = key[j] != NONE32;
-          const u32 b = ok ? pb_bucket(key[j], B) : 0u;
-          const u32 grp = __match_any_sync(0xffffffffu, ok ? (unsigned long long)b
-                                                           : ((1ull << 32) | lane));
-          const u32 leader = __ffs(grp) - 1;
-          u32 at = 0;
-          if (ok && lane == leader) at = atomicAdd(&s_cnt[b], (u32)__popc(grp));
-          at = __shfl_sync(0xffffffffu, at, leader);
-          if (ok) s_rank[q - lo] = (unsigned short)(at + __popc(grp & lt));
-        }
-      }
-      __syncthreads();
-      for (u32 x = threadIdx.x; x < B; x += blockDim.x) {
-        const u32 n = s_cnt[x];
-        if (n) s_base[x] = start[x] + atomicAdd(&cursor[x], n);
-      }
-      __syncthreads();
-      for (u64 q = lo + threadIdx.x; q < hi; q += blockDim.x) {
-        const u32 key = P.ktmp[ebase + (q - lo)];
-        if (key == NONE32) continue;
-        const u32 slot = s_base[pb_bucket(key, B)] + s_rank[q - lo];
-        P.ekey[slot] = key;
-        P.epos[slot] = (u32)(q - o0);
-        P.ew[slot] = A.w[q];
-      }
-      __syncthreads();
-      continue;
-    }
     // PB_FOLD_UNROLL entries per thread in flight; lanes bound for the same
     // bucket take their slots with one atomic (a heavy key fills one bucket)
     for (u64 w0 = lo + (threadIdx.x & ~31u); w0 < hi; w0 += 256 * PB_FOLD_UNROLL) {
