@@ -232,15 +232,20 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """Per-launch DRAM bytes of the evaluation kernel from the committed ncu
-    summary, scaled to the bench's launch (see profiles/)."""
-    p = os.path.join(ROOT, "profiles", "move_eval_traffic.json")
-    if os.path.exists(p):
-        try:
-            return json.load(open(p))
-        except Exception:
-            return None
+def committed_traffic(config=None):
+    """DRAM bytes per algorithmic byte of the movement evaluation from the
+    committed ncu summary of `config` (profiles/move_eval_traffic_<config>.json,
+    else the older single-configuration file), scaled to the bench's launch."""
+    names = ([f"move_eval_traffic_{config}.json"] if config else []) + ["move_eval_traffic.json"]
+    for name in names:
+        p = os.path.join(ROOT, "profiles", name)
+        if os.path.exists(p):
+            try:
+                tr = json.load(open(p))
+            except Exception:
+                continue
+            if config is None or tr.get("config") == config:
+                return tr
     return None
 
 
@@ -838,9 +843,9 @@ def run_rmat(args, cfg):
     dev_ms, host_s, launches, traversed, clk = _timed_steps(L, h, pinned[Wm:], n, rep,
                                                            Clocks(local))
     kernels = _kernel_table(L, h)
-    tr = committed_traffic()
-    ratio = (tr or {}).get("traffic_per_algorithmic_byte") if (tr or {}).get(
-        "config") == args.config else None
+    # the committed ratio is measured at scale 25; the small case has none
+    tr = None if args.ncu_small else committed_traffic(args.config)
+    ratio = (tr or {}).get("traffic_per_algorithmic_byte")
     config = {"workload": cfg["workload"], "scale": scale, "vertices": n, "edges": int(m),
               "batch_edges": k, "levels": st.levels, "parallelism": f"replicas{rep.world}",
               "l2": "inputs larger than L2 (resident CSR > 126 MB); no flush",
@@ -1001,9 +1006,8 @@ def main():
     L.check(L.lib.hl_reset_kernel_stats(h))
     dev_ms, host_s, launches, traversed, clk = _timed_steps(L, h, pinned, n, rep, Clocks(local))
     kernels = _kernel_table(L, h)
-    tr = committed_traffic()
-    ratio = (tr or {}).get("traffic_per_algorithmic_byte") if (tr or {}).get(
-        "config") == args.config else None
+    tr = None if args.ncu_small else committed_traffic(args.config)
+    ratio = (tr or {}).get("traffic_per_algorithmic_byte")
     config = {"workload": cfg["workload"], "vertices": n, "edges": int(len(s)),
               "batch_edges": k, "levels": st.levels, "parallelism": f"replicas{world}",
               "l2": "inputs larger than L2 (resident CSR > 126 MB); no flush",
