@@ -1019,7 +1019,6 @@ constexpr u32 PB_TAB = 512;     // table slots of a fold warp
 constexpr u32 PB_CHUNK = 4096;   // entries per block of the hist / scatter kernels
 constexpr u32 PB_HIST = 8192;    // buckets a block counts in shared memory
 constexpr u32 PB_FOLD_UNROLL = 4;  // chunks (or table slots) a fold thread has in flight
-constexpr u32 PB_HIST_UNROLL = 8;  // entries a hist thread gathers at a time
 
 __global__ void k_pb_plan(const u32* ovf, const u32* novf, const u32* verts, const u64* off,
                           u32* nb, u64* ne, u32* nc) {
@@ -1134,22 +1133,22 @@ __global__ void __launch_bounds__(256) k_pb_hist(EvalArgs A, PbArgs P) {
     double wc = 0.0;
     const u64 ebase = P.ebase[r] - P.e0 + (lo - o0);
     const u32 lane = threadIdx.x & 31;
-    // PB_HIST_UNROLL entries per thread in flight (neighbours, then their
+    // PB_FOLD_UNROLL entries per thread in flight (neighbours, then their
     // keys); lanes counting into the same bucket add once
-    for (u64 w0 = lo + (threadIdx.x & ~31u); w0 < hi; w0 += 256 * PB_HIST_UNROLL) {
-      u32 nb[PB_HIST_UNROLL], key[PB_HIST_UNROLL];
+    for (u64 w0 = lo + (threadIdx.x & ~31u); w0 < hi; w0 += 256 * PB_FOLD_UNROLL) {
+      u32 nb[PB_FOLD_UNROLL], key[PB_FOLD_UNROLL];
 #pragma unroll
-      for (u32 j = 0; j < PB_HIST_UNROLL; ++j) {
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
         const u64 q = w0 + j * 256 + lane;
         nb[j] = q < hi ? A.col[q] : NONE32;
       }
 #pragma unroll
-      for (u32 j = 0; j < PB_HIST_UNROLL; ++j) {
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
         key[j] = NONE32;
         if (nb[j] != NONE32 && !entry_key<KIND>(A, v, nb[j], fv, key[j])) key[j] = NONE32;
       }
 #pragma unroll
-      for (u32 j = 0; j < PB_HIST_UNROLL; ++j) {
+      for (u32 j = 0; j < PB_FOLD_UNROLL; ++j) {
         const u64 q = w0 + j * 256 + lane;
         if (q < hi) P.ktmp[ebase + (q - lo)] = key[j];
         const bool ok = key[j] != NONE32;
