@@ -383,6 +383,41 @@ def test_move_eval_hub_paths_bit_exact(defer):
         assert np.array_equal(to_o[pos], to_g[pos])
 
 
+# ---- integral weights too large for a 32-bit group sum (>= 2^26 each): the
+# lanes that share a key are added up by their leader instead -----------------
+@pytest.mark.parametrize("defer", [1, 0xFFFFFFFF])
+def test_move_eval_hub_large_integral_weights(defer):
+    rng = np.random.default_rng(7 + (defer & 3))
+    n = 30000
+    src, dst, w = gh.random_graph(rng, n, 20000, True)
+    w = w * float(1 << 27)
+    hubs = [(0, 1500), (1, 12000)]
+    hs, hd = [], []
+    for h, deg in hubs:
+        hs.append(np.full(deg, h, np.uint32))
+        hd.append(rng.choice(np.arange(10, n), deg, replace=False).astype(np.uint32))
+    hw = rng.integers(1 << 27, 1 << 30, sum(d for _, d in hubs)).astype(float)
+    g = O.Graph.from_edges(n, np.concatenate([src] + hs), np.concatenate([dst] + hd),
+                           np.concatenate([w, hw])).apply_delta([], [], [], keep_self_loops=True)
+    k = g.degrees()
+    tw = O.tree_sum(k)
+    assert tw < 2.0 ** 52  # integral sums stay exact
+    for ncomm in [5, 2000]:
+        f = gh.random_partition(rng, n, ncomm)
+        heavy = hd[-1][: len(hd[-1]) // 2]  # half of the big hub's row in one key
+        f[heavy] = f[hd[-1][0]]
+        d = np.zeros(2 * n + 2)
+        np.add.at(d, f, k)
+        verts = np.concatenate([np.arange(2, dtype=np.uint32),
+                                np.arange(2, n, 13, dtype=np.uint32)])
+        to_o, g_o = O.move_eval(g, f, d, k, tw, 1.0, verts)
+        with gh.hub_defer(defer):
+            to_g, g_g = gh.move_eval(g, f, d, k, tw, 1.0, verts)
+        assert gh.same_bits(g_o, g_g)
+        pos = g_o > 0
+        assert np.array_equal(to_o[pos], to_g[pos])
+
+
 # ---- very high degree vertices (block kernel, shared and global tables) -----
 @pytest.mark.parametrize("integral", [True, False])
 @pytest.mark.parametrize("hub_deg", [300, 3000, 6000, 20000])
