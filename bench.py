@@ -135,7 +135,8 @@ def parse():
     ap.add_argument("--cpu-variant-run", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-variant-mode", default="throughput", help=argparse.SUPPRESS)
     ap.add_argument("--ncu-small", action="store_true",
-                    help="small case for ncu captures (200k vertices)")
+                    help="small case for ncu captures (rmat25: R-MAT scale 20 with 1M/32-update "
+                         "batches; lfr1m: 200k vertices)")
     ap.add_argument("--workers", type=int, default=16,
                     help="host worker threads of the batching / serving forms")
     ap.add_argument("--scale", type=float, default=1.0,
