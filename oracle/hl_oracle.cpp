@@ -28,7 +28,7 @@
 //     bounds there (`community_degrees` sized n, hit_leiden.rs:1060-1066).
 //   * run()'s thread_rng shuffle is replaced by a seeded splitmix64 shuffle.
 //
-// Build: oracle/Makefile (g++ -O2 -ffp-contract=off, so that a*b+c is never
+// Build: oracle/Makefile (g++ -O3 -ffp-contract=off, so that a*b+c is never
 // fused: the gain formulas must round exactly like the reference's f64 code).
 
 #include <algorithm>
@@ -39,6 +39,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <set>
 #include <unordered_map>
 #include <unordered_set>
@@ -452,10 +453,163 @@ struct MoveOut {
 // hit_leiden.rs:1024-1192 (`inc_movement`) with the throughput branch
 // (:1068-1101 → throughput.rs:80-202) and the deterministic branch
 // (:1103-1191).
+// ---------------------------------------------------------------------------
+// Round-to-round hub key sums (OR_FLAG_HUB_CHECK; test infrastructure, not a
+// restatement of the reference).  Between two throughput rounds only the
+// moved vertices' labels change, so a long row's per-key weight sums can be
+// kept and corrected by its moved neighbours instead of being recomputed.
+// The table keeps, per key, the sum, the first CSR position, and whether that
+// position may be out of date (its entry moved to another key); it is
+// recomputed only when the key ties the best gain, the one place the tie
+// rule reads it.  Exact for integral weights, where sums do not depend on the
+// order of additions; the check compares every such evaluation with the full
+// one (eval_move).
+// ---------------------------------------------------------------------------
+constexpr u64 HUB_CHECK_DEG = 512;
+static std::atomic<unsigned long long> g_hub_check[6];  // see or_hub_check_counters
+
+struct HubCheck {
+  struct Ent {
+    double sum;
+    u64 first;
+    bool stale;
+  };
+  const Graph& g;
+  std::unordered_map<u32, std::unordered_map<u32, Ent>> tabs;
+  explicit HubCheck(const Graph& gr) : g(gr) {}
+
+  u64 first_pos(u32 v, u32 key, const std::vector<u32>& f) const {
+    for (u64 q = g.off[v]; q < g.off[v + 1]; ++q)
+      if (g.col[q] != v && f[g.col[q]] == key) return q - g.off[v];
+    return ~0ull;
+  }
+
+  // The evaluation eval_move makes (empty community allowed), from v's table.
+  Eval eval(u32 v, const std::vector<u32>& f, const std::vector<double>& d,
+            const std::vector<double>& k, double tw, double gamma) {
+    auto it = tabs.find(v);
+    if (it == tabs.end()) {
+      std::unordered_map<u32, Ent> tb;
+      for (u64 q = g.off[v]; q < g.off[v + 1]; ++q) {
+        const u32 nb = g.col[q];
+        if (nb == v) continue;
+        auto r = tb.find(f[nb]);
+        if (r == tb.end()) tb[f[nb]] = Ent{g.w[q], q - g.off[v], false};
+        else r->second.sum += g.w[q];
+      }
+      it = tabs.emplace(v, std::move(tb)).first;
+      ++g_hub_check[4];
+    }
+    auto& tb = it->second;
+    const u32 cur = f[v];
+    const double kv = k[v];
+    auto rc = tb.find(cur);
+    const double wcur = rc == tb.end() ? 0.0 : rc->second.sum;
+    const double dcur = d[cur];
+    u32 best = cur;
+    double bestg = 0.0;
+    for (auto& kvp : tb) {
+      ++g_hub_check[5];
+      const u32 c = kvp.first;
+      Ent& e = kvp.second;
+      if (c == cur || e.sum == 0.0) continue;
+      const double gn = move_gain(e.sum, wcur, tw, gamma, kv, dcur, d[c]);
+      if (gn <= bestg && !(gn == bestg && gn > 0.0)) continue;
+      if (gn == bestg) {  // a tie: the first position decides
+        for (Ent* x : {&e, &tb[best]})
+          if (x->stale) {
+            x->first = first_pos(v, x == &e ? c : best, f);
+            x->stale = false;
+            ++g_hub_check[2];
+          }
+        if (e.first < tb[best].first) best = c;
+        continue;
+      }
+      bestg = gn;
+      best = c;
+    }
+    const double eg = empty_gain(wcur, tw, gamma, kv, dcur);
+    if (eg > bestg) {
+      bestg = eg;
+      best = g.n + v;
+    }
+    return {best, bestg};
+  }
+
+  // The round's accepted moves: each moved vertex's entry in the tables of
+  // its neighbours, found by binary search (rows are sorted by neighbour).
+  void correct(const std::vector<Move>& sel) {
+    for (const Move& m : sel) {
+      for (u64 pm = g.off[m.node]; pm < g.off[m.node + 1]; ++pm) {
+        const u32 h = g.col[pm];
+        if (h == m.node) continue;
+        auto ih = tabs.find(h);
+        if (ih == tabs.end()) continue;
+        u64 lo = g.off[h], hi = g.off[h + 1];
+        while (hi - lo > 1) {
+          const u64 mid = (lo + hi) / 2;
+          if (g.col[mid] <= m.node) lo = mid;
+          else hi = mid;
+        }
+        const u64 q = lo - g.off[h];
+        const double w = g.w[lo];
+        auto& tb = ih->second;
+        Ent& ef = tb[m.from];
+        ef.sum -= w;
+        if (!ef.stale && ef.first == q) ef.stale = true;
+        auto rt = tb.find(m.to);
+        if (rt == tb.end() || rt->second.sum == 0.0) {
+          tb[m.to] = Ent{w, q, false};
+        } else {
+          rt->second.sum += w;
+          if (!rt->second.stale) rt->second.first = std::min(rt->second.first, q);
+        }
+        ++g_hub_check[3];
+      }
+    }
+  }
+};
+
+// A fixed case for the stale first position: hub 0 with unit edges to 1..7;
+// communities 10 = {1, 2, 7} and 20 = {3, 4} of equal degree.  Vertex 1 (the
+// first entry of key 10) moves to 40, so 10's first position goes stale and
+// 10 and 20 then tie (two entries each): the tie rule needs 10's true first
+// position (vertex 2) to pick 10.  Returns the rescans made, or -1 when an
+// evaluation differs from eval_move.
+static int hub_check_selftest() {
+  std::vector<Edge> e;
+  for (u32 x = 1; x <= 7; ++x) e.push_back({0, x, 1.0});
+  const Graph g = graph_from_edges(50, e);
+  std::vector<u32> f(50);
+  for (u32 x = 0; x < 50; ++x) f[x] = x;
+  f[1] = f[2] = f[7] = 10;
+  f[3] = f[4] = 20;
+  const std::vector<double> k = node_degrees(g);
+  const double tw = twice_total_weight(k);
+  std::vector<double> d(101, 0.0);
+  d[10] = d[20] = 3.0;
+  d[0] = k[0];
+  d[5] = d[6] = 10.0;  // the singletons 5 and 6 and the new community 40 lose
+  d[40] = 5.0;
+  MoveScratch sc;
+  sc.buf.assign(d.size() + g.n + 1, 0.0);
+  HubCheck hub(g);
+  const unsigned long long r0 = g_hub_check[2].load();
+  Eval a = hub.eval(0, f, d, k, tw, 1.0);
+  Eval b = eval_move(g, 0, f, d, k, tw, 1.0, true, sc);
+  if (a.to != b.to || a.gain != b.gain) return -1;
+  f[1] = 40;
+  hub.correct({Move{1, 10, 40, k[1], 0.0}});
+  a = hub.eval(0, f, d, k, tw, 1.0);
+  b = eval_move(g, 0, f, d, k, tw, 1.0, true, sc);
+  if (a.to != b.to || a.gain != b.gain || a.to != 10) return -1;
+  return (int)(g_hub_check[2].load() - r0);
+}
+
 static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std::vector<u32>& f,
                             const std::vector<u32>& s, double gamma, int mode, u32 max_rounds,
                             bool compact, bool mark_moved = false,
-                            const std::vector<u32>* extra_k = nullptr) {
+                            const std::vector<u32>* extra_k = nullptr, u64 hub_check_deg = 0) {
   u32 n = g.n;
   MoveOut out;
   out.changed.assign(n, 0);
@@ -490,6 +644,8 @@ static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std:
       if (active[i]) act.push_back(i);
     u32 it = 0;
     std::vector<Eval> ev;
+    std::unique_ptr<HubCheck> hub;
+    if (hub_check_deg) hub.reset(new HubCheck(g));
     while (!act.empty() && it < max_rounds) {
       // Every active vertex is evaluated on the same snapshot (the reference
       // runs these with rayon, throughput.rs:80-202), so the evaluations run
@@ -506,6 +662,14 @@ static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std:
           [&](size_t i, MoveScratch& tsc) {
             ev[i] = eval_move(g, act[i], f, d, k, tw, gamma, true, tsc);
           });
+      if (hub) {
+        for (size_t i = 0; i < act.size(); ++i) {
+          if (g.deg(act[i]) <= hub_check_deg) continue;
+          const Eval e = hub->eval(act[i], f, d, k, tw, gamma);
+          ++g_hub_check[0];
+          if (e.to != ev[i].to || e.gain != ev[i].gain) ++g_hub_check[1];
+        }
+      }
       std::vector<Move> cand;
       for (size_t i = 0; i < act.size(); ++i) {
         const u32 v = act[i];
@@ -534,6 +698,7 @@ static MoveOut inc_movement(const Graph& g, const std::vector<Edge>& delta, std:
         if (mark_moved) out.affected[m.node] = 1;
       }
       out.rounds_moves += sel.size();
+      if (hub) hub->correct(sel);
       for (const Move& m : sel) {
         for (u64 p = g.off[m.node]; p < g.off[m.node + 1]; ++p) {
           u32 nb = g.col[p];
@@ -1095,7 +1260,8 @@ static u32 hit_leiden(State& st, u32 delta_n, const std::vector<Edge>& delta, do
     grow_map(st.g[p], np);
     grow_map(st.s_pre[p], np);
     grow_map(st.s_cur[p], np);
-    MoveOut mo = inc_movement(st.sg[p], cur, st.f[p], st.s_cur[p], gamma, mode, max_rounds, compact);
+    MoveOut mo = inc_movement(st.sg[p], cur, st.f[p], st.s_cur[p], gamma, mode, max_rounds, compact,
+                              false, nullptr, (flags & OR_FLAG_HUB_CHECK) ? HUB_CHECK_DEG : 0);
     total_it += mo.iterations;
     RefineOut ro = inc_refinement(st.sg[p], st.f[p], st.s_cur[p], mo.affected, gamma, mode, faithful);
     if (stats) {
@@ -1189,7 +1355,8 @@ static u32 hit_leiden_ml(State& st, const std::vector<Edge>& delta, double gamma
     st.sg[p] = apply_delta(st.sg[p], std::max(cur_n, st.sg[p].n), cur, true);
     ensure_level_size(st, p, st.sg[p].n);
     MoveOut mo = inc_movement(st.sg[p], cur, st.f[p], st.s_cur[p], gamma, mode, max_rounds,
-                              compact, true, &gained);
+                              compact, true, &gained,
+                              (flags & OR_FLAG_HUB_CHECK) ? HUB_CHECK_DEG : 0);
     total_it += mo.iterations;
     RefineOut ro =
         inc_refinement(st.sg[p], st.f[p], st.s_cur[p], mo.affected, gamma, mode, faithful, true);
@@ -1995,6 +2162,12 @@ double or_run(uint32_t n, const uint32_t* src, const uint32_t* dst, const double
   if (out_part) std::memcpy(out_part, ro.part.data(), sizeof(u32) * n);
   if (out_levels) *out_levels = (uint32_t)ro.hierarchy.size();
   return ro.quality;
+}
+
+int or_hub_check_selftest(void) { return ora::hub_check_selftest(); }
+
+void or_hub_check_counters(uint64_t out[6]) {
+  for (int i = 0; i < 6; ++i) out[i] = ora::g_hub_check[i].exchange(0);
 }
 
 }  // extern "C"

@@ -23,8 +23,23 @@ enum {
   OR_FLAG_EDGE_WEIGHT_LOOPS = 1u << 2, /* self-loop transfer moves w, not 2w      */
   OR_FLAG_NO_COMPACT = 1u << 3,        /* never compact community ids >= n        */
   OR_FLAG_FAITHFUL_SCANS = 1u << 4,    /* T-filter with the reference's O(n) scans */
-  OR_FLAG_MULTILEVEL = 1u << 5         /* multi-level update semantics (M1-M7)    */
+  OR_FLAG_MULTILEVEL = 1u << 5,        /* multi-level update semantics (M1-M7)    */
+  OR_FLAG_HUB_CHECK = 1u << 6          /* check round-to-round hub key sums (below) */
 };
+
+/* Throughput movement with OR_FLAG_HUB_CHECK also evaluates every active row
+ * of more than 512 entries a second way: from a table of (key, sum, first
+ * position) per row, built at the row's first evaluation in the movement
+ * call and corrected after each round by the moves of its neighbours (first
+ * positions recomputed only when a key that lost its first entry ties the
+ * best gain).  Each such evaluation is compared with the full one.  This
+ * returns and resets the counters: evaluations, mismatches, first-position
+ * rescans, corrections, table builds, keys scanned.  Test infrastructure:
+ * the results of the update do not depend on the flag. */
+void or_hub_check_counters(uint64_t out[6]);
+/* The check's stale first-position path on a fixed case: the number of
+ * rescans it made (1 expected), or -1 if an evaluation differed. */
+int or_hub_check_selftest(void);
 
 typedef struct or_graph or_graph;
 typedef struct or_state or_state;

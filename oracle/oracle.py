@@ -26,6 +26,7 @@ FLAG_EDGE_WEIGHT_LOOPS = 1 << 2
 FLAG_NO_COMPACT = 1 << 3
 FLAG_FAITHFUL_SCANS = 1 << 4
 FLAG_MULTILEVEL = 1 << 5
+FLAG_HUB_CHECK = 1 << 6
 
 _lock = threading.Lock()
 _lib = None
@@ -82,6 +83,8 @@ def load():
         lib.or_select_decoupled.argtypes = [u32p, u32p, u32p, vp, f64p, C.c_uint64, u32p]
         lib.or_move_eval.argtypes = [vp, u32p, f64p, C.c_uint64, f64p, C.c_double, C.c_double,
                                      u32p, C.c_uint64, u32p, f64p]
+        lib.or_hub_check_counters.argtypes = [u64p]
+        lib.or_hub_check_selftest.restype = C.c_int
         lib.or_inc_movement.restype = C.c_uint32
         lib.or_inc_movement.argtypes = [vp, u32p, u32p, vp, C.c_uint64, u32p, u32p, C.c_double,
                                         C.c_int, C.c_uint32, C.c_int, C.c_int, u8p, u8p]
@@ -202,6 +205,22 @@ class Graph:
         s, d, wa, wp = _edges(src, dst, w)
         dn = self.n if delta_n is None else delta_n
         return Graph(lib.or_graph_apply_delta(self.h, dn, s, d, wp, len(s), int(keep_self_loops)))
+
+
+def hub_check_counters():
+    """Counters of the round-to-round hub key-sum check (FLAG_HUB_CHECK),
+    reset by the call: evaluations, mismatches, first-position rescans,
+    corrections, table builds, keys scanned."""
+    out = np.zeros(6, np.uint64)
+    load().or_hub_check_counters(out)
+    return dict(zip(("evals", "mismatches", "rescans", "corrections", "builds", "keys"),
+                    (int(x) for x in out)))
+
+
+def hub_check_selftest():
+    """The check's stale first-position path on its fixed case: rescans made
+    (1 expected), or -1 if an evaluation differed from the full one."""
+    return int(load().or_hub_check_selftest())
 
 
 def tree_sum(x):
