@@ -765,8 +765,8 @@ def _bench_line(rep, cfg_workload, config, K, Wm, k, n, dev_ms, host_s, launches
     lat = sorted(1000.0 * x for x in host_s)
     dlat = sorted(dev_ms)
     peak, peak_kind = measured_peak()
-    roof = _roof(kernels, "move_eval", "k_eval_* <EVAL_MOVE> (inc-movement best-move evaluation, "
-                 "all degree bins)", peak, peak_kind)
+    roof = _roof(kernels, "move_eval", "k_eval_* and k_pb_* <EVAL_MOVE> (inc-movement best-move "
+                 "evaluation: all degree bins and the partitioned hub pass)", peak, peak_kind)
     if roof is not None and roof_traffic:
         roof["traffic"] = roof["bytes_per_launch"] * roof_traffic
     mv = kernels.get("stage_move", {})
